@@ -1,0 +1,219 @@
+/*
+ * ldga_b200.h -- C ABI of the B200 (sm_100a) lDGA ladder library (libldga_b200.so).
+ *
+ * One handle (ldga_ctx) holds one k-grid / frequency box / parameter point and owns all device
+ * memory of the ladder chain: bubble -> Bethe-Salpeter (m, d) -> lambda_0 -> equation of motion
+ * -> lambda correction.  Every entry point replaces one function of LadderDGA.jl v0.15.1; the
+ * citation beside each declaration names the reference interface (file:line, paths inside the
+ * LadderDGA.jl repository).
+ *
+ * Conventions
+ *   - Complex arrays are interleaved (re, im) doubles: Julia ComplexF64, C double _Complex.
+ *   - Multi-dimensional arrays are column-major with the first index fastest, exactly the memory
+ *     layout of the Julia arrays the reference passes around (chi0.data[q, nu, w], Gamma[nu, nu', w],
+ *     chi.data[q, w], gamma.data[q, nu, w], Sigma_ladder[q, nu]).
+ *   - Array pointers may point to host or to device memory (CUDA unified addressing).  An output
+ *     pointer may be NULL: the result then stays on the device, inside the handle, and later calls
+ *     use it (pass NULL for the matching input).
+ *   - Every function returns LDGA_OK (0) or an error code; ldga_last_error() gives the message.
+ *     Calls are synchronous (the stream is synchronised before return) and a handle must not be
+ *     used from two threads at once, like the reference's kG caches.
+ *   - q runs over the point-group-irreducible wedge q_x >= q_y (>= q_z) >= 0, q_i <= N/2, in
+ *     lexicographic order (q = 0 first); ldga_kgrid() returns the wedge, kMult and eps_k.
+ */
+#ifndef LDGA_B200_H
+#define LDGA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ldga_ctx ldga_ctx;
+
+/* status codes */
+#define LDGA_OK          0
+#define LDGA_ERR_ARG     1   /* bad argument / shape: the reference's ArgumentError */
+#define LDGA_ERR_CUDA    2   /* CUDA runtime error or missing device */
+#define LDGA_ERR_STATE   3   /* prerequisite missing, or lambda applied twice (ErrorException) */
+#define LDGA_ERR_NUMERIC 4   /* non-finite data or a BSE matrix that could not be solved */
+#define LDGA_ERR_NOCONV  5   /* root finding failed (the reference returns NaN / converged=false) */
+#define LDGA_ERR_TYPE    6   /* channel not in {m, d}: error("Unkown type") */
+
+/* BSE precision modes (per handle) */
+#define LDGA_PREC_FP64_INV 0 /* full FP64 inverse of every (q, w) matrix: the reference's inv! */
+#define LDGA_PREC_FP64     1 /* FP64 elimination of the single right-hand side that chi/gamma use */
+#define LDGA_PREC_MIXED    2 /* FP32 elimination + FP64 iterative refinement against FP64 residuals */
+
+#define LDGA_CH_M 0
+#define LDGA_CH_D 1
+
+/* Lattice: simple cubic, eps_k = -2t sum_i cos k_i (2D adds -4t' cos kx cos ky - 2t''(cos 2kx + cos 2ky)).
+ * Replaces Dispersions.gen_kGrid("<dim>Dsc-t[-tp-tpp]", ns) (called at runHelpers.jl:88); ns = 1 is
+ * the one-point grid of the local quantities (gen_kGrid(kind, 1), runHelpers.jl:134). */
+typedef struct {
+    int32_t dim;            /* 2 or 3 */
+    int32_t ns;             /* points per axis */
+    double t, tp, tpp;
+} ldga_lattice;
+
+/* ModelParameters (Config.jl:39-47) */
+typedef struct {
+    double U, mu, beta, n, sVk, Epot_DMFT, Ekin_DMFT;
+} ldga_model;
+
+/* SimulationParameters (Config.jl:66-75); chi_helper must be `nothing` (plain path) */
+typedef struct {
+    int32_t n_iw, n_iv, n_iv_shell, shift;
+    int32_t fft_lo, fft_hi;               /* fft_range = fft_lo:fft_hi */
+    double usable_prct_reduction;
+    int32_t dbg_full_eom_omega;
+} ldga_sim;
+
+/* ---------------------------------------------------------------- handle ---------------- */
+
+/* Allocate a handle on CUDA device `device` (gen_kGrid, runHelpers.jl:88, plus the model and
+ * simulation parameter structs).  precision is one of LDGA_PREC_*. */
+int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* sp,
+                int32_t precision, int32_t device, ldga_ctx** out);
+int ldga_destroy(ldga_ctx* ctx);
+const char* ldga_last_error(const ldga_ctx* ctx);
+const char* ldga_status_string(int32_t status);
+int ldga_version(void);
+
+/* Replace the model parameters (e.g. a new mu); mutable ModelParameters, Config.jl:39. */
+int ldga_set_model(ldga_ctx* ctx, const ldga_model* mp);
+int ldga_set_precision(ldga_ctx* ctx, int32_t precision);
+
+/* k-grid of the handle: kG.kMult, kG.ϵkGrid and the wedge coordinates (Dispersions.jl; used at
+ * DataTypes.jl:230-241 and GFTools.jl:117-126).  Any output may be NULL. */
+int ldga_kgrid(const ldga_ctx* ctx, int32_t* nk, int32_t* nq, double* kmult, double* eps,
+               int32_t* wedge /* [nq * dim] */);
+
+/* ---------------------------------------------------------------- a1: G and its transforms -- */
+
+/* Lattice G(k, nu) = 1/(i nu_n + mu - eps_k - Sigma_loc(nu_n)) for nu_n in fft_range, and its
+ * k-space transform, kept on the device (setup loop runHelpers.jl:113-130, G_fft helpers.jl:153-183).
+ * sigma_loc: Sigma_loc(n) for n = 0..n_sigma-1 (n_sigma > max|fft_range|); negative n by
+ * conjugation.  gloc_out (may be NULL): gLoc[q, nu] [Nq, Nf]. */
+int ldga_gloc(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, double* gloc_out);
+
+/* Use a given G[q, nu] ([Nq, Nf], nu over fft_range) instead, e.g. a ladder G for the
+ * self-consistent loop (G_rfft!, helpers.jl:164-173). */
+int ldga_set_gloc(ldga_ctx* ctx, const double* gloc);
+
+/* ---------------------------------------------------------------- a2: bubble ----------------- */
+
+/* chi0[q, nu, w] = -beta/N_k sum_k G(k, nu) G(k+q, nu+w) (calc_bubble, BSETools.jl:157-172).
+ * chi0_out: [Nq, Nnu, Nw] complex or NULL. */
+int ldga_bubble(ldga_ctx* ctx, double* chi0_out);
+
+/* Upload an external chi0 [Nq, Nnu, Nw] (calc_chi_gamma(type, Gamma, chi0, ...) with a user chi0). */
+int ldga_set_chi0(ldga_ctx* ctx, const double* chi0);
+
+/* ---------------------------------------------------------------- a7: Bethe-Salpeter --------- */
+
+/* Per (q, w): A = Gamma_r(w) + diag(1/chi0(q, :, w)); chi_r(q,w) = Re(1^T A^-1 1)/beta^2;
+ * gamma_r(q, nu, w) = (1^T A^-1)_nu / (chi0(q,nu,w) (1 + s U chi_r)), s = -1 (d), +1 (m)
+ * (calc_χγ, BSETools.jl:192-248, inv! LapackWrapper.jl:64-72).
+ * gamma_r_in: Gamma_r [Nnu, Nnu, Nw] complex (NULL: reuse the last one of this channel).
+ * chi_out [Nq, Nw] real, gam_out [Nq, Nnu, Nw] complex, either may be NULL.
+ * n_fallback (may be NULL): matrices re-solved by the pivoted FP64 path. */
+int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* chi_out,
+             double* gam_out, int32_t* n_fallback);
+
+/* Upload chi_r [Nq, Nw] / gamma_r [Nq, Nnu, Nw] produced elsewhere (the chiT/gammaT data). */
+int ldga_set_chi(ldga_ctx* ctx, int32_t channel, const double* chi);
+int ldga_set_gamma(ldga_ctx* ctx, int32_t channel, const double* gam);
+
+/* ---------------------------------------------------------------- a5/a6: F and lambda_0 ------ */
+
+/* F_m(nu, nu', w) from the local chi_m(nu, nu', w) and G_imp (F_from_χ, BSETools.jl:40-53).
+ * gimp: G_imp(n) for n = 0..n_gimp-1 (negative n by conjugation).  F_out [Nnu, Nnu, Nw] or NULL. */
+int ldga_F_from_chi(ldga_ctx* ctx, const double* chi_loc, const double* gimp, int32_t n_gimp,
+                    double* F_out);
+
+/* lambda0[q, nu', w] = chi0[q, nu', w]/beta^2 * sum_nu F[nu, nu', w] (calc_λ0 plain branch,
+ * BSETools.jl:129-141).  F_in NULL: the F of the last ldga_F_from_chi.  lambda0_out or NULL. */
+int ldga_lambda0(ldga_ctx* ctx, const double* F_in, double* lambda0_out);
+int ldga_set_lambda0(ldga_ctx* ctx, const double* lambda0);
+
+/* ---------------------------------------------------------------- a8/a11: sums --------------- */
+
+/* sum_kω with the c2/w^2 tail (DataTypes.jl:215-249) of chi_r transformed by chi_lambda(., lam)
+ * (deriv = 0) or by its derivative dchi_lambda (deriv = 1) (LambdaCorrection/helpers.jl:18,61). */
+int ldga_sum_kw(ldga_ctx* ctx, int32_t channel, double lam, int32_t deriv, double* out);
+
+/* sum_ωk (DataTypes.jl:257-264): the same sum with the w sum taken first for every q, then the
+ * k integration (the reference's consistency check of sum_kω). */
+int ldga_sum_wk(ldga_ctx* ctx, int32_t channel, double lam, double* out);
+
+/* get_λ_min (LambdaCorrection/helpers.jl:217-220) of chi_r. */
+int ldga_lambda_min(ldga_ctx* ctx, int32_t channel, double* out);
+
+/* ---------------------------------------------------------------- a9/a10: EoM ---------------- */
+
+/* Sigma_ladder[q, nu_n], nu_n = 0..numax-1 (calc_Σ, ladderDGATools_singleCore.jl:108-136 with
+ * calc_Σ! :71-81, eom ladderDGATools.jl:260, conv_tmp_add! ladderDGATools.jl:147-160):
+ * Sigma = (1/beta) sum_w conv(K_{nu w}, G_{nu+w}) - U (sum_kω chi_m^lam - chiloc_m_sum)/(i nu_n)
+ *         + U n/2, K = eom(U, gamma_m, gamma_d, chi_m^lam_m, chi_d^lam_d, lambda0).
+ * tc = 0 drops the tail term.  sigma_out [Nq, numax] complex or NULL. */
+int ldga_eom(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc,
+             double chiloc_m_sum, double* sigma_out);
+
+/* calc_Σ_parts (ladderDGATools_singleCore.jl:153-189): [Nq, n_iv, 7] complex, contributions
+ * chi_m, gamma_m, chi_d, gamma_d, -U, lambda0 + Hartree, tail. */
+int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum,
+                   double* parts_out);
+
+/* ---------------------------------------------------------------- a12/a13: lambda_m ---------- */
+
+/* newton_right (LambdaCorrection/helpers.jl:133-153, nsteps 100, atol 1e-13) on
+ * f(l) = sum_kω chi_λ(chi_m, l) - rhs, start 0, bound get_λ_min (λm_correction,
+ * conditions_new.jl:144-154), all on the device.  iterations may be NULL. */
+int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iterations);
+
+/* ---------------------------------------------------------------- a15: G_ladder, energies ---- */
+
+/* From the Sigma_ladder of the last ldga_eom: fit mu to the filling n (fix_n != 0; G_from_Σladder!,
+ * GFTools.jl:162-186, filling_pos :255-273), build G_ladder over fft_range, and compute
+ * (E_kin, E_pot) (calc_E, thermodynamics.jl:142-168) and the filling n.
+ * sigma_loc (n = 0..n_sigma-1, NULL: the last one given to ldga_gloc) fills nu beyond numax.
+ * G_out [Nq, Nf] complex or NULL. */
+int ldga_g_ladder(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, int32_t fix_n,
+                  double mu_in, double* mu_out, double* G_out, double* e_kin, double* e_pot,
+                  double* n_out);
+
+/* Upload a Sigma_ladder [Nq, numax] (nu_n = 0..numax-1) as the handle's current self-energy, e.g. a
+ * user-modified one before ldga_g_ladder (G_from_Σladder takes Sigma as an argument, GFTools.jl:154). */
+int ldga_set_sigma(ldga_ctx* ctx, const double* sigma, int32_t numax);
+
+/* calc_E(G, Σ, μ, kG, mP) (thermodynamics.jl:142-168) for given G, Sigma [Nq, numax] over
+ * nu_n = 0..numax-1 (NULL: the handle's G_ladder / Sigma_ladder). */
+int ldga_calc_E(ldga_ctx* ctx, const double* G, const double* sigma, int32_t numax, double mu,
+                double* e_kin, double* e_pot);
+
+/* ---------------------------------------------------------------- a14: lambda_dm ------------- */
+
+/* λdm_correction plain branch (conditions_new.jl:219-324): 2-D newton_right with a forward-
+ * difference Jacobian (helpers.jl:165-208) on
+ *   F(lm, ld) = [ (sum chi_d^ld + sum chi_m^lm)/2 - n/2(1-n/2),  E_pot,1 - E_pot,2 ],
+ * each evaluation = EoM + mu fit + energies on the device.  numax <= 0: min(n_iv, floor(3 Nw/8)).
+ * out7 (may be NULL): [n, mu, E_kin, E_pot1, E_pot2, PP_p1, PP_p2] at the root; numax_out the
+ * EoM frequency count used; sigma_out [Nq, numax] and G_out [Nq, Nf] (may be NULL): Sigma_ladder
+ * and G_ladder at the root.
+ * Returns LDGA_ERR_NOCONV (with lam = NaN) when the root search fails, like the reference's
+ * [NaN, NaN]; *converged is the reference's validation flag. */
+int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam_min_delta,
+                   double atol, int32_t nsteps, double* lam_m, double* lam_d, int32_t* converged,
+                   double* out7, int32_t* numax_out, double* sigma_out, double* G_out);
+
+/* Number of residual evaluations of the last ldga_lambda_dm. */
+int ldga_lambda_dm_evals(const ldga_ctx* ctx, int32_t* n_evals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LDGA_B200_H */

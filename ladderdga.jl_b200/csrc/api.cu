@@ -1,0 +1,676 @@
+// C ABI of libldga_b200 (declarations and reference citations in include/ldga_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ldga_internal.cuh"
+
+double host_G_shell_sum(int N, double beta);
+int launch_fill_tail(ldga_ctx* ctx, int numax, double tnum, double2* out, int out_ld);
+int launch_calc_E(ldga_ctx* ctx, const double2* G, int ldg, const double2* sigma, int numax, double mu,
+                  double* d_out);
+
+static thread_local std::string g_create_error;
+
+int ctx_fail(ldga_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what) {
+    return ctx_fail(ctx, LDGA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+template <typename T>
+int dev_alloc(ldga_ctx* ctx, T** p, size_t n) {
+    if (*p) return LDGA_OK;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return ctx_cuda(ctx, e, "cudaMalloc");
+    return LDGA_OK;
+}
+
+// copy between any two pointers (host or device) on the handle's stream
+int copy(ldga_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return LDGA_OK;
+    LDGA_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+    return LDGA_OK;
+}
+
+int sync(ldga_ctx* ctx) {
+    LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    LDGA_CUDA(ctx, cudaGetLastError());
+    return LDGA_OK;
+}
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); }
+    ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
+};
+
+#define TRY(x) do { int _s = (x); if (_s != LDGA_OK) return _s; } while (0)
+#define NEED(ctx, cond, msg) do { if (!(cond)) return ctx_fail((ctx), LDGA_ERR_STATE, (msg)); } while (0)
+
+bool supported_grid(int dim, int M) {
+    static const int m2[] = {1, 2, 3, 4, 5, 6, 7, 9, 11, 13, 17, 21, 25, 33};
+    static const int m3[] = {1, 2, 3, 4, 5, 6, 7, 9, 11, 13, 17};
+    if (dim == 2) return std::find(std::begin(m2), std::end(m2), M) != std::end(m2);
+    if (dim == 3) return std::find(std::begin(m3), std::end(m3), M) != std::end(m3);
+    return false;
+}
+
+// point-group reduced simple-cubic grid: wedge (a >= b [>= c]), multiplicities, eps_k, T matrix
+void build_kgrid(ldga_ctx* c) {
+    const int N = c->ns, M = N / 2 + 1, d = c->dim;
+    c->M = M;
+    c->Nk = d == 2 ? N * N : N * N * N;
+    c->Nq = wedge_count(d, M);
+    c->kmult.assign(c->Nq, 0.0);
+    c->eps.assign(c->Nq, 0.0);
+    c->wedge.assign((size_t)c->Nq * d, 0);
+    auto fold = [N](int n) { return std::min(n, (N - n) % N); };
+    if (d == 2) {
+        for (int x = 0; x < N; ++x)
+            for (int y = 0; y < N; ++y) c->kmult[sidx2(fold(x), fold(y))] += 1.0;
+        for (int a = 0; a < M; ++a)
+            for (int b = 0; b <= a; ++b) {
+                const int q = widx2(a, b);
+                c->wedge[(size_t)q * 2] = a; c->wedge[(size_t)q * 2 + 1] = b;
+                const double kx = 2.0 * M_PI * a / N, ky = 2.0 * M_PI * b / N;
+                c->eps[q] = -2.0 * c->lat.t * (cos(kx) + cos(ky)) - 4.0 * c->lat.tp * cos(kx) * cos(ky) -
+                            2.0 * c->lat.tpp * (cos(2 * kx) + cos(2 * ky));
+            }
+    } else {
+        for (int x = 0; x < N; ++x)
+            for (int y = 0; y < N; ++y)
+                for (int z = 0; z < N; ++z) c->kmult[sidx3(fold(x), fold(y), fold(z))] += 1.0;
+        for (int a = 0; a < M; ++a)
+            for (int b = 0; b <= a; ++b)
+                for (int cc = 0; cc <= b; ++cc) {
+                    const int q = widx3(a, b, cc);
+                    c->wedge[(size_t)q * 3] = a; c->wedge[(size_t)q * 3 + 1] = b; c->wedge[(size_t)q * 3 + 2] = cc;
+                    c->eps[q] = -2.0 * c->lat.t * (cos(2.0 * M_PI * a / N) + cos(2.0 * M_PI * b / N) +
+                                                   cos(2.0 * M_PI * cc / N));
+                }
+    }
+    // T[q][m] = w_m cos(2 pi m q / N); w_m = 1 for m = 0 and m = N/2 (N even), else 2
+    c->Tmat.assign((size_t)M * M, 0.0);
+    for (int q = 0; q < M; ++q)
+        for (int m = 0; m < M; ++m) {
+            const double w = (m == 0 || (N % 2 == 0 && 2 * m == N)) ? 1.0 : 2.0;
+            // exact integer reduction of the phase keeps the cosines symmetric to the last bit
+            const long ph = ((long)m * q) % N;
+            c->Tmat[(size_t)q * M + m] = w * cos(2.0 * M_PI * (double)ph / (double)N);
+        }
+}
+
+int alloc_all(ldga_ctx* c) {
+    const size_t nq = c->Nq, nnu = c->Nnu, nw = c->Nw, nf = c->Nf;
+    TRY(dev_alloc(c, &c->d_kmult, nq));
+    TRY(dev_alloc(c, &c->d_eps, nq));
+    TRY(dev_alloc(c, &c->d_ghat, nq * nf));
+    TRY(dev_alloc(c, &c->d_gloc, nq * nf));
+    TRY(dev_alloc(c, &c->d_chi0, nq * nnu * nw));
+    for (int r = 0; r < 2; ++r) {
+        TRY(dev_alloc(c, &c->d_Gamma[r], nnu * nnu * nw));
+        TRY(dev_alloc(c, &c->d_chi[r], nq * nw));
+        TRY(dev_alloc(c, &c->d_gam[r], nq * nnu * nw));
+    }
+    TRY(dev_alloc(c, &c->d_F, nnu * nnu * nw));
+    TRY(dev_alloc(c, &c->d_lambda0, nq * nnu * nw));
+    TRY(dev_alloc(c, &c->d_sigma, nq * std::max<size_t>(nnu, 1)));
+    TRY(dev_alloc(c, &c->d_gladder, nq * nf));
+    TRY(dev_alloc(c, &c->d_red, 64 + 2 * nnu * nw + 64));
+    TRY(dev_alloc(c, &c->d_flags, nq * nw));
+    TRY(dev_alloc(c, &c->d_list, nq * nw));
+    TRY(dev_alloc(c, &c->d_count, 4));
+    TRY(copy(c, c->d_kmult, c->kmult.data(), nq * sizeof(double)));
+    TRY(copy(c, c->d_eps, c->eps.data(), nq * sizeof(double)));
+    return sync(c);
+}
+
+void free_all(ldga_ctx* c) {
+    void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
+                    c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
+                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}
+
+int set_sigma_loc(ldga_ctx* ctx, const double* sigma_loc, int n_sigma) {
+    const int L = std::max(std::abs(ctx->sp.fft_lo), std::abs(ctx->sp.fft_hi));
+    if (n_sigma <= L)
+        return ctx_fail(ctx, LDGA_ERR_ARG, "Sigma_loc must cover n = 0..max|fft_range| (" + std::to_string(L + 1) +
+                                               " values), got " + std::to_string(n_sigma));
+    if (n_sigma > ctx->n_sigma_loc) {
+        if (ctx->d_sigma_loc) cudaFree(ctx->d_sigma_loc);
+        ctx->d_sigma_loc = nullptr;
+        TRY(dev_alloc(ctx, &ctx->d_sigma_loc, (size_t)n_sigma));
+    }
+    ctx->n_sigma_loc = n_sigma;
+    return copy(ctx, ctx->d_sigma_loc, sigma_loc, (size_t)n_sigma * sizeof(double2));
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+int ldga_version(void) { return 1; }
+
+const char* ldga_status_string(int32_t s) {
+    switch (s) {
+        case LDGA_OK: return "ok";
+        case LDGA_ERR_ARG: return "invalid argument";
+        case LDGA_ERR_CUDA: return "CUDA error";
+        case LDGA_ERR_STATE: return "invalid state";
+        case LDGA_ERR_NUMERIC: return "numerical failure";
+        case LDGA_ERR_NOCONV: return "root finding did not converge";
+        case LDGA_ERR_TYPE: return "unknown channel type";
+        default: return "unknown status";
+    }
+}
+
+const char* ldga_last_error(const ldga_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* sp, int32_t precision,
+                int32_t device, ldga_ctx** out) {
+    if (!lat || !mp || !sp || !out) return ctx_fail(nullptr, LDGA_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (lat->dim != 2 && lat->dim != 3) return ctx_fail(nullptr, LDGA_ERR_ARG, "lattice dimension must be 2 or 3");
+    if (lat->ns < 1 || lat->ns > 64) return ctx_fail(nullptr, LDGA_ERR_ARG, "points per axis must be 1..64");
+    if (sp->n_iv < 1 || sp->n_iw < 0) return ctx_fail(nullptr, LDGA_ERR_ARG, "n_iv >= 1 and n_iw >= 0 required");
+    if (sp->n_iv_shell != 0)
+        return ctx_fail(nullptr, LDGA_ERR_ARG, "only the plain path (n_iv_shell = 0, chi_helper = nothing) is built");
+    if (precision < LDGA_PREC_FP64_INV || precision > LDGA_PREC_MIXED)
+        return ctx_fail(nullptr, LDGA_ERR_ARG, "unknown precision mode");
+    // G(nu) and G(nu + w) of the bubble and G(nu_n + w_n) of the EoM must lie inside fft_range
+    const int need_hi = 2 * sp->n_iv + sp->n_iw - 1;
+    const int need_lo = -(sp->n_iv + sp->n_iw + (sp->shift ? (sp->n_iw + 1) / 2 : 0));
+    if (sp->fft_lo > need_lo || sp->fft_hi < need_hi)
+        return ctx_fail(nullptr, LDGA_ERR_ARG, "fft_range too small for the frequency box");
+    const int M = lat->ns / 2 + 1;
+    if (!supported_grid(lat->dim, M))
+        return ctx_fail(nullptr, LDGA_ERR_ARG, "k-grid size " + std::to_string(lat->ns) + " not built for dim " +
+                                                   std::to_string(lat->dim));
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return ctx_fail(nullptr, LDGA_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return ctx_fail(nullptr, LDGA_ERR_ARG, "device index out of range");
+    ldga_ctx* c = new (std::nothrow) ldga_ctx();
+    if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
+    DeviceGuard g(device);
+    c->device = device;
+    c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;
+    c->dim = lat->dim; c->ns = lat->ns;
+    c->Nnu = 2 * sp->n_iv; c->Nw = 2 * sp->n_iw + 1;
+    c->Nf = sp->fft_hi - sp->fft_lo + 1; c->fft_lo = sp->fft_lo;
+    build_kgrid(c);
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { g_create_error = cudaGetErrorString(e); delete c; return LDGA_ERR_CUDA; }
+    int st = alloc_all(c);
+    if (st != LDGA_OK) { g_create_error = c->err; free_all(c); cudaStreamDestroy(c->stream); delete c; return st; }
+    *out = c;
+    return LDGA_OK;
+}
+
+int ldga_destroy(ldga_ctx* ctx) {
+    if (!ctx) return LDGA_OK;
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return LDGA_OK;
+}
+
+int ldga_set_model(ldga_ctx* ctx, const ldga_model* mp) {
+    if (!ctx || !mp) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    ctx->mp = *mp;
+    return LDGA_OK;
+}
+
+int ldga_set_precision(ldga_ctx* ctx, int32_t precision) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (precision < LDGA_PREC_FP64_INV || precision > LDGA_PREC_MIXED)
+        return ctx_fail(ctx, LDGA_ERR_ARG, "unknown precision mode");
+    ctx->prec = precision;
+    return LDGA_OK;
+}
+
+int ldga_kgrid(const ldga_ctx* ctx, int32_t* nk, int32_t* nq, double* kmult, double* eps, int32_t* wedge) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (nk) *nk = ctx->Nk;
+    if (nq) *nq = ctx->Nq;
+    if (kmult) std::memcpy(kmult, ctx->kmult.data(), ctx->Nq * sizeof(double));
+    if (eps) std::memcpy(eps, ctx->eps.data(), ctx->Nq * sizeof(double));
+    if (wedge) std::memcpy(wedge, ctx->wedge.data(), ctx->wedge.size() * sizeof(int32_t));
+    return LDGA_OK;
+}
+
+int ldga_gloc(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, double* gloc_out) {
+    if (!ctx || !sigma_loc) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    TRY(set_sigma_loc(ctx, sigma_loc, n_sigma));
+    TRY(launch_gloc_transform(ctx, true));
+    ctx->have_ghat = true;
+    if (gloc_out) TRY(copy(ctx, gloc_out, ctx->d_gloc, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_set_gloc(ldga_ctx* ctx, const double* gloc) {
+    if (!ctx || !gloc) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_gloc, gloc, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
+    TRY(launch_gloc_transform(ctx, false));
+    ctx->have_ghat = true;
+    return sync(ctx);
+}
+
+int ldga_bubble(ldga_ctx* ctx, double* chi0_out) {
+    if (!ctx) return LDGA_ERR_ARG;
+    NEED(ctx, ctx->have_ghat, "calc_bubble: call ldga_gloc or ldga_set_gloc first");
+    DeviceGuard g(ctx->device);
+    TRY(launch_bubble(ctx));
+    ctx->have_chi0 = true;
+    if (chi0_out) TRY(copy(ctx, chi0_out, ctx->d_chi0, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_set_chi0(ldga_ctx* ctx, const double* chi0) {
+    if (!ctx || !chi0) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_chi0, chi0, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    ctx->have_chi0 = true;
+    return sync(ctx);
+}
+
+int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* chi_out, double* gam_out,
+             int32_t* n_fallback) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi0, "calc_χγ: bubble chi0 missing (call ldga_bubble or ldga_set_chi0)");
+    DeviceGuard g(ctx->device);
+    if (gamma_r_in) {
+        TRY(copy(ctx, ctx->d_Gamma[channel], gamma_r_in, (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw * sizeof(double2)));
+        ctx->have_Gamma[channel] = true;
+    }
+    NEED(ctx, ctx->have_Gamma[channel], "calc_χγ: Gamma_r missing");
+    int nfb = 0;
+    TRY(launch_bse(ctx, channel, &nfb));
+    ctx->have_chi[channel] = ctx->have_gam[channel] = true;
+    if (n_fallback) *n_fallback = nfb;
+    if (chi_out) TRY(copy(ctx, chi_out, ctx->d_chi[channel], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
+    if (gam_out) TRY(copy(ctx, gam_out, ctx->d_gam[channel], (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_set_chi(ldga_ctx* ctx, int32_t channel, const double* chi) {
+    if (!ctx || !chi) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_chi[channel], chi, (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
+    ctx->have_chi[channel] = true;
+    return sync(ctx);
+}
+
+int ldga_set_gamma(ldga_ctx* ctx, int32_t channel, const double* gam) {
+    if (!ctx || !gam) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_gam[channel], gam, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    ctx->have_gam[channel] = true;
+    return sync(ctx);
+}
+
+int ldga_F_from_chi(ldga_ctx* ctx, const double* chi_loc, const double* gimp, int32_t n_gimp, double* F_out) {
+    if (!ctx || !chi_loc || !gimp) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    const int need = 2 * ctx->sp.n_iv + ctx->sp.n_iw + (ctx->sp.shift ? ctx->sp.n_iw : 0);
+    if (n_gimp < need) return ctx_fail(ctx, LDGA_ERR_ARG, "G_imp too short for the frequency box");
+    DeviceGuard g(ctx->device);
+    const size_t nF = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw;
+    double2* d_chi = nullptr;
+    double2* d_g = nullptr;
+    LDGA_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_chi), nF * sizeof(double2), ctx->stream));
+    LDGA_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_g), (size_t)n_gimp * sizeof(double2), ctx->stream));
+    int st = copy(ctx, d_chi, chi_loc, nF * sizeof(double2));
+    if (!st) st = copy(ctx, d_g, gimp, (size_t)n_gimp * sizeof(double2));
+    if (!st) st = launch_F_from_chi(ctx, d_chi, d_g, n_gimp);
+    cudaFreeAsync(d_chi, ctx->stream);
+    cudaFreeAsync(d_g, ctx->stream);
+    TRY(st);
+    ctx->have_F = true;
+    if (F_out) TRY(copy(ctx, F_out, ctx->d_F, nF * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_lambda0(ldga_ctx* ctx, const double* F_in, double* lambda0_out) {
+    if (!ctx) return LDGA_ERR_ARG;
+    NEED(ctx, ctx->have_chi0, "calc_λ0: bubble chi0 missing");
+    DeviceGuard g(ctx->device);
+    const size_t nF = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw;
+    if (F_in) { TRY(copy(ctx, ctx->d_F, F_in, nF * sizeof(double2))); ctx->have_F = true; }
+    NEED(ctx, ctx->have_F, "calc_λ0: F missing (call ldga_F_from_chi or pass F)");
+    TRY(launch_lambda0(ctx));
+    ctx->have_lambda0 = true;
+    if (lambda0_out) TRY(copy(ctx, lambda0_out, ctx->d_lambda0, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_set_lambda0(ldga_ctx* ctx, const double* lambda0) {
+    if (!ctx || !lambda0) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_lambda0, lambda0, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    ctx->have_lambda0 = true;
+    return sync(ctx);
+}
+
+int ldga_sum_kw(ldga_ctx* ctx, int32_t channel, double lam, int32_t deriv, double* out) {
+    if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi[channel], "sum_kω: chi missing");
+    DeviceGuard g(ctx->device);
+    TRY(launch_sum_kw(ctx, channel, lam, deriv ? 1 : 0, ctx->d_red));
+    TRY(copy(ctx, out, ctx->d_red, sizeof(double)));
+    return sync(ctx);
+}
+
+int ldga_sum_wk(ldga_ctx* ctx, int32_t channel, double lam, double* out) {
+    if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi[channel], "sum_ωk: chi missing");
+    DeviceGuard g(ctx->device);
+    TRY(launch_sum_kw(ctx, channel, lam, 2, ctx->d_red));
+    TRY(copy(ctx, out, ctx->d_red, sizeof(double)));
+    return sync(ctx);
+}
+
+int ldga_lambda_min(ldga_ctx* ctx, int32_t channel, double* out) {
+    if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi[channel], "get_λ_min: chi missing");
+    DeviceGuard g(ctx->device);
+    TRY(launch_lambda_min(ctx, channel, ctx->d_red));
+    TRY(copy(ctx, out, ctx->d_red, sizeof(double)));
+    return sync(ctx);
+}
+
+namespace {
+int eom_inputs_ready(ldga_ctx* ctx) {
+    NEED(ctx, ctx->have_ghat, "calc_Σ: G transform missing");
+    NEED(ctx, ctx->have_chi[0] && ctx->have_chi[1], "calc_Σ: chi_m / chi_d missing");
+    NEED(ctx, ctx->have_gam[0] && ctx->have_gam[1], "calc_Σ: gamma_m / gamma_d missing");
+    NEED(ctx, ctx->have_lambda0, "calc_Σ: lambda0 missing");
+    return LDGA_OK;
+}
+
+// EoM into d_sigma (all on the stream, no sync)
+int eom_device(ldga_ctx* ctx, double lam_m, double lam_d, int numax, int tc, double chiloc_m_sum) {
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
+    if (tc) TRY(launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8));
+    TRY(launch_eom(ctx, numax, lam_m, lam_d, -1, ctx->d_red + 8, tc, chiloc_m_sum, ctx->d_sigma, ctx->Nq, 1));
+    ctx->have_sigma = true;
+    ctx->sigma_numax = numax;
+    return LDGA_OK;
+}
+}  // namespace
+
+int ldga_eom(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, double chiloc_m_sum,
+             double* sigma_out) {
+    if (!ctx) return LDGA_ERR_ARG;
+    TRY(eom_inputs_ready(ctx));
+    if (!std::isfinite(lam_m) || !std::isfinite(lam_d)) return ctx_fail(ctx, LDGA_ERR_ARG, "λ must be finite");
+    DeviceGuard g(ctx->device);
+    TRY(eom_device(ctx, lam_m, lam_d, numax, tc, chiloc_m_sum));
+    if (sigma_out) TRY(copy(ctx, sigma_out, ctx->d_sigma, (size_t)ctx->Nq * numax * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum, double* parts_out) {
+    if (!ctx || !parts_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(eom_inputs_ready(ctx));
+    DeviceGuard g(ctx->device);
+    const int numax = ctx->sp.n_iv;
+    const size_t blk = (size_t)ctx->Nq * numax;
+    double2* d_parts = nullptr;
+    LDGA_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_parts), 7 * blk * sizeof(double2), ctx->stream));
+    int st = LDGA_OK;
+    for (int p = 0; p < 6 && st == LDGA_OK; ++p)
+        st = launch_eom(ctx, numax, lam_m, lam_d, p, ctx->d_red, 0, 0.0, d_parts + p * blk, ctx->Nq, p == 5 ? 1 : 0);
+    double tnum = 0.0;
+    if (st == LDGA_OK && tc) {
+        st = launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8);
+        double s = 0.0;
+        if (st == LDGA_OK) st = copy(ctx, &s, ctx->d_red + 8, sizeof(double));
+        if (st == LDGA_OK) st = sync(ctx);
+        tnum = -ctx->mp.U * (s - chiloc_m_sum);
+    }
+    if (st == LDGA_OK) st = launch_fill_tail(ctx, numax, tnum, d_parts + 6 * blk, ctx->Nq);
+    if (st == LDGA_OK) st = copy(ctx, parts_out, d_parts, 7 * blk * sizeof(double2));
+    cudaFreeAsync(d_parts, ctx->stream);
+    TRY(st);
+    return sync(ctx);
+}
+
+int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iterations) {
+    if (!ctx || !lam_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    NEED(ctx, ctx->have_chi[LDGA_CH_M], "λm_correction: chi_m missing");
+    DeviceGuard g(ctx->device);
+    TRY(launch_lambda_m(ctx, rhs, ctx->d_red + 16));
+    double r[2];
+    TRY(copy(ctx, r, ctx->d_red + 16, 2 * sizeof(double)));
+    TRY(sync(ctx));
+    *lam_out = r[0];
+    if (iterations) *iterations = (int32_t)r[1];
+    return LDGA_OK;
+}
+
+int ldga_g_ladder(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, int32_t fix_n, double mu_in,
+                  double* mu_out, double* G_out, double* e_kin, double* e_pot, double* n_out) {
+    if (!ctx) return LDGA_ERR_ARG;
+    NEED(ctx, ctx->have_sigma, "G_from_Σladder: no Sigma_ladder on the device (call ldga_eom)");
+    DeviceGuard g(ctx->device);
+    if (sigma_loc) TRY(set_sigma_loc(ctx, sigma_loc, n_sigma));
+    NEED(ctx, ctx->d_sigma_loc != nullptr, "G_from_Σladder: Sigma_loc missing");
+    TRY(launch_g_ladder(ctx, ctx->sigma_numax, fix_n, mu_in, ctx->d_red + 24));
+    double r[4];
+    TRY(copy(ctx, r, ctx->d_red + 24, 4 * sizeof(double)));
+    TRY(sync(ctx));
+    if (G_out) {
+        TRY(launch_g_ladder_full(ctx, ctx->sigma_numax, r[0]));
+        TRY(copy(ctx, G_out, ctx->d_gladder, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
+        TRY(sync(ctx));
+    }
+    if (mu_out) *mu_out = r[0];
+    if (e_kin) *e_kin = r[1];
+    if (e_pot) *e_pot = r[2];
+    if (n_out) *n_out = r[3];
+    if (!std::isfinite(r[0])) return ctx_fail(ctx, LDGA_ERR_NOCONV, "μ determination failed");
+    return LDGA_OK;
+}
+
+int ldga_set_sigma(ldga_ctx* ctx, const double* sigma, int32_t numax) {
+    if (!ctx || !sigma) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    DeviceGuard g(ctx->device);
+    TRY(copy(ctx, ctx->d_sigma, sigma, (size_t)ctx->Nq * numax * sizeof(double2)));
+    ctx->have_sigma = true;
+    ctx->sigma_numax = numax;
+    return sync(ctx);
+}
+
+int ldga_calc_E(ldga_ctx* ctx, const double* G, const double* sigma, int32_t numax, double mu, double* e_kin,
+                double* e_pot) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    DeviceGuard g(ctx->device);
+    const size_t blk = (size_t)ctx->Nq * numax;
+    double2* d_tmp = nullptr;
+    const double2* dG = nullptr;
+    const double2* dS = ctx->d_sigma;
+    int ldg = ctx->Nq;
+    if (G || sigma) LDGA_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_tmp), 2 * blk * sizeof(double2), ctx->stream));
+    int st = LDGA_OK;
+    if (G) { st = copy(ctx, d_tmp, G, blk * sizeof(double2)); dG = d_tmp; }
+    else { dG = ctx->d_gladder - ctx->fft_lo * (ptrdiff_t)ctx->Nq; }   // column nu_n = 0 of G_ladder
+    if (!st && sigma) { st = copy(ctx, d_tmp + blk, sigma, blk * sizeof(double2)); dS = d_tmp + blk; }
+    if (!st) st = launch_calc_E(ctx, dG, ldg, dS, numax, mu, ctx->d_red + 48);
+    double r[2] = {0.0, 0.0};
+    if (!st) st = copy(ctx, r, ctx->d_red + 48, 2 * sizeof(double));
+    if (d_tmp) cudaFreeAsync(d_tmp, ctx->stream);
+    TRY(st);
+    TRY(sync(ctx));
+    if (e_kin) *e_kin = r[0];
+    if (e_pot) *e_pot = r[1];
+    return LDGA_OK;
+}
+
+// ------------------------------------------------------------------------------- lambda_dm --
+namespace {
+
+struct DmState {
+    ldga_ctx* ctx;
+    double chiloc_m_sum;
+    int numax;
+    double mu;
+    double rhs_c1;
+    int evals = 0;
+    int status = LDGA_OK;
+    double last[7];
+};
+
+// residual_vals (conditions_new.jl:250-270): returns false on a CUDA/argument error
+bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
+    ldga_ctx* ctx = s.ctx;
+    s.evals++;
+    if (lm > 1e5 || ld > 1e5) { F[0] = F[1] = NAN; return true; }
+    int st = eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum);
+    if (!st) st = launch_g_ladder(ctx, s.numax, 1, s.mu, ctx->d_red + 24);
+    if (!st) st = launch_sum_kw(ctx, LDGA_CH_M, lm, 0, ctx->d_red + 32);
+    if (!st) st = launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33);
+    double r[10];
+    if (!st) st = copy(ctx, r, ctx->d_red + 24, 10 * sizeof(double));
+    if (!st) st = sync(ctx);
+    if (st) { s.status = st; return false; }
+    const double mu = r[0], ek = r[1], ep1 = r[2], n = r[3], xm = r[8], xd = r[9];
+    s.mu = mu;
+    const double lhs = (xd + xm) / 2.0;
+    const double U = ctx->mp.U, nn = ctx->mp.n;
+    const double ep2 = (U / 2.0) * (xd - xm) + U * (nn / 2.0 * nn / 2.0);
+    F[0] = lhs - s.rhs_c1;
+    F[1] = ep1 - ep2;
+    s.last[0] = n; s.last[1] = mu; s.last[2] = ek; s.last[3] = ep1; s.last[4] = ep2; s.last[5] = s.rhs_c1;
+    s.last[6] = lhs;
+    return true;
+}
+
+double fd_step(double x) {
+    const double r = std::sqrt(2.220446049250313e-16);
+    return std::max(r * std::fabs(x), r);
+}
+
+}  // namespace
+
+int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam_min_delta, double atol,
+                   int32_t nsteps, double* lam_m, double* lam_d, int32_t* converged, double* out7,
+                   int32_t* numax_out, double* sigma_out, double* G_out) {
+    if (!ctx || !lam_m || !lam_d) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(eom_inputs_ready(ctx));
+    NEED(ctx, ctx->d_sigma_loc != nullptr, "λdm_correction: Sigma_loc missing (call ldga_gloc)");
+    DeviceGuard g(ctx->device);
+    const int nw_use = ctx->Nw;   // usable range = full range (chi built with full_range = true)
+    int nu_auto = std::min(ctx->sp.n_iv, (int)std::floor(3.0 * nw_use / 8.0));
+    if (ctx->sp.dbg_full_eom_omega) nu_auto = std::min(ctx->sp.n_iv, (int)std::floor(3.0 * ctx->Nw / 8.0));
+    const int nu = numax < 1 ? nu_auto : std::min(nu_auto, (int)numax);
+    if (nu < 1) return ctx_fail(ctx, LDGA_ERR_ARG, "λdm: no fermionic frequencies for the EoM");
+    if (numax_out) *numax_out = nu;
+    DmState s;
+    s.ctx = ctx; s.chiloc_m_sum = chiloc_m_sum; s.numax = nu; s.mu = ctx->mp.mu;
+    s.rhs_c1 = ctx->mp.n / 2.0 * (1.0 - ctx->mp.n / 2.0);
+    // bounds: lambda_min + delta |lambda_min| (conditions_new.jl:290-293)
+    double lmin[2];
+    TRY(launch_lambda_min(ctx, LDGA_CH_M, ctx->d_red + 40));
+    TRY(launch_lambda_min(ctx, LDGA_CH_D, ctx->d_red + 41));
+    TRY(copy(ctx, lmin, ctx->d_red + 40, 2 * sizeof(double)));
+    TRY(sync(ctx));
+    const double xmin[2] = {lmin[0] + lam_min_delta * std::fabs(lmin[0]), lmin[1] + lam_min_delta * std::fabs(lmin[1])};
+    // newton_right, N-D (LambdaCorrection/helpers.jl:165-208)
+    const double start[2] = {0.0, 0.0};
+    double xi[2] = {start[0], start[1]};
+    int i = 1, reset_i = 1;
+    bool bis_fail = false, failed = false;
+    const int max_reset = 5;
+    const double reset_backoff = 1.0;
+    while (true) {
+        double fi[2], f0[2], f1[2], J[2][2];
+        if (!dm_residual(s, xi[0], xi[1], fi)) return s.status;
+        // forward-difference Jacobian; FiniteDiff evaluates f(x) again
+        if (!dm_residual(s, xi[0], xi[1], f0)) return s.status;
+        for (int j = 0; j < 2; ++j) {
+            double x1[2] = {xi[0], xi[1]};
+            const double e = fd_step(xi[j]);
+            x1[j] += e;
+            if (!dm_residual(s, x1[0], x1[1], f1)) return s.status;
+            J[0][j] = (f1[0] - f0[0]) / e;
+            J[1][j] = (f1[1] - f0[1]) / e;
+        }
+        const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        const double inv[2][2] = {{J[1][1] / det, -J[0][1] / det}, {-J[1][0] / det, J[0][0] / det}};
+        const double last[2] = {xi[0], xi[1]};
+        xi[0] = xi[0] - (inv[0][0] * fi[0] + inv[0][1] * fi[1]);
+        xi[1] = xi[1] - (inv[1][0] * fi[0] + inv[1][1] * fi[1]);
+        for (int l = 0; l < 2; ++l) {
+            if (xi[l] < xmin[l]) {
+                xi[l] = xmin[l] + std::fabs(last[l] - xmin[l]) / 2.0;
+                if (std::fabs(last[l] - xmin[l]) / 2.0 < 1e-8) bis_fail = true;
+            }
+        }
+        if (bis_fail || !std::isfinite(fi[0]) || !std::isfinite(fi[1])) {
+            bis_fail = false;
+            if (reset_i >= max_reset) { failed = true; break; }
+            reset_i += 1;
+            xi[0] = start[0] + reset_i * reset_backoff * std::fabs(xmin[0]);
+            xi[1] = start[1] + reset_i * reset_backoff * std::fabs(xmin[1]);
+        }
+        if (std::fabs(std::sqrt(fi[0] * fi[0] + fi[1] * fi[1])) < atol) break;
+        if (i >= nsteps) break;
+        i += 1;
+    }
+    ctx->lambda_dm_evals = s.evals;
+    if (failed || !std::isfinite(xi[0]) || !std::isfinite(xi[1])) {
+        *lam_m = NAN; *lam_d = NAN;
+        if (converged) *converged = 0;
+        if (out7) for (int k = 0; k < 7; ++k) out7[k] = NAN;
+        return ctx_fail(ctx, LDGA_ERR_NOCONV, "λ root-finding failed after " + std::to_string(i) + " iterations");
+    }
+    double F[2];
+    if (!dm_residual(s, xi[0], xi[1], F)) return s.status;
+    ctx->lambda_dm_evals = s.evals;
+    *lam_m = xi[0];
+    *lam_d = xi[1];
+    const bool conv = std::fabs(s.rhs_c1 - s.last[6]) <= 1e-8 && std::fabs(s.last[3] - s.last[4]) <= 1e-8;
+    if (converged) *converged = conv ? 1 : 0;
+    if (out7) for (int k = 0; k < 7; ++k) out7[k] = s.last[k];
+    if (sigma_out) TRY(copy(ctx, sigma_out, ctx->d_sigma, (size_t)ctx->Nq * nu * sizeof(double2)));
+    if (G_out) {
+        TRY(launch_g_ladder_full(ctx, nu, s.mu));
+        TRY(copy(ctx, G_out, ctx->d_gladder, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
+    }
+    return sync(ctx);
+}
+
+int ldga_lambda_dm_evals(const ldga_ctx* ctx, int32_t* n_evals) {
+    if (!ctx || !n_evals) return LDGA_ERR_ARG;
+    *n_evals = ctx->lambda_dm_evals;
+    return LDGA_OK;
+}
+
+}  // extern "C"

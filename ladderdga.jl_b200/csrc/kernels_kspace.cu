@@ -1,0 +1,367 @@
+// k-space kernels: lattice G and its transform (setup), the bubble chi0, and the equation of motion.
+// All of them are built on the symmetry-reduced transform of transform.cuh; one CTA processes a
+// batch of independent (nu, w) vectors entirely in shared memory.
+#include <cmath>
+
+#include "transform.cuh"
+
+using namespace ldga;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr size_t kSmemBudget = 200 * 1024;
+
+template <int DIM, int M>
+int pairs_per_cta(int total) {
+    using S = TransformSmem<DIM, M>;
+    const size_t per = (size_t)(S::BUF_A + S::BUF_B) * sizeof(double2);
+    int np = (int)(kSmemBudget / per);
+    if (np > 16) np = 16;
+    if (np < 1) np = 1;
+    if (np > total) np = total;
+    return np;
+}
+
+template <int DIM, int M>
+size_t smem_bytes(int np) {
+    using S = TransformSmem<DIM, M>;
+    return (size_t)np * (S::BUF_A + S::BUF_B) * sizeof(double2);
+}
+
+template <int M>
+TMat<M> make_T(const ldga_ctx* ctx) {
+    TMat<M> T;
+    for (int i = 0; i < M * M; ++i) T.t[i] = ctx->Tmat[i];
+    return T;
+}
+
+// ---------------------------------------------------------------------------------------------
+// a1: G(k, nu) for nu in fft_range and Ghat = S(G)
+// ---------------------------------------------------------------------------------------------
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_gloc_transform(
+    const TMat<M> T, int nf, int fft_lo, double beta, double mu, const double* __restrict__ eps,
+    const double2* __restrict__ sigma_loc, int n_sigma, double2* __restrict__ gloc, int from_sigma,
+    double2* __restrict__ ghat) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)(gridDim.y);   // pairs per CTA passed through gridDim.y
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, nf - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int f = p0 + p;
+        double2 g;
+        if (from_sigma) {
+            const int vn = fft_lo + f;
+            const double2 s = vn < 0 ? cconj(sigma_loc[-vn - 1]) : sigma_loc[vn];
+            const double2 z = make_double2(mu - eps[q] - s.x, (2.0 * vn + 1.0) * M_PI / beta - s.y);
+            g = cinv(z);
+            gloc[(size_t)f * NQ + q] = g;
+        } else {
+            g = gloc[(size_t)f * NQ + q];
+        }
+        bufA[p * NQ + q] = g;
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        ghat[(size_t)(p0 + p) * NQ + q] = v;
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// a2: chi0[q, nu, w] = -beta/N_k^2 S(Ghat(nu) Ghat(nu+w))(q)
+// ---------------------------------------------------------------------------------------------
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_bubble(
+    const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double scale,
+    const double2* __restrict__ ghat, double2* __restrict__ chi0) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int total = nnu * nw;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, total - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int pi = p0 + p;
+        const int wi = pi / nnu, vi = pi - wi * nnu;
+        const int wn = wi - n_iw;
+        const int vn = (vi - n_iv) - shift * (wn / 2);    // C division truncates like trunc(Int, .)
+        const double2 a = ghat[(size_t)(vn - fft_lo) * NQ + q];
+        const double2 b = ghat[(size_t)(vn + wn - fft_lo) * NQ + q];
+        bufA[p * NQ + q] = cmul(a, b);
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        chi0[(size_t)(p0 + p) * NQ + q] = cscale(v, scale);
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// a9/a10: EoM.  Forward: for one nu_n and a chunk of w, K(q) = eom(...) -> S(K) * Ghat(nu+w),
+// summed over the chunk in a fixed order -> partial[chunk][nu][q].  The inverse kernel then sums
+// the chunks (fixed order), applies S, and adds 1/beta, the tail and the Hartree term.
+// ---------------------------------------------------------------------------------------------
+struct EomArgs {
+    int nnu, nw, n_iv, n_iw, shift, fft_lo, numax, w_per_chunk;
+    double U, lam_m, lam_d;
+    int part;   // -1: full eom; 0..5: calc_Σ_parts contributions
+};
+
+__device__ __forceinline__ double chi_lam(double x, double lam) {
+    return lam == 0.0 ? x : x / (lam * x + 1.0);
+}
+
+__device__ __forceinline__ double2 eom_value(const EomArgs& a, double2 gm, double2 gd, double xm, double xd,
+                                             double2 l0) {
+    const double U = a.U;
+    switch (a.part) {
+        case 0: {  // eom_χ_m = U*(γm*1.5*(U*χm))
+            const double f = 1.5 * (U * xm);
+            return make_double2(U * (gm.x * f), U * (gm.y * f));
+        }
+        case 1:    // eom_γ_m = U*(γm*1.5)
+            return make_double2(U * (gm.x * 1.5), U * (gm.y * 1.5));
+        case 2: {  // eom_χ_d = -U*(γd*0.5*(-U*χd))
+            const double f = 0.5 * (-U * xd);
+            return make_double2(-U * (gd.x * f), -U * (gd.y * f));
+        }
+        case 3:    // eom_γ_d = -U*(γd*0.5)
+            return make_double2(-U * (gd.x * 0.5), -U * (gd.y * 0.5));
+        case 4:    // eom_rest_01 = -U*1.0 + 0im
+            return make_double2(-U * 1.0, 0.0);
+        case 5:    // eom_rest = U*λ₀
+            return make_double2(U * l0.x, U * l0.y);
+        default: {
+            // eom = U*(γm*1.5*(1+U*χm) - γd*0.5*(1-U*χd) - 1.5 + 0.5 + λ₀), left to right
+            const double fm = 1.5 * (1.0 + U * xm);
+            const double fd = 0.5 * (1.0 - U * xd);
+            double re = gm.x * fm - gd.x * fd;
+            double im = gm.y * fm - gd.y * fd;
+            re = re - 1.5;
+            re = re + 0.5;
+            re = re + l0.x;
+            im = im + l0.y;
+            return make_double2(U * re, U * im);
+        }
+    }
+}
+
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_eom_forward(
+    const TMat<M> T, const EomArgs a, const double2* __restrict__ ghat, const double* __restrict__ chi_m,
+    const double2* __restrict__ gam_m, const double* __restrict__ chi_d, const double2* __restrict__ gam_d,
+    const double2* __restrict__ lambda0, double2* __restrict__ partial) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = a.w_per_chunk;
+    const int chunk = blockIdx.x, nu_n = blockIdx.y;
+    const int w0 = chunk * np_max;
+    const int np = min(np_max, a.nw - w0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    double2* outb = smem + np_max * (S::BUF_A + S::BUF_B);     // [np_max][NQ] products
+    __shared__ int s_vi[16];
+    if (threadIdx.x < np) {
+        const int wi = w0 + threadIdx.x;
+        const int wn = wi - a.n_iw;
+        const int v0 = a.n_iv + a.shift * ((wi - a.n_iw) / 2);          // ν0Index_of_ωIndex - 1
+        const int len = min(a.numax, 2 * a.n_iv - v0);
+        s_vi[threadIdx.x] = (nu_n < len && v0 + nu_n >= 0) ? v0 + nu_n : -1;
+        (void)wn;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int wi = w0 + p;
+        const int vi = s_vi[p];
+        double2 K = make_double2(0.0, 0.0);
+        if (vi >= 0) {
+            const size_t iq = (size_t)q + (size_t)NQ * wi;
+            const size_t iv = (size_t)q + (size_t)NQ * (vi + (size_t)a.nnu * wi);
+            const double xm = chi_lam(chi_m[iq], a.lam_m);
+            const double xd = chi_lam(chi_d[iq], a.lam_d);
+            K = eom_value(a, gam_m[iv], gam_d[iv], xm, xd, lambda0[iv]);
+        }
+        bufA[p * NQ + q] = K;
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        const int wi = w0 + p;
+        const int wn = wi - a.n_iw;
+        double2 r = make_double2(0.0, 0.0);
+        if (s_vi[p] >= 0) r = cmul(v, ghat[(size_t)(nu_n + wn - a.fft_lo) * NQ + q]);
+        outb[p * NQ + q] = r;
+    });
+    for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int p = 0; p < np; ++p) acc = cadd(acc, outb[p * NQ + q]);
+        partial[((size_t)chunk * a.numax + nu_n) * NQ + q] = acc;
+    }
+}
+
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_eom_inverse(
+    const TMat<M> T, int numax, int nchunk, double scale, double beta, double U, double hartree,
+    const double* __restrict__ tail_sum, int tc, double chiloc_m_sum, const double2* __restrict__ partial,
+    double2* __restrict__ out, int out_ld, int add_hartree) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, numax - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int nu = p0 + p;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int c = 0; c < nchunk; ++c) acc = cadd(acc, partial[((size_t)c * numax + nu) * NQ + q]);
+        bufA[p * NQ + q] = acc;
+    }
+    __syncthreads();
+    // tail: (tc ? -U (sum_kω χm - χloc_m_sum) : 0) / (i ν_n), ν_n = (2n+1)π/β
+    const double tnum = tc ? -U * (tail_sum[0] - chiloc_m_sum) : 0.0;
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        const int nu = p0 + p;
+        const double w = (2.0 * nu + 1.0) * M_PI / beta;
+        // tnum / (i w) = -i tnum / w
+        double re = v.x * scale / beta + 0.0;
+        double im = v.y * scale / beta - tnum / w;
+        if (add_hartree) re += hartree;
+        out[(size_t)nu * out_ld + q] = make_double2(re, im);
+    });
+}
+
+// ---------------------------------------------------------------------------------------------
+// host-side dispatch on (DIM, M)
+// ---------------------------------------------------------------------------------------------
+template <int DIM, int M>
+int run_gloc(ldga_ctx* ctx, bool from_sigma) {
+    const int np = pairs_per_cta<DIM, M>(ctx->Nf);
+    const size_t sm = smem_bytes<DIM, M>(np);
+    auto kern = k_gloc_transform<DIM, M>;
+    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid((ctx->Nf + np - 1) / np, np);
+    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, ctx->fft_lo, ctx->mp.beta, ctx->mp.mu,
+                                               ctx->d_eps, ctx->d_sigma_loc, ctx->n_sigma_loc, ctx->d_gloc,
+                                               from_sigma ? 1 : 0, ctx->d_ghat);
+    LDGA_LAUNCHED(ctx, "k_gloc_transform");
+    return LDGA_OK;
+}
+
+template <int DIM, int M>
+int run_bubble(ldga_ctx* ctx) {
+    const int total = ctx->Nnu * ctx->Nw;
+    const int np = pairs_per_cta<DIM, M>(total);
+    const size_t sm = smem_bytes<DIM, M>(np);
+    auto kern = k_bubble<DIM, M>;
+    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid((total + np - 1) / np, np);
+    const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
+    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
+                                               ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_chi0);
+    LDGA_LAUNCHED(ctx, "k_bubble");
+    return LDGA_OK;
+}
+
+template <int DIM, int M>
+int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, int& nchunk_out) {
+    using S = TransformSmem<DIM, M>;
+    const size_t per = (size_t)(S::BUF_A + S::BUF_B + S::NQ) * sizeof(double2);
+    int wpc = (int)(kSmemBudget / per);
+    if (wpc > 16) wpc = 16;
+    if (wpc < 1) wpc = 1;
+    // spread the w axis over enough CTAs to fill the machine
+    const int target_ctas = 2 * 148;
+    while (wpc > 1 && (long)numax * ((ctx->Nw + wpc - 1) / wpc) < target_ctas) --wpc;
+    const int nchunk = (ctx->Nw + wpc - 1) / wpc;
+    const size_t need = (size_t)nchunk * numax * ctx->Nq;
+    if (need > ctx->partial_elems) {
+        if (ctx->d_partial) cudaFree(ctx->d_partial);
+        ctx->d_partial = nullptr;
+        LDGA_CUDA(ctx, cudaMalloc(&ctx->d_partial, need * sizeof(double2)));
+        ctx->partial_elems = need;
+    }
+    EomArgs a;
+    a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
+    a.fft_lo = ctx->fft_lo; a.numax = numax; a.w_per_chunk = wpc;
+    a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = part;
+    const size_t sm = (size_t)wpc * per;
+    auto kern = k_eom_forward<DIM, M>;
+    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid(nchunk, numax);
+    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_ghat, ctx->d_chi[0], ctx->d_gam[0],
+                                               ctx->d_chi[1], ctx->d_gam[1], ctx->d_lambda0, ctx->d_partial);
+    LDGA_LAUNCHED(ctx, "k_eom_forward");
+    nchunk_out = nchunk;
+    return LDGA_OK;
+}
+
+template <int DIM, int M>
+int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, int tc, double chiloc_m_sum,
+                    double2* out, int out_ld, int add_hartree) {
+    const int np = pairs_per_cta<DIM, M>(numax);
+    const size_t sm = smem_bytes<DIM, M>(np);
+    auto kern = k_eom_inverse<DIM, M>;
+    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid((numax + np - 1) / np, np);
+    const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);
+    const double hartree = ctx->mp.n * ctx->mp.U / 2.0;
+    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
+                                               hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,
+                                               add_hartree);
+    LDGA_LAUNCHED(ctx, "k_eom_inverse");
+    return LDGA_OK;
+}
+
+}  // namespace
+
+#define LDGA_CASE(D, MM)                                  \
+    if (ctx->dim == D && ctx->M == MM) { return BODY(D, MM); }
+
+int launch_gloc_transform(ldga_ctx* ctx, bool from_sigma) {
+#define BODY(D, MM) run_gloc<D, MM>(ctx, from_sigma)
+    LDGA_FOR_EACH_GRID(LDGA_CASE)
+#undef BODY
+    return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}
+
+int launch_bubble(ldga_ctx* ctx) {
+#define BODY(D, MM) run_bubble<D, MM>(ctx)
+    LDGA_FOR_EACH_GRID(LDGA_CASE)
+#undef BODY
+    return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}
+
+// EoM: forward kernel then inverse kernel; `part` selects the contribution (-1: full EoM; 0..5 the
+// calc_Σ_parts pieces).  d_tail: device scalar sum_kω(chi_m^lam) (read only when tc != 0).
+namespace {
+template <int DIM, int M>
+int run_eom_all(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
+                double chiloc_m_sum, double2* out, int out_ld, int add_hartree) {
+    int nchunk = 0;
+    int st = run_eom<DIM, M>(ctx, numax, lam_m, lam_d, part, nchunk);
+    if (st != LDGA_OK) return st;
+    return run_eom_inverse<DIM, M>(ctx, numax, nchunk, d_tail, tc, chiloc_m_sum, out, out_ld, add_hartree);
+}
+}  // namespace
+
+int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
+               double chiloc_m_sum, double2* out, int out_ld, int add_hartree) {
+#define BODY(D, MM) run_eom_all<D, MM>(ctx, numax, lam_m, lam_d, part, d_tail, tc, chiloc_m_sum, out, out_ld, add_hartree)
+    LDGA_FOR_EACH_GRID(LDGA_CASE)
+#undef BODY
+    return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}
+

@@ -1,0 +1,142 @@
+// Internal definitions of libldga_b200: handle layout, complex helpers, k-grid wedge indexing and
+// the symmetry-reduced k-space transform shared by the G setup, the bubble and the EoM kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ldga_b200.h"
+
+#define LDGA_MAX_M 33        // wedge points per axis: N/2 + 1 for N <= 64
+#define LDGA_MAX_NNU 128     // fermionic box size handled by the BSE kernels
+
+// ------------------------------------------------------------------------------------------
+// complex helpers (interleaved double2 / float2)
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ double2 cmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// 1/z computed as conj(z)/|z|^2 with a scaling step so that |z|^2 cannot overflow.
+__host__ __device__ __forceinline__ double2 cinv(double2 z) {
+    double s = fabs(z.x) > fabs(z.y) ? fabs(z.x) : fabs(z.y);
+    if (s == 0.0) return make_double2(1.0 / 0.0, 0.0);
+    double xr = z.x / s, xi = z.y / s;
+    double d = (xr * xr + xi * xi) * s;
+    return make_double2(xr / d, -xi / d);
+}
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) { return cmul(a, cinv(b)); }
+
+__host__ __device__ __forceinline__ float2 fadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 fmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// ------------------------------------------------------------------------------------------
+// wedge indexing: irreducible points (a >= b [>= c] >= 0), lexicographic order
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int widx2(int a, int b) { return a * (a + 1) / 2 + b; }
+__host__ __device__ __forceinline__ int widx3(int a, int b, int c) {
+    return a * (a + 1) * (a + 2) / 6 + b * (b + 1) / 2 + c;
+}
+__host__ __device__ __forceinline__ int sidx2(int a, int b) { return a >= b ? widx2(a, b) : widx2(b, a); }
+__host__ __device__ __forceinline__ int sidx3(int a, int b, int c) {
+    int x = a, y = b, z = c, t;
+    if (x < y) { t = x; x = y; y = t; }
+    if (y < z) { t = y; y = z; z = t; }
+    if (x < y) { t = x; x = y; y = t; }
+    return widx3(x, y, z);
+}
+__host__ __device__ __forceinline__ int wedge_count(int dim, int M) {
+    return dim == 2 ? M * (M + 1) / 2 : M * (M + 1) * (M + 2) / 6;
+}
+
+// ------------------------------------------------------------------------------------------
+// transform matrix, passed by value so that the coefficients sit in the kernel-parameter
+// constant bank and feed the FMAs directly:  T[q][m] = w_m cos(2 pi m q / N), w = 1 at m = 0 and
+// m = N/2, 2 otherwise.  For a function even in every axis (every array of this library is
+// point-group symmetric) the full-grid DFT along one axis equals this cosine sum over m <= N/2.
+// ------------------------------------------------------------------------------------------
+template <int M>
+struct TMat {
+    double t[M * M];
+};
+
+// ------------------------------------------------------------------------------------------
+// handle
+// ------------------------------------------------------------------------------------------
+struct ldga_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ldga_lattice lat{};
+    ldga_model mp{};
+    ldga_sim sp{};
+    int prec = LDGA_PREC_FP64;
+
+    int dim = 0, ns = 0, M = 0, Nk = 0, Nq = 0, Nnu = 0, Nw = 0, Nf = 0, fft_lo = 0;
+    std::vector<double> kmult, eps, Tmat;   // Tmat: M*M row-major T[q][m]
+    std::vector<int32_t> wedge;
+
+    // device arrays (column-major reference layouts, first index fastest)
+    double* d_kmult = nullptr;     // [Nq]
+    double* d_eps = nullptr;       // [Nq]
+    double2* d_ghat = nullptr;     // [Nq, Nf]   transformed G, R on the wedge
+    double2* d_gloc = nullptr;     // [Nq, Nf]   G(k, nu)
+    double2* d_sigma_loc = nullptr;
+    int n_sigma_loc = 0;
+    double2* d_chi0 = nullptr;     // [Nq, Nnu, Nw]
+    double2* d_Gamma[2] = {nullptr, nullptr};   // [Nnu, Nnu, Nw]
+    double* d_chi[2] = {nullptr, nullptr};      // [Nq, Nw]
+    double2* d_gam[2] = {nullptr, nullptr};     // [Nq, Nnu, Nw]
+    double2* d_F = nullptr;        // [Nnu, Nnu, Nw]
+    double2* d_lambda0 = nullptr;  // [Nq, Nnu, Nw]
+    double2* d_sigma = nullptr;    // [Nq, numax]
+    int sigma_numax = 0;
+    double2* d_gladder = nullptr;  // [Nq, Nf]
+    double2* d_partial = nullptr;  // EoM partial sums [nchunk, Nq, numax]
+    size_t partial_elems = 0;
+    double* d_red = nullptr;       // reduction scratch
+    int32_t* d_flags = nullptr;    // BSE fallback flags [Nq*Nw]
+    int32_t* d_list = nullptr;     // compacted fallback list
+    int32_t* d_count = nullptr;
+
+    bool have_ghat = false, have_chi0 = false, have_F = false, have_lambda0 = false, have_sigma = false;
+    bool have_Gamma[2] = {false, false}, have_chi[2] = {false, false}, have_gam[2] = {false, false};
+    int lambda_dm_evals = 0;
+
+    std::string err;
+};
+
+// error helpers (host)
+int ctx_fail(ldga_ctx* ctx, int code, const std::string& msg);
+int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what);
+#define LDGA_CUDA(ctx, call)                                        \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return ctx_cuda((ctx), _e, #call);   \
+    } while (0)
+#define LDGA_LAUNCHED(ctx, what)                                    \
+    do {                                                            \
+        cudaError_t _e = cudaGetLastError();                        \
+        if (_e != cudaSuccess) return ctx_cuda((ctx), _e, what);    \
+    } while (0)
+
+// kernel launchers implemented in the .cu files
+int launch_gloc_transform(ldga_ctx* ctx, bool from_sigma);
+int launch_bubble(ldga_ctx* ctx);
+int launch_bse(ldga_ctx* ctx, int channel, int* n_fallback);
+int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp);
+int launch_lambda0(ldga_ctx* ctx);
+int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
+               double chiloc_m_sum, double2* out, int out_ld, int add_hartree);
+int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int deriv, double* d_out);
+int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
+int launch_lambda_m(ldga_ctx* ctx, double rhs, double* d_out /*[2]*/);
+int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[8]*/);
+int launch_g_ladder_full(ldga_ctx* ctx, int numax, double mu);
