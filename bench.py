@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Throughput of the lDGA ladder chain on B200.
+
+One step = the whole hot path for one parameter point of the 3D simple-cubic workload
+(eps_k = -2t sum cos k_i, N_k = 32^3 -> 969 irreducible q, beta = 20, U = 1.5, Nnu = 40, Nw = 41):
+lattice G and its transform -> bubble chi0 -> Bethe-Salpeter (m, d) -> F_m, lambda_0 -> lambda_m
+correction (device Newton) -> EoM Sigma_ladder(lambda_m) -> mu fit, G_ladder, energies.
+metric = (q, w)-points per second = N_q * N_w per step, summed over ranks (each rank runs its own
+seeded parameter point: weak scaling, no data-path collective).
+
+  value  device-resident inputs; per-step CUDA-event time on the stream the library launches on
+  e2e    the same chain through the C ABI from pinned HOST buffers (inputs copied in, Sigma_ladder,
+         chi_m, chi_d, lambda, mu, energies copied out inside the timed region)
+  --impl reference  the CPU restatement (oracle/) of the reference algorithm on all host cores
+
+L2 is flushed (256 MiB write) before every timed step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(cfg=3, dim=3, ns=32, beta=20.0, U=1.5, n_iv=20, n_iw=20)
+WORKLOAD_NAME = "3D sc Nk=32^3 (969 irreducible q), beta=20, U=1.5, Nnu=40, Nw=41, lambda_m"
+METRIC = "(q,w)-points/s"
+PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--prec", default="mixed", choices=list(PREC_NAMES))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--out", default=None, help="also write the JSON line to this file")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ----------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return self.summary()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, n in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU baseline: the oracle restatement of the reference algorithm on the host cores
+# ----------------------------------------------------------------------------------------------
+def cpu_chain_seconds(inp) -> float:
+    from oracle import ldga_ref as R
+    R.set_workers(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    R.run_chain(inp, lambda_type="m")
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(inp, points: int) -> dict:
+    t = cpu_chain_seconds(inp)
+    return {"value": points / t, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"one full chain of the workload ({t:.1f} s): NumPy/SciPy FP64 restatement of the "
+                      "reference algorithm (oracle/ldga_ref.py), scipy.fft workers and OpenBLAS threads = all cores"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from ladderdga_b200 import synthetic as S
+    inp = S.config_input(WORKLOAD["cfg"])
+    points = 969 * (2 * WORKLOAD["n_iw"] + 1)
+    for _ in range(args.warmup):
+        cpu_chain_seconds(inp)
+    ts = [cpu_chain_seconds(inp) for _ in range(args.steps)]
+    ms = 1000.0 * float(np.mean(ts))
+    value = points / (ms / 1000.0)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD_NAME, "global_batch": 1, "l2": "inputs resident in host memory"},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": "full chain of the workload per step on the CPU restatement (oracle/)"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if args.out:
+        open(args.out, "w").write(json.dumps(line) + "\n")
+    return 0
+
+
+# ----------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------
+class Chain:
+    """The device chain for one parameter point, driven through the C ABI."""
+
+    def __init__(self, inp, prec: int, device: int):
+        import torch
+        import ladderdga_b200 as L
+        self.L, self.torch = L, torch
+        self.inp = inp
+        self.h = L.setup_synthetic(inp, precision=prec, device=device)
+        self.ctx = self.h.ctx
+        self.lib = self.ctx.lib
+        self.stream = torch.cuda.current_stream(device)
+        self.ctx.call("ldga_set_stream", C.c_void_p(self.stream.cuda_stream))
+        h = self.h
+        dev = torch.device("cuda", device)
+
+        def cplx(a):
+            return np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+
+        host = {"sigma_loc": cplx(h.Σ_loc), "gamma_m": cplx(h.Γ_m), "gamma_d": cplx(h.Γ_d),
+                "chi_loc_m": cplx(h.χDMFT_m), "gimp": cplx(h.gImp)}
+        self.h2d_bytes = sum(v.nbytes for v in host.values())
+        # pinned host copies (e2e) and device-resident copies (value)
+        self.pin = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
+        self.dev = {k: torch.from_numpy(v).to(dev) for k, v in host.items()}
+        self.n_sigma = len(h.Σ_loc)
+        self.n_gimp = len(h.gImp)
+        nq, nw, numax = self.ctx.Nq, self.ctx.Nw, h.sP.n_iν
+        self.numax = numax
+        self.out_sigma = torch.empty(nq * numax * 2, dtype=torch.float64).pin_memory()
+        self.out_chi_m = torch.empty(nq * nw, dtype=torch.float64).pin_memory()
+        self.out_chi_d = torch.empty(nq * nw, dtype=torch.float64).pin_memory()
+        self.d2h_bytes = (self.out_sigma.numel() + self.out_chi_m.numel() + self.out_chi_d.numel()) * 8 + 5 * 8
+        self.points = nq * nw
+
+    def step(self, src: dict, outputs: bool, graph: bool = True):
+        """One parameter point through ldga_chain_m (captured once in a CUDA graph, then replayed)."""
+        p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        sc = (C.c_double * 8)()
+        self.ctx.call("ldga_chain_m", p(src["sigma_loc"]), self.n_sigma, p(src["gamma_m"]), p(src["gamma_d"]),
+                      p(src["chi_loc_m"]), p(src["gimp"]), self.n_gimp, self.h.imp_density, self.h.χloc_m_sum,
+                      int(graph), p(self.out_sigma) if outputs else None, p(self.out_chi_m) if outputs else None,
+                      p(self.out_chi_d) if outputs else None, sc)
+        return list(sc)
+
+
+def stage_times(chain):
+    from ladderdga_b200._lib import STAGES
+    ms = (C.c_double * 10)()
+    cnt = (C.c_int32 * 10)()
+    chain.ctx.call("ldga_stage_times", ms, cnt)
+    return {STAGES[i]: (ms[i], cnt[i]) for i in range(10)}
+
+
+def roofline(stages: dict, chain, peaks: dict) -> dict:
+    """Dominant stage of the step and its roofline (algorithmic work per launch / CUDA-event time)."""
+    name = max(stages, key=lambda k: stages[k][0])
+    tot, cnt = stages[name]
+    t = tot / max(cnt, 1) / 1e3   # seconds per launch
+    nq, nnu, nw = chain.ctx.Nq, chain.ctx.Nnu, chain.ctx.Nw
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    if name == "bse":
+        # per (q, w): complex elimination of [B | 1], N^3/2 complex multiply-adds (8 flops each);
+        # one launch = one channel, N_q N_w matrices
+        flops = nq * nw * 8.0 * nnu**3 / 2
+        ach = flops / t / 1e12
+        # bound: FP32 (mixed) / FP64 CUDA-core pipes, nominal B200 rates at the measured max clock
+        sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+        fp = "fp32" if chain.ctx.precision == 2 else "fp64"
+        lanes = 128 if fp == "fp32" else 64
+        peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
+        return {"kernel": "k_bse_gj (" + fp + ")", "bound": fp, "achieved": ach, "peak": peak,
+                "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "peak_source": f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz"}
+    # HBM-bound stages: algorithmic bytes per launch
+    byts = {
+        "bubble": (nq * (nnu + 1) * 16 * 2 + nq * nnu * nw * 16),
+        "eom_forward": nq * chain.numax * nw * (3 * 16 + 2 * 8) + nq * chain.numax * 16,
+        "gloc": nq * chain.ctx.Nf * 16 * 2,
+    }.get(name, nq * nnu * nw * 16)
+    ach = byts / t / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": None, "peak_source": "measured hbm_gbs"}
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from ladderdga_b200 import synthetic as S
+    inp = S.config_input(WORKLOAD["cfg"], point=rank)
+    chain = Chain(inp, PREC_NAMES[args.prec], local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+    def timed(src, outputs):
+        times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(chain.stream)
+            chain.step(src, outputs)
+            b.record(chain.stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        return times
+
+    # the stage events are recorded inside the graph, so profiling is on for capture and timing
+    chain.ctx.call("ldga_profile", 1)
+    for _ in range(max(args.warmup, 3)):
+        scal = chain.step(chain.dev, False)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    stage_times(chain)
+    n0 = C.c_int64()
+    chain.ctx.call("ldga_launch_count", C.byref(n0))
+    t_dev = timed(chain.dev, False)
+    n1 = C.c_int64()
+    chain.ctx.call("ldga_launch_count", C.byref(n1))
+    stages = stage_times(chain)
+    for _ in range(max(args.warmup, 3)):
+        chain.step(chain.pin, True)
+    t_e2e = timed(chain.pin, True)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    chain.ctx.call("ldga_profile", 0)
+    ms = float(np.mean(t_dev))
+    ms_e2e = float(np.mean(t_e2e))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    value = world * chain.points / (ms / 1e3)
+    e2e = world * chain.points / (ms_e2e / 1e3)
+    launches = int(n1.value - n0.value)
+    if rank == 0:
+        rl = roofline(stages, chain, peaks)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
+                "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
+                "config": {"workload": WORKLOAD_NAME, "global_batch": world, "seq_len": None,
+                           "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
+                           "points_per_step_per_gpu": chain.points},
+                "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": chain.h2d_bytes,
+                        "d2h_bytes_per_step": chain.d2h_bytes, "ms_per_step": ms_e2e,
+                        "path": "C ABI (ldga_*) from pinned host buffers"},
+                "roofline": rl,
+                "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items() if v[1]},
+                "gpu_launches": launches,
+                "result": {"lambda_m": scal[0], "mu": scal[1], "E_kin": scal[2], "E_pot1": scal[3],
+                           "newton_iterations": scal[6]},
+                "clocks": clk}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(inp, chain.points)
+        print(json.dumps(line), flush=True)
+        if args.out:
+            open(args.out, "w").write(json.dumps(line) + "\n")
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -82,6 +82,29 @@ const char* ldga_last_error(const ldga_ctx* ctx);
 const char* ldga_status_string(int32_t status);
 int ldga_version(void);
 
+/* Run the handle's work on the caller's CUDA stream (a cudaStream_t; NULL: the handle's own
+ * stream).  No reference counterpart: lets a host application order the ladder kernels with its own. */
+int ldga_set_stream(ldga_ctx* ctx, void* stream);
+
+/* Per-stage device timing with CUDA events on the handle's stream (no reference counterpart; the
+ * reference times stages with TimerOutputs, DepsInit.jl:71).  enable != 0 starts accumulating;
+ * ldga_stage_times returns, per stage, total milliseconds and launch counts (LDGA_N_STAGES each). */
+#define LDGA_N_STAGES 10
+#define LDGA_STAGE_GLOC 0
+#define LDGA_STAGE_BUBBLE 1
+#define LDGA_STAGE_BSE 2
+#define LDGA_STAGE_BSE_FALLBACK 3
+#define LDGA_STAGE_LAMBDA0 4
+#define LDGA_STAGE_SUMS 5
+#define LDGA_STAGE_LAMBDA_NEWTON 6
+#define LDGA_STAGE_EOM_FORWARD 7
+#define LDGA_STAGE_EOM_INVERSE 8
+#define LDGA_STAGE_GLADDER 9
+int ldga_profile(ldga_ctx* ctx, int32_t enable);
+int ldga_stage_times(ldga_ctx* ctx, double* ms, int32_t* counts);
+/* Number of kernels this handle has launched since it was created. */
+int ldga_launch_count(const ldga_ctx* ctx, int64_t* n);
+
 /* Replace the model parameters (e.g. a new mu); mutable ModelParameters, Config.jl:39. */
 int ldga_set_model(ldga_ctx* ctx, const ldga_model* mp);
 int ldga_set_precision(ldga_ctx* ctx, int32_t precision);
@@ -122,6 +145,17 @@ int ldga_set_chi0(ldga_ctx* ctx, const double* chi0);
  * n_fallback (may be NULL): matrices re-solved by the pivoted FP64 path. */
 int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* chi_out,
              double* gam_out, int32_t* n_fallback);
+
+/* Copy a device-resident array of the handle to `out` (host or device) without recomputing it.
+ * No reference counterpart: the reference's arrays live in Julia memory; here they stay in HBM
+ * until asked for.  what: one of LDGA_GET_*; channel only for chi and gamma. */
+#define LDGA_GET_CHI0 0      /* [Nq, Nnu, Nw] complex */
+#define LDGA_GET_CHI 1       /* [Nq, Nw] real */
+#define LDGA_GET_GAMMA 2     /* [Nq, Nnu, Nw] complex */
+#define LDGA_GET_LAMBDA0 3   /* [Nq, Nnu, Nw] complex */
+#define LDGA_GET_SIGMA 4     /* [Nq, numax] complex, numax of the last EoM */
+#define LDGA_GET_GLOC 5      /* [Nq, Nf] complex */
+int ldga_get(ldga_ctx* ctx, int32_t what, int32_t channel, double* out);
 
 /* Upload chi_r [Nq, Nw] / gamma_r [Nq, Nnu, Nw] produced elsewhere (the chiT/gammaT data). */
 int ldga_set_chi(ldga_ctx* ctx, int32_t channel, const double* chi);
@@ -193,6 +227,22 @@ int ldga_set_sigma(ldga_ctx* ctx, const double* sigma, int32_t numax);
  * nu_n = 0..numax-1 (NULL: the handle's G_ladder / Sigma_ladder). */
 int ldga_calc_E(ldga_ctx* ctx, const double* G, const double* sigma, int32_t numax, double mu,
                 double* e_kin, double* e_pot);
+
+/* ---------------------------------------------------------------- fused chain ---------------- */
+
+/* The plain lambda_m chain of scripts/run_minimal.jl:7-14 for one parameter point, as one call:
+ * ldga_gloc -> ldga_bubble -> ldga_bse(m) -> ldga_bse(d) -> ldga_F_from_chi -> ldga_lambda0 ->
+ * λm_correction_full (conditions_new.jl:174-190: rhs = 2 imp_density - sum_kω chi_d, device Newton,
+ * EoM at numax = Nnu/2, μ fit, energies).  Everything is enqueued without host round trips; with
+ * use_graph != 0 and pinned-host or device pointers the sequence is captured once in a CUDA graph
+ * and replayed while the pointers and scalars stay the same.
+ * Inputs (host or device): sigma_loc [n_sigma], gamma_m, gamma_d, chi_loc_m [Nnu, Nnu, Nw], gimp [n_gimp].
+ * Outputs (may be NULL): sigma_out [Nq, Nnu/2], chi_m_out, chi_d_out [Nq, Nw], scalars_out[8] =
+ * {λm, μ, E_kin, E_pot1, E_pot2, PP_p2, Newton iterations, filling}. */
+int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const double* gamma_m,
+                 const double* gamma_d, const double* chi_loc_m, const double* gimp, int32_t n_gimp,
+                 double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
+                 double* chi_m_out, double* chi_d_out, double* scalars_out);
 
 /* ---------------------------------------------------------------- a14: lambda_dm ------------- */
 

@@ -25,8 +25,12 @@ EXPORTS = [
     "ldga_set_chi0", "ldga_bse", "ldga_set_chi", "ldga_set_gamma", "ldga_F_from_chi", "ldga_lambda0",
     "ldga_set_lambda0", "ldga_sum_kw", "ldga_sum_wk", "ldga_lambda_min", "ldga_eom", "ldga_eom_parts",
     "ldga_lambda_m", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
-    "ldga_lambda_dm_evals",
+    "ldga_lambda_dm_evals", "ldga_set_stream", "ldga_profile", "ldga_stage_times", "ldga_launch_count",
+    "ldga_get", "ldga_chain_m",
 ]
+GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
+STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
+          "eom_inverse", "g_ladder"]
 
 
 class LibraryMissing(RuntimeError):
@@ -96,6 +100,12 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_g_ladder": (C.c_int, [P, P, I32, I32, D, PD, P, PD, PD, PD]),
         "ldga_lambda_dm": (C.c_int, [P, D, I32, D, D, I32, PD, PD, PI32, P, PI32, P, P]),
         "ldga_lambda_dm_evals": (C.c_int, [P, PI32]),
+        "ldga_set_stream": (C.c_int, [P, P]),
+        "ldga_profile": (C.c_int, [P, I32]),
+        "ldga_stage_times": (C.c_int, [P, PD, PI32]),
+        "ldga_launch_count": (C.c_int, [P, C.POINTER(C.c_int64)]),
+        "ldga_get": (C.c_int, [P, I32, I32, P]),
+        "ldga_chain_m": (C.c_int, [P, P, I32, P, P, P, P, I32, D, D, I32, P, P, P, P]),
         "ldga_set_sigma": (C.c_int, [P, P, I32]),
         "ldga_calc_E": (C.c_int, [P, P, P, I32, D, PD, PD]),
     }

@@ -838,19 +838,27 @@ def setup_LDGA(kGridStr, mP: ModelParameters, sP: SimulationParameters, inputs, 
                       χDMFT_d, χ_m_loc, γ_m_loc, χ_d_loc, γ_d_loc, χ0Loc, gimp, ctx=ctx, ctx_loc=ctx_loc)
 
 
-def _fetch(ctx: Context, what: str) -> np.ndarray:
+def _fetch(ctx: Context, what: str, ch: int = 0) -> np.ndarray:
+    """Copy a device-resident array of the handle to the host (ldga_get)."""
     if what == "chi0":
         out = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
-        # re-running the bubble is the only device->host path for χ0 through the C ABI
-        ctx.call("ldga_bubble", ptr(out))
-        return out
-    raise KeyError(what)
+        ctx.call("ldga_get", _lib.GET_CHI0, 0, ptr(out))
+    elif what == "gamma":
+        out = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+        ctx.call("ldga_get", _lib.GET_GAMMA, ch, ptr(out))
+    elif what == "lambda0":
+        out = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+        ctx.call("ldga_get", _lib.GET_LAMBDA0, 0, ptr(out))
+    elif what == "gloc":
+        out = _lib.cplx_out((ctx.Nq, ctx.Nf))
+        ctx.call("ldga_get", _lib.GET_GLOC, 0, ptr(out))
+    else:
+        raise KeyError(what)
+    return out
 
 
 def _fetch_gloc(ctx: Context, Σ_loc: np.ndarray) -> np.ndarray:
-    out = _lib.cplx_out((ctx.Nq, ctx.Nf))
-    ctx.call("ldga_gloc", ptr(Σ_loc), len(Σ_loc), ptr(out))
-    return out
+    return _fetch(ctx, "gloc")
 
 
 def setup_synthetic(inp, precision: int = PREC_FP64, device: int = 0, usable_prct_reduction: float = 0.0) -> lDΓAHelper:
@@ -880,9 +888,7 @@ def _bse(ctx: Context, ch: int, Γ, mP, χ0: χ0T | None = None):
     ctx.call("ldga_bse", ch, ptr(as_fc(Γ)) if Γ is not None else None, ptr(χ), None, _lib.C.byref(nfb))
 
     def fetch_gamma():
-        out = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
-        ctx.call("ldga_bse", ch, None, None, ptr(out), None)
-        return out
+        return _fetch(ctx, "gamma", ch)
 
     c = χT(χ, mP.β, tail_c=[0.0, 0.0, mP.Ekin_DMFT])._bind(ctx, ch)
     c.n_fallback = nfb.value
@@ -936,12 +942,7 @@ def calc_λ0(χ0: χ0T, h: lDΓAHelper, Fr=None) -> DeviceArray:
     else:
         ctx.call("ldga_lambda0", ptr(as_fc(Fr)), None)
 
-    def fetch():
-        out = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
-        ctx.call("ldga_lambda0", None, ptr(out))
-        return out
-
-    arr = DeviceArray(ctx, fetch, (ctx.Nq, ctx.Nnu, ctx.Nw))
+    arr = DeviceArray(ctx, lambda: _fetch(ctx, "lambda0"), (ctx.Nq, ctx.Nnu, ctx.Nw))
     arr._is_lambda0 = True
     return arr
 

@@ -26,6 +26,29 @@ int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what) {
     return ctx_fail(ctx, LDGA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// While a graph is captured the two event records become graph nodes; their (stage, slot) pairs are
+// kept with the graph and read after every replay (ldga_chain_m).
+StageTimer::StageTimer(ldga_ctx* ctx, int st) : c(ctx), stage(st), slot(-1) {
+    if (!c || !c->profiling) return;
+    if (c->ev_free.empty()) {
+        ldga_ctx::EvPair p;
+        if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) return;
+        c->ev_pool.push_back(p);
+        c->ev_free.push_back((int)c->ev_pool.size() - 1);
+    }
+    slot = c->ev_free.back();
+    c->ev_free.pop_back();
+    // inside a capture only "external" records become event-record nodes that can be timed later
+    cudaEventRecordWithFlags(c->ev_pool[slot].a, c->stream, c->capturing ? cudaEventRecordExternal : 0);
+}
+
+StageTimer::~StageTimer() {
+    if (slot < 0) return;
+    cudaEventRecordWithFlags(c->ev_pool[slot].b, c->stream, c->capturing ? cudaEventRecordExternal : 0);
+    if (c->capturing) c->graph_ev.emplace_back(stage, slot);
+    else c->ev_pending.emplace_back(stage, slot);
+}
+
 namespace {
 
 template <typename T>
@@ -213,10 +236,11 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     c->Nnu = 2 * sp->n_iv; c->Nw = 2 * sp->n_iw + 1;
     c->Nf = sp->fft_hi - sp->fft_lo + 1; c->fft_lo = sp->fft_lo;
     build_kgrid(c);
-    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { g_create_error = cudaGetErrorString(e); delete c; return LDGA_ERR_CUDA; }
+    c->stream = c->own_stream;
     int st = alloc_all(c);
-    if (st != LDGA_OK) { g_create_error = c->err; free_all(c); cudaStreamDestroy(c->stream); delete c; return st; }
+    if (st != LDGA_OK) { g_create_error = c->err; free_all(c); cudaStreamDestroy(c->own_stream); delete c; return st; }
     *out = c;
     return LDGA_OK;
 }
@@ -226,8 +250,55 @@ int ldga_destroy(ldga_ctx* ctx) {
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     free_all(ctx);
-    cudaStreamDestroy(ctx->stream);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    if (ctx->d_chiloc) cudaFree(ctx->d_chiloc);
+    if (ctx->d_gimp) cudaFree(ctx->d_gimp);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    for (auto& p : ctx->ev_pool) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return LDGA_OK;
+}
+
+int ldga_set_stream(ldga_ctx* ctx, void* stream) {
+    if (!ctx) return LDGA_ERR_ARG;
+    DeviceGuard g(ctx->device);
+    LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return LDGA_OK;
+}
+
+int ldga_profile(ldga_ctx* ctx, int32_t enable) {
+    if (!ctx) return LDGA_ERR_ARG;
+    ctx->profiling = enable != 0;
+    return LDGA_OK;
+}
+
+int ldga_launch_count(const ldga_ctx* ctx, int64_t* n) {
+    if (!ctx || !n) return LDGA_ERR_ARG;
+    *n = ctx->n_launches;
+    return LDGA_OK;
+}
+
+int ldga_stage_times(ldga_ctx* ctx, double* ms, int32_t* counts) {
+    if (!ctx) return LDGA_ERR_ARG;
+    DeviceGuard g(ctx->device);
+    LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (auto& pr : ctx->ev_pending) {
+        float t = 0.f;
+        LDGA_CUDA(ctx, cudaEventElapsedTime(&t, ctx->ev_pool[pr.second].a, ctx->ev_pool[pr.second].b));
+        ctx->stage_ms[pr.first] += t;
+        ctx->stage_cnt[pr.first] += 1;
+        ctx->ev_free.push_back(pr.second);
+    }
+    ctx->ev_pending.clear();
+    for (int i = 0; i < LDGA_N_STAGES; ++i) {
+        if (ms) ms[i] = ctx->stage_ms[i];
+        if (counts) counts[i] = ctx->stage_cnt[i];
+        ctx->stage_ms[i] = 0.0;
+        ctx->stage_cnt[i] = 0;
+    }
     return LDGA_OK;
 }
 
@@ -303,12 +374,55 @@ int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* c
         ctx->have_Gamma[channel] = true;
     }
     NEED(ctx, ctx->have_Gamma[channel], "calc_χγ: Gamma_r missing");
-    int nfb = 0;
-    TRY(launch_bse(ctx, channel, &nfb));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    TRY(launch_bse(ctx, channel, ctx->d_count + 1));
+    int32_t cnt[2] = {0, 0};
+    TRY(copy(ctx, cnt, ctx->d_count, 2 * sizeof(int32_t)));
+    TRY(sync(ctx));
     ctx->have_chi[channel] = ctx->have_gam[channel] = true;
-    if (n_fallback) *n_fallback = nfb;
+    if (n_fallback) *n_fallback = bse_has_fast_path(ctx->Nnu) ? cnt[0] : ctx->Nq * ctx->Nw;
+    if (cnt[1] > 0)
+        return ctx_fail(ctx, LDGA_ERR_NUMERIC, std::to_string(cnt[1]) + " BSE matrices are singular or non-finite");
     if (chi_out) TRY(copy(ctx, chi_out, ctx->d_chi[channel], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
     if (gam_out) TRY(copy(ctx, gam_out, ctx->d_gam[channel], (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    return sync(ctx);
+}
+
+int ldga_get(ldga_ctx* ctx, int32_t what, int32_t channel, double* out) {
+    if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw;
+    const bool ch_ok = channel == LDGA_CH_M || channel == LDGA_CH_D;
+    switch (what) {
+        case LDGA_GET_CHI0:
+            NEED(ctx, ctx->have_chi0, "chi0 not computed");
+            TRY(copy(ctx, out, ctx->d_chi0, qvw * sizeof(double2)));
+            break;
+        case LDGA_GET_CHI:
+            if (!ch_ok) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+            NEED(ctx, ctx->have_chi[channel], "chi not computed");
+            TRY(copy(ctx, out, ctx->d_chi[channel], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
+            break;
+        case LDGA_GET_GAMMA:
+            if (!ch_ok) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+            NEED(ctx, ctx->have_gam[channel], "gamma not computed");
+            TRY(copy(ctx, out, ctx->d_gam[channel], qvw * sizeof(double2)));
+            break;
+        case LDGA_GET_LAMBDA0:
+            NEED(ctx, ctx->have_lambda0, "lambda0 not computed");
+            TRY(copy(ctx, out, ctx->d_lambda0, qvw * sizeof(double2)));
+            break;
+        case LDGA_GET_SIGMA:
+            NEED(ctx, ctx->have_sigma, "Sigma_ladder not computed");
+            TRY(copy(ctx, out, ctx->d_sigma, (size_t)ctx->Nq * ctx->sigma_numax * sizeof(double2)));
+            break;
+        case LDGA_GET_GLOC:
+            NEED(ctx, ctx->have_ghat, "G not set");
+            TRY(copy(ctx, out, ctx->d_gloc, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
+            break;
+        default:
+            return ctx_fail(ctx, LDGA_ERR_ARG, "unknown array id");
+    }
     return sync(ctx);
 }
 
@@ -416,7 +530,8 @@ int eom_device(ldga_ctx* ctx, double lam_m, double lam_d, int numax, int tc, dou
     if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
     if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
     if (tc) TRY(launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8));
-    TRY(launch_eom(ctx, numax, lam_m, lam_d, -1, ctx->d_red + 8, tc, chiloc_m_sum, ctx->d_sigma, ctx->Nq, 1));
+    TRY(launch_eom(ctx, numax, lam_m, lam_d, nullptr, nullptr, -1, ctx->d_red + 8, tc, chiloc_m_sum, ctx->d_sigma,
+                   ctx->Nq, 1));
     ctx->have_sigma = true;
     ctx->sigma_numax = numax;
     return LDGA_OK;
@@ -444,7 +559,8 @@ int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double
     LDGA_CUDA(ctx, cudaMallocAsync(reinterpret_cast<void**>(&d_parts), 7 * blk * sizeof(double2), ctx->stream));
     int st = LDGA_OK;
     for (int p = 0; p < 6 && st == LDGA_OK; ++p)
-        st = launch_eom(ctx, numax, lam_m, lam_d, p, ctx->d_red, 0, 0.0, d_parts + p * blk, ctx->Nq, p == 5 ? 1 : 0);
+        st = launch_eom(ctx, numax, lam_m, lam_d, nullptr, nullptr, p, ctx->d_red, 0, 0.0, d_parts + p * blk, ctx->Nq,
+                        p == 5 ? 1 : 0);
     double tnum = 0.0;
     if (st == LDGA_OK && tc) {
         st = launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8);
@@ -464,7 +580,7 @@ int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iteration
     if (!ctx || !lam_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
     NEED(ctx, ctx->have_chi[LDGA_CH_M], "λm_correction: chi_m missing");
     DeviceGuard g(ctx->device);
-    TRY(launch_lambda_m(ctx, rhs, ctx->d_red + 16));
+    TRY(launch_lambda_m(ctx, rhs, nullptr, ctx->d_red + 16));
     double r[2];
     TRY(copy(ctx, r, ctx->d_red + 16, 2 * sizeof(double)));
     TRY(sync(ctx));
@@ -485,7 +601,7 @@ int ldga_g_ladder(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, int32
     TRY(copy(ctx, r, ctx->d_red + 24, 4 * sizeof(double)));
     TRY(sync(ctx));
     if (G_out) {
-        TRY(launch_g_ladder_full(ctx, ctx->sigma_numax, r[0]));
+        TRY(launch_g_ladder_full(ctx, ctx->sigma_numax, ctx->d_red + 24));
         TRY(copy(ctx, G_out, ctx->d_gladder, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
         TRY(sync(ctx));
     }
@@ -530,6 +646,162 @@ int ldga_calc_E(ldga_ctx* ctx, const double* G, const double* sigma, int32_t num
     TRY(sync(ctx));
     if (e_kin) *e_kin = r[0];
     if (e_pot) *e_pot = r[1];
+    return LDGA_OK;
+}
+
+// -------------------------------------------------------------------------- fused lambda_m chain --
+namespace {
+
+bool host_pageable(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return true; }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+struct ChainArgs {
+    const double *sigma_loc, *gamma_m, *gamma_d, *chi_loc_m, *gimp;
+    int n_sigma, n_gimp;
+    double imp_density, chiloc_m_sum;
+    double *sigma_out, *chi_m_out, *chi_d_out;
+};
+
+// Enqueue the whole chain on ctx->stream; nothing here waits for the device.
+int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
+    const size_t nG = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw * sizeof(double2);
+    const int numax = ctx->Nnu / 2;
+    TRY(copy(ctx, ctx->d_sigma_loc, a.sigma_loc, (size_t)a.n_sigma * sizeof(double2)));
+    TRY(copy(ctx, ctx->d_Gamma[0], a.gamma_m, nG));
+    TRY(copy(ctx, ctx->d_Gamma[1], a.gamma_d, nG));
+    TRY(copy(ctx, ctx->d_chiloc, a.chi_loc_m, nG));
+    TRY(copy(ctx, ctx->d_gimp, a.gimp, (size_t)a.n_gimp * sizeof(double2)));
+    TRY(launch_gloc_transform(ctx, true));                       // a1
+    TRY(launch_bubble(ctx));                                     // a2
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    TRY(launch_bse(ctx, LDGA_CH_M, ctx->d_count + 1));           // a7
+    TRY(launch_bse(ctx, LDGA_CH_D, ctx->d_count + 1));
+    TRY(launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp));   // a5
+    TRY(launch_lambda0(ctx));                                    // a6
+    // λm_correction_full (conditions_new.jl:174-190): rhs = 2 imp_density - sum_kω(chi_d)
+    TRY(launch_sum_kw(ctx, LDGA_CH_D, 0.0, 0, ctx->d_red + 56));
+    TRY(launch_lambda_m(ctx, 2.0 * a.imp_density, ctx->d_red + 56, ctx->d_red + 16));
+    TRY(launch_sum_kw(ctx, LDGA_CH_M, 0.0, 0, ctx->d_red + 8, ctx->d_red + 16));   // sum_kω(chi_m, λ = λm)
+    TRY(launch_eom(ctx, numax, 0.0, 0.0, ctx->d_red + 16, nullptr, -1, ctx->d_red + 8, 1, a.chiloc_m_sum,
+                   ctx->d_sigma, ctx->Nq, 1));                   // a10 at λm
+    TRY(launch_g_ladder(ctx, numax, 1, ctx->mp.mu, ctx->d_red + 24));   // a15: μ fit, energies
+    if (a.sigma_out) TRY(copy(ctx, a.sigma_out, ctx->d_sigma, (size_t)ctx->Nq * numax * sizeof(double2)));
+    if (a.chi_m_out) TRY(copy(ctx, a.chi_m_out, ctx->d_chi[0], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
+    if (a.chi_d_out) TRY(copy(ctx, a.chi_d_out, ctx->d_chi[1], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
+    TRY(copy(ctx, ctx->h_stage, ctx->d_red, 64 * sizeof(double)));
+    TRY(copy(ctx, ctx->h_stage + 64, ctx->d_count, 4 * sizeof(int32_t)));
+    return LDGA_OK;
+}
+
+uint64_t dbits(double x) { uint64_t u; std::memcpy(&u, &x, 8); return u; }
+
+}  // namespace
+
+int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const double* gamma_m,
+                 const double* gamma_d, const double* chi_loc_m, const double* gimp, int32_t n_gimp,
+                 double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
+                 double* chi_m_out, double* chi_d_out, double* scalars_out) {
+    if (!ctx || !sigma_loc || !gamma_m || !gamma_d || !chi_loc_m || !gimp)
+        return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    const int L = std::max(std::abs(ctx->sp.fft_lo), std::abs(ctx->sp.fft_hi));
+    if (n_sigma <= L) return ctx_fail(ctx, LDGA_ERR_ARG, "Sigma_loc must cover n = 0..max|fft_range|");
+    const int need_g = 2 * ctx->sp.n_iv + ctx->sp.n_iw + (ctx->sp.shift ? ctx->sp.n_iw : 0);
+    if (n_gimp < need_g) return ctx_fail(ctx, LDGA_ERR_ARG, "G_imp too short for the frequency box");
+    // buffers (allocated outside any capture)
+    if (n_sigma > ctx->n_sigma_loc) {
+        if (ctx->d_sigma_loc) cudaFree(ctx->d_sigma_loc);
+        ctx->d_sigma_loc = nullptr;
+        TRY(dev_alloc(ctx, &ctx->d_sigma_loc, (size_t)n_sigma));
+        ctx->n_sigma_loc = n_sigma;
+    }
+    ctx->n_sigma_loc = std::max(ctx->n_sigma_loc, (int)n_sigma);
+    TRY(dev_alloc(ctx, &ctx->d_chiloc, (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw));
+    if (n_gimp > ctx->n_gimp_alloc) {
+        if (ctx->d_gimp) cudaFree(ctx->d_gimp);
+        ctx->d_gimp = nullptr;
+        TRY(dev_alloc(ctx, &ctx->d_gimp, (size_t)n_gimp));
+        ctx->n_gimp_alloc = n_gimp;
+    }
+    if (!ctx->h_stage) LDGA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), 64 * sizeof(double) + 16));
+    ChainArgs a{sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, n_sigma, n_gimp, imp_density, chiloc_m_sum,
+                sigma_out, chi_m_out, chi_d_out};
+    const void* ptrs[] = {sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, sigma_out, chi_m_out, chi_d_out};
+    bool graphable = use_graph != 0;
+    for (const void* p : ptrs)
+        if (host_pageable(p)) graphable = false;   // stream capture needs pinned or device memory
+    std::vector<uint64_t> key;
+    if (graphable) {
+        for (const void* p : ptrs) key.push_back((uint64_t)(uintptr_t)p);
+        key.insert(key.end(), {(uint64_t)n_sigma, (uint64_t)n_gimp, dbits(imp_density), dbits(chiloc_m_sum),
+                               dbits(ctx->mp.U), dbits(ctx->mp.mu), dbits(ctx->mp.beta), dbits(ctx->mp.n),
+                               dbits(ctx->mp.Ekin_DMFT), (uint64_t)ctx->prec, (uint64_t)(uintptr_t)ctx->stream,
+                               (uint64_t)ctx->profiling});
+    }
+    bool replayed = false;
+    if (graphable && ctx->graph_exec && key == ctx->graph_key) {
+        LDGA_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+        ctx->n_launches += ctx->graph_launches;
+        replayed = true;
+    } else {
+        TRY(chain_m_enqueue(ctx, a));   // the uncaptured run computes this call's results
+        if (graphable) {
+            if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+            if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+            for (auto& pr : ctx->graph_ev) ctx->ev_free.push_back(pr.second);
+            ctx->graph_ev.clear();
+            ctx->capturing = true;
+            const int64_t n0 = ctx->n_launches;
+            cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+            int st = e == cudaSuccess ? chain_m_enqueue(ctx, a) : LDGA_ERR_CUDA;
+            cudaGraph_t gr = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &gr);
+            ctx->capturing = false;
+            ctx->graph_launches = ctx->n_launches - n0;   // kernels in the graph (nothing ran yet)
+            ctx->n_launches = n0;
+            if (e != cudaSuccess || st != LDGA_OK || e2 != cudaSuccess || !gr) {
+                if (gr) cudaGraphDestroy(gr);
+                cudaGetLastError();
+                return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("CUDA graph capture of the chain failed: ") +
+                                                        cudaGetErrorString(e != cudaSuccess ? e : e2));
+            }
+            LDGA_CUDA(ctx, cudaGraphInstantiate(&ctx->graph_exec, gr, 0));
+            ctx->graph = gr;
+            ctx->graph_key = key;
+        }
+    }
+    TRY(sync(ctx));
+    if (replayed && ctx->profiling) {
+        for (auto& pr : ctx->graph_ev) {
+            float t = 0.f;
+            LDGA_CUDA(ctx, cudaEventElapsedTime(&t, ctx->ev_pool[pr.second].a, ctx->ev_pool[pr.second].b));
+            ctx->stage_ms[pr.first] += t;
+            ctx->stage_cnt[pr.first] += 1;
+        }
+    }
+    const double* r = ctx->h_stage;
+    int32_t fails = 0;
+    std::memcpy(&fails, reinterpret_cast<const char*>(ctx->h_stage + 64) + sizeof(int32_t), sizeof(int32_t));
+    ctx->have_ghat = ctx->have_chi0 = ctx->have_F = ctx->have_lambda0 = ctx->have_sigma = true;
+    ctx->have_Gamma[0] = ctx->have_Gamma[1] = ctx->have_chi[0] = ctx->have_chi[1] = true;
+    ctx->have_gam[0] = ctx->have_gam[1] = true;
+    ctx->sigma_numax = ctx->Nnu / 2;
+    if (scalars_out) {
+        const double xm = r[8], xd = r[56], U = ctx->mp.U, nn = ctx->mp.n;
+        scalars_out[0] = r[16];                                     // λm
+        scalars_out[1] = r[24];                                     // μ
+        scalars_out[2] = r[25];                                     // E_kin
+        scalars_out[3] = r[26];                                     // E_pot,1
+        scalars_out[4] = (U / 2.0) * (xd - xm) + U * (nn / 2.0 * nn / 2.0);   // E_pot,2
+        scalars_out[5] = (xd + xm) / 2.0;                           // PP_p2 (lhs of the sum rule)
+        scalars_out[6] = r[17];                                     // Newton iterations
+        scalars_out[7] = r[27];                                     // filling n at μ
+    }
+    if (fails > 0) return ctx_fail(ctx, LDGA_ERR_NUMERIC, std::to_string(fails) + " BSE matrices are singular or non-finite");
     return LDGA_OK;
 }
 
@@ -661,7 +933,7 @@ int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam
     if (out7) for (int k = 0; k < 7; ++k) out7[k] = s.last[k];
     if (sigma_out) TRY(copy(ctx, sigma_out, ctx->d_sigma, (size_t)ctx->Nq * nu * sizeof(double2)));
     if (G_out) {
-        TRY(launch_g_ladder_full(ctx, nu, s.mu));
+        TRY(launch_g_ladder_full(ctx, nu, ctx->d_red + 24));
         TRY(copy(ctx, G_out, ctx->d_gladder, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
     }
     return sync(ctx);

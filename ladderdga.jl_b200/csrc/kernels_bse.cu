@@ -310,13 +310,15 @@ __global__ void __launch_bounds__(((N * H + 31) / 32) * 32) k_bse_gj(const BseAr
 
 // Fallback: partial-pivoting FP64 LU of B = A^T (one matrix per CTA, shared memory), used for flagged
 // matrices and for box sizes without an unrolled instantiation.  list == nullptr: all (q, w).
-__global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int32_t* list, int count) {
+__global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int32_t* list, int count,
+                                                       const int32_t* count_dev) {
     extern __shared__ double2 sm[];
     const int N = a.nnu;
     double2* B = sm;                 // [N][N+1] row-major, last column = rhs
     double* red = reinterpret_cast<double*>(B + N * (N + 1));
     int* piv_s = reinterpret_cast<int*>(red + 64);
     const int ld = N + 1;
+    if (count_dev) count = count_dev[0];
     for (int item = blockIdx.x; item < count; item += gridDim.x) {
         const int lin = list ? list[item] : item;
         const int q = lin % a.nq, w = lin / a.nq;
@@ -410,12 +412,13 @@ int run_gj(ldga_ctx* ctx, const BseArgs& a0) {
     const size_t sm = (size_t)N * N * sizeof(double2) + 2 * (N + 1) * sizeof(V) + N * sizeof(double2) +
                       32 * sizeof(double) + N * sizeof(V) + 64;
     auto kern = k_bse_gj<N, H, TF, MODE>;
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     // q chunk: enough CTAs for several waves, but reuse Gamma(w) for many q
     int chunk = 8;
     while (chunk > 1 && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk /= 2;
     a.qchunk = chunk;
     dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
+    StageTimer st_(ctx, LDGA_STAGE_BSE);
     kern<<<grid, threads, sm, ctx->stream>>>(a);
     LDGA_LAUNCHED(ctx, "k_bse_gj");
     return LDGA_OK;
@@ -432,7 +435,14 @@ int run_mode(ldga_ctx* ctx, const BseArgs& a) {
 
 }  // namespace
 
-int launch_bse(ldga_ctx* ctx, int channel, int* n_fallback) {
+bool bse_has_fast_path(int nnu) {
+    switch (nnu) {
+        case 4: case 6: case 8: case 10: case 12: case 16: case 20: case 30: case 40: case 60: return true;
+        default: return false;
+    }
+}
+
+int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     BseArgs a;
     a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
     a.beta = ctx->mp.beta; a.U = ctx->mp.U;
@@ -461,31 +471,23 @@ int launch_bse(ldga_ctx* ctx, int channel, int* n_fallback) {
     if (st != LDGA_OK) return st;
     const size_t smp = (size_t)ctx->Nnu * (ctx->Nnu + 1) * sizeof(double2) + 64 * sizeof(double) + 16;
     if (smp > 220 * 1024) return ctx_fail(ctx, LDGA_ERR_ARG, "fermionic box too large for the BSE kernels");
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(k_bse_lu_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+    LDGA_CUDA(ctx, set_smem(ctx, k_bse_lu_pivot, smp));
     if (generic) {
-        k_bse_lu_pivot<<<4 * 148, 256, smp, ctx->stream>>>(a, nullptr, n);
+        StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
+        k_bse_lu_pivot<<<4 * 148, 256, smp, ctx->stream>>>(a, nullptr, n, nullptr);
         LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
-        if (n_fallback) *n_fallback = n;
     } else {
+        // flagged matrices: compacted on the device, re-solved by a grid-stride pivoted kernel that reads
+        // the count from device memory (zero work when nothing was flagged)
         LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, sizeof(int32_t), ctx->stream));
         k_compact_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, ctx->d_list, ctx->d_count);
         LDGA_LAUNCHED(ctx, "k_compact_flags");
-        int32_t cnt = 0;
-        LDGA_CUDA(ctx, cudaMemcpyAsync(&cnt, ctx->d_count, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-        LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        if (cnt > 0) {
-            k_bse_lu_pivot<<<cnt < 4 * 148 ? cnt : 4 * 148, 256, smp, ctx->stream>>>(a, ctx->d_list, cnt);
-            LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
-        }
-        if (n_fallback) *n_fallback = cnt;
+        StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
+        k_bse_lu_pivot<<<2 * 148, 256, smp, ctx->stream>>>(a, ctx->d_list, 0, ctx->d_count);
+        LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
     }
-    // matrices that stayed non-finite after the pivoted solve
-    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, sizeof(int32_t), ctx->stream));
-    k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, ctx->d_count);
+    // matrices that stayed non-finite after the pivoted solve, accumulated into *d_fail
+    k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, d_fail);
     LDGA_LAUNCHED(ctx, "k_count_flags");
-    int32_t bad = 0;
-    LDGA_CUDA(ctx, cudaMemcpyAsync(&bad, ctx->d_count, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (bad > 0) return ctx_fail(ctx, LDGA_ERR_NUMERIC, std::to_string(bad) + " BSE matrices are singular or non-finite");
     return LDGA_OK;
 }

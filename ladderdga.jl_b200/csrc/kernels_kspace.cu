@@ -113,6 +113,8 @@ __global__ void __launch_bounds__(kThreads) k_bubble(
 struct EomArgs {
     int nnu, nw, n_iv, n_iw, shift, fft_lo, numax, w_per_chunk;
     double U, lam_m, lam_d;
+    const double* lam_m_dev;   // device scalars added to lam_m / lam_d (may be null)
+    const double* lam_d_dev;
     int part;   // -1: full eom; 0..5: calc_Σ_parts contributions
 };
 
@@ -188,8 +190,10 @@ __global__ void __launch_bounds__(kThreads) k_eom_forward(
         if (vi >= 0) {
             const size_t iq = (size_t)q + (size_t)NQ * wi;
             const size_t iv = (size_t)q + (size_t)NQ * (vi + (size_t)a.nnu * wi);
-            const double xm = chi_lam(chi_m[iq], a.lam_m);
-            const double xd = chi_lam(chi_d[iq], a.lam_d);
+            const double lm = a.lam_m + (a.lam_m_dev ? a.lam_m_dev[0] : 0.0);
+            const double ld = a.lam_d + (a.lam_d_dev ? a.lam_d_dev[0] : 0.0);
+            const double xm = chi_lam(chi_m[iq], lm);
+            const double xd = chi_lam(chi_d[iq], ld);
             K = eom_value(a, gam_m[iv], gam_d[iv], xm, xd, lambda0[iv]);
         }
         bufA[p * NQ + q] = K;
@@ -251,8 +255,9 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
     const int np = pairs_per_cta<DIM, M>(ctx->Nf);
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_gloc_transform<DIM, M>;
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((ctx->Nf + np - 1) / np, np);
+    StageTimer st_(ctx, LDGA_STAGE_GLOC);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, ctx->fft_lo, ctx->mp.beta, ctx->mp.mu,
                                                ctx->d_eps, ctx->d_sigma_loc, ctx->n_sigma_loc, ctx->d_gloc,
                                                from_sigma ? 1 : 0, ctx->d_ghat);
@@ -266,9 +271,10 @@ int run_bubble(ldga_ctx* ctx) {
     const int np = pairs_per_cta<DIM, M>(total);
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_bubble<DIM, M>;
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((total + np - 1) / np, np);
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
+    StageTimer st_(ctx, LDGA_STAGE_BUBBLE);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
                                                ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_chi0);
     LDGA_LAUNCHED(ctx, "k_bubble");
@@ -276,7 +282,8 @@ int run_bubble(ldga_ctx* ctx) {
 }
 
 template <int DIM, int M>
-int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, int& nchunk_out) {
+int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lm_dev, const double* ld_dev,
+            int part, int& nchunk_out) {
     using S = TransformSmem<DIM, M>;
     const size_t per = (size_t)(S::BUF_A + S::BUF_B + S::NQ) * sizeof(double2);
     int wpc = (int)(kSmemBudget / per);
@@ -297,10 +304,12 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, int&
     a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
     a.fft_lo = ctx->fft_lo; a.numax = numax; a.w_per_chunk = wpc;
     a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = part;
+    a.lam_m_dev = lm_dev; a.lam_d_dev = ld_dev;
     const size_t sm = (size_t)wpc * per;
     auto kern = k_eom_forward<DIM, M>;
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid(nchunk, numax);
+    StageTimer st_(ctx, LDGA_STAGE_EOM_FORWARD);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_ghat, ctx->d_chi[0], ctx->d_gam[0],
                                                ctx->d_chi[1], ctx->d_gam[1], ctx->d_lambda0, ctx->d_partial);
     LDGA_LAUNCHED(ctx, "k_eom_forward");
@@ -314,10 +323,11 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
     const int np = pairs_per_cta<DIM, M>(numax);
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_eom_inverse<DIM, M>;
-    LDGA_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((numax + np - 1) / np, np);
     const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);
     const double hartree = ctx->mp.n * ctx->mp.U / 2.0;
+    StageTimer st_(ctx, LDGA_STAGE_EOM_INVERSE);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
                                                hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,
                                                add_hartree);
@@ -348,18 +358,22 @@ int launch_bubble(ldga_ctx* ctx) {
 // calc_Σ_parts pieces).  d_tail: device scalar sum_kω(chi_m^lam) (read only when tc != 0).
 namespace {
 template <int DIM, int M>
-int run_eom_all(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
-                double chiloc_m_sum, double2* out, int out_ld, int add_hartree) {
+int run_eom_all(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lm_dev, const double* ld_dev,
+                int part, const double* d_tail, int tc, double chiloc_m_sum, double2* out, int out_ld,
+                int add_hartree) {
     int nchunk = 0;
-    int st = run_eom<DIM, M>(ctx, numax, lam_m, lam_d, part, nchunk);
+    int st = run_eom<DIM, M>(ctx, numax, lam_m, lam_d, lm_dev, ld_dev, part, nchunk);
     if (st != LDGA_OK) return st;
     return run_eom_inverse<DIM, M>(ctx, numax, nchunk, d_tail, tc, chiloc_m_sum, out, out_ld, add_hartree);
 }
 }  // namespace
 
-int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
-               double chiloc_m_sum, double2* out, int out_ld, int add_hartree) {
-#define BODY(D, MM) run_eom_all<D, MM>(ctx, numax, lam_m, lam_d, part, d_tail, tc, chiloc_m_sum, out, out_ld, add_hartree)
+int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lam_m_dev,
+               const double* lam_d_dev, int part, const double* d_tail, int tc, double chiloc_m_sum,
+               double2* out, int out_ld, int add_hartree) {
+#define BODY(D, MM)                                                                                      \
+    run_eom_all<D, MM>(ctx, numax, lam_m, lam_d, lam_m_dev, lam_d_dev, part, d_tail, tc, chiloc_m_sum, out, \
+                       out_ld, add_hartree)
     LDGA_FOR_EACH_GRID(LDGA_CASE)
 #undef BODY
     return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");

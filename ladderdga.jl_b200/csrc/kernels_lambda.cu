@@ -1,33 +1,60 @@
 // a5/a6 (F, lambda_0), a8/a11-a13 (Matsubara sums, lambda_m Newton) and a15 (mu fit, G_ladder,
-// energies).  The root finders run inside one CTA so that no host round trip sits between
-// iterations; every reduction has a fixed summation order, so reruns are bitwise identical.
+// energies).
+//
+// The reductions and root finders run on one 8-CTA thread-block cluster: every Newton iteration's
+// sums are reduced inside each CTA, exchanged through distributed shared memory after a hardware
+// cluster barrier, and added in rank order by every CTA, which then takes the same Newton step.
+// No host round trip sits between iterations, the inputs (lambda, rhs, lambda_min) can come from
+// device memory written earlier on the stream, and the summation order is fixed, so reruns are
+// bitwise identical.
+#include <cooperative_groups.h>
+
 #include <cmath>
 
 #include "ldga_internal.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace {
 
-constexpr int kRedThreads = 1024;
+constexpr int kCluster = 8;
+constexpr int kClThreads = 512;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
-// Deterministic block sum; result valid in every thread.  `red` holds >= 33 doubles.
-__device__ double block_sum(double v, double* red) {
-    v = warp_sum(v);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) red[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        double r = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
-        r = warp_sum(r);
-        if (l == 0) red[32] = r;
+
+// Cluster-wide sums of NV values, fixed order; every thread of every CTA receives the totals.
+// red: shared [NV * 32]; part: shared [2 * NV] exchange slots; parity alternates between calls.
+template <int NV>
+__device__ void cluster_sum(double (&v)[NV], double* red, double* part, int& parity) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+    if (l == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) red[j * 32 + w] = v[j];
     }
     __syncthreads();
-    return red[32];
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int i = 0; i < nwarp; ++i) s += red[threadIdx.x * 32 + i];
+        part[parity * NV + threadIdx.x] = s;
+    }
+    cl.sync();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double s = 0.0;
+        for (int r = 0; r < kCluster; ++r) s += cl.map_shared_rank(part, r)[parity * NV + j];
+        v[j] = s;
+    }
+    parity ^= 1;
 }
+
+__device__ __forceinline__ int cl_tid() { return cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int cl_nth() { return kCluster * blockDim.x; }
 
 // ---------------------------------------------------------------------------------------------
 // F_from_χ (BSETools.jl:40-53) and lambda_0 (BSETools.jl:129-141)
@@ -76,63 +103,59 @@ __global__ void k_lambda0(int nq, int nnu, int nw, double inv_beta2, const doubl
 
 // ---------------------------------------------------------------------------------------------
 // sum_kω (DataTypes.jl:230-249):  (sum_w [ sum_q kMult f(chi)/N_k - c2/(i w)^2 ] - beta^2 c2/12)/beta
-// f = chi_lambda(., lam) (deriv 0) or dchi_lambda (deriv 1)
 // ---------------------------------------------------------------------------------------------
 struct SumArgs {
     int nq, nw, n_iw;
     double beta, c2, inv_nk;
 };
 
-__device__ __forceinline__ double chi_l(double x, double lam) { return x / (lam * x + 1.0); }
-
-__device__ double sum_kw_block(const SumArgs& a, const double* __restrict__ chi, const double* __restrict__ kmult,
-                               double lam, int deriv, double* red) {
-    double acc = 0.0;
-    const int total = a.nq * a.nw;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int q = e % a.nq;
-        double v = chi[e];
-        if (deriv) {
-            const double t = chi_l(v, lam);
-            v = -t * t;
-        } else if (lam != 0.0) {
-            v = chi_l(v, lam);
-        }
-        acc = fma(kmult[q], v, acc);
-    }
-    const double s = block_sum(acc, red) * a.inv_nk;
-    // tail: sum over w != 0 of real(c2/(i w_m)^2) = -c2 beta^2/(4 pi^2 m^2)
+// sum over w != 0 of real(c2/(i w_m)^2) = -c2 beta^2/(4 pi^2 m^2)
+__device__ __forceinline__ double w2_tail(const SumArgs& a) {
     double tail = 0.0;
     for (int m = 1; m <= a.n_iw; ++m) tail += 2.0 * (-a.c2 * a.beta * a.beta / (4.0 * M_PI * M_PI * (double)m * m));
-    return (s - tail + (-a.beta * a.beta / 12.0) * a.c2) / a.beta;
+    return tail;
+}
+__device__ __forceinline__ double finish_kw(const SumArgs& a, double s) {
+    return (s * a.inv_nk - w2_tail(a) + (-a.beta * a.beta / 12.0) * a.c2) / a.beta;
 }
 
-// sum_ωk order: per q, (sum_w [chi - tail] - beta^2 c2/12)/beta, then the kMult-weighted mean
-__device__ double sum_wk_block(const SumArgs& a, const double* __restrict__ chi, const double* __restrict__ kmult,
-                               double lam, double* red) {
-    double tail = 0.0;
-    for (int m = 1; m <= a.n_iw; ++m) tail += 2.0 * (-a.c2 * a.beta * a.beta / (4.0 * M_PI * M_PI * (double)m * m));
-    double acc = 0.0;
-    for (int q = threadIdx.x; q < a.nq; q += blockDim.x) {
-        double s = 0.0;
-        for (int w = 0; w < a.nw; ++w) {
-            const double v = chi[(size_t)w * a.nq + q];
-            s += lam != 0.0 ? chi_l(v, lam) : v;
+// mode 0: chi_lambda, 1: dchi_lambda, 2: sum_ωk order (per q over w first, then kMult)
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+k_sum_kw(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double lam,
+         const double* lam_dev, int mode, double* out) {
+    __shared__ double red[32];
+    __shared__ double part[2];
+    int parity = 0;
+    if (lam_dev) lam += lam_dev[0];
+    double v[1] = {0.0};
+    if (mode == 2) {
+        const double tail = w2_tail(a);
+        for (int q = cl_tid(); q < a.nq; q += cl_nth()) {
+            double s = 0.0;
+            for (int w = 0; w < a.nw; ++w) {
+                const double x = chi[(size_t)w * a.nq + q];
+                s += lam != 0.0 ? x / (lam * x + 1.0) : x;
+            }
+            s = (s - tail + a.c2 * (-a.beta * a.beta / 12.0)) / a.beta;
+            v[0] = fma(kmult[q], s, v[0]);
         }
-        s = (s - tail + a.c2 * (-a.beta * a.beta / 12.0)) / a.beta;
-        acc = fma(kmult[q], s, acc);
+        cluster_sum<1>(v, red, part, parity);
+        if (cl_tid() == 0) out[0] = v[0] * a.inv_nk;
+    } else {
+        const int total = a.nq * a.nw;
+        for (int e = cl_tid(); e < total; e += cl_nth()) {
+            const int q = e % a.nq;
+            const double x = chi[e];
+            const double t = lam != 0.0 ? x / (lam * x + 1.0) : x;
+            v[0] = fma(kmult[q], mode == 1 ? -t * t : t, v[0]);
+        }
+        cluster_sum<1>(v, red, part, parity);
+        if (cl_tid() == 0) out[0] = finish_kw(a, v[0]);
     }
-    return block_sum(acc, red) * a.inv_nk;
+    cg::this_cluster().sync();
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_sum_kw(SumArgs a, const double* chi, const double* kmult,
-                                                          double lam, int deriv, double* out) {
-    __shared__ double red[40];
-    const double r = deriv == 2 ? sum_wk_block(a, chi, kmult, lam, red) : sum_kw_block(a, chi, kmult, lam, deriv, red);
-    if (threadIdx.x == 0) out[0] = r;
-}
-
-__global__ void __launch_bounds__(kRedThreads) k_lambda_min(int nq, int w0, const double* chi, double* out) {
+__global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const double* chi, double* out) {
     __shared__ double red[33];
     double mn = INFINITY;
     for (int q = threadIdx.x; q < nq; q += blockDim.x) mn = fmin(mn, 1.0 / chi[(size_t)w0 * nq + q]);
@@ -149,16 +172,31 @@ __global__ void __launch_bounds__(kRedThreads) k_lambda_min(int nq, int w0, cons
 
 // newton_right, 1-D (LambdaCorrection/helpers.jl:133-153), iteration for iteration; f and df are the
 // reference's f_c1/df_c1 (conditions_new.jl:152-153): both carry the tail terms of sum_kω.
-__global__ void __launch_bounds__(kRedThreads) k_lambda_m(SumArgs a, const double* chi, const double* kmult,
-                                                            double rhs, double xmin, int nsteps, double atol,
-                                                            double* out) {
-    __shared__ double red[40];
+// rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0); xmin = xmin_dev[0] (get_λ_min, computed on the stream).
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
+           const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out) {
+    __shared__ double red[64];
+    __shared__ double part[4];
+    int parity = 0;
+    const double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
+    const double xmin = xmin_dev[0];
     const double delta = 1e-4;
+    const int total = a.nq * a.nw;
     double x0 = 0.0, xi = x0;
     int i = 1;
     while (true) {
-        const double fi = sum_kw_block(a, chi, kmult, xi, 0, red) - rhs;
-        const double dfi = sum_kw_block(a, chi, kmult, xi, 1, red);
+        double v[2] = {0.0, 0.0};
+        for (int e = cl_tid(); e < total; e += cl_nth()) {
+            const double x = chi[e];
+            const double t = x / (xi * x + 1.0);
+            const double km = kmult[e % a.nq];
+            v[0] = fma(km, t, v[0]);
+            v[1] = fma(km, -t * t, v[1]);
+        }
+        cluster_sum<2>(v, red, part, parity);
+        const double fi = finish_kw(a, v[0]) - rhs;
+        const double dfi = finish_kw(a, v[1]);
         const double dfii = 1.0 / dfi;
         xi = x0 - dfii * fi;
         if (fabs(fi) < atol) break;
@@ -167,7 +205,8 @@ __global__ void __launch_bounds__(kRedThreads) k_lambda_m(SumArgs a, const doubl
         if (i >= nsteps) break;
         ++i;
     }
-    if (threadIdx.x == 0) { out[0] = xi; out[1] = (double)i; }
+    if (cl_tid() == 0) { out[0] = xi; out[1] = (double)i; }
+    cg::this_cluster().sync();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -184,37 +223,31 @@ __device__ __forceinline__ double2 g_at(double mu, double eps, double2 sig, int 
     return cinv(make_double2(mu - eps - sig.x, (2.0 * nn + 1.0) * M_PI / beta - sig.y));
 }
 
-// f(mu) = filling_pos - n and df/dmu, summed over q (kMult) and nu_n < numax
-__device__ void filling_f_df(const GArgs& a, const double* kmult, const double* eps, const double2* sigma,
-                             double mu, double* red, double& f, double& df) {
-    double sre = 0.0, dre = 0.0;
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restrict__ eps,
+                const double2* __restrict__ sigma, int fix_n, double mu_in, double* out) {
+    __shared__ double red[3 * 32];
+    __shared__ double part[6];
+    int parity = 0;
     const int total = a.nq * a.numax;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int q = e % a.nq, nn = e / a.nq;
-        const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
-        const double2 G2 = cmul(G, G);
-        sre = fma(kmult[q], G.x, sre);
-        dre = fma(kmult[q], -G2.x, dre);
-    }
-    const double sG = block_sum(sre, red) * a.inv_nk;
-    const double dG = block_sum(dre, red) * a.inv_nk;
-    f = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell) - a.n;
-    df = 2.0 * (2.0 * dG / a.beta + a.shell) / (1.0 + a.U * a.shell);
-}
-
-__global__ void __launch_bounds__(kRedThreads) k_mu_fit_energy(GArgs a, const double* kmult, const double* eps,
-                                                                 const double2* sigma, int fix_n, double mu_in,
-                                                                 double mu_ref, double* out) {
-    __shared__ double red[40];
     double mu = mu_in;
     bool failed = false;
     if (fix_n) {
-        // safeguarded Newton (same method as the oracle's mu_newton)
+        // safeguarded Newton (same method as the oracle's mu_newton); f = filling_pos - n
         double lo = -INFINITY, hi = INFINITY;
         const double tol = 1e-14;
         for (int it = 0; it < 100; ++it) {
-            double f, df;
-            filling_f_df(a, kmult, eps, sigma, mu, red, f, df);
+            double v[2] = {0.0, 0.0};
+            for (int e = cl_tid(); e < total; e += cl_nth()) {
+                const int q = e % a.nq, nn = e / a.nq;
+                const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
+                v[0] = fma(kmult[q], G.x, v[0]);
+                v[1] = fma(kmult[q], -(G.x * G.x - G.y * G.y), v[1]);
+            }
+            cluster_sum<2>(v, red, part, parity);
+            const double sG = v[0] * a.inv_nk, dG = v[1] * a.inv_nk;
+            const double f = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell) - a.n;
+            const double df = 2.0 * (2.0 * dG / a.beta + a.shell) / (1.0 + a.U * a.shell);
             if (!isfinite(f)) { failed = true; break; }
             if (fabs(f) < tol) break;
             if (f > 0) hi = fmin(hi, mu); else lo = fmax(lo, mu);
@@ -229,11 +262,10 @@ __global__ void __launch_bounds__(kRedThreads) k_mu_fit_energy(GArgs a, const do
         }
     }
     if (failed) mu = NAN;
-    // energies at mu (calc_E with mu_ref = the chemical potential handed to calc_E) and filling
+    // energies at mu (calc_E with the fitted mu) and the filling
     const double hartree = a.n * a.U / 2.0;
-    double ekin = 0.0, epot = 0.0, sre = 0.0;
-    const int total = a.nq * a.numax;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int e = cl_tid(); e < total; e += cl_nth()) {
         const int q = e % a.nq, nn = e / a.nq;
         const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
         const double wn = (2.0 * nn + 1.0) * M_PI / a.beta;
@@ -241,38 +273,38 @@ __global__ void __launch_bounds__(kRedThreads) k_mu_fit_energy(GArgs a, const do
         const double ekin_tc = eps[q] + hartree - mu;
         const double epot_tc = a.U * a.U * 0.5 * a.n * (1.0 - 0.5 * a.n) + hartree * (eps[q] + hartree - mu);
         const double2 GS = cmul(G, sigma[e]);
-        const double ep = GS.x - epot_tc * tail;
-        const double ek = eps[q] * (G.x - ekin_tc * tail);
-        ekin = fma(kmult[q], 4.0 * ek, ekin);
-        epot = fma(kmult[q], 2.0 * ep, epot);
-        sre = fma(kmult[q], G.x, sre);
+        v[0] = fma(kmult[q], 4.0 * (eps[q] * (G.x - ekin_tc * tail)), v[0]);
+        v[1] = fma(kmult[q], 2.0 * (GS.x - epot_tc * tail), v[1]);
+        v[2] = fma(kmult[q], G.x, v[2]);
     }
-    // tail_inv terms (once per q)
-    for (int q = threadIdx.x; q < a.nq; q += blockDim.x) {
+    for (int q = cl_tid(); q < a.nq; q += cl_nth()) {     // tail_inv terms, once per q
         const double ekin_tc = eps[q] + hartree - mu;
         const double epot_tc = a.U * a.U * 0.5 * a.n * (1.0 - 0.5 * a.n) + hartree * (eps[q] + hartree - mu);
-        const double epot_inv = (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc;
-        const double ekin_inv = (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc);
-        ekin = fma(kmult[q], ekin_inv, ekin);
-        epot = fma(kmult[q], epot_inv, epot);
+        v[0] = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), v[0]);
+        v[1] = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, v[1]);
     }
-    const double Ek = block_sum(ekin, red) * a.inv_nk / a.beta;
-    const double Ep = block_sum(epot, red) * a.inv_nk / a.beta;
-    const double sG = block_sum(sre, red) * a.inv_nk;
-    const double nfill = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell);
-    (void)mu_ref;
-    if (threadIdx.x == 0) { out[0] = mu; out[1] = Ek; out[2] = Ep; out[3] = nfill; }
+    cluster_sum<3>(v, red, part, parity);
+    if (cl_tid() == 0) {
+        const double sG = v[2] * a.inv_nk;
+        out[0] = mu;
+        out[1] = v[0] * a.inv_nk / a.beta;
+        out[2] = v[1] * a.inv_nk / a.beta;
+        out[3] = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell);
+    }
+    cg::this_cluster().sync();
 }
 
 // calc_E for a given G (column stride ldg) and Sigma over nu_n = 0..numax-1 (thermodynamics.jl:142-168)
-__global__ void __launch_bounds__(kRedThreads) k_calc_E(GArgs a, const double* kmult, const double* eps,
-                                                          const double2* G, int ldg, const double2* sigma,
-                                                          double mu, double* out) {
-    __shared__ double red[40];
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+k_calc_E(GArgs a, const double* kmult, const double* eps, const double2* G, int ldg, const double2* sigma,
+         double mu, double* out) {
+    __shared__ double red[2 * 32];
+    __shared__ double part[4];
+    int parity = 0;
     const double hartree = a.n * a.U / 2.0;
-    double ekin = 0.0, epot = 0.0;
+    double v[2] = {0.0, 0.0};
     const int total = a.nq * a.numax;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    for (int e = cl_tid(); e < total; e += cl_nth()) {
         const int q = e % a.nq, nn = e / a.nq;
         const double2 g = G[(size_t)nn * ldg + q];
         const double wn = (2.0 * nn + 1.0) * M_PI / a.beta;
@@ -280,24 +312,24 @@ __global__ void __launch_bounds__(kRedThreads) k_calc_E(GArgs a, const double* k
         const double ekin_tc = eps[q] + hartree - mu;
         const double epot_tc = a.U * a.U * 0.5 * a.n * (1.0 - 0.5 * a.n) + hartree * (eps[q] + hartree - mu);
         const double2 GS = cmul(g, sigma[e]);
-        ekin = fma(kmult[q], 4.0 * (eps[q] * (g.x - ekin_tc * tail)), ekin);
-        epot = fma(kmult[q], 2.0 * (GS.x - epot_tc * tail), epot);
+        v[0] = fma(kmult[q], 4.0 * (eps[q] * (g.x - ekin_tc * tail)), v[0]);
+        v[1] = fma(kmult[q], 2.0 * (GS.x - epot_tc * tail), v[1]);
     }
-    for (int q = threadIdx.x; q < a.nq; q += blockDim.x) {
+    for (int q = cl_tid(); q < a.nq; q += cl_nth()) {
         const double ekin_tc = eps[q] + hartree - mu;
         const double epot_tc = a.U * a.U * 0.5 * a.n * (1.0 - 0.5 * a.n) + hartree * (eps[q] + hartree - mu);
-        ekin = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), ekin);
-        epot = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, epot);
+        v[0] = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), v[0]);
+        v[1] = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, v[1]);
     }
-    const double Ek = block_sum(ekin, red) * a.inv_nk / a.beta;
-    const double Ep = block_sum(epot, red) * a.inv_nk / a.beta;
-    if (threadIdx.x == 0) { out[0] = Ek; out[1] = Ep; }
+    cluster_sum<2>(v, red, part, parity);
+    if (cl_tid() == 0) { out[0] = v[0] * a.inv_nk / a.beta; out[1] = v[1] * a.inv_nk / a.beta; }
+    cg::this_cluster().sync();
 }
 
 // G_ladder over fft_range: Sigma_ladder for nu_n < numax, Sigma_loc beyond, negative nu by conjugation
-__global__ void k_g_ladder_full(int nq, int nf, int fft_lo, int numax, double beta, double mu,
-                                const double* eps, const double2* sigma, const double2* sigma_loc,
-                                double2* G) {
+__global__ void k_g_ladder_full(int nq, int nf, int fft_lo, int numax, double beta, const double* mu_dev,
+                                const double* eps, const double2* sigma, const double2* sigma_loc, double2* G) {
+    const double mu = mu_dev[0];
     const int L = fft_lo + nf - 1;    // last index
     const size_t total = (size_t)nq * nf;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
@@ -308,7 +340,7 @@ __global__ void k_g_ladder_full(int nq, int nf, int fft_lo, int numax, double be
             const double2 s = vn < numax ? sigma[(size_t)vn * nq + q] : sigma_loc[vn];
             g = g_at(mu, eps[q], s, vn, beta);
         } else {
-            // G(-n-1)... G_new[:, first:-1] = conj(G_new[:, last-1:-1:0])
+            // G_new[:, first:-1] = conj(G_new[:, last-1:-1:0])  (GFTools.jl:183-184)
             const int src = (L - 1) - (vn - fft_lo);
             const double2 s = src < numax ? sigma[(size_t)src * nq + q] : sigma_loc[src];
             g = cconj(g_at(mu, eps[q], s, src, beta));
@@ -326,10 +358,21 @@ __global__ void k_fill_tail(int nq, int numax, double beta, double tnum, double2
     }
 }
 
+// lambda_m right-hand side and bounds on the stream (no host round trip):
+// out[0] = 2 imp_density - sum_kω(chi_d) is formed inside k_lambda_m from these pieces.
+
 SumArgs sum_args(const ldga_ctx* ctx) {
     SumArgs a;
     a.nq = ctx->Nq; a.nw = ctx->Nw; a.n_iw = ctx->sp.n_iw;
     a.beta = ctx->mp.beta; a.c2 = ctx->mp.Ekin_DMFT; a.inv_nk = 1.0 / (double)ctx->Nk;
+    return a;
+}
+
+GArgs g_args(const ldga_ctx* ctx, int numax, double shell) {
+    GArgs a;
+    a.nq = ctx->Nq; a.numax = numax; a.beta = ctx->mp.beta; a.U = ctx->mp.U; a.n = ctx->mp.n;
+    a.inv_nk = 1.0 / (double)ctx->Nk;
+    a.shell = shell;
     return a;
 }
 
@@ -355,6 +398,7 @@ double host_G_shell_sum(int N, double beta) {
 
 int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp) {
     (void)n_gimp;
+    StageTimer st_(ctx, LDGA_STAGE_LAMBDA0);
     k_F_from_chi<<<256, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw, ctx->sp.shift,
                                               ctx->mp.beta, d_chi_loc, d_gimp, ctx->d_F);
     LDGA_LAUNCHED(ctx, "k_F_from_chi");
@@ -363,6 +407,7 @@ int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_
 
 int launch_lambda0(ldga_ctx* ctx) {
     double2* colF = reinterpret_cast<double2*>(ctx->d_red + 64);
+    StageTimer st_(ctx, LDGA_STAGE_LAMBDA0);
     k_colsum_F<<<64, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
     LDGA_LAUNCHED(ctx, "k_colsum_F");
     k_lambda0<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, ctx->Nw, 1.0 / (ctx->mp.beta * ctx->mp.beta),
@@ -371,56 +416,57 @@ int launch_lambda0(ldga_ctx* ctx) {
     return LDGA_OK;
 }
 
-int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int deriv, double* d_out) {
-    k_sum_kw<<<1, kRedThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[channel], ctx->d_kmult, lam, deriv, d_out);
+// mode 0: chi_lambda, 1: dchi_lambda, 2: sum_ωk order.  lam_dev (may be null) is added to lam.
+int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev) {
+    StageTimer st_(ctx, LDGA_STAGE_SUMS);
+    k_sum_kw<<<kCluster, kClThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[channel], ctx->d_kmult, lam, lam_dev,
+                                                       mode, d_out);
     LDGA_LAUNCHED(ctx, "k_sum_kw");
     return LDGA_OK;
 }
 
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
     const int w0 = (ctx->Nw + 1) / 2 - 1;   // ω0_index = ceil(Nw/2), 1-based
-    k_lambda_min<<<1, kRedThreads, 0, ctx->stream>>>(ctx->Nq, w0, ctx->d_chi[channel], d_out);
+    StageTimer st_(ctx, LDGA_STAGE_SUMS);
+    k_lambda_min<<<1, 1024, 0, ctx->stream>>>(ctx->Nq, w0, ctx->d_chi[channel], d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_min");
     return LDGA_OK;
 }
 
-int launch_lambda_m(ldga_ctx* ctx, double rhs, double* d_out) {
-    // lambda_min first (device), then the Newton loop reads it back from the host copy
+// lambda_m Newton: rhs = rhs_const - *rhs_sub_dev (if given); d_out[0] = lambda, d_out[1] = iterations;
+// d_out[2] receives lambda_min.
+int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out) {
     int st = launch_lambda_min(ctx, LDGA_CH_M, d_out + 2);
     if (st) return st;
-    double xmin = 0.0;
-    LDGA_CUDA(ctx, cudaMemcpyAsync(&xmin, d_out + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    LDGA_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    k_lambda_m<<<1, kRedThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs, xmin,
-                                                   100, 1e-13, d_out);
+    StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
+    k_lambda_m<<<kCluster, kClThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[LDGA_CH_M], ctx->d_kmult,
+                                                         rhs_const, rhs_sub_dev, d_out + 2, 100, 1e-13, d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");
     return LDGA_OK;
 }
 
 int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out) {
-    GArgs a;
-    a.nq = ctx->Nq; a.numax = numax; a.beta = ctx->mp.beta; a.U = ctx->mp.U; a.n = ctx->mp.n;
-    a.inv_nk = 1.0 / (double)ctx->Nk;
-    a.shell = host_G_shell_sum(numax + 1, ctx->mp.beta);
-    k_mu_fit_energy<<<1, kRedThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n, mu_in,
-                                                        mu_in, d_out);
+    GArgs a = g_args(ctx, numax, host_G_shell_sum(numax + 1, ctx->mp.beta));
+    StageTimer st_(ctx, LDGA_STAGE_GLADDER);
+    k_mu_fit_energy<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n,
+                                                              mu_in, d_out);
     LDGA_LAUNCHED(ctx, "k_mu_fit_energy");
     return LDGA_OK;
 }
 
 int launch_calc_E(ldga_ctx* ctx, const double2* G, int ldg, const double2* sigma, int numax, double mu,
                   double* d_out) {
-    GArgs a;
-    a.nq = ctx->Nq; a.numax = numax; a.beta = ctx->mp.beta; a.U = ctx->mp.U; a.n = ctx->mp.n;
-    a.inv_nk = 1.0 / (double)ctx->Nk;
-    a.shell = 0.0;
-    k_calc_E<<<1, kRedThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, G, ldg, sigma, mu, d_out);
+    GArgs a = g_args(ctx, numax, 0.0);
+    StageTimer st_(ctx, LDGA_STAGE_GLADDER);
+    k_calc_E<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, G, ldg, sigma, mu, d_out);
     LDGA_LAUNCHED(ctx, "k_calc_E");
     return LDGA_OK;
 }
 
-int launch_g_ladder_full(ldga_ctx* ctx, int numax, double mu) {
-    k_g_ladder_full<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nf, ctx->fft_lo, numax, ctx->mp.beta, mu,
+// mu_dev: device scalar with the chemical potential (e.g. the output of k_mu_fit_energy)
+int launch_g_ladder_full(ldga_ctx* ctx, int numax, const double* mu_dev) {
+    StageTimer st_(ctx, LDGA_STAGE_GLADDER);
+    k_g_ladder_full<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nf, ctx->fft_lo, numax, ctx->mp.beta, mu_dev,
                                                       ctx->d_eps, ctx->d_sigma, ctx->d_sigma_loc, ctx->d_gladder);
     LDGA_LAUNCHED(ctx, "k_g_ladder_full");
     return LDGA_OK;

@@ -106,6 +106,30 @@ struct ldga_ctx {
     int32_t* d_list = nullptr;     // compacted fallback list
     int32_t* d_count = nullptr;
 
+    cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
+    bool capturing = false;              // a CUDA graph of the chain is being captured
+
+    // fused chain (ldga_chain_m): persistent input buffers and the captured graph
+    double2* d_chiloc = nullptr;   // [Nnu, Nnu, Nw] local chi_m
+    double2* d_gimp = nullptr;
+    int n_gimp_alloc = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<uint64_t> graph_key;
+    std::vector<std::pair<int, int>> graph_ev;   // stage events recorded inside the captured graph
+    int64_t graph_launches = 0;                  // kernels per replay of the captured graph
+    double* h_stage = nullptr;     // pinned host staging for the chain's scalars (64 doubles + 4 ints)
+
+    // stage timing (ldga_profile / ldga_stage_times)
+    bool profiling = false;
+    struct EvPair { cudaEvent_t a = nullptr, b = nullptr; };
+    std::vector<EvPair> ev_pool;
+    std::vector<int> ev_free;
+    std::vector<std::pair<int, int>> ev_pending;   // (stage, slot)
+    double stage_ms[LDGA_N_STAGES] = {0};
+    int stage_cnt[LDGA_N_STAGES] = {0};
+    int64_t n_launches = 0;        // kernels launched by this handle
+
     bool have_ghat = false, have_chi0 = false, have_F = false, have_lambda0 = false, have_sigma = false;
     bool have_Gamma[2] = {false, false}, have_chi[2] = {false, false}, have_gam[2] = {false, false};
     int lambda_dm_evals = 0;
@@ -123,20 +147,48 @@ int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what);
     } while (0)
 #define LDGA_LAUNCHED(ctx, what)                                    \
     do {                                                            \
+        (ctx)->n_launches++;                                        \
         cudaError_t _e = cudaGetLastError();                        \
         if (_e != cudaSuccess) return ctx_cuda((ctx), _e, what);    \
     } while (0)
 
+// Dynamic shared-memory opt-in for a kernel; skipped while a CUDA graph is being captured (the
+// uncaptured warm-up run of the same sequence has already set it).
+template <typename F>
+inline cudaError_t set_smem(ldga_ctx* c, F* f, size_t sm) {
+    if (c->capturing) return cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+}
+
+bool bse_has_fast_path(int nnu);
+
+// Records CUDA events around one stage when the handle is profiling (no-op otherwise).
+struct StageTimer {
+    ldga_ctx* c;
+    int stage;
+    int slot;
+    StageTimer(ldga_ctx* ctx, int st);
+    ~StageTimer();
+};
+
 // kernel launchers implemented in the .cu files
 int launch_gloc_transform(ldga_ctx* ctx, bool from_sigma);
 int launch_bubble(ldga_ctx* ctx);
-int launch_bse(ldga_ctx* ctx, int channel, int* n_fallback);
+// BSE for one channel; enqueues the fallback for flagged matrices on the device (no host sync).
+// d_fail (device int32) receives the number of matrices that stayed unsolved.
+int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail);
 int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp);
 int launch_lambda0(ldga_ctx* ctx);
-int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int part, const double* d_tail, int tc,
-               double chiloc_m_sum, double2* out, int out_ld, int add_hartree);
-int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int deriv, double* d_out);
+// EoM forward + inverse.  lam_*_dev (may be null) are device scalars added to lam_m / lam_d.
+int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lam_m_dev,
+               const double* lam_d_dev, int part, const double* d_tail, int tc, double chiloc_m_sum,
+               double2* out, int out_ld, int add_hartree);
+int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev = nullptr);
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
-int launch_lambda_m(ldga_ctx* ctx, double rhs, double* d_out /*[2]*/);
-int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[8]*/);
-int launch_g_ladder_full(ldga_ctx* ctx, int numax, double mu);
+int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out /*[3]*/);
+int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[4]*/);
+int launch_g_ladder_full(ldga_ctx* ctx, int numax, const double* mu_dev);
+int launch_calc_E(ldga_ctx* ctx, const double2* G, int ldg, const double2* sigma, int numax, double mu,
+                  double* d_out);
+int launch_fill_tail(ldga_ctx* ctx, int numax, double tnum, double2* out, int out_ld);
+double host_G_shell_sum(int N, double beta);

@@ -177,6 +177,35 @@ def test_lambda_dm_correction(case):
     assert abs(res_g.EPot_p1 - res_g.EPot_p2) < 1e-8
 
 
+def test_fused_chain_matches_stepwise(case):
+    """ldga_chain_m (one call, CUDA graph on replay) gives the step-by-step API's λm result."""
+    import ctypes as C
+    import torch
+    name, inp, ref = case
+    g = gpu_chain(inp)
+    res = L.λ_correction("m", g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], g["h"])
+    h = L.setup_synthetic(inp)
+    ctx = h.ctx
+
+    def pinned(a):
+        v = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+        return torch.from_numpy(v.copy()).pin_memory()
+
+    src = [pinned(x) for x in (h.Σ_loc, h.Γ_m, h.Γ_d, h.χDMFT_m, h.gImp)]
+    numax = h.sP.n_iν
+    for use_graph in (0, 1, 1, 1):
+        S_out = torch.zeros(ctx.Nq * numax * 2, dtype=torch.float64).pin_memory()
+        sc = (C.c_double * 8)()
+        p = [C.c_void_p(t.data_ptr()) for t in src]
+        ctx.call("ldga_chain_m", p[0], len(h.Σ_loc), p[1], p[2], p[3], p[4], len(h.gImp), h.imp_density,
+                 h.χloc_m_sum, use_graph, C.c_void_p(S_out.data_ptr()), None, None, sc)
+        S = S_out.numpy().view(np.complex128).reshape((ctx.Nq, numax), order="F")
+        assert abs(sc[0] - res.λm) <= 1e-12 * max(1.0, abs(res.λm)), (use_graph, sc[0], res.λm)
+        assert rel(S, res.Σ_ladder) < 1e-12
+        assert abs(sc[1] - res.μ) < 1e-12
+        assert abs(sc[3] - res.EPot_p1) <= 1e-12 * max(1.0, abs(res.EPot_p1))
+
+
 def test_errors(case):
     name, inp, ref = case
     g = gpu_chain(inp)
