@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--prec", default="mixed", choices=list(PREC_NAMES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ns", type=int, default=None, help="smaller k-grid (points per axis) for profiling captures")
     ap.add_argument("--out", default=None, help="also write the JSON line to this file")
     return ap.parse_args()
 
@@ -248,7 +249,8 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from ladderdga_b200 import synthetic as S
-    inp = S.config_input(WORKLOAD["cfg"], point=rank)
+    over = {"ns": args.ns} if args.ns else {}
+    inp = S.config_input(WORKLOAD["cfg"], point=rank, **over)
     chain = Chain(inp, PREC_NAMES[args.prec], local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = {}

@@ -4,27 +4,33 @@
 // and only uses y = (1^T A^-1)^T, i.e. the solution of B y = 1 with B = A^T:
 //     chi_r(q, w) = Re(sum_nu y_nu) / beta^2,   gamma_r(q, nu, w) = y_nu / (chi0(q,nu,w)(1 + s U chi_r)).
 //
-// Kernel layout: one CTA per (w, chunk of q); Gamma(w) is staged once in shared memory (FP64) and
-// reused by every q of the chunk.  Row i of B lives in the registers of H adjacent lanes (lane h
-// of the group holds the columns j = s*H + h), so a Gauss-Jordan step k is: the owners of row k
-// publish it to shared memory (double-buffered, one barrier per step), every other row computes
-// its multiplier m = b_ik / b_kk in the lane that owns column k, broadcasts it within the group by
-// shuffle, and updates its remaining columns.  All loops are unrolled at compile time, so every
-// register index is static and the column bound j > k costs no predicated work outside one slot.
+// Layout.  One CTA per (w, chunk of q); Gamma(w) is staged once in shared memory (FP64) and shared
+// by MPC independent matrix groups.  A group of TR x TC threads owns one matrix [B | 1] (N rows,
+// N + 1 columns) as a 2D cyclic register tile: thread (tr, tc) holds rows tr + TR*a and columns
+// tc + TC*c.  The TC threads of a row group are adjacent lanes of one warp.
+//
+// Gauss-Jordan step k (unrolled; every register index is static):
+//   1. the row group of row k writes its part of row k (columns >= k) to a double-buffered shared
+//      row; the owner of the pivot also writes the pivot's reciprocal (FP32 rcp seed + two FP64
+//      Newton steps: no IEEE divide on the critical path);
+//   2. one named barrier over the group's threads (other groups of the CTA run on);
+//   3. in every row group the lane owning column k forms the multipliers m = b_ik / b_kk of its rows
+//      and shuffles them to the other lanes of the group, which update their columns > k.
+// The multipliers replace the eliminated column (kept for refinement).  Work is ~N^3/2 complex
+// multiply-adds: only the tile column that straddles k carries a runtime predicate.
 //
 // Modes:
 //   LDGA_PREC_FP64_INV  in-place FP64 Gauss-Jordan inverse (N^3, the reference's formulation);
 //                       y = row sums of B^-1.
-//   LDGA_PREC_FP64      FP64 Gauss-Jordan elimination of [B | 1] (N^3/2).
-//   LDGA_PREC_MIXED     FP32 elimination with the multipliers kept, then FP64 iterative refinement:
-//                       r = 1 - B y in FP64 (Gamma from shared memory), delta from the stored FP32
-//                       elimination, y += delta, until the update is below FP64 resolution.
+//   LDGA_PREC_FP64      FP64 elimination of [B | 1].
+//   LDGA_PREC_MIXED     FP32 elimination, then FP64 iterative refinement: r = 1 - B y in FP64
+//                       (Gamma from shared memory), the correction from the stored FP32 multipliers,
+//                       y += delta, until the backward error reaches FP64 resolution.
 // No pivoting is done in the fast path.  Every solution is verified by its FP64 backward error
 // |1 - B y|_inf / (|B|_inf |y|_inf + 1); a matrix above 1e-12 (or with a non-finite y) is flagged
 // and re-solved by a partial-pivoting FP64 LU kernel, which is also the path for box sizes that
-// have no unrolled instantiation.
+// have no tiled instantiation.
 #include <cmath>
-#include <cstdio>
 
 #include "ldga_internal.cuh"
 
@@ -49,27 +55,40 @@ __device__ __forceinline__ void vfnms(V& a, V m, V b) {
     a.y = fma(-m.x, b.y, a.y);
     a.y = fma(-m.y, b.x, a.y);
 }
-template <typename V>
-__device__ __forceinline__ V vinv(V z) {
-    using R = decltype(z.x);
-    R s = fabs(z.x) > fabs(z.y) ? fabs(z.x) : fabs(z.y);
-    R xr = z.x / s, xi = z.y / s;
-    R d = (xr * xr + xi * xi) * s;
-    V r; r.x = xr / d; r.y = -xi / d; return r;
+// 1/z = conj(z)/|z|^2, 1/|z|^2 from an FP32 rcp seed refined by Newton steps (FP64: two steps,
+// relative error ~ seed^4, below rounding).  |z|^2 outside the FP32 range gives a non-finite
+// result, which the backward-error check routes to the pivoted FP64 path.
+__device__ __forceinline__ double2 vinv(double2 z) {
+    const double d = z.x * z.x + z.y * z.y;
+    double r = (double)__frcp_rn((float)d);
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    return make_double2(z.x * r, -z.y * r);
+}
+__device__ __forceinline__ float2 vinv(float2 z) {
+    const float d = z.x * z.x + z.y * z.y;
+    const float r = __frcp_rn(d);
+    return make_float2(z.x * r, -z.y * r);
 }
 
 template <typename V>
-__device__ __forceinline__ V shfl_v(V v, int src, int width) {
+__device__ __forceinline__ V shfl_v(V v, int src) {
     V r;
-    r.x = __shfl_sync(0xffffffffu, v.x, src, width);
-    r.y = __shfl_sync(0xffffffffu, v.y, src, width);
+    r.x = __shfl_sync(0xffffffffu, v.x, src);
+    r.y = __shfl_sync(0xffffffffu, v.y, src);
     return r;
+}
+
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 struct BseArgs {
     int nq, nnu, nw, qchunk;
     double beta, U;
-    int s;            // -1 for d, +1 for m
+    int s;                  // -1 for d, +1 for m
     const double2* Gamma;   // [Nnu, Nnu, Nw]
     const double2* chi0;    // [Nq, Nnu, Nw]
     double* chi;            // [Nq, Nw]
@@ -79,7 +98,311 @@ struct BseArgs {
 
 __device__ __forceinline__ double2 dmk(double r, double i) { return make_double2(r, i); }
 
-// Block-wide sum in a fixed order (deterministic): lanes -> warps -> warp 0.
+// Group-wide reduction of NV values (op 1: max, 0: sum) over the group's G threads, fixed order.
+// red: per-group shared scratch [NV * (G/32)].  Result in every thread of the group.
+template <int NV, int G>
+__device__ __forceinline__ void group_reduce(double (&v)[NV], const int (&op)[NV], double* red, int bar_id,
+                                             int t) {
+    constexpr int NWG = G / 32;
+    const int wg = t >> 5, l = t & 31;
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_down_sync(0xffffffffu, v[j], o);
+            v[j] = op[j] ? fmax(v[j], x) : v[j] + x;
+        }
+    named_barrier(bar_id, G);   // previous readers of red are done
+    if (l == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) red[j * NWG + wg] = v[j];
+    }
+    named_barrier(bar_id, G);
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double r = 0.0;
+        for (int i = 0; i < NWG; ++i) r = op[j] ? fmax(r, red[j * NWG + i]) : r + red[j * NWG + i];
+        v[j] = r;
+    }
+}
+
+template <int N, int TR, int TC>
+struct Tile {
+    static constexpr int RT = (N + TR - 1) / TR;          // tile rows
+    static constexpr int NC = N + 1;                      // columns incl. the right-hand side
+    static constexpr int CT = (NC + TC - 1) / TC;         // tile columns
+    static constexpr int G = TR * TC;                     // threads per matrix group
+    static constexpr int RW = N + 2;                      // published row: columns, rhs, reciprocal
+};
+
+template <int N, int TR, int TC, typename V>
+constexpr size_t group_smem() {
+    using T = Tile<N, TR, TC>;
+    // rowbuf [2][RW] V, pinv [N] V, rk [2] V, ysm [N] double2, red [8 * G/32] double
+    return 2 * T::RW * sizeof(V) + N * sizeof(V) + 2 * sizeof(V) + N * sizeof(double2) +
+           8 * (T::G / 32) * sizeof(double) + 16;
+}
+
+// MINB: resident CTAs per SM the register allocation must allow
+template <int N, int TR, int TC, int MPC, int MINB, typename TF, int MODE>
+__global__ void __launch_bounds__(TR * TC * MPC, MINB) k_bse_tile(const BseArgs a) {
+    using V = typename C2<TF>::T;
+    using TL = Tile<N, TR, TC>;
+    static_assert(TR == TC, "the blocked elimination needs a square thread grid");
+    constexpr int T = TC;
+    constexpr int RT = TL::RT, CT = TL::CT, G = TL::G, RW = TL::RW;
+    constexpr bool MIXED = MODE == LDGA_PREC_MIXED;
+    constexpr bool INV = MODE == LDGA_PREC_FP64_INV;
+    constexpr int TCN = N % TC, CN = N / TC;              // owner lane / slot of the rhs column
+    extern __shared__ double2 sm[];
+    double2* Gsm = sm;                                    // [N*N] Gamma(w), G[j + N*i]
+    const int tid = threadIdx.x;
+    const int g = tid / G, t = tid - g * G;
+    const int tr = t / TC, tc = t - (t / TC) * TC;
+    const int lane = tid & 31;
+    const int gbase = lane - tc;                          // first lane of this row group
+    const int bar = g + 1;
+    char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * group_smem<N, TR, TC, V>();
+    V* rowbuf = reinterpret_cast<V*>(gs);                 // [2][RW]
+    V* pinv = rowbuf + 2 * RW;                            // [N]
+    V* rkbuf = pinv + N;                                  // [2]
+    double2* ysm = reinterpret_cast<double2*>(rkbuf + 2); // [N]
+    double* red = reinterpret_cast<double*>(ysm + N);     // [8 * G/32]
+
+    const int w = blockIdx.y;
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    {
+        const double2* Gw = a.Gamma + (size_t)w * N * N;
+        for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+    }
+    __syncthreads();
+
+    for (int q = q0 + g; q < q1; q += MPC) {
+        const double2* c0p = a.chi0 + (size_t)q + (size_t)a.nq * ((size_t)N * w);
+        // ---- load the tile of [B | 1], B_ij = Gamma[j, i] + delta_ij / chi0(q, i, w)
+        V b[RT][CT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + TR * ra;
+#pragma unroll
+            for (int c = 0; c < CT; ++c) {
+                const int j = tc + TC * c;
+                double2 v = dmk(0.0, 0.0);
+                if (i < N) {
+                    if (j < N) {
+                        v = Gsm[i * N + j];
+                        if (j == i) v = cadd(v, cinv(c0p[(size_t)a.nq * i]));
+                    } else if (j == N) {
+                        v = dmk(1.0, 0.0);
+                    }
+                }
+                b[ra][c] = vmk<V>(v.x, v.y);
+            }
+        }
+
+        // ---- elimination.  Step k = ktc + T kc: row k is tile row kc of row group ktc and column k is
+        // tile column kc of lane ktc, so kc is a compile-time index (unrolled blocks) while ktc runs
+        // as an ordinary loop -- static register indices with a small code footprint.
+#pragma unroll
+        for (int kc = 0; kc < (N + T - 1) / T; ++kc) {
+            const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+            for (int ktc = 0; ktc < kend; ++ktc) {
+                const int k = ktc + T * kc;
+                V* rb = rowbuf + (k & 1) * RW;
+                if (tr == ktc) {
+#pragma unroll
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + T * c;
+                        if ((INV || c >= kc) && j <= N) rb[j] = b[kc][c];
+                    }
+                    if (tc == ktc) {
+                        const V iv = vinv(b[kc][kc]);
+                        rb[N + 1] = iv;
+                        pinv[k] = iv;
+                    }
+                }
+                named_barrier(bar, G);
+                const V inv = rb[N + 1];
+                if (INV) {
+                    // in-place Gauss-Jordan inverse on the N x N part: row k scaled by 1/p (b_kk -> 1/p);
+                    // other rows b_ij -= b_ik row_k[j] / p, b_ik -> -b_ik / p
+                    V u[CT];
+#pragma unroll
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + T * c;
+                        u[c] = (j == k) ? inv : (j < N ? vmul<V>(rb[j], inv) : vmk<V>(0.0, 0.0));
+                    }
+#pragma unroll
+                    for (int ra = 0; ra < RT; ++ra) {
+                        V f = tc == ktc ? b[ra][kc] : vmk<V>(0.0, 0.0);
+                        f = shfl_v<V>(f, gbase + ktc);
+                        if (ra == kc && tr == ktc) {
+#pragma unroll
+                            for (int c = 0; c < CT; ++c) b[ra][c] = u[c];
+                        } else {
+                            if (tc == ktc) b[ra][kc] = vmk<V>(0.0, 0.0);
+#pragma unroll
+                            for (int c = 0; c < CT; ++c) vfnms<V>(b[ra][c], f, u[c]);
+                        }
+                    }
+                } else {
+                    V u[CT];
+#pragma unroll
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + T * c;
+                        if (c >= kc) u[c] = (j > k && j <= N) ? rb[j] : vmk<V>(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int ra = 0; ra < RT; ++ra) {
+                        const bool rowk = (ra == kc) && (tr == ktc);
+                        V m = vmk<V>(0.0, 0.0);
+                        if (tc == ktc && !rowk) {
+                            m = vmul<V>(b[ra][kc], inv);
+                            b[ra][kc] = m;                     // the multiplier replaces column k
+                        }
+                        m = shfl_v<V>(m, gbase + ktc);
+                        if (!rowk) {
+#pragma unroll
+                            for (int c = 0; c < CT; ++c) {
+                                if (c > kc || (c == kc && tc > ktc)) vfnms<V>(b[ra][c], m, u[c]);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+
+        // ---- solution y (FP64), shared through ysm
+        double2 y[RT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + TR * ra;
+            if (INV) {
+                double2 part = dmk(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < CT; ++c) {
+                    const int j = tc + TC * c;
+                    if (j < N) part = cadd(part, dmk((double)b[ra][c].x, (double)b[ra][c].y));
+                }
+#pragma unroll
+                for (int o = 1; o < TC; o <<= 1) {
+                    part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
+                    part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
+                }
+                y[ra] = part;
+            } else {
+                V z = tc == TCN ? b[ra][CN] : vmk<V>(0.0, 0.0);
+                z = shfl_v<V>(z, gbase + TCN);
+                const V tv = i < N ? vmul<V>(z, pinv[i]) : vmk<V>(0.0, 0.0);
+                y[ra] = dmk((double)tv.x, (double)tv.y);
+            }
+            if (i < N && tc == 0) ysm[i] = y[ra];
+        }
+        named_barrier(bar, G);
+
+        // ---- FP64 backward error (all modes) and, for MIXED, iterative refinement
+        double ysum = 0.0, berr = 0.0;
+        constexpr int max_ref = MIXED ? 6 : 0;
+        for (int it = 0; it <= max_ref; ++it) {
+            double2 r[RT];
+            double st[4] = {0.0, 0.0, 0.0, 0.0};
+            const int op[4] = {1, 1, 1, 0};
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) {
+                const int i = tr + TR * ra;
+                double2 acc = dmk(0.0, 0.0);
+                double rown = 0.0;
+                if (i < N) {
+#pragma unroll
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + TC * c;
+                        if (j < N) {
+                            double2 gv = Gsm[i * N + j];
+                            if (j == i) gv = cadd(gv, cinv(c0p[(size_t)a.nq * i]));
+                            acc = cadd(acc, cmul(gv, ysm[j]));
+                            rown += fabs(gv.x) + fabs(gv.y);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int o = 1; o < TC; o <<= 1) {
+                    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+                    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+                    rown += __shfl_xor_sync(0xffffffffu, rown, o);
+                }
+                r[ra] = i < N ? dmk(1.0 - acc.x, -acc.y) : dmk(0.0, 0.0);
+                if (i < N && tc == 0) {
+                    st[0] = fmax(st[0], fabs(r[ra].x) + fabs(r[ra].y));
+                    st[1] = fmax(st[1], fabs(y[ra].x) + fabs(y[ra].y));
+                    st[2] = fmax(st[2], rown);
+                    st[3] += y[ra].x;
+                }
+            }
+            group_reduce<4, G>(st, op, red, bar, t);
+            berr = st[0] / (st[2] * st[1] + 1.0);
+            ysum = st[3];
+            // refinement stops once the FP64 backward error is below 1e-14 (the verification bar is 1e-12)
+            if (!MIXED || it == max_ref || !isfinite(berr) || berr <= 1e-14) break;
+            // correction: replay the stored FP32 elimination on r (r replicated across each row group)
+            V rv[RT];
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) rv[ra] = vmk<V>(r[ra].x, r[ra].y);
+#pragma unroll
+            for (int kc = 0; kc < (N + T - 1) / T; ++kc) {
+                const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+                for (int ktc = 0; ktc < kend; ++ktc) {
+                    const int k = ktc + T * kc;
+                    if (tr == ktc && tc == 0) rkbuf[k & 1] = rv[kc];
+                    named_barrier(bar, G);
+                    const V rk = rkbuf[k & 1];
+#pragma unroll
+                    for (int ra = 0; ra < RT; ++ra) {
+                        const bool rowk = (ra == kc) && (tr == ktc);
+                        V tv = (tc == ktc && !rowk) ? vmul<V>(b[ra][kc], rk) : vmk<V>(0.0, 0.0);
+                        tv = shfl_v<V>(tv, gbase + ktc);
+                        if (!rowk) { rv[ra].x -= tv.x; rv[ra].y -= tv.y; }
+                    }
+                }
+            }
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) {
+                const int i = tr + TR * ra;
+                if (i < N) {
+                    const V d = vmul<V>(rv[ra], pinv[i]);
+                    y[ra] = cadd(y[ra], dmk((double)d.x, (double)d.y));
+                }
+            }
+            named_barrier(bar, G);
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) {
+                const int i = tr + TR * ra;
+                if (i < N && tc == 0) ysm[i] = y[ra];
+            }
+            named_barrier(bar, G);
+        }
+
+        // ---- chi and gamma
+        const double chi = ysum / (a.beta * a.beta);
+        const bool ok = isfinite(berr) && berr <= 1e-12;
+        if (t == 0) {
+            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+        }
+        const double f = 1.0 + a.s * a.U * chi;
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + TR * ra;
+            if (i < N && tc == 0) {
+                const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+                a.gam[ci] = cdiv(y[ra], cscale(a.chi0[ci], f));
+            }
+        }
+        named_barrier(bar, G);   // ysm / pinv of this matrix are read before the next one writes
+    }
+}
+
 __device__ __forceinline__ double block_sum_det(double v, double* red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -91,225 +414,10 @@ __device__ __forceinline__ double block_sum_det(double v, double* red) {
     for (int i = 0; i < nw; ++i) r += red[i];
     return r;
 }
-__device__ __forceinline__ double block_max(double v, double* red) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) red[w] = v;
-    __syncthreads();
-    double r = 0.0;
-    const int nw = (blockDim.x + 31) >> 5;
-    for (int i = 0; i < nw; ++i) r = fmax(r, red[i]);
-    return r;
-}
-
-template <int N, int H, typename TF, int MODE>
-__global__ void __launch_bounds__(((N * H + 31) / 32) * 32) k_bse_gj(const BseArgs a) {
-    using V = typename C2<TF>::T;
-    constexpr int S = (N + H - 1) / H;
-    extern __shared__ double2 sm[];
-    double2* Gsm = sm;                               // [N*N] Gamma(w), Julia layout G[j + N*i]
-    V* rowbuf = reinterpret_cast<V*>(Gsm + N * N);   // [2][N + 1] published row k (+ rhs)
-    double2* ysm = reinterpret_cast<double2*>(rowbuf + 2 * (N + 1));   // [N]
-    double* red = reinterpret_cast<double*>(ysm + N);                 // [32]
-    V* zsm = reinterpret_cast<V*>(red + 32);                           // [N] refinement rhs
-
-    const int w = blockIdx.y;
-    const int q0 = blockIdx.x * a.qchunk;
-    const int q1 = min(a.nq, q0 + a.qchunk);
-    const int tid = threadIdx.x;
-    const int i = tid / H, h = tid - (tid / H) * H;
-    const bool act = i < N;
-    const int lane = tid & 31;
-    const int gbase = lane - h;      // first lane of this row's group
-
-    const double2* Gw = a.Gamma + (size_t)w * N * N;
-    for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
-    __syncthreads();
-
-    for (int q = q0; q < q1; ++q) {
-        // ---- load row i of B = A^T: B_ij = Gamma[j, i] + delta_ij / chi0(q, i, w)
-        const size_t ci = act ? ((size_t)q + (size_t)a.nq * (i + (size_t)N * w)) : 0;
-        double2 c0 = act ? a.chi0[ci] : dmk(1.0, 0.0);
-        double2 dii = cinv(c0);
-        V b[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int j = s * H + h;
-            double2 g = (act && j < N) ? Gsm[i * N + j] : dmk(0.0, 0.0);
-            if (j == i) g = cadd(g, dii);
-            b[s] = vmk<V>(g.x, g.y);
-        }
-        V z = vmk<V>(1.0, 0.0);
-        V mypiv = vmk<V>(1.0, 0.0);
-
-        // ---- elimination
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const int sk = k / H, hk = k - (k / H) * H;
-            V* rb = rowbuf + (k & 1) * (N + 1);
-            if (act && i == k) {
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const int j = s * H + h;
-                    if (MODE == LDGA_PREC_FP64_INV) {
-                        if (j < N) rb[j] = b[s];
-                    } else {
-                        if (s >= sk && j < N) rb[j] = b[s];
-                    }
-                }
-                if (h == 0) rb[N] = z;
-            }
-            __syncthreads();
-            const V piv = rb[k];
-            const V inv = vinv<V>(piv);
-            if (i == k) mypiv = piv;
-            if (MODE == LDGA_PREC_FP64_INV) {
-                // in-place Gauss-Jordan inverse: row k scaled by 1/p (b_kk -> 1/p), others
-                // b_ij -= b_ik * row_k[j] / p with b_ik -> -b_ik / p
-                V f = vmk<V>(0.0, 0.0);
-                if (h == hk) f = b[sk];
-                f = shfl_v<V>(f, gbase + hk, 32);
-                if (i == k) {
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        const int j = s * H + h;
-                        if (j == k) b[s] = inv; else b[s] = vmul<V>(b[s], inv);
-                    }
-                } else {
-                    if (h == hk) b[sk] = vmk<V>(0.0, 0.0);
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        const int j = s * H + h;
-                        if (j < N) {
-                            V u = (j == k) ? inv : vmul<V>(rb[j], inv);
-                            vfnms<V>(b[s], f, u);
-                        }
-                    }
-                }
-            } else {
-                V m = vmk<V>(0.0, 0.0);
-                if (h == hk) {
-                    m = vmul<V>(b[sk], inv);
-                    if (i != k) b[sk] = m;          // keep the multiplier for refinement
-                }
-                m = shfl_v<V>(m, gbase + hk, 32);
-                if (i != k) {
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        if (s >= sk) {
-                            const int j = s * H + h;
-                            if (j > k && j < N) vfnms<V>(b[s], m, rb[j]);
-                        }
-                    }
-                    vfnms<V>(z, m, rb[N]);
-                }
-            }
-        }
-
-        // ---- solution y (FP64)
-        double2 y = dmk(0.0, 0.0);
-        if (MODE == LDGA_PREC_FP64_INV) {
-            // y_i = sum_j X_ij
-            double2 part = dmk(0.0, 0.0);
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const int j = s * H + h;
-                if (j < N) part = cadd(part, dmk((double)b[s].x, (double)b[s].y));
-            }
-#pragma unroll
-            for (int o = 1; o < H; o <<= 1) {
-                part.x += __shfl_xor_sync(0xffffffffu, part.x, o, 32);
-                part.y += __shfl_xor_sync(0xffffffffu, part.y, o, 32);
-            }
-            y = part;
-        } else {
-            const V t = vmul<V>(z, vinv<V>(mypiv));
-            y = dmk((double)t.x, (double)t.y);
-        }
-        if (act && h == 0) ysm[i] = y;
-        __syncthreads();
-
-        // ---- FP64 residual r_i = 1 - sum_j B_ij y_j and (MIXED) refinement
-        bool ok = true;
-        const int max_ref = (MODE == LDGA_PREC_MIXED) ? 6 : 0;
-        double bnorm_row = 0.0;
-        for (int it = 0; it <= max_ref; ++it) {
-            double2 acc = dmk(0.0, 0.0);
-            double rown = 0.0;
-            if (act) {
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const int j = s * H + h;
-                    if (j < N) {
-                        double2 g = Gsm[i * N + j];
-                        if (j == i) g = cadd(g, dii);
-                        acc = cadd(acc, cmul(g, ysm[j]));
-                        rown += fabs(g.x) + fabs(g.y);
-                    }
-                }
-            }
-#pragma unroll
-            for (int o = 1; o < H; o <<= 1) {
-                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o, 32);
-                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o, 32);
-                rown += __shfl_xor_sync(0xffffffffu, rown, o, 32);
-            }
-            const double2 r = dmk(1.0 - acc.x, -acc.y);
-            const double rabs = act ? fabs(r.x) + fabs(r.y) : 0.0;
-            const double yabs = act ? fabs(y.x) + fabs(y.y) : 0.0;
-            const double rmax = block_max(rabs, red);
-            const double ymax = block_max(yabs, red);
-            bnorm_row = block_max(act ? rown : 0.0, red);
-            const double berr = rmax / (bnorm_row * ymax + 1.0);
-            const bool finite = isfinite(berr);
-            if (MODE != LDGA_PREC_MIXED || it == max_ref) {
-                ok = finite && berr <= 1e-12;
-                break;
-            }
-            if (!finite) { ok = false; break; }
-            if (berr <= 2e-16) { ok = true; break; }
-            // delta = (stored FP32 elimination) applied to r
-            if (act && h == 0) zsm[i] = vmk<V>(r.x, r.y);
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const int sk = k / H, hk = k - (k / H) * H;
-                const V zk = zsm[k];
-                if (act && i != k && h == hk) {
-                    V zi = zsm[i];
-                    vfnms<V>(zi, b[sk], zk);
-                    zsm[i] = zi;
-                }
-                __syncthreads();
-            }
-            if (act && h == 0) {
-                const V d = vmul<V>(zsm[i], vinv<V>(mypiv));
-                y = cadd(y, dmk((double)d.x, (double)d.y));
-                ysm[i] = y;
-            }
-            // other lanes of the group need the updated y only through ysm
-            __syncthreads();
-            if (act) y = ysm[i];
-        }
-
-        // ---- chi and gamma
-        const double ysum = block_sum_det((act && h == 0) ? y.x : 0.0, red);
-        const double chi = ysum / (a.beta * a.beta);
-        if (tid == 0) {
-            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
-            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
-        }
-        if (act && h == 0) {
-            const double f = 1.0 + a.s * a.U * chi;
-            a.gam[ci] = cdiv(y, cscale(c0, f));
-        }
-        __syncthreads();
-    }
-}
 
 // Fallback: partial-pivoting FP64 LU of B = A^T (one matrix per CTA, shared memory), used for flagged
-// matrices and for box sizes without an unrolled instantiation.  list == nullptr: all (q, w).
+// matrices and for box sizes without a tiled instantiation.  list == nullptr: all (q, w);
+// count_dev (may be null) holds the number of list entries (written earlier on the stream).
 __global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int32_t* list, int count,
                                                        const int32_t* count_dev) {
     extern __shared__ double2 sm[];
@@ -404,32 +512,33 @@ __global__ void k_count_flags(const int32_t* flags, int n, int32_t* count) {
         if (flags[e] != 0) atomicAdd(count, 1);
 }
 
-template <int N, int H, typename TF, int MODE>
-int run_gj(ldga_ctx* ctx, const BseArgs& a0) {
+template <int N, int TR, int TC, int MPC, int MINB, typename TF, int MODE>
+int run_tile(ldga_ctx* ctx, const BseArgs& a0) {
     BseArgs a = a0;
     using V = typename C2<TF>::T;
-    const int threads = ((N * H + 31) / 32) * 32;
-    const size_t sm = (size_t)N * N * sizeof(double2) + 2 * (N + 1) * sizeof(V) + N * sizeof(double2) +
-                      32 * sizeof(double) + N * sizeof(V) + 64;
-    auto kern = k_bse_gj<N, H, TF, MODE>;
+    const int threads = TR * TC * MPC;
+    const size_t sm = (size_t)N * N * sizeof(double2) + MPC * group_smem<N, TR, TC, V>();
+    auto kern = k_bse_tile<N, TR, TC, MPC, MINB, TF, MODE>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-    // q chunk: enough CTAs for several waves, but reuse Gamma(w) for many q
-    int chunk = 8;
-    while (chunk > 1 && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk /= 2;
+    // q chunk: every group of the CTA takes several q of the same w (Gamma(w) staged once)
+    int chunk = 4 * MPC;
+    while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
     a.qchunk = chunk;
     dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     kern<<<grid, threads, sm, ctx->stream>>>(a);
-    LDGA_LAUNCHED(ctx, "k_bse_gj");
+    LDGA_LAUNCHED(ctx, "k_bse_tile");
     return LDGA_OK;
 }
 
-template <int N, int H, int H32>
+// TR x TC thread grid per matrix (TC lanes of a row group inside one warp); MPC matrices per CTA
+// MINB of the FP64 elimination (the register-heaviest variant that still spills little when capped)
+template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1>
 int run_mode(ldga_ctx* ctx, const BseArgs& a) {
     switch (ctx->prec) {
-        case LDGA_PREC_FP64_INV: return run_gj<N, H, double, LDGA_PREC_FP64_INV>(ctx, a);
-        case LDGA_PREC_FP64: return run_gj<N, H, double, LDGA_PREC_FP64>(ctx, a);
-        default: return run_gj<N, H32, float, LDGA_PREC_MIXED>(ctx, a);
+        case LDGA_PREC_FP64_INV: return run_tile<N, TR, TC, MPC64, 1, double, LDGA_PREC_FP64_INV>(ctx, a);
+        case LDGA_PREC_FP64: return run_tile<N, TR, TC, MPC64, MINB64, double, LDGA_PREC_FP64>(ctx, a);
+        default: return run_tile<N, TR, TC, MPC32, 1, float, LDGA_PREC_MIXED>(ctx, a);
     }
 }
 
@@ -455,17 +564,17 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     const int n = ctx->Nq * ctx->Nw;
     int st = LDGA_OK;
     bool generic = false;
-    switch (ctx->Nnu) {
-        case 4: st = run_mode<4, 1, 1>(ctx, a); break;
-        case 6: st = run_mode<6, 1, 1>(ctx, a); break;
-        case 8: st = run_mode<8, 1, 1>(ctx, a); break;
-        case 10: st = run_mode<10, 1, 1>(ctx, a); break;
-        case 12: st = run_mode<12, 1, 1>(ctx, a); break;
-        case 16: st = run_mode<16, 2, 1>(ctx, a); break;
-        case 20: st = run_mode<20, 2, 1>(ctx, a); break;
-        case 30: st = run_mode<30, 2, 2>(ctx, a); break;
-        case 40: st = run_mode<40, 2, 2>(ctx, a); break;
-        case 60: st = run_mode<60, 4, 2>(ctx, a); break;
+    switch (ctx->Nnu) {       // T x T thread grid: tiles of ceil(N/T) x ceil((N+1)/T) per thread
+        case 4: st = run_mode<4, 8, 8, 2, 2>(ctx, a); break;
+        case 6: st = run_mode<6, 8, 8, 2, 2>(ctx, a); break;
+        case 8: st = run_mode<8, 8, 8, 2, 2>(ctx, a); break;
+        case 10: st = run_mode<10, 8, 8, 2, 2>(ctx, a); break;
+        case 12: st = run_mode<12, 8, 8, 2, 2>(ctx, a); break;
+        case 16: st = run_mode<16, 8, 8, 2, 4>(ctx, a); break;
+        case 20: st = run_mode<20, 8, 8, 2, 4>(ctx, a); break;
+        case 30: st = run_mode<30, 8, 8, 2, 2>(ctx, a); break;
+        case 40: st = run_mode<40, 8, 8, 2, 2, 3>(ctx, a); break;
+        case 60: st = run_mode<60, 16, 16, 1, 1>(ctx, a); break;
         default: generic = true; break;
     }
     if (st != LDGA_OK) return st;
