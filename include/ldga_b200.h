@@ -173,6 +173,19 @@ int ldga_F_from_chi(ldga_ctx* ctx, const double* chi_loc, const double* gimp, in
 int ldga_lambda0(ldga_ctx* ctx, const double* F_in, double* lambda0_out);
 int ldga_set_lambda0(ldga_ctx* ctx, const double* lambda0);
 
+/* lambda_0 without any device allocation (no counterpart in the reference; it exists for callers
+ * that cannot allocate device memory: a host application whose device memory is entirely owned by
+ * its own pool allocator, or code that enqueues work while a stream capture forbids cudaMalloc).
+ * Same arithmetic as ldga_lambda0; no handle is needed.  chi0 [nq, nnu, nw], F [nnu, nnu, nw] and
+ * lambda0_out [nq, nnu, nw] must be device pointers on the current device; work is enqueued on
+ * `stream` (NULL: the legacy default stream) and the call returns without synchronising.
+ * Scratch: a built-in device array of 32768 (nu', w) columns (512 KiB, held by every GPU that loads
+ * the library until exit); nnu*nw above that is rejected with LDGA_ERR_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture.  Calls share the array: calls that overlap on one GPU race. */
+int ldga_lambda0_noalloc(const double* chi0, const double* F, int32_t nq, int32_t nnu, int32_t nw,
+                         double beta, double* lambda0_out, void* stream);
+
 /* ---------------------------------------------------------------- a8/a11: sums --------------- */
 
 /* sum_kω with the c2/w^2 tail (DataTypes.jl:215-249) of chi_r transformed by chi_lambda(., lam)

@@ -10,6 +10,7 @@
 #include <cooperative_groups.h>
 
 #include <cmath>
+#include <mutex>
 
 #include "ldga_internal.cuh"
 
@@ -469,6 +470,68 @@ int launch_g_ladder_full(ldga_ctx* ctx, int numax, const double* mu_dev) {
     k_g_ladder_full<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nf, ctx->fft_lo, numax, ctx->mp.beta, mu_dev,
                                                       ctx->d_eps, ctx->d_sigma, ctx->d_sigma_loc, ctx->d_gladder);
     LDGA_LAUNCHED(ctx, "k_g_ladder_full");
+    return LDGA_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free lambda_0 (ldga_lambda0_noalloc).
+//
+// Its one piece of scratch, the column sums colF[nu', w] = sum_nu F[nu, nu', w], lives in this
+// file-scope device array instead of memory from cudaMalloc.  Every GPU that loads the library holds
+// the array (LDGA_NOALLOC_MAX_COLS complex doubles, 512 KiB) until the process exits.  All calls share
+// it: the column-sum kernel writes every entry the lambda_0 kernel reads, so nothing needs clearing,
+// but two calls that run at the same time on one GPU (different streams, or host threads) race on it.
+// ---------------------------------------------------------------------------------------------
+#define LDGA_NOALLOC_MAX_COLS 32768
+static __device__ __align__(256) double2 g_noalloc_colF[LDGA_NOALLOC_MAX_COLS];
+
+namespace {
+// Device address of g_noalloc_colF per device.  In host code the symbol's name is only a host-side
+// stand-in; cudaGetSymbolAddress, called with the device current, gives the address a kernel can use.
+double2* noalloc_colF(int device, cudaError_t* err) {
+    static double2* addr[64] = {nullptr};
+    static std::mutex mu;
+    if (device < 0 || device >= 64) { *err = cudaErrorInvalidDevice; return nullptr; }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        double2* p = nullptr;
+        *err = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_colF);
+        if (*err != cudaSuccess) return nullptr;
+        addr[device] = p;
+    }
+    *err = cudaSuccess;
+    return addr[device];
+}
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
+extern "C" int ldga_lambda0_noalloc(const double* chi0, const double* F, int32_t nq, int32_t nnu, int32_t nw,
+                                    double beta, double* lambda0_out, void* stream) {
+    if (!chi0 || !F || !lambda0_out) return ctx_fail(nullptr, LDGA_ERR_ARG, "ldga_lambda0_noalloc: null argument");
+    if (nq < 1 || nnu < 1 || nw < 1) return ctx_fail(nullptr, LDGA_ERR_ARG, "ldga_lambda0_noalloc: sizes must be positive");
+    if ((long)nnu * nw > LDGA_NOALLOC_MAX_COLS)
+        return ctx_fail(nullptr, LDGA_ERR_ARG,
+                        "ldga_lambda0_noalloc: Nnu*Nw = " + std::to_string((long)nnu * nw) +
+                            " exceeds the built-in scratch of " + std::to_string(LDGA_NOALLOC_MAX_COLS) +
+                            " (nu', w) columns");
+    if (!is_device_ptr(chi0) || !is_device_ptr(F) || !is_device_ptr(lambda0_out))
+        return ctx_fail(nullptr, LDGA_ERR_ARG, "ldga_lambda0_noalloc: chi0, F and lambda0_out must be device memory");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    double2* colF = noalloc_colF(dev, &e);
+    if (!colF) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_colsum_F<<<64, 256, 0, s>>>(nnu, nw, reinterpret_cast<const double2*>(F), colF);
+    k_lambda0<<<4 * 148, 256, 0, s>>>(nq, nnu, nw, 1.0 / (beta * beta), reinterpret_cast<const double2*>(chi0), colF,
+                                      reinterpret_cast<double2*>(lambda0_out));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("ldga_lambda0_noalloc launch: ") + cudaGetErrorString(e));
     return LDGA_OK;
 }
 
