@@ -403,6 +403,246 @@ __global__ void __launch_bounds__(TR * TC * MPC, MINB) k_bse_tile(const BseArgs 
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// FP64 single right-hand side by LU: forward elimination below the pivot only (~N^3/3 complex
+// multiply-adds instead of Gauss-Jordan's N^3/2), then a blocked back substitution.
+//
+// Same 2-D cyclic register tile as k_bse_tile (thread (tr, tc) of a T x T group holds rows tr + T a,
+// columns tc + T c of [B | 1]).  Step k = ktc + T kc:
+//   1. the row group of row k writes row k (columns > k) to a double-buffered shared row, the lanes
+//      owning column k write column k (rows >= k, pivot included) to a double-buffered shared column,
+//      and the row group also keeps the row's part inside the diagonal block kc for the back
+//      substitution;
+//   2. one named barrier per matrix group;
+//   3. every thread forms 1/pivot itself (FP32 rcp seed + two FP64 Newton steps), scales the row
+//      entries of its columns and updates its active tile: tile rows >= kc (the boundary tile row
+//      predicated on tr > ktc) times tile columns >= kc (boundary predicated on tc > ktc).
+// Both broadcasts are shared-memory reads (one 16-byte load per value); no shuffles.
+// Back substitution, tile row r from the last to the first: the row groups fold the lanes' partial
+// sums of the rows of block r (three xor shuffles), the rhs lane publishes z_i - sum, warp 0 of the
+// group solves the T x T upper-triangular diagonal block with lanes as rows (T shuffle broadcasts),
+// publishes y of the block, and every lane adds u_ij y_j of its column of block r into the partial
+// sums of the rows above.  Two named barriers per block.
+// The solution is verified by its FP64 backward error exactly like k_bse_tile (flag above 1e-12).
+template <int N, int T>
+struct LuSmem {
+    static constexpr int RT = (N + T - 1) / T;
+    static constexpr int NC = N + 1;
+    static constexpr int G = T * T;
+    // rowbuf [2][NC], colbuf [2][N], diag [RT][T][T], pinv [N], dinv [N], zbuf [T], ysm [N] (double2),
+    // red [8 * G/32] (double)
+    static constexpr size_t bytes =
+        (2 * NC + 2 * N + RT * T * T + N + N + T + N) * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
+};
+
+template <int N, int T, int MPC, int MINB>
+__global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
+    using LS = LuSmem<N, T>;
+    constexpr int RT = LS::RT, NC = LS::NC, G = LS::G;
+    constexpr int CT = (NC + T - 1) / T;
+    constexpr int TCN = N % T, CN = N / T;                // owner lane / tile column of the rhs
+    static_assert(T <= 32 && 32 % T == 0, "a row group must sit inside one warp");
+    extern __shared__ double2 sm[];
+    double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
+    const int tid = threadIdx.x;
+    const int g = tid / G, t = tid - g * G;
+    const int tr = t / T, tc = t - (t / T) * T;
+    const int lane = tid & 31;
+        const int bar = g + 1;
+    char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * LS::bytes;
+    double2* rowbuf = reinterpret_cast<double2*>(gs);     // [2][NC]
+    double2* colbuf = rowbuf + 2 * NC;                    // [2][N]
+    double2* diag = colbuf + 2 * N;                       // [RT][T][T]
+    double2* pinv = diag + RT * T * T;                    // [N]
+    double2* dinv = pinv + N;                             // [N] 1/chi0(q, i, w)
+    double2* zbuf = dinv + N;                             // [T]
+    double2* ysm = zbuf + T;                              // [N]
+    double* red = reinterpret_cast<double*>(ysm + N);     // [8 * G/32]
+
+    const int w = blockIdx.y;
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    {
+        const double2* Gw = a.Gamma + (size_t)w * N * N;
+        for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+    }
+    __syncthreads();
+
+    for (int q = q0 + g; q < q1; q += MPC) {
+        const double2* c0p = a.chi0 + (size_t)q + (size_t)a.nq * ((size_t)N * w);
+        for (int i = t; i < N; i += G) dinv[i] = cinv(c0p[(size_t)a.nq * i]);
+        named_barrier(bar, G);
+        // ---- load the tile of [B | 1], B_ij = Gamma[j, i] + delta_ij / chi0(q, i, w); the diagonal
+        // i == j can only fall into tile (ra, ra) of the threads with tr == tc
+        double2 b[RT][CT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+#pragma unroll
+            for (int c = 0; c < CT; ++c) {
+                const int j = tc + T * c;
+                double2 v = dmk(0.0, 0.0);
+                if (i < N) {
+                    if (j < N) {
+                        v = Gsm[i * N + j];
+                        if (c == ra && tr == tc) v = cadd(v, dinv[i]);
+                    } else if (j == N) {
+                        v = dmk(1.0, 0.0);
+                    }
+                }
+                b[ra][c] = v;
+            }
+        }
+
+        // ---- forward elimination (rows below the pivot)
+#pragma unroll
+        for (int kc = 0; kc < RT; ++kc) {
+            const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+            for (int ktc = 0; ktc < kend; ++ktc) {
+                const int k = ktc + T * kc;
+                double2* rb = rowbuf + (k & 1) * NC;
+                double2* cb = colbuf + (k & 1) * N;
+                if (tr == ktc) {
+#pragma unroll
+                    for (int c = kc; c < CT; ++c) {
+                        const int j = tc + T * c;
+                        if (j > k && j <= N) rb[j] = b[kc][c];
+                    }
+                    if (tc > ktc) diag[(kc * T + ktc) * T + tc] = b[kc][kc];
+                }
+                if (tc == ktc) {
+#pragma unroll
+                    for (int ra = kc; ra < RT; ++ra) {
+                        const int i = tr + T * ra;
+                        if (i >= k && i < N) cb[i] = b[ra][kc];
+                    }
+                }
+                named_barrier(bar, G);
+                const double2 inv = vinv(cb[k]);
+                if (t == 0) pinv[k] = inv;
+                double2 u[CT];
+#pragma unroll
+                for (int c = kc; c < CT; ++c) {
+                    const int j = tc + T * c;
+                    u[c] = (j > k && j <= N) ? vmul<double2>(rb[j], inv) : dmk(0.0, 0.0);
+                }
+#pragma unroll
+                for (int ra = kc; ra < RT; ++ra) {
+                    const int i = tr + T * ra;
+                    if ((ra > kc || tr > ktc) && i < N) {
+                        const double2 m = cb[i];
+#pragma unroll
+                        for (int c = kc; c < CT; ++c) {
+                            if (c > kc || tc > ktc) vfnms<double2>(b[ra][c], m, u[c]);
+                        }
+                    }
+                }
+            }
+        }
+
+        // ---- back substitution, one diagonal block (tile row) at a time from the bottom
+        double2 acc[RT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) acc[ra] = dmk(0.0, 0.0);
+#pragma unroll
+        for (int r = RT - 1; r >= 0; --r) {
+            const int nb = (N - T * r) < T ? (N - T * r) : T;
+            double2 s = acc[r];
+#pragma unroll
+            for (int o = 1; o < T; o <<= 1) {
+                s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+                s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+            }
+            if (tc == TCN && tr < nb) zbuf[tr] = csub(b[r][CN], s);
+            named_barrier(bar, G);
+            if (t < 32) {
+                // lanes a < nb hold row a of the diagonal block; y of the block from the last row up
+                const int ar = lane < nb ? lane : 0;
+                double2 z = zbuf[ar];
+                double2 yv = dmk(0.0, 0.0);
+#pragma unroll
+                for (int tt = T - 1; tt >= 0; --tt) {
+                    if (tt < nb) {
+                        double2 yt = lane == tt ? cmul(z, pinv[T * r + tt]) : dmk(0.0, 0.0);
+                        yt.x = __shfl_sync(0xffffffffu, yt.x, tt);
+                        yt.y = __shfl_sync(0xffffffffu, yt.y, tt);
+                        if (lane == tt) yv = yt;
+                        if (lane < tt) z = csub(z, cmul(diag[(r * T + lane) * T + tt], yt));
+                    }
+                }
+                if (lane < nb) ysm[T * r + lane] = yv;
+            }
+            named_barrier(bar, G);
+            if (r > 0 && T * r + tc < N) {
+                const double2 yj = ysm[T * r + tc];
+#pragma unroll
+                for (int ra = 0; ra < r; ++ra) acc[ra] = cadd(acc[ra], cmul(b[ra][r], yj));
+            }
+        }
+
+        // ---- FP64 backward error |1 - B y| / (|B| |y| + 1)
+        double2 y[RT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+            y[ra] = i < N ? ysm[i] : dmk(0.0, 0.0);
+        }
+        double st[4] = {0.0, 0.0, 0.0, 0.0};
+        const int op[4] = {1, 1, 1, 0};
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+            double2 accr = dmk(0.0, 0.0);
+            double rown = 0.0;
+            if (i < N) {
+#pragma unroll
+                for (int c = 0; c < CT; ++c) {
+                    const int j = tc + T * c;
+                    if (j < N) {
+                        double2 gv = Gsm[i * N + j];
+                        if (c == ra && tr == tc) gv = cadd(gv, dinv[i]);
+                        accr = cadd(accr, cmul(gv, ysm[j]));
+                        rown += fabs(gv.x) + fabs(gv.y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < T; o <<= 1) {
+                accr.x += __shfl_xor_sync(0xffffffffu, accr.x, o);
+                accr.y += __shfl_xor_sync(0xffffffffu, accr.y, o);
+                rown += __shfl_xor_sync(0xffffffffu, rown, o);
+            }
+            if (i < N && tc == 0) {
+                st[0] = fmax(st[0], fabs(1.0 - accr.x) + fabs(accr.y));
+                st[1] = fmax(st[1], fabs(y[ra].x) + fabs(y[ra].y));
+                st[2] = fmax(st[2], rown);
+                st[3] += y[ra].x;
+            }
+        }
+        group_reduce<4, G>(st, op, red, bar, t);
+        const double berr = st[0] / (st[2] * st[1] + 1.0);
+
+        // ---- chi and gamma = y / (chi0 (1 + s U chi))
+        const double chi = st[3] / (a.beta * a.beta);
+        const bool ok = isfinite(berr) && berr <= 1e-12;
+        if (t == 0) {
+            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+        }
+        const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+            if (i < N && tc == 0) {
+                const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+                a.gam[ci] = cscale(cmul(y[ra], dinv[i]), rf);
+            }
+        }
+        named_barrier(bar, G);   // shared buffers of this matrix are read before the next one writes
+    }
+}
+
 __device__ __forceinline__ double block_sum_det(double v, double* red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -531,13 +771,30 @@ int run_tile(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
+template <int N, int T, int MPC, int MINB>
+int run_lu(ldga_ctx* ctx, const BseArgs& a0) {
+    BseArgs a = a0;
+    const int threads = T * T * MPC;
+    const size_t sm = (size_t)N * N * sizeof(double2) + MPC * LuSmem<N, T>::bytes;
+    auto kern = k_bse_lu<N, T, MPC, MINB>;
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+    int chunk = 4 * MPC;
+    while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
+    a.qchunk = chunk;
+    dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
+    StageTimer st_(ctx, LDGA_STAGE_BSE);
+    kern<<<grid, threads, sm, ctx->stream>>>(a);
+    LDGA_LAUNCHED(ctx, "k_bse_lu");
+    return LDGA_OK;
+}
+
 // TR x TC thread grid per matrix (TC lanes of a row group inside one warp); MPC matrices per CTA
 // MINB of the FP64 elimination (the register-heaviest variant that still spills little when capped)
 template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1>
 int run_mode(ldga_ctx* ctx, const BseArgs& a) {
     switch (ctx->prec) {
         case LDGA_PREC_FP64_INV: return run_tile<N, TR, TC, MPC64, 1, double, LDGA_PREC_FP64_INV>(ctx, a);
-        case LDGA_PREC_FP64: return run_tile<N, TR, TC, MPC64, MINB64, double, LDGA_PREC_FP64>(ctx, a);
+        case LDGA_PREC_FP64: return run_lu<N, TC, MPC64, MINB64>(ctx, a);
         default: return run_tile<N, TR, TC, MPC32, 1, float, LDGA_PREC_MIXED>(ctx, a);
     }
 }

@@ -26,31 +26,51 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Cluster-wide sums of NV values, fixed order; every thread of every CTA receives the totals.
-// red: shared [NV * 32]; part: shared [2 * NV] exchange slots; parity alternates between calls.
+// Shared state of cluster_sum: per-warp partials, two exchange slots read by the other CTAs of the
+// cluster (alternating between calls), and the broadcast of the totals inside the CTA.
 template <int NV>
-__device__ void cluster_sum(double (&v)[NV], double* red, double* part, int& parity) {
+struct ClRed {
+    double red[NV * 32];
+    double part[2 * NV];
+    double bcast[NV];
+};
+
+// Cluster-wide sums of NV values in a fixed order; every thread of every CTA receives the totals.
+// Per call: warp shuffles, one CTA barrier, warp 0 folds the warp partials and publishes them, one
+// cluster barrier, then warp 0 alone reads the kCluster remote partials (one distributed-shared-
+// memory load per lane) and broadcasts the totals through shared memory.  Slot reuse is safe: a
+// slot written in call i + 2 was last read before every CTA arrived at the barrier of call i + 1.
+// parity: a register of every thread, flipped identically by all of them.
+template <int NV>
+__device__ void cluster_sum(double (&v)[NV], ClRed<NV>& s, int& parity) {
     cg::cluster_group cl = cg::this_cluster();
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const int slot = parity * NV;
 #pragma unroll
     for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
     if (l == 0) {
 #pragma unroll
-        for (int j = 0; j < NV; ++j) red[j * 32 + w] = v[j];
+        for (int j = 0; j < NV; ++j) s.red[j * 32 + w] = v[j];
     }
     __syncthreads();
-    if (threadIdx.x < NV) {
-        double s = 0.0;
-        for (int i = 0; i < nwarp; ++i) s += red[threadIdx.x * 32 + i];
-        part[parity * NV + threadIdx.x] = s;
+    if (w == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const double x = warp_sum(l < nwarp ? s.red[j * 32 + l] : 0.0);
+            if (l == 0) s.part[slot + j] = x;
+        }
     }
     cl.sync();
+    if (w == 0) {
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        double s = 0.0;
-        for (int r = 0; r < kCluster; ++r) s += cl.map_shared_rank(part, r)[parity * NV + j];
-        v[j] = s;
+        for (int j = 0; j < NV; ++j) {
+            const double x = warp_sum(l < kCluster ? cl.map_shared_rank(s.part, l)[slot + j] : 0.0);
+            if (l == 0) s.bcast[j] = x;
+        }
     }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = s.bcast[j];
     parity ^= 1;
 }
 
@@ -124,8 +144,7 @@ __device__ __forceinline__ double finish_kw(const SumArgs& a, double s) {
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_sum_kw(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double lam,
          const double* lam_dev, int mode, double* out) {
-    __shared__ double red[32];
-    __shared__ double part[2];
+    __shared__ ClRed<1> cr;
     int parity = 0;
     if (lam_dev) lam += lam_dev[0];
     double v[1] = {0.0};
@@ -140,7 +159,7 @@ k_sum_kw(SumArgs a, const double* __restrict__ chi, const double* __restrict__ k
             s = (s - tail + a.c2 * (-a.beta * a.beta / 12.0)) / a.beta;
             v[0] = fma(kmult[q], s, v[0]);
         }
-        cluster_sum<1>(v, red, part, parity);
+        cluster_sum<1>(v, cr, parity);
         if (cl_tid() == 0) out[0] = v[0] * a.inv_nk;
     } else {
         const int total = a.nq * a.nw;
@@ -150,7 +169,7 @@ k_sum_kw(SumArgs a, const double* __restrict__ chi, const double* __restrict__ k
             const double t = lam != 0.0 ? x / (lam * x + 1.0) : x;
             v[0] = fma(kmult[q], mode == 1 ? -t * t : t, v[0]);
         }
-        cluster_sum<1>(v, red, part, parity);
+        cluster_sum<1>(v, cr, parity);
         if (cl_tid() == 0) out[0] = finish_kw(a, v[0]);
     }
     cg::this_cluster().sync();
@@ -174,30 +193,53 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 // newton_right, 1-D (LambdaCorrection/helpers.jl:133-153), iteration for iteration; f and df are the
 // reference's f_c1/df_c1 (conditions_new.jl:152-153): both carry the tail terms of sum_kω.
 // rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0); xmin = xmin_dev[0] (get_λ_min, computed on the stream).
+// K > 0: every thread keeps its K elements of chi and their kMult weights in registers for the whole
+// loop (elements e = tid + j * threads, the order the K = 0 streaming form sums in); the constant
+// tail of sum_kω is formed once.  An iteration is then K divisions, one cluster_sum and the step.
+template <int K>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
            const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out) {
-    __shared__ double red[64];
-    __shared__ double part[4];
+    __shared__ ClRed<2> cr;
     int parity = 0;
     const double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
     const double xmin = xmin_dev[0];
     const double delta = 1e-4;
     const int total = a.nq * a.nw;
+    const int tid = cl_tid(), nth = cl_nth();
+    // finish_kw(s) = (s inv_nk - tail + c) / beta with the tail and constant hoisted out of the loop
+    const double tail = w2_tail(a);
+    const double cst = (-a.beta * a.beta / 12.0) * a.c2;
+    double xv[K > 0 ? K : 1], kv[K > 0 ? K : 1];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int e = tid + j * nth;
+        xv[j] = e < total ? chi[e] : 0.0;
+        kv[j] = e < total ? kmult[e % a.nq] : 0.0;
+    }
     double x0 = 0.0, xi = x0;
     int i = 1;
     while (true) {
         double v[2] = {0.0, 0.0};
-        for (int e = cl_tid(); e < total; e += cl_nth()) {
-            const double x = chi[e];
-            const double t = x / (xi * x + 1.0);
-            const double km = kmult[e % a.nq];
-            v[0] = fma(km, t, v[0]);
-            v[1] = fma(km, -t * t, v[1]);
+        if (K > 0) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const double t = xv[j] / (xi * xv[j] + 1.0);
+                v[0] = fma(kv[j], t, v[0]);
+                v[1] = fma(kv[j], -t * t, v[1]);
+            }
+        } else {
+            for (int e = tid; e < total; e += nth) {
+                const double x = chi[e];
+                const double t = x / (xi * x + 1.0);
+                const double km = kmult[e % a.nq];
+                v[0] = fma(km, t, v[0]);
+                v[1] = fma(km, -t * t, v[1]);
+            }
         }
-        cluster_sum<2>(v, red, part, parity);
-        const double fi = finish_kw(a, v[0]) - rhs;
-        const double dfi = finish_kw(a, v[1]);
+        cluster_sum<2>(v, cr, parity);
+        const double fi = (v[0] * a.inv_nk - tail + cst) / a.beta - rhs;
+        const double dfi = (v[1] * a.inv_nk - tail + cst) / a.beta;
         const double dfii = 1.0 / dfi;
         xi = x0 - dfii * fi;
         if (fabs(fi) < atol) break;
@@ -206,7 +248,7 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
         if (i >= nsteps) break;
         ++i;
     }
-    if (cl_tid() == 0) { out[0] = xi; out[1] = (double)i; }
+    if (tid == 0) { out[0] = xi; out[1] = (double)i; }
     cg::this_cluster().sync();
 }
 
@@ -224,28 +266,55 @@ __device__ __forceinline__ double2 g_at(double mu, double eps, double2 sig, int 
     return cinv(make_double2(mu - eps - sig.x, (2.0 * nn + 1.0) * M_PI / beta - sig.y));
 }
 
+// K > 0: the Newton loop keeps every thread's K (q, nu) elements (kMult, eps_q, Sigma, nu_n) in
+// registers; K = 0 streams them from memory each iteration.
+template <int K>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restrict__ eps,
                 const double2* __restrict__ sigma, int fix_n, double mu_in, double* out) {
-    __shared__ double red[3 * 32];
-    __shared__ double part[6];
+    __shared__ ClRed<2> cr2;
+    __shared__ ClRed<3> cr3;
     int parity = 0;
     const int total = a.nq * a.numax;
     double mu = mu_in;
     bool failed = false;
+    double ck[K > 0 ? K : 1], ce[K > 0 ? K : 1], cw[K > 0 ? K : 1];
+    double2 cs[K > 0 ? K : 1];
+    if (fix_n) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int e = cl_tid() + j * cl_nth();
+            const bool in = e < total;
+            const int q = in ? e % a.nq : 0, nn = in ? e / a.nq : 0;
+            ck[j] = in ? kmult[q] : 0.0;       // padding elements carry weight 0
+            ce[j] = in ? eps[q] : 0.0;
+            cs[j] = in ? sigma[e] : make_double2(0.0, 0.0);
+            cw[j] = (2.0 * nn + 1.0) * M_PI / a.beta;
+        }
+    }
     if (fix_n) {
         // safeguarded Newton (same method as the oracle's mu_newton); f = filling_pos - n
         double lo = -INFINITY, hi = INFINITY;
         const double tol = 1e-14;
         for (int it = 0; it < 100; ++it) {
             double v[2] = {0.0, 0.0};
-            for (int e = cl_tid(); e < total; e += cl_nth()) {
-                const int q = e % a.nq, nn = e / a.nq;
-                const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
-                v[0] = fma(kmult[q], G.x, v[0]);
-                v[1] = fma(kmult[q], -(G.x * G.x - G.y * G.y), v[1]);
+            if (K > 0) {
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    // g_at(mu, eps, sigma, nn, beta) with its operands from registers
+                    const double2 G = cinv(make_double2(mu - ce[j] - cs[j].x, cw[j] - cs[j].y));
+                    v[0] = fma(ck[j], G.x, v[0]);
+                    v[1] = fma(ck[j], -(G.x * G.x - G.y * G.y), v[1]);
+                }
+            } else {
+                for (int e = cl_tid(); e < total; e += cl_nth()) {
+                    const int q = e % a.nq, nn = e / a.nq;
+                    const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
+                    v[0] = fma(kmult[q], G.x, v[0]);
+                    v[1] = fma(kmult[q], -(G.x * G.x - G.y * G.y), v[1]);
+                }
             }
-            cluster_sum<2>(v, red, part, parity);
+            cluster_sum<2>(v, cr2, parity);
             const double sG = v[0] * a.inv_nk, dG = v[1] * a.inv_nk;
             const double f = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell) - a.n;
             const double df = 2.0 * (2.0 * dG / a.beta + a.shell) / (1.0 + a.U * a.shell);
@@ -284,7 +353,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
         v[0] = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), v[0]);
         v[1] = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, v[1]);
     }
-    cluster_sum<3>(v, red, part, parity);
+    cluster_sum<3>(v, cr3, parity);
     if (cl_tid() == 0) {
         const double sG = v[2] * a.inv_nk;
         out[0] = mu;
@@ -299,8 +368,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_calc_E(GArgs a, const double* kmult, const double* eps, const double2* G, int ldg, const double2* sigma,
          double mu, double* out) {
-    __shared__ double red[2 * 32];
-    __shared__ double part[4];
+    __shared__ ClRed<2> cr;
     int parity = 0;
     const double hartree = a.n * a.U / 2.0;
     double v[2] = {0.0, 0.0};
@@ -322,7 +390,7 @@ k_calc_E(GArgs a, const double* kmult, const double* eps, const double2* G, int 
         v[0] = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), v[0]);
         v[1] = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, v[1]);
     }
-    cluster_sum<2>(v, red, part, parity);
+    cluster_sum<2>(v, cr, parity);
     if (cl_tid() == 0) { out[0] = v[0] * a.inv_nk / a.beta; out[1] = v[1] * a.inv_nk / a.beta; }
     cg::this_cluster().sync();
 }
@@ -440,8 +508,11 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
     int st = launch_lambda_min(ctx, LDGA_CH_M, d_out + 2);
     if (st) return st;
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
-    k_lambda_m<<<kCluster, kClThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[LDGA_CH_M], ctx->d_kmult,
-                                                         rhs_const, rhs_sub_dev, d_out + 2, 100, 1e-13, d_out);
+    const SumArgs sa = sum_args(ctx);
+    const int per = (sa.nq * sa.nw + kCluster * kClThreads - 1) / (kCluster * kClThreads);
+    auto kern = per <= 4 ? k_lambda_m<4> : per <= 8 ? k_lambda_m<8> : per <= 16 ? k_lambda_m<16> : k_lambda_m<0>;
+    kern<<<kCluster, kClThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
+                                                   d_out + 2, 100, 1e-13, d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");
     return LDGA_OK;
 }
@@ -449,8 +520,9 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
 int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out) {
     GArgs a = g_args(ctx, numax, host_G_shell_sum(numax + 1, ctx->mp.beta));
     StageTimer st_(ctx, LDGA_STAGE_GLADDER);
-    k_mu_fit_energy<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n,
-                                                              mu_in, d_out);
+    const int per = (a.nq * a.numax + kCluster * kClThreads - 1) / (kCluster * kClThreads);
+    auto kern = per <= 4 ? k_mu_fit_energy<4> : per <= 8 ? k_mu_fit_energy<8> : k_mu_fit_energy<0>;
+    kern<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n, mu_in, d_out);
     LDGA_LAUNCHED(ctx, "k_mu_fit_energy");
     return LDGA_OK;
 }
