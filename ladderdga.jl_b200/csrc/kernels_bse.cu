@@ -404,35 +404,40 @@ __global__ void __launch_bounds__(TR * TC * MPC, MINB) k_bse_tile(const BseArgs 
 }
 
 // ------------------------------------------------------------------------------------------------
-// FP64 single right-hand side by LU: forward elimination below the pivot only (~N^3/3 complex
-// multiply-adds instead of Gauss-Jordan's N^3/2), then a blocked back substitution.
+// FP64 single right-hand side by LU with Gauss-Jordan inside the diagonal blocks: forward elimination
+// of the rows below the pivot plus the rows above it in the same T-row block (~N^3/3 + N^2 T/2 complex
+// multiply-adds instead of full Gauss-Jordan's N^3/2), then a block back substitution without any
+// sequential triangular solve.
 //
 // Same 2-D cyclic register tile as k_bse_tile (thread (tr, tc) of a T x T group holds rows tr + T a,
 // columns tc + T c of [B | 1]).  Step k = ktc + T kc:
-//   1. the row group of row k writes row k (columns > k) to a double-buffered shared row, the lanes
-//      owning column k write column k (rows >= k, pivot included) to a double-buffered shared column,
-//      and the row group also keeps the row's part inside the diagonal block kc for the back
-//      substitution;
+//   1. the row group of row k shuffles the pivot b_kk from lane ktc, forms 1/b_kk (FP32 rcp seed +
+//      two FP64 Newton steps) and writes row k scaled by it (columns >= T kc) to a double-buffered
+//      shared row; the lanes owning column k write column k (rows >= T kc) to a double-buffered
+//      shared column;
 //   2. one named barrier per matrix group;
-//   3. every thread forms 1/pivot itself (FP32 rcp seed + two FP64 Newton steps), scales the row
-//      entries of its columns and updates its active tile: tile rows >= kc (the boundary tile row
-//      predicated on tr > ktc) times tile columns >= kc (boundary predicated on tc > ktc).
-// Both broadcasts are shared-memory reads (one 16-byte load per value); no shuffles.
-// Back substitution, tile row r from the last to the first: the row groups fold the lanes' partial
-// sums of the rows of block r (three xor shuffles), the rhs lane publishes z_i - sum, warp 0 of the
-// group solves the T x T upper-triangular diagonal block with lanes as rows (T shuffle broadcasts),
-// publishes y of the block, and every lane adds u_ij y_j of its column of block r into the partial
-// sums of the rows above.  Two named barriers per block.
+//   3. every thread updates its tile rows >= kc except row k (so the rows of tile row kc above the
+//      pivot are eliminated too: the block becomes diagonal) times its tile columns > k.  The rows
+//      above the pivot in tile row kc cost no extra issue slots: that tile row is issued anyway,
+//      under a runtime predicate.
+// Padding rows (i >= N) and columns (j > N) hold zeros and stay zero, so no step needs a bounds
+// predicate.  Both broadcasts are shared-memory reads (one 16-byte load per value).
+// Back substitution, tile row r from the last to the first: every row of block r only needs the
+// solution of later blocks: the row group folds its lanes' partial sums (three xor shuffles), the rhs
+// lane writes y_i = (z_i - sum) / b_ii, one named barrier, and every lane adds u_ij y_j of its column
+// of block r into the partial sums of the rows above.
 // The solution is verified by its FP64 backward error exactly like k_bse_tile (flag above 1e-12).
 template <int N, int T>
 struct LuSmem {
     static constexpr int RT = (N + T - 1) / T;
     static constexpr int NC = N + 1;
+    static constexpr int CT = (NC + T - 1) / T;
     static constexpr int G = T * T;
-    // rowbuf [2][NC], colbuf [2][N], diag [RT][T][T], pinv [N], dinv [N], zbuf [T], ysm [N] (double2),
-    // red [8 * G/32] (double)
+    static constexpr int RW = CT * T;   // published row, padded to whole tile columns
+    static constexpr int CW = RT * T;   // published column, padded to whole tile rows
+    // rowbuf [2][RW], colbuf [2][CW], pinv [N], dinv [N], ysm [N] (double2), red [8 * G/32] (double)
     static constexpr size_t bytes =
-        (2 * NC + 2 * N + RT * T * T + N + N + T + N) * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
+        (2 * RW + 2 * CW + N + N + N) * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
 };
 
 template <int N, int T, int MPC, int MINB>
@@ -450,13 +455,11 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     const int lane = tid & 31;
         const int bar = g + 1;
     char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * LS::bytes;
-    double2* rowbuf = reinterpret_cast<double2*>(gs);     // [2][NC]
-    double2* colbuf = rowbuf + 2 * NC;                    // [2][N]
-    double2* diag = colbuf + 2 * N;                       // [RT][T][T]
-    double2* pinv = diag + RT * T * T;                    // [N]
+    double2* rowbuf = reinterpret_cast<double2*>(gs);     // [2][RW]
+    double2* colbuf = rowbuf + 2 * LS::RW;                // [2][CW]
+    double2* pinv = colbuf + 2 * LS::CW;                  // [N] 1/b_kk
     double2* dinv = pinv + N;                             // [N] 1/chi0(q, i, w)
-    double2* zbuf = dinv + N;                             // [T]
-    double2* ysm = zbuf + T;                              // [N]
+    double2* ysm = dinv + N;                              // [N]
     double* red = reinterpret_cast<double*>(ysm + N);     // [8 * G/32]
 
     const int w = blockIdx.y;
@@ -494,44 +497,40 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
             }
         }
 
-        // ---- forward elimination (rows below the pivot)
+        // ---- forward elimination (rows below the pivot).  Padding rows (i >= N) and columns (j > N)
+        // of the tile hold zeros and stay zero (their published values are zero), so no step needs
+        // a bounds predicate; entries at or left of the pivot are published but never read.
+        const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
 #pragma unroll
         for (int kc = 0; kc < RT; ++kc) {
             const int kend = (N - T * kc) < T ? (N - T * kc) : T;
 #pragma unroll 1
             for (int ktc = 0; ktc < kend; ++ktc) {
                 const int k = ktc + T * kc;
-                double2* rb = rowbuf + (k & 1) * NC;
-                double2* cb = colbuf + (k & 1) * N;
+                double2* rb = rowbuf + (k & 1) * LS::RW;
+                double2* cb = colbuf + (k & 1) * LS::CW;
                 if (tr == ktc) {
+                    // the row group of row k scales its row by 1/b_kk (pivot shuffled from lane ktc)
+                    double2 p;
+                    p.x = __shfl_sync(gmask, b[kc][kc].x, ktc, T);
+                    p.y = __shfl_sync(gmask, b[kc][kc].y, ktc, T);
+                    const double2 inv = vinv(p);
+                    if (tc == ktc) pinv[k] = inv;
 #pragma unroll
-                    for (int c = kc; c < CT; ++c) {
-                        const int j = tc + T * c;
-                        if (j > k && j <= N) rb[j] = b[kc][c];
-                    }
-                    if (tc > ktc) diag[(kc * T + ktc) * T + tc] = b[kc][kc];
+                    for (int c = kc; c < CT; ++c) rb[tc + T * c] = vmul<double2>(b[kc][c], inv);
                 }
                 if (tc == ktc) {
 #pragma unroll
-                    for (int ra = kc; ra < RT; ++ra) {
-                        const int i = tr + T * ra;
-                        if (i >= k && i < N) cb[i] = b[ra][kc];
-                    }
+                    for (int ra = kc; ra < RT; ++ra) cb[tr + T * ra] = b[ra][kc];
                 }
                 named_barrier(bar, G);
-                const double2 inv = vinv(cb[k]);
-                if (t == 0) pinv[k] = inv;
                 double2 u[CT];
 #pragma unroll
-                for (int c = kc; c < CT; ++c) {
-                    const int j = tc + T * c;
-                    u[c] = (j > k && j <= N) ? vmul<double2>(rb[j], inv) : dmk(0.0, 0.0);
-                }
+                for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
 #pragma unroll
                 for (int ra = kc; ra < RT; ++ra) {
-                    const int i = tr + T * ra;
-                    if ((ra > kc || tr > ktc) && i < N) {
-                        const double2 m = cb[i];
+                    if (ra > kc || tr != ktc) {
+                        const double2 m = cb[tr + T * ra];
 #pragma unroll
                         for (int c = kc; c < CT; ++c) {
                             if (c > kc || tc > ktc) vfnms<double2>(b[ra][c], m, u[c]);
@@ -554,25 +553,7 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
                 s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
                 s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
             }
-            if (tc == TCN && tr < nb) zbuf[tr] = csub(b[r][CN], s);
-            named_barrier(bar, G);
-            if (t < 32) {
-                // lanes a < nb hold row a of the diagonal block; y of the block from the last row up
-                const int ar = lane < nb ? lane : 0;
-                double2 z = zbuf[ar];
-                double2 yv = dmk(0.0, 0.0);
-#pragma unroll
-                for (int tt = T - 1; tt >= 0; --tt) {
-                    if (tt < nb) {
-                        double2 yt = lane == tt ? cmul(z, pinv[T * r + tt]) : dmk(0.0, 0.0);
-                        yt.x = __shfl_sync(0xffffffffu, yt.x, tt);
-                        yt.y = __shfl_sync(0xffffffffu, yt.y, tt);
-                        if (lane == tt) yv = yt;
-                        if (lane < tt) z = csub(z, cmul(diag[(r * T + lane) * T + tt], yt));
-                    }
-                }
-                if (lane < nb) ysm[T * r + lane] = yv;
-            }
+            if (tc == TCN && tr < nb) ysm[T * r + tr] = cmul(csub(b[r][CN], s), pinv[T * r + tr]);
             named_barrier(bar, G);
             if (r > 0 && T * r + tc < N) {
                 const double2 yj = ysm[T * r + tc];
@@ -794,7 +775,7 @@ template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1>
 int run_mode(ldga_ctx* ctx, const BseArgs& a) {
     switch (ctx->prec) {
         case LDGA_PREC_FP64_INV: return run_tile<N, TR, TC, MPC64, 1, double, LDGA_PREC_FP64_INV>(ctx, a);
-        case LDGA_PREC_FP64: return run_lu<N, TC, MPC64, MINB64>(ctx, a);
+        case LDGA_PREC_FP64: return run_lu<N, TC, 1, MINB64 * MPC64>(ctx, a);   // one matrix per CTA
         default: return run_tile<N, TR, TC, MPC32, 1, float, LDGA_PREC_MIXED>(ctx, a);
     }
 }

@@ -74,6 +74,46 @@ __device__ void cluster_sum(double (&v)[NV], ClRed<NV>& s, int& parity) {
     parity ^= 1;
 }
 
+// One-barrier cluster all-reduce for loops that reduce every iteration (Newton).  Each warp folds
+// its NV values with shuffles and lanes 0..kCluster-1 store them into slot [parity] of every CTA of
+// the cluster (lane r writes CTA r); after one cluster barrier every warp of every CTA sums all
+// kCluster * warps partials itself, in the same fixed order, so all threads hold identical totals
+// with no further CTA barrier.  A slot written in call i + 2 was last read before every thread
+// arrived at the barrier of call i + 1.
+constexpr int kClWarps = kClThreads / 32;
+template <int NV>
+struct ClAll {
+    double part[2][NV][kCluster * kClWarps];
+};
+
+template <int NV>
+__device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV>& s, int& parity) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int src = (int)cl.block_rank() * kClWarps + w;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[j] = x;
+    }
+    if (l < kCluster) {
+        ClAll<NV>* dst = cl.map_shared_rank(&s, l);
+#pragma unroll
+        for (int j = 0; j < NV; ++j) dst->part[parity][j][src] = v[j];
+    }
+    cl.sync();
+    constexpr int P = kCluster * kClWarps;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = 0.0;
+        for (int i = l; i < P; i += 32) x += s.part[parity][j][i];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[j] = x;
+    }
+    parity ^= 1;
+}
+
 __device__ __forceinline__ int cl_tid() { return cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int cl_nth() { return kCluster * blockDim.x; }
 
@@ -200,7 +240,7 @@ template <int K>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
            const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out) {
-    __shared__ ClRed<2> cr;
+    __shared__ ClAll<2> ca;
     int parity = 0;
     const double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
     const double xmin = xmin_dev[0];
@@ -237,7 +277,7 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
                 v[1] = fma(km, -t * t, v[1]);
             }
         }
-        cluster_sum<2>(v, cr, parity);
+        cluster_allsum<2>(v, ca, parity);
         const double fi = (v[0] * a.inv_nk - tail + cst) / a.beta - rhs;
         const double dfi = (v[1] * a.inv_nk - tail + cst) / a.beta;
         const double dfii = 1.0 / dfi;
@@ -272,7 +312,7 @@ template <int K>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restrict__ eps,
                 const double2* __restrict__ sigma, int fix_n, double mu_in, double* out) {
-    __shared__ ClRed<2> cr2;
+    __shared__ ClAll<2> ca2;
     __shared__ ClRed<3> cr3;
     int parity = 0;
     const int total = a.nq * a.numax;
@@ -314,7 +354,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
                     v[1] = fma(kmult[q], -(G.x * G.x - G.y * G.y), v[1]);
                 }
             }
-            cluster_sum<2>(v, cr2, parity);
+            cluster_allsum<2>(v, ca2, parity);
             const double sG = v[0] * a.inv_nk, dG = v[1] * a.inv_nk;
             const double f = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell) - a.n;
             const double df = 2.0 * (2.0 * dG / a.beta + a.shell) / (1.0 + a.U * a.shell);
@@ -510,7 +550,9 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
     const SumArgs sa = sum_args(ctx);
     const int per = (sa.nq * sa.nw + kCluster * kClThreads - 1) / (kCluster * kClThreads);
-    auto kern = per <= 4 ? k_lambda_m<4> : per <= 8 ? k_lambda_m<8> : per <= 16 ? k_lambda_m<16> : k_lambda_m<0>;
+    auto kern = per <= 2 ? k_lambda_m<2> : per <= 4 ? k_lambda_m<4> : per <= 6 ? k_lambda_m<6>
+              : per <= 8 ? k_lambda_m<8> : per <= 10 ? k_lambda_m<10> : per <= 12 ? k_lambda_m<12>
+              : per <= 16 ? k_lambda_m<16> : k_lambda_m<0>;
     kern<<<kCluster, kClThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
                                                    d_out + 2, 100, 1e-13, d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");
@@ -521,7 +563,8 @@ int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d
     GArgs a = g_args(ctx, numax, host_G_shell_sum(numax + 1, ctx->mp.beta));
     StageTimer st_(ctx, LDGA_STAGE_GLADDER);
     const int per = (a.nq * a.numax + kCluster * kClThreads - 1) / (kCluster * kClThreads);
-    auto kern = per <= 4 ? k_mu_fit_energy<4> : per <= 8 ? k_mu_fit_energy<8> : k_mu_fit_energy<0>;
+    auto kern = per <= 2 ? k_mu_fit_energy<2> : per <= 4 ? k_mu_fit_energy<4> : per <= 6 ? k_mu_fit_energy<6>
+              : per <= 8 ? k_mu_fit_energy<8> : k_mu_fit_energy<0>;
     kern<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n, mu_in, d_out);
     LDGA_LAUNCHED(ctx, "k_mu_fit_energy");
     return LDGA_OK;
