@@ -37,13 +37,17 @@ WORKLOAD_NAME = "3D sc Nk=32^3 (969 irreducible q), beta=20, U=1.5, Nnu=40, Nw=4
 METRIC = "(q,w)-points/s"
 PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
 REF_BUDGET_S = 120.0
-# DRAM bytes per BSE matrix (Nnu = 40, FP64) from one ncu capture (profiles/k_bse_tile_n40_fp64_3d16.md)
-BSE_DRAM_BYTES_PER_MATRIX = 5534720 / 6765
+# DRAM bytes per BSE matrix (Nnu = 40, FP64) from one ncu capture (profiles/k_bse_lu_n40_fp64_3d16.md)
+BSE_DRAM_BYTES_PER_MATRIX = 5423872 / 6765
+BSE_TILE = 8   # rows per diagonal block of the LU kernels at Nnu = 40
 
 
-def BSE_EXEC_CMACS(n: int) -> float:
-    """Complex multiply-adds of the kernel's Gauss-Jordan elimination of [B | 1] (N^3/2)."""
-    return n**3 / 2.0
+def BSE_EXEC_CMACS(n: int, t: int = BSE_TILE) -> float:
+    """Complex multiply-adds the LU kernels execute for one matrix: the forward elimination of
+    [B | 1] (step k updates the rows of its diagonal block and below, except row k, in the columns
+    right of k), the block back substitution (N^2/2) and the FP64 backward-error product (N^2)."""
+    fwd = sum((n - t * (k // t) - 1) * (n - k) for k in range(n))
+    return fwd + n * n / 2.0 + n * n
 
 
 def parse():
@@ -245,14 +249,16 @@ def roofline(stages: dict, chain, peaks: dict) -> dict:
         fp = "fp32" if chain.ctx.precision == 2 else "fp64"
         lanes = 128 if fp == "fp32" else 64
         peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
-        return {"kernel": "k_bse_tile (" + fp + ")", "bound": fp, "achieved": ach, "peak": peak,
+        kname = "k_bse_lu32 (FP32 LU + FP64 refinement)" if fp == "fp32" else "k_bse_lu (FP64 LU)"
+        return {"kernel": kname, "bound": fp, "achieved": ach, "peak": peak,
                 "unit": "TFLOP/s", "frac": ach / peak,
                 "work": "8 N^3 + 8 N^2 flops per matrix (the reference's LU + inverse formulation)",
                 "executed": {"tflops": exe, "frac": exe / peak,
-                             "work": "flops of the single-right-hand-side elimination the kernel runs"},
+                             "work": "flops of the LU solve of [B | 1], its back substitution and the "
+                                     "backward-error check (one pass; refinement sweeps not counted)"},
                 "traffic": BSE_DRAM_BYTES_PER_MATRIX * nq * nw,
-                "traffic_source": "ncu dram__bytes_read+write of one launch on 3D 16^3 (6765 matrices, "
-                                  "818 B each), scaled by the matrix count",
+                "traffic_source": "ncu dram__bytes_read+write of one FP64 launch on 3D 16^3 (6765 matrices, "
+                                  "802 B each), scaled by the matrix count",
                 "peak_source": f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz "
                                "(no FP64 figure is measured; the CUDA-core pipe, not HBM or tensor cores, "
                                "bounds this kernel)"}

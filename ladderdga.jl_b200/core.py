@@ -834,8 +834,11 @@ def setup_LDGA(kGridStr, mP: ModelParameters, sP: SimulationParameters, inputs, 
     if not silent:
         print(f"Inputs Read. imp_density = {imp_density}, χloc_m_sum = {χloc_m_sum}")
 
-    return lDΓAHelper(sP, mP, kG, Σ_ladderLoc, Σ_loc, imp_density, gloc, Γ_m, Γ_d, χloc_m_sum, χDMFT_m,
-                      χDMFT_d, χ_m_loc, γ_m_loc, χ_d_loc, γ_d_loc, χ0Loc, gimp, ctx=ctx, ctx_loc=ctx_loc)
+    h = lDΓAHelper(sP, mP, kG, Σ_ladderLoc, Σ_loc, imp_density, gloc, Γ_m, Γ_d, χloc_m_sum, χDMFT_m,
+                   χDMFT_d, χ_m_loc, γ_m_loc, χ_d_loc, γ_d_loc, χ0Loc, gimp, ctx=ctx, ctx_loc=ctx_loc)
+    _CTX_BY_GRID[id(kG)] = ctx
+    _HELPER_BY_GRID[id(kG)] = h
+    return h
 
 
 def _fetch(ctx: Context, what: str, ch: int = 0) -> np.ndarray:
@@ -1006,6 +1009,7 @@ def G_from_Σladder(Σ_ladder: np.ndarray, Σloc, kG: KGrid, mP: ModelParameters
 
 
 _CTX_BY_GRID: dict = {}
+_HELPER_BY_GRID: dict = {}
 
 
 def _current_ctx(kG: KGrid) -> Context:
@@ -1159,6 +1163,120 @@ def λ_correction(type_, χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHe
     raise RuntimeError(f"λ-correction type '{type_}' not recognized!")
 
 
+# =============================================================================================
+# parallel API (ladderDGATools.jl:46-245, parallelization_helpers.jl:197-240, 358-420)
+# =============================================================================================
+# The reference keeps ω blocks of χ₀, χ, γ and the EoM caches on Distributed.jl workers and
+# `collect_*` gathers them.  Here the GPU handle of the k-grid is the worker pool: the arrays stay
+# in its HBM and `collect_*` copies them out.  Results are identical to the single-call API.
+_EOM_STATE: dict = {}
+
+
+def _helper_of(h_or_kG) -> lDΓAHelper:
+    if isinstance(h_or_kG, lDΓAHelper):
+        return h_or_kG
+    h = _HELPER_BY_GRID.get(id(h_or_kG))
+    if h is None:
+        raise RuntimeError("Add workers and run lDGA_setup before calling parallel functions! "
+                           "(no GPU handle was set up for this k-grid)")
+    return h
+
+
+def calc_bubble_par(h_or_kG, mP=None, sP=None, collect_data: bool = True):
+    """``calc_bubble_par(h; collect_data)`` / ``(kG, mP, sP; collect_data)`` (ladderDGATools.jl:44-57):
+    χ₀ is computed on the device; with ``collect_data`` it is returned (``collect_χ0``)."""
+    h = _helper_of(h_or_kG)
+    h.ctx.call("ldga_bubble", None)
+    return collect_χ0(h) if collect_data else None
+
+
+def collect_χ0(h_or_kG, mP=None, sP=None) -> χ0T:
+    """``collect_χ0`` (ladderDGATools.jl:59-90): the device χ₀ of the last ``calc_bubble_par``."""
+    h = _helper_of(h_or_kG)
+    ctx = h.ctx
+    dev = DeviceArray(ctx, lambda: _fetch(ctx, "chi0"), (ctx.Nq, ctx.Nnu, ctx.Nw))
+    return χ0T(dev, h.mP.β, range(-h.sP.n_iω, h.sP.n_iω + 1), h.sP.n_iν, h.sP.shift, ctx=ctx)
+
+
+def calc_χγ_par(type_, h_or_Γ, kG=None, mP=None, sP=None, collect_data: bool = True):
+    """``calc_χγ_par(type, h; collect_data)`` / ``(type, Γr, kG, mP, sP; collect_data)``
+    (ladderDGATools.jl:128-145): the BSE of the device χ₀; results stay on the device unless
+    ``collect_data``."""
+    ch = _channel(type_)
+    if isinstance(h_or_Γ, lDΓAHelper):
+        h, Γ = h_or_Γ, (h_or_Γ.Γ_m if ch == CH_M else h_or_Γ.Γ_d)
+    else:
+        h, Γ = _helper_of(kG), h_or_Γ
+    χ, γ = _bse(h.ctx, ch, Γ, h.mP)
+    _log_q0_χ_check(h.ctx, χ, type_)
+    h._par_χγ = getattr(h, "_par_χγ", {})
+    h._par_χγ[ch] = (χ, γ)
+    return (χ, γ) if collect_data else None
+
+
+def collect_χ(type_, h_or_kG, mP=None, sP=None) -> χT:
+    """``collect_χ`` (parallelization_helpers.jl:358-383): χ_r of the last ``calc_χγ_par``."""
+    h, ch = _helper_of(h_or_kG), _channel(type_)
+    if ch not in getattr(h, "_par_χγ", {}):
+        raise RuntimeError(f"collect_χ: call calc_χγ_par(:{type_}, ...) first")
+    return h._par_χγ[ch][0]
+
+
+def collect_γ(type_, h_or_kG, mP=None, sP=None) -> γT:
+    """``collect_γ`` (parallelization_helpers.jl:385-410): γ_r of the last ``calc_χγ_par``."""
+    h, ch = _helper_of(h_or_kG), _channel(type_)
+    if ch not in getattr(h, "_par_χγ", {}):
+        raise RuntimeError(f"collect_γ: call calc_χγ_par(:{type_}, ...) first")
+    return h._par_χγ[ch][1]
+
+
+def initialize_EoM(h: lDΓAHelper, λ0, νGrid, force_reinit: bool = False, χ_m: χT | None = None,
+                   γ_m: γT | None = None, χ_d: χT | None = None, γ_d: γT | None = None) -> None:
+    """``initialize_EoM(h, λ₀, νGrid; χ_m, γ_m, χ_d, γ_d)`` (parallelization_helpers.jl:207-240):
+    binds the EoM inputs (default: the last ``calc_χγ_par`` results) to the device handle."""
+    νGrid = list(νGrid)
+    if νGrid != list(range(νGrid[0], νGrid[0] + len(νGrid))) or νGrid[0] != 0:
+        raise ValueError("νGrid must be 0:νmax-1 (the range calc_Σ_par fills)")
+    χ_m = collect_χ("m", h) if χ_m is None else χ_m
+    γ_m = collect_γ("m", h) if γ_m is None else γ_m
+    χ_d = collect_χ("d", h) if χ_d is None else χ_d
+    γ_d = collect_γ("d", h) if γ_d is None else γ_d
+    _prepare_eom(h, χ_m, γ_m, χ_d, γ_d, λ0)
+    _EOM_STATE.clear()
+    _EOM_STATE.update(h=h, χm=χ_m, γm=γ_m, χd=χ_d, γd=γ_d, λ0=λ0, νmax=len(νGrid))
+
+
+def calc_Σ_par(λm: float = 0.0, λd: float = 0.0, collect_data: bool = True, tc: bool = True):
+    """``calc_Σ_par(; λm, λd, collect_data, tc)`` (ladderDGATools.jl:223-229) on the inputs bound by
+    ``initialize_EoM``.  Σ_ladder[q, ν_n], ν_n = 0..νmax-1, Hartree term included."""
+    if not _EOM_STATE:
+        raise RuntimeError("Call initialize_EoM before calc_Σ_par in order to initialize worker caches.")
+    st = _EOM_STATE
+    out = calc_Σ(st["χm"], st["γm"], st["χd"], st["γd"], st["λ0"], st["h"], νmax=st["νmax"], λm=λm, λd=λd, tc=tc)
+    return out if collect_data else None
+
+
+def calc_Σ_par_(Σ_ladder: np.ndarray, λm: float = 0.0, λd: float = 0.0, collect_data: bool = True,
+                tc: bool = True):
+    """``calc_Σ_par!`` (ladderDGATools.jl:231-245): fills ``Σ_ladder`` in place."""
+    res = calc_Σ_par(λm=λm, λd=λd, collect_data=True, tc=tc)
+    if collect_data:
+        Σ_ladder[...] = res
+    return Σ_ladder if collect_data else None
+
+
+def gen_ω_part(sP: SimulationParameters, N: int):
+    """``gen_ω_part`` (parallelization_helpers.jl:49-53); see ``parallel``."""
+    from . import parallel
+    return parallel.gen_ω_part(sP, N)
+
+
+def par_partition(set_, N: int):
+    """``par_partition`` (parallelization_helpers.jl:22-29); see ``parallel``."""
+    from . import parallel
+    return parallel.par_partition(set_, N)
+
+
 # ASCII aliases
 chi0T, chiT, gammaT = χ0T, χT, γT   # the reference's χ₀T / λ₀ are χ0T / λ0 (no subscripts in identifiers)
 calc_chi_gamma = calc_χγ
@@ -1177,3 +1295,5 @@ G_from_Sigma, G_from_Sigma_ladder = G_from_Σ, G_from_Σladder
 find_usable_chi_interval, usable_windices = find_usable_χ_interval, usable_ωindices
 LDGAHelper = lDΓAHelper
 F_from_chi = F_from_χ
+calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_χγ_par, collect_χ0, collect_χ, collect_γ
+calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_part

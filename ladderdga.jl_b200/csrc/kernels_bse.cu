@@ -624,6 +624,584 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// MIXED: the k_bse_lu elimination in FP32 on packed f32x2 FMAs, then FP64 iterative refinement.
+//
+// A complex value of the tile is one 64-bit register pair (re, im).  b -= m u costs two f32x2 FMAs:
+//     b = fma2((m.x, m.x), (-u.x, -u.y), b);   b = fma2((m.y, m.y), (u.y, -u.x), b)
+// The publishing threads store both operands pre-arranged, so every broadcast is one 16-byte
+// shared-memory load: the pivot row as (-u.x, -u.y, u.y, -u.x) per column, the pivot column as
+// (m.x, m.x, m.y, m.y) per row.
+//
+// Refinement (all modes verify with the same FP64 backward error):
+//   r = 1 - B y in FP64 (Gamma from shared memory, 1/chi0 in FP64);
+//   forward replay of the stored FP32 elimination on r: z_i -= b_ik z_k / b_kk for the same rows
+//   as step k (the elimination leaves column k of every row it touched holding b_ik), one named
+//   barrier per step, z in shared memory;
+//   block back substitution with the stored U exactly like the first solve;  y += delta (FP64).
+// It stops once the backward error is below 1e-14; the flag threshold is 1e-12 as everywhere.
+typedef unsigned long long f2p;
+__device__ __forceinline__ f2p p2(float x, float y) {
+    f2p r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+    return r;
+}
+__device__ __forceinline__ float2 u2(f2p v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
+    f2p d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ float2 finv(float2 z) {
+    const float r = __frcp_rn(z.x * z.x + z.y * z.y);
+    return make_float2(z.x * r, -z.y * r);
+}
+
+template <int N, int T>
+struct Lu32Smem {
+    static constexpr int RT = (N + T - 1) / T;
+    static constexpr int CT = (N + 1 + T - 1) / T;
+    static constexpr int G = T * T;
+    static constexpr int RW = CT * T;
+    static constexpr int CW = RT * T;
+    // rowbuf [2][RW] float4, colbuf [2][CW] float4, pinv [N] float2, zsm [RT*T] float2,
+    // dinv [N] double2, ysm [N] double2, red [8 * G/32] double
+    static constexpr size_t bytes = (2 * RW + 2 * CW) * sizeof(float4) + (N + RT * T) * sizeof(float2) +
+                                    2 * N * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
+};
+
+template <int N, int T, int MPC, int MINB>
+__global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu32(const BseArgs a) {
+    using LS = Lu32Smem<N, T>;
+    constexpr int RT = LS::RT, CT = LS::CT, G = LS::G;
+    constexpr int TCN = N % T, CN = N / T;                // owner lane / tile column of the rhs
+    constexpr int MAX_REF = 6;
+    static_assert(T <= 32 && 32 % T == 0, "a row group must sit inside one warp");
+    static_assert((N * N * sizeof(double2)) % 16 == 0, "16-byte alignment of the group buffers");
+    extern __shared__ double2 sm[];
+    double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
+    const int tid = threadIdx.x;
+    const int g = tid / G, t = tid - g * G;
+    const int tr = t / T, tc = t - (t / T) * T;
+    const int lane = tid & 31;
+    const int bar = g + 1;
+    char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * LS::bytes;
+    float4* rowbuf = reinterpret_cast<float4*>(gs);       // [2][RW]
+    float4* colbuf = rowbuf + 2 * LS::RW;                 // [2][CW]
+    float2* pinv = reinterpret_cast<float2*>(colbuf + 2 * LS::CW);   // [N] 1/b_kk (FP32)
+    float2* zsm = pinv + N;                               // [RT*T] refinement right-hand side
+    double2* dinv = reinterpret_cast<double2*>(zsm + RT * T);        // [N] 1/chi0(q, i, w)
+    double2* ysm = dinv + N;                              // [N] solution (FP64)
+    double* red = reinterpret_cast<double*>(ysm + N);     // [8 * G/32]
+
+    const int w = blockIdx.y;
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    {
+        const double2* Gw = a.Gamma + (size_t)w * N * N;
+        for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+    }
+    __syncthreads();
+    const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
+
+    for (int q = q0 + g; q < q1; q += MPC) {
+        const double2* c0p = a.chi0 + (size_t)q + (size_t)a.nq * ((size_t)N * w);
+        for (int i = t; i < N; i += G) dinv[i] = cinv(c0p[(size_t)a.nq * i]);
+        named_barrier(bar, G);
+        // ---- FP32 tile of [B | 1]; padding rows / columns are zero and stay zero
+        f2p b[RT][CT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+#pragma unroll
+            for (int c = 0; c < CT; ++c) {
+                const int j = tc + T * c;
+                double2 v = dmk(0.0, 0.0);
+                if (i < N) {
+                    if (j < N) {
+                        v = Gsm[i * N + j];
+                        if (c == ra && tr == tc) v = cadd(v, dinv[i]);
+                    } else if (j == N) {
+                        v = dmk(1.0, 0.0);
+                    }
+                }
+                b[ra][c] = p2((float)v.x, (float)v.y);
+            }
+        }
+
+        // ---- forward elimination (LU with Gauss-Jordan inside the diagonal blocks), FP32
+#pragma unroll
+        for (int kc = 0; kc < RT; ++kc) {
+            const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+            for (int ktc = 0; ktc < kend; ++ktc) {
+                const int k = ktc + T * kc;
+                float4* rb = rowbuf + (k & 1) * LS::RW;
+                float4* cb = colbuf + (k & 1) * LS::CW;
+                if (tr == ktc) {
+                    const float2 pv = u2(b[kc][kc]);
+                    float2 p;
+                    p.x = __shfl_sync(gmask, pv.x, ktc, T);
+                    p.y = __shfl_sync(gmask, pv.y, ktc, T);
+                    const float2 inv = finv(p);
+                    if (tc == ktc) pinv[k] = inv;
+#pragma unroll
+                    for (int c = kc; c < CT; ++c) {
+                        const float2 u = fmul(u2(b[kc][c]), inv);
+                        rb[tc + T * c] = make_float4(-u.x, -u.y, u.y, -u.x);
+                    }
+                }
+                if (tc == ktc) {
+#pragma unroll
+                    for (int ra = kc; ra < RT; ++ra) {
+                        const float2 m = u2(b[ra][kc]);
+                        cb[tr + T * ra] = make_float4(m.x, m.x, m.y, m.y);
+                    }
+                }
+                named_barrier(bar, G);
+                f2p un[CT], us[CT];
+#pragma unroll
+                for (int c = kc; c < CT; ++c) {
+                    const float4 v = rb[tc + T * c];
+                    un[c] = p2(v.x, v.y);
+                    us[c] = p2(v.z, v.w);
+                }
+#pragma unroll
+                for (int ra = kc; ra < RT; ++ra) {
+                    if (ra > kc || tr != ktc) {
+                        const float4 mv = cb[tr + T * ra];
+                        const f2p mx = p2(mv.x, mv.y), my = p2(mv.z, mv.w);
+#pragma unroll
+                        for (int c = kc; c < CT; ++c) {
+                            if (c > kc || tc > ktc) b[ra][c] = fma2(my, us[c], fma2(mx, un[c], b[ra][c]));
+                        }
+                    }
+                }
+            }
+        }
+
+        // ---- block back substitution: z in the rhs column (lane TCN, tile column CN) -> ysm.
+        // sol: FP32 solution of the current block, written to dst (FP64 y, or the correction in zsm)
+        auto back_substitute = [&](bool first) {
+            f2p acc[RT];
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) acc[ra] = p2(0.f, 0.f);
+#pragma unroll
+            for (int r = RT - 1; r >= 0; --r) {
+                const int nb = (N - T * r) < T ? (N - T * r) : T;
+                float2 s = u2(acc[r]);
+#pragma unroll
+                for (int o = 1; o < T; o <<= 1) {
+                    s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+                    s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+                }
+                if (tc == TCN && tr < nb) {
+                    const int i = T * r + tr;
+                    const float2 z = first ? u2(b[r][CN]) : zsm[i];
+                    const float2 yi = fmul(make_float2(z.x - s.x, z.y - s.y), pinv[i]);
+                    zsm[i] = yi;
+                }
+                named_barrier(bar, G);
+                if (r > 0 && T * r + tc < N) {
+                    const float2 yj = zsm[T * r + tc];
+                    const f2p yx = p2(yj.x, yj.x), yy = p2(yj.y, yj.y);
+#pragma unroll
+                    for (int ra = 0; ra < r; ++ra) {
+                        // acc += b * yj:  (b.x yj.x - b.y yj.y, b.y yj.x + b.x yj.y)
+                        const float2 bv = u2(b[ra][r]);
+                        acc[ra] = fma2(yy, p2(-bv.y, bv.x), fma2(yx, b[ra][r], acc[ra]));
+                    }
+                }
+            }
+        };
+        back_substitute(true);
+        for (int i = t; i < N; i += G) {
+            const float2 v = zsm[i];
+            ysm[i] = dmk((double)v.x, (double)v.y);
+        }
+        named_barrier(bar, G);
+
+        // ---- FP64 backward error and refinement
+        double berr = 0.0, ysum = 0.0;
+        for (int it = 0; it <= MAX_REF; ++it) {
+            double st[4] = {0.0, 0.0, 0.0, 0.0};
+            const int op[4] = {1, 1, 1, 0};
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) {
+                const int i = tr + T * ra;
+                double2 accr = dmk(0.0, 0.0);
+                double rown = 0.0;
+                if (i < N) {
+#pragma unroll
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + T * c;
+                        if (j < N) {
+                            double2 gv = Gsm[i * N + j];
+                            if (c == ra && tr == tc) gv = cadd(gv, dinv[i]);
+                            accr = cadd(accr, cmul(gv, ysm[j]));
+                            rown += fabs(gv.x) + fabs(gv.y);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int o = 1; o < T; o <<= 1) {
+                    accr.x += __shfl_xor_sync(0xffffffffu, accr.x, o);
+                    accr.y += __shfl_xor_sync(0xffffffffu, accr.y, o);
+                    rown += __shfl_xor_sync(0xffffffffu, rown, o);
+                }
+                if (i < N && tc == 0) {
+                    const double2 yi = ysm[i];
+                    const double2 ri = dmk(1.0 - accr.x, -accr.y);
+                    zsm[i] = make_float2((float)ri.x, (float)ri.y);
+                    st[0] = fmax(st[0], fabs(ri.x) + fabs(ri.y));
+                    st[1] = fmax(st[1], fabs(yi.x) + fabs(yi.y));
+                    st[2] = fmax(st[2], rown);
+                    st[3] += yi.x;
+                }
+            }
+            group_reduce<4, G>(st, op, red, bar, t);   // its barriers also publish zsm
+            berr = st[0] / (st[2] * st[1] + 1.0);
+            ysum = st[3];
+            if (it == MAX_REF || !isfinite(berr) || berr <= 1e-14) break;
+            // forward replay of the FP32 elimination on z = r
+#pragma unroll
+            for (int kc = 0; kc < RT; ++kc) {
+                const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+                for (int ktc = 0; ktc < kend; ++ktc) {
+                    const int k = ktc + T * kc;
+                    if (tc == ktc) {
+                        const float2 zk = fmul(zsm[k], pinv[k]);
+#pragma unroll
+                        for (int ra = kc; ra < RT; ++ra) {
+                            const int i = tr + T * ra;
+                            if (i < N && i != k) {
+                                const float2 m = u2(b[ra][kc]);
+                                const float2 d = fmul(m, zk);
+                                float2 zi = zsm[i];
+                                zi.x -= d.x; zi.y -= d.y;
+                                zsm[i] = zi;
+                            }
+                        }
+                    }
+                    named_barrier(bar, G);
+                }
+            }
+            // back substitution on the corrected rhs (reads z_i, writes delta_i into zsm)
+            back_substitute(false);
+            for (int i = t; i < N; i += G) {
+                const float2 d = zsm[i];
+                ysm[i] = cadd(ysm[i], dmk((double)d.x, (double)d.y));
+            }
+            named_barrier(bar, G);
+        }
+
+        // ---- chi and gamma = y / (chi0 (1 + s U chi))
+        const double chi = ysum / (a.beta * a.beta);
+        const bool ok = isfinite(berr) && berr <= 1e-12;
+        if (t == 0) {
+            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+        }
+        const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+        for (int i = t; i < N; i += G) {
+            const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+            a.gam[ci] = cscale(cmul(ysm[i], dinv[i]), rf);
+        }
+        named_barrier(bar, G);   // shared buffers of this matrix are read before the next one writes
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// MIXED, one matrix per warp: the FP32 f32x2 elimination and the FP64 refinement of k_bse_lu32
+// without any named barrier.  The warp holds [B | 1] as a TR x TC lane grid (TR * TC = 32; lane
+// tr * TC + tc owns rows tr + TR a and columns tc + TC c), so every broadcast is a shared-memory
+// store, __syncwarp and a 16-byte load, and every reduction is a shuffle.
+//
+// Steps are grouped so that both the tile row of row k (k / TR) and the tile column of column k
+// (k / TC) are compile-time indices: the coarse tiling (P = max(TR, TC) rows or columns) is
+// unrolled, inside it the fine one (m = min(TR, TC)), and only the m steps of a fine block run as
+// a loop.  The diagonal blocks of the LU are the TR-row tiles (Gauss-Jordan inside them, as in
+// k_bse_lu), so the back substitution walks the tile rows from the bottom.
+// The multipliers are masked instead of branched: row k and the columns <= k of tile column
+// k / TC see a zero operand, which keeps the warp converged.
+template <int N, int TR, int TC>
+struct Warp32Smem {
+    static constexpr int RT = (N + TR - 1) / TR;
+    static constexpr int CT = (N + 1 + TC - 1) / TC;
+    // rowbuf [2][CT*TC] float4, colbuf [2][RT*TR] float4, pinv [RT*TR] float2, zsm [RT*TR] float2,
+    // dinv [N] double2, ysm [N] double2
+    static constexpr size_t bytes =
+        (2 * CT * TC + 2 * RT * TR) * sizeof(float4) + 2 * RT * TR * sizeof(float2) + 2 * N * sizeof(double2);
+};
+
+template <int N, int TR, int TC, int WPC, int MINB>
+__global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) {
+    using WS = Warp32Smem<N, TR, TC>;
+    constexpr int RT = WS::RT, CT = WS::CT;
+    constexpr int P = TR > TC ? TR : TC, MF = TR > TC ? TC : TR;   // coarse / fine tile size
+    constexpr int NO = (N + P - 1) / P, NH = P / MF;
+    constexpr int TCN = N % TC, CN = N / TC;              // owner lane / tile column of the rhs
+    constexpr int MAX_REF = 6;
+    static_assert(TR * TC == 32 && P % MF == 0, "a TR x TC lane grid filling one warp");
+    extern __shared__ double2 sm[];
+    double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int tr = lane / TC, tc = lane - (lane / TC) * TC;
+    char* gs = reinterpret_cast<char*>(Gsm + N * N) + wp * WS::bytes;
+    float4* rowbuf = reinterpret_cast<float4*>(gs);       // [2][CT*TC]
+    float4* colbuf = rowbuf + 2 * CT * TC;                // [2][RT*TR]
+    float2* pinv = reinterpret_cast<float2*>(colbuf + 2 * RT * TR);  // [RT*TR] 1/b_kk (FP32)
+    float2* zsm = pinv + RT * TR;                         // [RT*TR] solution / refinement rhs
+    double2* dinv = reinterpret_cast<double2*>(zsm + RT * TR);       // [N] 1/chi0(q, i, w)
+    double2* ysm = dinv + N;                              // [N] solution (FP64)
+
+    const int w = blockIdx.y;
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    {
+        const double2* Gw = a.Gamma + (size_t)w * N * N;
+        for (int e = threadIdx.x; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+    }
+    __syncthreads();
+    const unsigned rmask = (TC == 32 ? 0xffffffffu : ((1u << TC) - 1u)) << (lane & ~(TC - 1));
+    const f2p zero = p2(0.f, 0.f);
+
+    for (int q = q0 + wp; q < q1; q += WPC) {
+        const double2* c0p = a.chi0 + (size_t)q + (size_t)a.nq * ((size_t)N * w);
+        for (int i = lane; i < N; i += 32) dinv[i] = cinv(c0p[(size_t)a.nq * i]);
+        __syncwarp();
+        f2p b[RT][CT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + TR * ra;
+#pragma unroll
+            for (int c = 0; c < CT; ++c) {
+                const int j = tc + TC * c;
+                double2 v = dmk(0.0, 0.0);
+                if (i < N) {
+                    if (j < N) {
+                        v = Gsm[i * N + j];
+                        if (i == j) v = cadd(v, dinv[i]);
+                    } else if (j == N) {
+                        v = dmk(1.0, 0.0);
+                    }
+                }
+                b[ra][c] = p2((float)v.x, (float)v.y);
+            }
+        }
+
+        // ---- forward elimination, FP32 (LU with Gauss-Jordan inside the TR-row diagonal blocks)
+#pragma unroll
+        for (int o = 0; o < NO; ++o) {
+#pragma unroll
+            for (int h = 0; h < NH; ++h) {
+                const int k0 = P * o + MF * h;
+                if (k0 >= N) break;
+                const int rak = k0 / TR, ck = k0 / TC;
+                const int kend = (N - k0) < MF ? (N - k0) : MF;
+#pragma unroll 1
+                for (int jj = 0; jj < kend; ++jj) {
+                    const int k = k0 + jj;
+                    const int ktr = k % TR, ktc = k % TC;
+                    float4* rb = rowbuf + (k & 1) * (CT * TC);
+                    float4* cb = colbuf + (k & 1) * (RT * TR);
+                    if (tr == ktr) {
+                        const float2 pv = u2(b[rak][ck]);
+                        float2 p;
+                        p.x = __shfl_sync(rmask, pv.x, ktc, TC);
+                        p.y = __shfl_sync(rmask, pv.y, ktc, TC);
+                        const float2 inv = finv(p);
+                        if (tc == ktc) pinv[k] = inv;
+#pragma unroll
+                        for (int c = ck; c < CT; ++c) {
+                            const float2 u = fmul(u2(b[rak][c]), inv);
+                            rb[tc + TC * c] = make_float4(-u.x, -u.y, u.y, -u.x);
+                        }
+                    }
+                    if (tc == ktc) {
+#pragma unroll
+                        for (int ra = rak; ra < RT; ++ra) {
+                            const float2 m = u2(b[ra][ck]);
+                            cb[tr + TR * ra] = make_float4(m.x, m.x, m.y, m.y);
+                        }
+                    }
+                    __syncwarp();
+                    f2p mx[RT], my[RT];
+#pragma unroll
+                    for (int ra = rak; ra < RT; ++ra) {
+                        const float4 mv = cb[tr + TR * ra];
+                        const bool rowk = ra == rak && tr == ktr;
+                        mx[ra] = rowk ? zero : p2(mv.x, mv.y);
+                        my[ra] = rowk ? zero : p2(mv.z, mv.w);
+                    }
+#pragma unroll
+                    for (int c = ck; c < CT; ++c) {
+                        const float4 v = rb[tc + TC * c];
+                        const bool keep = c == ck && tc <= ktc;   // columns <= k hold multipliers
+                        const f2p un = keep ? zero : p2(v.x, v.y), us = keep ? zero : p2(v.z, v.w);
+#pragma unroll
+                        for (int ra = rak; ra < RT; ++ra) b[ra][c] = fma2(my[ra], us, fma2(mx[ra], un, b[ra][c]));
+                    }
+                }
+            }
+        }
+
+        // ---- block back substitution over the TR-row tiles; z from the rhs column (first) or zsm
+        auto back_substitute = [&](bool first) {
+            f2p acc[RT];
+#pragma unroll
+            for (int ra = 0; ra < RT; ++ra) acc[ra] = zero;
+#pragma unroll
+            for (int r = RT - 1; r >= 0; --r) {
+                const int nb = (N - TR * r) < TR ? (N - TR * r) : TR;
+                float2 s = u2(acc[r]);
+#pragma unroll
+                for (int o = 1; o < TC; o <<= 1) {
+                    s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+                    s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+                }
+                if (tc == TCN && tr < nb) {
+                    const int i = TR * r + tr;
+                    const float2 z = first ? u2(b[r][CN]) : zsm[i];
+                    zsm[i] = fmul(make_float2(z.x - s.x, z.y - s.y), pinv[i]);
+                }
+                __syncwarp();
+                if (r > 0) {
+                    // columns TR r .. TR r + nb - 1 live in tile columns (TR r) / TC .. (TR r + TR - 1) / TC
+#pragma unroll
+                    for (int c = (TR * r) / TC; c <= (TR * r + TR - 1) / TC; ++c) {
+                        const int j = tc + TC * c;
+                        if (j >= TR * r && j < TR * r + nb) {
+                            const float2 yj = zsm[j];
+                            const f2p yx = p2(yj.x, yj.x), yy = p2(yj.y, yj.y);
+#pragma unroll
+                            for (int ra = 0; ra < r; ++ra) {
+                                const float2 bv = u2(b[ra][c]);
+                                acc[ra] = fma2(yy, p2(-bv.y, bv.x), fma2(yx, b[ra][c], acc[ra]));
+                            }
+                        }
+                    }
+                }
+            }
+        };
+        back_substitute(true);
+        for (int i = lane; i < N; i += 32) {
+            const float2 v = zsm[i];
+            ysm[i] = dmk((double)v.x, (double)v.y);
+        }
+        __syncwarp();
+
+        // ---- FP64 backward error and refinement
+        double berr = 0.0, ysum = 0.0;
+        for (int it = 0; it <= MAX_REF; ++it) {
+            double e_r = 0.0, e_y = 0.0, e_b = 0.0, sy = 0.0;
+#pragma unroll 1
+            for (int ra = 0; ra < RT; ++ra) {
+                const int i = tr + TR * ra;
+                double2 accr = dmk(0.0, 0.0);
+                double rown = 0.0;
+                if (i < N) {
+#pragma unroll 1
+                    for (int c = 0; c < CT; ++c) {
+                        const int j = tc + TC * c;
+                        if (j < N) {
+                            double2 gv = Gsm[i * N + j];
+                            if (i == j) gv = cadd(gv, dinv[i]);
+                            accr = cadd(accr, cmul(gv, ysm[j]));
+                            rown += fabs(gv.x) + fabs(gv.y);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int o = 1; o < TC; o <<= 1) {
+                    accr.x += __shfl_xor_sync(0xffffffffu, accr.x, o);
+                    accr.y += __shfl_xor_sync(0xffffffffu, accr.y, o);
+                    rown += __shfl_xor_sync(0xffffffffu, rown, o);
+                }
+                if (i < N && tc == 0) {
+                    const double2 yi = ysm[i];
+                    const double2 ri = dmk(1.0 - accr.x, -accr.y);
+                    zsm[i] = make_float2((float)ri.x, (float)ri.y);
+                    e_r = fmax(e_r, fabs(ri.x) + fabs(ri.y));
+                    e_y = fmax(e_y, fabs(yi.x) + fabs(yi.y));
+                    e_b = fmax(e_b, rown);
+                    sy += yi.x;
+                }
+            }
+            // warp reduction in a fixed order (xor butterfly over the row groups' lane 0 values)
+#pragma unroll
+            for (int o = TC; o < 32; o <<= 1) {
+                e_r = fmax(e_r, __shfl_xor_sync(0xffffffffu, e_r, o));
+                e_y = fmax(e_y, __shfl_xor_sync(0xffffffffu, e_y, o));
+                e_b = fmax(e_b, __shfl_xor_sync(0xffffffffu, e_b, o));
+                sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            }
+            e_r = __shfl_sync(0xffffffffu, e_r, 0);
+            e_y = __shfl_sync(0xffffffffu, e_y, 0);
+            e_b = __shfl_sync(0xffffffffu, e_b, 0);
+            sy = __shfl_sync(0xffffffffu, sy, 0);
+            __syncwarp();
+            berr = e_r / (e_b * e_y + 1.0);
+            ysum = sy;
+            if (it == MAX_REF || !isfinite(berr) || berr <= 1e-14) break;
+            // forward replay of the FP32 elimination on z = r
+#pragma unroll
+            for (int o = 0; o < NO; ++o) {
+#pragma unroll
+                for (int h = 0; h < NH; ++h) {
+                    const int k0 = P * o + MF * h;
+                    if (k0 >= N) break;
+                    const int rak = k0 / TR, ck = k0 / TC;
+                    const int kend = (N - k0) < MF ? (N - k0) : MF;
+#pragma unroll 1
+                    for (int jj = 0; jj < kend; ++jj) {
+                        const int k = k0 + jj;
+                        if (tc == k % TC) {
+                            const float2 zk = fmul(zsm[k], pinv[k]);
+#pragma unroll
+                            for (int ra = rak; ra < RT; ++ra) {
+                                const int i = tr + TR * ra;
+                                if (i < N && i != k) {
+                                    const float2 d = fmul(u2(b[ra][ck]), zk);
+                                    float2 zi = zsm[i];
+                                    zi.x -= d.x; zi.y -= d.y;
+                                    zsm[i] = zi;
+                                }
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+            back_substitute(false);
+            for (int i = lane; i < N; i += 32) {
+                const float2 d = zsm[i];
+                ysm[i] = cadd(ysm[i], dmk((double)d.x, (double)d.y));
+            }
+            __syncwarp();
+        }
+
+        // ---- chi and gamma = y / (chi0 (1 + s U chi))
+        const double chi = ysum / (a.beta * a.beta);
+        const bool ok = isfinite(berr) && berr <= 1e-12;
+        if (lane == 0) {
+            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+        }
+        const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+        for (int i = lane; i < N; i += 32) {
+            const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+            a.gam[ci] = cscale(cmul(ysm[i], dinv[i]), rf);
+        }
+        __syncwarp();   // shared buffers of this matrix are read before the next one writes
+    }
+}
+
 __device__ __forceinline__ double block_sum_det(double v, double* red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -769,14 +1347,50 @@ int run_lu(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
+template <int N, int T, int MPC, int MINB>
+int run_lu32(ldga_ctx* ctx, const BseArgs& a0) {
+    BseArgs a = a0;
+    const int threads = T * T * MPC;
+    const size_t sm = (size_t)N * N * sizeof(double2) + MPC * Lu32Smem<N, T>::bytes;
+    auto kern = k_bse_lu32<N, T, MPC, MINB>;
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+    int chunk = 4 * MPC;
+    while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
+    a.qchunk = chunk;
+    dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
+    StageTimer st_(ctx, LDGA_STAGE_BSE);
+    kern<<<grid, threads, sm, ctx->stream>>>(a);
+    LDGA_LAUNCHED(ctx, "k_bse_lu32");
+    return LDGA_OK;
+}
+
+template <int N, int TR, int TC, int WPC, int MINB>
+int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
+    BseArgs a = a0;
+    const int threads = 32 * WPC;
+    const size_t sm = (size_t)N * N * sizeof(double2) + WPC * Warp32Smem<N, TR, TC>::bytes;
+    auto kern = k_bse_warp32<N, TR, TC, WPC, MINB>;
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+    int chunk = 4 * WPC;
+    while (chunk > WPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= WPC;
+    a.qchunk = chunk;
+    dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
+    StageTimer st_(ctx, LDGA_STAGE_BSE);
+    kern<<<grid, threads, sm, ctx->stream>>>(a);
+    LDGA_LAUNCHED(ctx, "k_bse_warp32");
+    return LDGA_OK;
+}
+
 // TR x TC thread grid per matrix (TC lanes of a row group inside one warp); MPC matrices per CTA
 // MINB of the FP64 elimination (the register-heaviest variant that still spills little when capped)
-template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1>
+template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1, int MINB32 = 1>
 int run_mode(ldga_ctx* ctx, const BseArgs& a) {
     switch (ctx->prec) {
         case LDGA_PREC_FP64_INV: return run_tile<N, TR, TC, MPC64, 1, double, LDGA_PREC_FP64_INV>(ctx, a);
         case LDGA_PREC_FP64: return run_lu<N, TC, 1, MINB64 * MPC64>(ctx, a);   // one matrix per CTA
-        default: return run_tile<N, TR, TC, MPC32, 1, float, LDGA_PREC_MIXED>(ctx, a);
+        default:
+            if constexpr (N <= 40) return run_warp32<N, 8, 4, 4, MINB32>(ctx, a);   // one matrix per warp
+            else return run_lu32<N, TC, MPC32, MINB32>(ctx, a);
     }
 }
 
@@ -811,7 +1425,7 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
         case 16: st = run_mode<16, 8, 8, 2, 4>(ctx, a); break;
         case 20: st = run_mode<20, 8, 8, 2, 4>(ctx, a); break;
         case 30: st = run_mode<30, 8, 8, 2, 2>(ctx, a); break;
-        case 40: st = run_mode<40, 8, 8, 2, 2, 3>(ctx, a); break;
+        case 40: st = run_mode<40, 8, 8, 2, 2, 3, 1>(ctx, a); break;
         case 60: st = run_mode<60, 16, 16, 1, 1>(ctx, a); break;
         default: generic = true; break;
     }

@@ -229,3 +229,30 @@ def test_rerun_bitwise(case):
     Sa = L.calc_Σ(a["chi_m"], a["gamma_m"], a["chi_d"], a["gamma_d"], a["lambda0"], a["h"], λm=0.3)
     Sb = L.calc_Σ(b["chi_m"], b["gamma_m"], b["chi_d"], b["gamma_d"], b["lambda0"], b["h"], λm=0.3)
     assert np.array_equal(Sa, Sb)
+
+
+def test_parallel_api_matches_single_call_api(case):
+    """calc_bubble_par / calc_χγ_par / initialize_EoM / calc_Σ_par (ladderDGATools.jl:46-245) give
+    the single-call results and the oracle's, with the handle as the worker pool."""
+    name, inp, ref = case
+    h = L.setup_synthetic(inp)
+    assert L.calc_bubble_par(h, collect_data=False) is None
+    chi0 = L.collect_χ0(h)
+    assert rel(chi0.data, ref["chi0"]) < RTOL
+    assert L.calc_χγ_par("m", h, collect_data=False) is None
+    xd, gd = L.calc_χγ_par("d", h.Γ_d, h.kG, h.mP, h.sP)
+    xm, gm = L.collect_χ("m", h), L.collect_γ("m", h)
+    assert rel(xm.data, ref["chi_m"].data) < RTOL and rel(gd.data, ref["gamma_d"]) < RTOL
+    l0 = L.calc_λ0(chi0, h)
+    numax = h.sP.n_iν
+    L.initialize_EoM(h, l0, range(0, numax))
+    s_par = L.calc_Σ_par(λm=0.1, λd=0.0)
+    s_one = L.calc_Σ(xm, gm, xd, gd, l0, h, νmax=numax, λm=0.1)
+    assert np.array_equal(s_par, s_one)
+    S_ = np.zeros_like(s_one)
+    L.calc_Σ_par_(S_, λm=0.1)
+    assert np.array_equal(S_, s_one)
+    r = ref["h"]
+    s_ref = R.calc_Sigma(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], r.chiloc_m_sum, ref["lambda0"],
+                         r.grhat, r.kG, r.mP, r.sP, numax=numax, lam_m=0.1)
+    assert rel(s_par, s_ref) < RTOL
