@@ -917,18 +917,29 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu32(const BseArgs a)
 }
 
 // ------------------------------------------------------------------------------------------------
-// MIXED, one matrix per warp: the FP32 f32x2 elimination and the FP64 refinement of k_bse_lu32
-// without any named barrier.  The warp holds [B | 1] as a TR x TC lane grid (TR * TC = 32; lane
-// tr * TC + tc owns rows tr + TR a and columns tc + TC c), so every broadcast is a shared-memory
-// store, __syncwarp and a 16-byte load, and every reduction is a shuffle.
+// MIXED, one matrix per warp: the FP32 f32x2 elimination of k_bse_lu32 and an FP64-refined solve
+// without any barrier.  The warp holds [B | 1] as a TR x TC lane grid (TR * TC = 32, TR >= TC;
+// lane tr * TC + tc owns rows tr + TR a and columns tc + TC c).
 //
-// Steps are grouped so that both the tile row of row k (k / TR) and the tile column of column k
-// (k / TC) are compile-time indices: the coarse tiling (P = max(TR, TC) rows or columns) is
-// unrolled, inside it the fine one (m = min(TR, TC)), and only the m steps of a fine block run as
-// a loop.  The diagonal blocks of the LU are the TR-row tiles (Gauss-Jordan inside them, as in
-// k_bse_lu), so the back substitution walks the tile rows from the bottom.
-// The multipliers are masked instead of branched: row k and the columns <= k of tile column
-// k / TC see a zero operand, which keeps the warp converged.
+// Elimination step k (row tile k / TR and column tile k / TC are compile-time indices: the row
+// tiles are unrolled, inside them the TR / TC column tiles, and only the TC steps of one column
+// tile run as a loop):
+//   1. the row group of row k shuffles the pivot, forms 1/b_kk and stores row k scaled by it as
+//      (-u.x, -u.y, u.y, -u.x); the lanes owning column k store it as (m.x, m.x, m.y, m.y).  The
+//      publishers store zeros where nothing may change (row k itself, the columns <= k of the
+//      pivot's tile column), so the consumers need no predicate;
+//   2. __syncwarp; every lane loads its multipliers and row values (16-byte shared loads) and
+//      updates b -= m u with two f32x2 FMAs per complex element:
+//          b = fma2((m.y, m.y), (u.y, -u.x), fma2((m.x, m.x), (-u.x, -u.y), b)).
+// Gauss-Jordan inside the TR-row diagonal blocks (as in k_bse_lu) leaves those blocks diagonal,
+// so the back substitution walks the row tiles from the bottom with one shuffle reduction each.
+//
+// Refinement (FP64 residual, FP32 correction from the stored factors, y += delta) until the FP64
+// backward error |1 - B y|_inf / (|B|_inf |y|_inf + 1) is below 1e-14; the flag threshold for the
+// pivoted FP64 fallback is 1e-12 as in every mode.  The correction's forward replay is blocked:
+// per row tile, TR fully unrolled shuffle steps inside the diagonal block, then one matrix-vector
+// update of all rows below (partial sums over the TC lanes of a row group, xor-shuffle reduced).
+// z is replicated across the TC lanes of each row group, so no shared memory is involved.
 template <int N, int TR, int TC>
 struct Warp32Smem {
     static constexpr int RT = (N + TR - 1) / TR;
@@ -943,11 +954,10 @@ template <int N, int TR, int TC, int WPC, int MINB>
 __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) {
     using WS = Warp32Smem<N, TR, TC>;
     constexpr int RT = WS::RT, CT = WS::CT;
-    constexpr int P = TR > TC ? TR : TC, MF = TR > TC ? TC : TR;   // coarse / fine tile size
-    constexpr int NO = (N + P - 1) / P, NH = P / MF;
+    constexpr int NH = TR / TC;                           // tile columns per tile row
     constexpr int TCN = N % TC, CN = N / TC;              // owner lane / tile column of the rhs
     constexpr int MAX_REF = 6;
-    static_assert(TR * TC == 32 && P % MF == 0, "a TR x TC lane grid filling one warp");
+    static_assert(TR * TC == 32 && TR >= TC && TR % TC == 0, "a TR x TC lane grid filling one warp");
     extern __shared__ double2 sm[];
     double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -956,7 +966,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
     float4* rowbuf = reinterpret_cast<float4*>(gs);       // [2][CT*TC]
     float4* colbuf = rowbuf + 2 * CT * TC;                // [2][RT*TR]
     float2* pinv = reinterpret_cast<float2*>(colbuf + 2 * RT * TR);  // [RT*TR] 1/b_kk (FP32)
-    float2* zsm = pinv + RT * TR;                         // [RT*TR] solution / refinement rhs
+    float2* zsm = pinv + RT * TR;                         // [RT*TR] solution of one solve
     double2* dinv = reinterpret_cast<double2*>(zsm + RT * TR);       // [N] 1/chi0(q, i, w)
     double2* ysm = dinv + N;                              // [N] solution (FP64)
 
@@ -995,63 +1005,79 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
             }
         }
 
-        // ---- forward elimination, FP32 (LU with Gauss-Jordan inside the TR-row diagonal blocks)
+        // ---- forward elimination, FP32
 #pragma unroll
-        for (int o = 0; o < NO; ++o) {
+        for (int rak = 0; rak < RT; ++rak) {
 #pragma unroll
             for (int h = 0; h < NH; ++h) {
-                const int k0 = P * o + MF * h;
+                const int k0 = TR * rak + TC * h;
                 if (k0 >= N) break;
-                const int rak = k0 / TR, ck = k0 / TC;
-                const int kend = (N - k0) < MF ? (N - k0) : MF;
+                const int ck = rak * NH + h;
+                const int kend = (N - k0) < TC ? (N - k0) : TC;
 #pragma unroll 1
-                for (int jj = 0; jj < kend; ++jj) {
-                    const int k = k0 + jj;
-                    const int ktr = k % TR, ktc = k % TC;
+                for (int ktc = 0; ktc < kend; ++ktc) {
+                    const int k = k0 + ktc;
+                    const int ktr = TC * h + ktc;
                     float4* rb = rowbuf + (k & 1) * (CT * TC);
                     float4* cb = colbuf + (k & 1) * (RT * TR);
-                    if (tr == ktr) {
+                    // pivot to every lane; the lanes of column k scale it (RT values per lane, fewer
+                    // than the CT of a row), the row group of row k stores row k unscaled
+                    float2 p;
+                    {
                         const float2 pv = u2(b[rak][ck]);
-                        float2 p;
-                        p.x = __shfl_sync(rmask, pv.x, ktc, TC);
-                        p.y = __shfl_sync(rmask, pv.y, ktc, TC);
-                        const float2 inv = finv(p);
+                        p.x = __shfl_sync(0xffffffffu, pv.x, ktr * TC + ktc);
+                        p.y = __shfl_sync(0xffffffffu, pv.y, ktr * TC + ktc);
+                    }
+                    const float2 inv = finv(p);
+                    if (tr == ktr) {
                         if (tc == ktc) pinv[k] = inv;
+                        {
+                            const float2 u = u2(b[rak][ck]);
+                            rb[tc + TC * ck] = tc <= ktc ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(u.x, u.y, u.y, u.x);
+                        }
 #pragma unroll
-                        for (int c = ck; c < CT; ++c) {
-                            const float2 u = fmul(u2(b[rak][c]), inv);
-                            rb[tc + TC * c] = make_float4(-u.x, -u.y, u.y, -u.x);
+                        for (int c = ck + 1; c < CT; ++c) {
+                            const float2 u = u2(b[rak][c]);
+                            rb[tc + TC * c] = make_float4(u.x, u.y, u.y, u.x);
                         }
                     }
                     if (tc == ktc) {
+                        {
+                            const float2 m = fmul(u2(b[rak][ck]), inv);
+                            cb[tr + TR * rak] = tr == ktr ? make_float4(0.f, 0.f, 0.f, 0.f)
+                                                          : make_float4(-m.x, -m.x, m.y, -m.y);
+                        }
 #pragma unroll
-                        for (int ra = rak; ra < RT; ++ra) {
-                            const float2 m = u2(b[ra][ck]);
-                            cb[tr + TR * ra] = make_float4(m.x, m.x, m.y, m.y);
+                        for (int ra = rak + 1; ra < RT; ++ra) {
+                            const float2 m = fmul(u2(b[ra][ck]), inv);
+                            cb[tr + TR * ra] = make_float4(-m.x, -m.x, m.y, -m.y);
                         }
                     }
                     __syncwarp();
+                    // b -= m u:  b += (-m.x, -m.x) (u.x, u.y);  b += (m.y, -m.y) (u.y, u.x)
                     f2p mx[RT], my[RT];
 #pragma unroll
                     for (int ra = rak; ra < RT; ++ra) {
                         const float4 mv = cb[tr + TR * ra];
-                        const bool rowk = ra == rak && tr == ktr;
-                        mx[ra] = rowk ? zero : p2(mv.x, mv.y);
-                        my[ra] = rowk ? zero : p2(mv.z, mv.w);
+                        mx[ra] = p2(mv.x, mv.y);
+                        my[ra] = p2(mv.z, mv.w);
                     }
 #pragma unroll
                     for (int c = ck; c < CT; ++c) {
                         const float4 v = rb[tc + TC * c];
-                        const bool keep = c == ck && tc <= ktc;   // columns <= k hold multipliers
-                        const f2p un = keep ? zero : p2(v.x, v.y), us = keep ? zero : p2(v.z, v.w);
+                        const f2p u1 = p2(v.x, v.y), u2v = p2(v.z, v.w);
 #pragma unroll
-                        for (int ra = rak; ra < RT; ++ra) b[ra][c] = fma2(my[ra], us, fma2(mx[ra], un, b[ra][c]));
+                        for (int ra = rak; ra < RT; ++ra) b[ra][c] = fma2(mx[ra], u1, b[ra][c]);
+#pragma unroll
+                        for (int ra = rak; ra < RT; ++ra) b[ra][c] = fma2(my[ra], u2v, b[ra][c]);
                     }
                 }
             }
         }
 
-        // ---- block back substitution over the TR-row tiles; z from the rhs column (first) or zsm
+        // ---- block back substitution over the TR-row tiles: rhs z from the rhs column of the tile
+        // (first solve) or from zr (replicated on the row group), FP32 solution into zsm
+        float2 zr[RT];
         auto back_substitute = [&](bool first) {
             f2p acc[RT];
 #pragma unroll
@@ -1067,16 +1093,15 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
                 }
                 if (tc == TCN && tr < nb) {
                     const int i = TR * r + tr;
-                    const float2 z = first ? u2(b[r][CN]) : zsm[i];
+                    const float2 z = first ? u2(b[r][CN]) : zr[r];
                     zsm[i] = fmul(make_float2(z.x - s.x, z.y - s.y), pinv[i]);
                 }
                 __syncwarp();
                 if (r > 0) {
-                    // columns TR r .. TR r + nb - 1 live in tile columns (TR r) / TC .. (TR r + TR - 1) / TC
 #pragma unroll
-                    for (int c = (TR * r) / TC; c <= (TR * r + TR - 1) / TC; ++c) {
+                    for (int c = r * NH; c < r * NH + NH; ++c) {
                         const int j = tc + TC * c;
-                        if (j >= TR * r && j < TR * r + nb) {
+                        if (j < TR * r + nb) {
                             const float2 yj = zsm[j];
                             const f2p yx = p2(yj.x, yj.x), yy = p2(yj.y, yj.y);
 #pragma unroll
@@ -1097,10 +1122,10 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
         __syncwarp();
 
         // ---- FP64 backward error and refinement
-        double berr = 0.0, ysum = 0.0;
+        double berr = 0.0, ysum = 0.0, bnorm = 0.0;
         for (int it = 0; it <= MAX_REF; ++it) {
-            double e_r = 0.0, e_y = 0.0, e_b = 0.0, sy = 0.0;
-#pragma unroll 1
+            double e_r = 0.0, e_y = 0.0, sy = 0.0;
+#pragma unroll
             for (int ra = 0; ra < RT; ++ra) {
                 const int i = tr + TR * ra;
                 double2 accr = dmk(0.0, 0.0);
@@ -1112,8 +1137,10 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
                         if (j < N) {
                             double2 gv = Gsm[i * N + j];
                             if (i == j) gv = cadd(gv, dinv[i]);
-                            accr = cadd(accr, cmul(gv, ysm[j]));
-                            rown += fabs(gv.x) + fabs(gv.y);
+                            const double2 yj = ysm[j];
+                            accr.x = fma(gv.x, yj.x, fma(-gv.y, yj.y, accr.x));
+                            accr.y = fma(gv.x, yj.y, fma(gv.y, yj.x, accr.y));
+                            if (it == 0) rown += fabs(gv.x) + fabs(gv.y);
                         }
                     }
                 }
@@ -1121,61 +1148,74 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
                 for (int o = 1; o < TC; o <<= 1) {
                     accr.x += __shfl_xor_sync(0xffffffffu, accr.x, o);
                     accr.y += __shfl_xor_sync(0xffffffffu, accr.y, o);
-                    rown += __shfl_xor_sync(0xffffffffu, rown, o);
+                    if (it == 0) rown += __shfl_xor_sync(0xffffffffu, rown, o);
                 }
-                if (i < N && tc == 0) {
+                const double2 ri = i < N ? dmk(1.0 - accr.x, -accr.y) : dmk(0.0, 0.0);
+                zr[ra] = make_float2((float)ri.x, (float)ri.y);
+                if (i < N) {
                     const double2 yi = ysm[i];
-                    const double2 ri = dmk(1.0 - accr.x, -accr.y);
-                    zsm[i] = make_float2((float)ri.x, (float)ri.y);
                     e_r = fmax(e_r, fabs(ri.x) + fabs(ri.y));
                     e_y = fmax(e_y, fabs(yi.x) + fabs(yi.y));
-                    e_b = fmax(e_b, rown);
+                    if (it == 0) bnorm = fmax(bnorm, rown);
                     sy += yi.x;
                 }
             }
-            // warp reduction in a fixed order (xor butterfly over the row groups' lane 0 values)
+            // every lane of a row group holds its rows' values: reduce across row groups only
+            // (xor over the lane bits above tc), a fixed order
 #pragma unroll
             for (int o = TC; o < 32; o <<= 1) {
                 e_r = fmax(e_r, __shfl_xor_sync(0xffffffffu, e_r, o));
                 e_y = fmax(e_y, __shfl_xor_sync(0xffffffffu, e_y, o));
-                e_b = fmax(e_b, __shfl_xor_sync(0xffffffffu, e_b, o));
+                if (it == 0) bnorm = fmax(bnorm, __shfl_xor_sync(0xffffffffu, bnorm, o));
                 sy += __shfl_xor_sync(0xffffffffu, sy, o);
             }
-            e_r = __shfl_sync(0xffffffffu, e_r, 0);
-            e_y = __shfl_sync(0xffffffffu, e_y, 0);
-            e_b = __shfl_sync(0xffffffffu, e_b, 0);
-            sy = __shfl_sync(0xffffffffu, sy, 0);
-            __syncwarp();
-            berr = e_r / (e_b * e_y + 1.0);
+            berr = e_r / (bnorm * e_y + 1.0);
             ysum = sy;
             if (it == MAX_REF || !isfinite(berr) || berr <= 1e-14) break;
-            // forward replay of the FP32 elimination on z = r
+
+            // forward replay of the FP32 elimination on z = r, one row tile (diagonal block) at a time
 #pragma unroll
-            for (int o = 0; o < NO; ++o) {
+            for (int o = 0; o < RT; ++o) {
+                f2p mine[NH];                     // w of the columns this lane owns in the block
 #pragma unroll
-                for (int h = 0; h < NH; ++h) {
-                    const int k0 = P * o + MF * h;
-                    if (k0 >= N) break;
-                    const int rak = k0 / TR, ck = k0 / TC;
-                    const int kend = (N - k0) < MF ? (N - k0) : MF;
-#pragma unroll 1
-                    for (int jj = 0; jj < kend; ++jj) {
-                        const int k = k0 + jj;
-                        if (tc == k % TC) {
-                            const float2 zk = fmul(zsm[k], pinv[k]);
+                for (int h = 0; h < NH; ++h) mine[h] = zero;
 #pragma unroll
-                            for (int ra = rak; ra < RT; ++ra) {
-                                const int i = tr + TR * ra;
-                                if (i < N && i != k) {
-                                    const float2 d = fmul(u2(b[ra][ck]), zk);
-                                    float2 zi = zsm[i];
-                                    zi.x -= d.x; zi.y -= d.y;
-                                    zsm[i] = zi;
-                                }
-                            }
-                        }
-                        __syncwarp();
+                for (int s = 0; s < TR; ++s) {
+                    const int k = TR * o + s;
+                    if (k < N) {
+                        const int h = s / TC, ktc = s % TC, ck = o * NH + h;
+                        // w_k = z_k / b_kk (z_k lives on row group s)
+                        float2 zk;
+                        zk.x = __shfl_sync(0xffffffffu, zr[o].x, s * TC);
+                        zk.y = __shfl_sync(0xffffffffu, zr[o].y, s * TC);
+                        const float2 wk = fmul(zk, pinv[k]);
+                        if (tc == ktc) mine[h] = p2(wk.x, wk.y);
+                        // rows of the block except k: z_i -= b_ik w_k (b_ik on lane ktc of the row group)
+                        float2 d = fmul(u2(b[o][ck]), wk);
+                        d.x = __shfl_sync(0xffffffffu, d.x, tr * TC + ktc);
+                        d.y = __shfl_sync(0xffffffffu, d.y, tr * TC + ktc);
+                        if (tr != s) { zr[o].x -= d.x; zr[o].y -= d.y; }
                     }
+                }
+                // rows below the block: z_i -= sum_k b_ik w_k over the block's columns
+#pragma unroll
+                for (int ra = o + 1; ra < RT; ++ra) {
+                    f2p part = zero;
+#pragma unroll
+                    for (int h = 0; h < NH; ++h) {
+                        const float2 wv = u2(mine[h]);
+                        const f2p wx = p2(wv.x, wv.x), wy = p2(wv.y, wv.y);
+                        const float2 bv = u2(b[ra][o * NH + h]);
+                        part = fma2(wy, p2(-bv.y, bv.x), fma2(wx, b[ra][o * NH + h], part));
+                    }
+                    float2 ps = u2(part);
+#pragma unroll
+                    for (int x = 1; x < TC; x <<= 1) {
+                        ps.x += __shfl_xor_sync(0xffffffffu, ps.x, x);
+                        ps.y += __shfl_xor_sync(0xffffffffu, ps.y, x);
+                    }
+                    zr[ra].x -= ps.x;
+                    zr[ra].y -= ps.y;
                 }
             }
             back_substitute(false);
@@ -1425,7 +1465,7 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
         case 16: st = run_mode<16, 8, 8, 2, 4>(ctx, a); break;
         case 20: st = run_mode<20, 8, 8, 2, 4>(ctx, a); break;
         case 30: st = run_mode<30, 8, 8, 2, 2>(ctx, a); break;
-        case 40: st = run_mode<40, 8, 8, 2, 2, 3, 1>(ctx, a); break;
+        case 40: st = run_mode<40, 8, 8, 2, 2, 3, 3>(ctx, a); break;
         case 60: st = run_mode<60, 16, 16, 1, 1>(ctx, a); break;
         default: generic = true; break;
     }
