@@ -257,6 +257,33 @@ int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const 
                  double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
                  double* chi_m_out, double* chi_d_out, double* scalars_out);
 
+/* Arguments of ldga_chain_m for one parameter point of a batch. */
+typedef struct ldga_chain_io {
+    const double* sigma_loc;
+    int32_t n_sigma;
+    const double* gamma_m;
+    const double* gamma_d;
+    const double* chi_loc_m;
+    const double* gimp;
+    int32_t n_gimp;
+    double imp_density;
+    double chiloc_m_sum;
+    double* sigma_out;     /* may be NULL */
+    double* chi_m_out;     /* may be NULL */
+    double* chi_d_out;     /* may be NULL */
+    double* scalars_out;   /* [8] as ldga_chain_m, may be NULL */
+} ldga_chain_io;
+
+/* The lambda_m chain for n parameter points, one handle each (any mix of k-grids, frequency boxes
+ * and devices): an uneven (U, β) scan in one call.  The reference runs such scans as separate
+ * jobs (one run_minimal.jl per point); its per-point path is what ldga_chain_m replaces.  Every
+ * point's chain (its captured graph after the first call) is enqueued on its handle's stream
+ * before the first host wait, so points of different Nν overlap on the GPU.
+ * status[i] (may be NULL) receives each point's status; the return value is the first non-zero
+ * one (ldga_last_error of that handle has the message). */
+int ldga_batch_chain_m(int32_t n, ldga_ctx* const* ctxs, const ldga_chain_io* io, int32_t use_graph,
+                       int32_t* status);
+
 /* ---------------------------------------------------------------- a14: lambda_dm ------------- */
 
 /* λdm_correction plain branch (conditions_new.jl:219-324): 2-D newton_right with a forward-

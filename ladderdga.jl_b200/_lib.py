@@ -26,7 +26,7 @@ EXPORTS = [
     "ldga_set_lambda0", "ldga_sum_kw", "ldga_sum_wk", "ldga_lambda_min", "ldga_eom", "ldga_eom_parts",
     "ldga_lambda_m", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
     "ldga_lambda_dm_evals", "ldga_set_stream", "ldga_profile", "ldga_stage_times", "ldga_launch_count",
-    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc",
+    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m",
 ]
 GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
 STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
@@ -50,6 +50,14 @@ class Lattice(C.Structure):
 class Model(C.Structure):
     _fields_ = [("U", C.c_double), ("mu", C.c_double), ("beta", C.c_double), ("n", C.c_double),
                 ("sVk", C.c_double), ("Epot_DMFT", C.c_double), ("Ekin_DMFT", C.c_double)]
+
+
+class ChainIO(C.Structure):
+    """``ldga_chain_io``: the arguments of ldga_chain_m for one point of ldga_batch_chain_m."""
+    _fields_ = [("sigma_loc", C.c_void_p), ("n_sigma", C.c_int32), ("gamma_m", C.c_void_p), ("gamma_d", C.c_void_p),
+                ("chi_loc_m", C.c_void_p), ("gimp", C.c_void_p), ("n_gimp", C.c_int32), ("imp_density", C.c_double),
+                ("chiloc_m_sum", C.c_double), ("sigma_out", C.c_void_p), ("chi_m_out", C.c_void_p),
+                ("chi_d_out", C.c_void_p), ("scalars_out", C.c_void_p)]
 
 
 class Sim(C.Structure):
@@ -107,6 +115,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_get": (C.c_int, [P, I32, I32, P]),
         "ldga_lambda0_noalloc": (C.c_int, [P, P, I32, I32, I32, D, P, P]),
         "ldga_chain_m": (C.c_int, [P, P, I32, P, P, P, P, I32, D, D, I32, P, P, P, P]),
+        "ldga_batch_chain_m": (C.c_int, [I32, P, P, I32, PI32]),
         "ldga_set_sigma": (C.c_int, [P, P, I32]),
         "ldga_calc_E": (C.c_int, [P, P, P, I32, D, PD, PD]),
     }

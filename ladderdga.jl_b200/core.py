@@ -1164,6 +1164,83 @@ def λ_correction(type_, χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHe
 
 
 # =============================================================================================
+# uneven parameter scans: the λm chain of many points in one call
+# =============================================================================================
+@dataclass
+class ChainResult:
+    """One point of ``λm_chain_batch``: the λm chain's outputs (Σ_ladder on ν_n = 0..Nν/2-1)."""
+    λm: float
+    μ: float
+    EKin: float
+    EPot_p1: float
+    EPot_p2: float
+    PP_p2: float
+    newton_iterations: int
+    n: float
+    Σ_ladder: np.ndarray
+    χ_m: np.ndarray
+    χ_d: np.ndarray
+
+
+def _pinned(shape, dtype) -> np.ndarray:
+    """A numpy view of page-locked host memory: copies from and to it stay asynchronous, so the
+    points of a batch overlap (pageable memory would make every copy wait for its stream)."""
+    import torch
+    t = torch.empty(int(np.prod(shape)) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
+    return t.numpy().view(dtype).reshape(shape, order="F"), t
+
+
+def _chain_host_inputs(h: lDΓAHelper, keep: list) -> dict:
+    out = {}
+    for k, a in (("sigma_loc", h.Σ_loc), ("gamma_m", h.Γ_m), ("gamma_d", h.Γ_d), ("chi_loc_m", h.χDMFT_m),
+                 ("gimp", h.gImp)):
+        src = np.asarray(a, dtype=np.complex128).reshape(-1, order="F")
+        buf, t = _pinned(src.shape, np.complex128)
+        buf[...] = src
+        keep.append(t)
+        out[k] = buf
+    return out
+
+
+def λm_chain_batch(hs, use_graph: bool = False) -> list:
+    """bubble → BSE (m, d) → λ₀ → λm correction → EoM → μ, energies (``run_minimal.jl:7-14`` with
+    λ_correction(:m)) for every helper of ``hs`` in one ``ldga_batch_chain_m`` call: all points'
+    chains are in flight on the GPU together.  Each helper keeps its own handle (k-grid, box, U, β)."""
+    hs = list(hs)
+    n = len(hs)
+    ios = (_lib.ChainIO * max(n, 1))()
+    keep, outs = [], []
+    for i, h in enumerate(hs):
+        ctx = h.ctx
+        x = _chain_host_inputs(h, keep)
+        numax = ctx.Nnu // 2
+        S, t1 = _pinned((ctx.Nq, numax), np.complex128)
+        xm, t2 = _pinned((ctx.Nq, ctx.Nw), np.float64)
+        xd, t3 = _pinned((ctx.Nq, ctx.Nw), np.float64)
+        sc, t4 = _pinned((8,), np.float64)
+        keep.extend([x, t1, t2, t3, t4])
+        outs.append((S, xm, xd, sc))
+        ios[i] = _lib.ChainIO(x["sigma_loc"].ctypes.data, len(h.Σ_loc), x["gamma_m"].ctypes.data,
+                              x["gamma_d"].ctypes.data, x["chi_loc_m"].ctypes.data, x["gimp"].ctypes.data,
+                              len(h.gImp), h.imp_density, h.χloc_m_sum, S.ctypes.data, xm.ctypes.data,
+                              xd.ctypes.data, sc.ctypes.data)
+    handles = (_lib.C.c_void_p * max(n, 1))(*[h.ctx.h.value for h in hs])
+    status = (_lib.C.c_int32 * max(n, 1))()
+    lib = _lib.load()
+    st = lib.ldga_batch_chain_m(n, handles, ios, int(bool(use_graph)), status)
+    if st != _lib.LDGA_OK:
+        bad = [i for i in range(n) if status[i] != _lib.LDGA_OK]
+        msgs = "; ".join(f"point {i}: {lib.ldga_last_error(hs[i].ctx.h).decode()}" for i in bad)
+        raise _lib.LdgaError(st, msgs)
+    res = []
+    for S, xm, xd, sc in outs:
+        res.append(ChainResult(float(sc[0]), float(sc[1]), float(sc[2]), float(sc[3]), float(sc[4]), float(sc[5]),
+                               int(sc[6]), float(sc[7]), np.array(S, order="F"), np.array(xm, order="F"),
+                               np.array(xd, order="F")))
+    return res
+
+
+# =============================================================================================
 # parallel API (ladderDGATools.jl:46-245, parallelization_helpers.jl:197-240, 358-420)
 # =============================================================================================
 # The reference keeps ω blocks of χ₀, χ, γ and the EoM caches on Distributed.jl workers and
@@ -1297,3 +1374,4 @@ LDGAHelper = lDΓAHelper
 F_from_chi = F_from_χ
 calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_χγ_par, collect_χ0, collect_χ, collect_γ
 calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_part
+lambda_m_chain_batch = λm_chain_batch

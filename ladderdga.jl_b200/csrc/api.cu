@@ -154,6 +154,8 @@ int alloc_all(ldga_ctx* c) {
     TRY(dev_alloc(c, &c->d_flags, nq * nw));
     TRY(dev_alloc(c, &c->d_list, nq * nw));
     TRY(dev_alloc(c, &c->d_count, 4));
+    if (bse_pivot_smem((int)nnu) > LDGA_PIVOT_SMEM_MAX)
+        TRY(dev_alloc(c, &c->d_pivot_scratch, (size_t)LDGA_PIVOT_GRID * nnu * (nnu + 1)));
     TRY(copy(c, c->d_kmult, c->kmult.data(), nq * sizeof(double)));
     TRY(copy(c, c->d_eps, c->eps.data(), nq * sizeof(double)));
     return sync(c);
@@ -162,7 +164,8 @@ int alloc_all(ldga_ctx* c) {
 void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
-                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count};
+                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
+                    c->d_pivot_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -701,13 +704,17 @@ uint64_t dbits(double x) { uint64_t u; std::memcpy(&u, &x, 8); return u; }
 
 }  // namespace
 
-int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const double* gamma_m,
-                 const double* gamma_d, const double* chi_loc_m, const double* gimp, int32_t n_gimp,
-                 double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
-                 double* chi_m_out, double* chi_d_out, double* scalars_out) {
-    if (!ctx || !sigma_loc || !gamma_m || !gamma_d || !chi_loc_m || !gimp)
+namespace {
+
+// Checks the inputs, allocates the chain's persistent buffers and enqueues the chain on the handle's
+// stream: a replay of the captured graph when pointers and scalars are unchanged, otherwise an
+// uncaptured run (it computes this call's results) followed by a capture.  Nothing waits for the
+// device, so several handles' chains can be in flight at once.
+int chain_m_submit(ldga_ctx* ctx, const ChainArgs& a, bool use_graph, bool* replayed_out) {
+    *replayed_out = false;
+    if (!a.sigma_loc || !a.gamma_m || !a.gamma_d || !a.chi_loc_m || !a.gimp)
         return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
-    DeviceGuard g(ctx->device);
+    const int n_sigma = a.n_sigma, n_gimp = a.n_gimp;
     const int L = std::max(std::abs(ctx->sp.fft_lo), std::abs(ctx->sp.fft_hi));
     if (n_sigma <= L) return ctx_fail(ctx, LDGA_ERR_ARG, "Sigma_loc must cover n = 0..max|fft_range|");
     const int need_g = 2 * ctx->sp.n_iv + ctx->sp.n_iw + (ctx->sp.shift ? ctx->sp.n_iw : 0);
@@ -728,52 +735,54 @@ int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const 
         ctx->n_gimp_alloc = n_gimp;
     }
     if (!ctx->h_stage) LDGA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), 64 * sizeof(double) + 16));
-    ChainArgs a{sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, n_sigma, n_gimp, imp_density, chiloc_m_sum,
-                sigma_out, chi_m_out, chi_d_out};
-    const void* ptrs[] = {sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, sigma_out, chi_m_out, chi_d_out};
-    bool graphable = use_graph != 0;
+    const void* ptrs[] = {a.sigma_loc, a.gamma_m, a.gamma_d, a.chi_loc_m, a.gimp, a.sigma_out, a.chi_m_out, a.chi_d_out};
+    bool graphable = use_graph;
     for (const void* p : ptrs)
         if (host_pageable(p)) graphable = false;   // stream capture needs pinned or device memory
     std::vector<uint64_t> key;
     if (graphable) {
         for (const void* p : ptrs) key.push_back((uint64_t)(uintptr_t)p);
-        key.insert(key.end(), {(uint64_t)n_sigma, (uint64_t)n_gimp, dbits(imp_density), dbits(chiloc_m_sum),
+        key.insert(key.end(), {(uint64_t)n_sigma, (uint64_t)n_gimp, dbits(a.imp_density), dbits(a.chiloc_m_sum),
                                dbits(ctx->mp.U), dbits(ctx->mp.mu), dbits(ctx->mp.beta), dbits(ctx->mp.n),
                                dbits(ctx->mp.Ekin_DMFT), (uint64_t)ctx->prec, (uint64_t)(uintptr_t)ctx->stream,
                                (uint64_t)ctx->profiling});
     }
-    bool replayed = false;
     if (graphable && ctx->graph_exec && key == ctx->graph_key) {
         LDGA_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
         ctx->n_launches += ctx->graph_launches;
-        replayed = true;
-    } else {
-        TRY(chain_m_enqueue(ctx, a));   // the uncaptured run computes this call's results
-        if (graphable) {
-            if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
-            if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
-            for (auto& pr : ctx->graph_ev) ctx->ev_free.push_back(pr.second);
-            ctx->graph_ev.clear();
-            ctx->capturing = true;
-            const int64_t n0 = ctx->n_launches;
-            cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
-            int st = e == cudaSuccess ? chain_m_enqueue(ctx, a) : LDGA_ERR_CUDA;
-            cudaGraph_t gr = nullptr;
-            cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &gr);
-            ctx->capturing = false;
-            ctx->graph_launches = ctx->n_launches - n0;   // kernels in the graph (nothing ran yet)
-            ctx->n_launches = n0;
-            if (e != cudaSuccess || st != LDGA_OK || e2 != cudaSuccess || !gr) {
-                if (gr) cudaGraphDestroy(gr);
-                cudaGetLastError();
-                return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("CUDA graph capture of the chain failed: ") +
-                                                        cudaGetErrorString(e != cudaSuccess ? e : e2));
-            }
-            LDGA_CUDA(ctx, cudaGraphInstantiate(&ctx->graph_exec, gr, 0));
-            ctx->graph = gr;
-            ctx->graph_key = key;
-        }
+        *replayed_out = true;
+        return LDGA_OK;
     }
+    TRY(chain_m_enqueue(ctx, a));   // the uncaptured run computes this call's results
+    if (graphable) {
+        if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+        for (auto& pr : ctx->graph_ev) ctx->ev_free.push_back(pr.second);
+        ctx->graph_ev.clear();
+        ctx->capturing = true;
+        const int64_t n0 = ctx->n_launches;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        int st = e == cudaSuccess ? chain_m_enqueue(ctx, a) : LDGA_ERR_CUDA;
+        cudaGraph_t gr = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &gr);
+        ctx->capturing = false;
+        ctx->graph_launches = ctx->n_launches - n0;   // kernels in the graph (nothing ran yet)
+        ctx->n_launches = n0;
+        if (e != cudaSuccess || st != LDGA_OK || e2 != cudaSuccess || !gr) {
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("CUDA graph capture of the chain failed: ") +
+                                                    cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        LDGA_CUDA(ctx, cudaGraphInstantiate(&ctx->graph_exec, gr, 0));
+        ctx->graph = gr;
+        ctx->graph_key = key;
+    }
+    return LDGA_OK;
+}
+
+// Waits for the handle's stream and unpacks the chain's scalars (layout of ldga_chain_m).
+int chain_m_collect(ldga_ctx* ctx, bool replayed, double* scalars_out) {
     TRY(sync(ctx));
     if (replayed && ctx->profiling) {
         for (auto& pr : ctx->graph_ev) {
@@ -803,6 +812,53 @@ int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const 
     }
     if (fails > 0) return ctx_fail(ctx, LDGA_ERR_NUMERIC, std::to_string(fails) + " BSE matrices are singular or non-finite");
     return LDGA_OK;
+}
+
+}  // namespace
+
+int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const double* gamma_m,
+                 const double* gamma_d, const double* chi_loc_m, const double* gimp, int32_t n_gimp,
+                 double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
+                 double* chi_m_out, double* chi_d_out, double* scalars_out) {
+    if (!ctx) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    ChainArgs a{sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, n_sigma, n_gimp, imp_density, chiloc_m_sum,
+                sigma_out, chi_m_out, chi_d_out};
+    bool replayed = false;
+    TRY(chain_m_submit(ctx, a, use_graph != 0, &replayed));
+    return chain_m_collect(ctx, replayed, scalars_out);
+}
+
+int ldga_batch_chain_m(int32_t n, ldga_ctx* const* ctxs, const ldga_chain_io* io, int32_t use_graph,
+                       int32_t* status) {
+    if (n < 0 || (n > 0 && (!ctxs || !io))) return ctx_fail(nullptr, LDGA_ERR_ARG, "null argument");
+    std::vector<int> st(n, LDGA_OK);
+    std::vector<char> rep(n, 0);
+    for (int i = 0; i < n; ++i) {        // every point's chain is in flight before the first wait
+        ldga_ctx* c = ctxs[i];
+        if (!c) { st[i] = LDGA_ERR_ARG; continue; }
+        DeviceGuard g(c->device);
+        const ldga_chain_io& x = io[i];
+        ChainArgs a{x.sigma_loc, x.gamma_m, x.gamma_d, x.chi_loc_m, x.gimp, x.n_sigma, x.n_gimp, x.imp_density,
+                    x.chiloc_m_sum, x.sigma_out, x.chi_m_out, x.chi_d_out};
+        bool r = false;
+        st[i] = chain_m_submit(c, a, use_graph != 0, &r);
+        rep[i] = r;
+    }
+    int first = LDGA_OK;
+    for (int i = 0; i < n; ++i) {
+        if (st[i] == LDGA_OK) {
+            DeviceGuard g(ctxs[i]->device);
+            st[i] = chain_m_collect(ctxs[i], rep[i] != 0, io[i].scalars_out);
+        } else if (ctxs[i]) {
+            DeviceGuard g(ctxs[i]->device);
+            cudaStreamSynchronize(ctxs[i]->stream);   // whatever was enqueued before the failure
+        }
+        if (status) status[i] = st[i];
+        if (first == LDGA_OK && st[i] != LDGA_OK) first = st[i];
+    }
+    if (first != LDGA_OK) g_create_error = "ldga_batch_chain_m: see status[] and ldga_last_error of each handle";
+    return first;
 }
 
 // ------------------------------------------------------------------------------- lambda_dm --

@@ -440,7 +440,7 @@ struct LuSmem {
         (2 * RW + 2 * CW + N + N + N) * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
 };
 
-template <int N, int T, int MPC, int MINB>
+template <int N, int T, int MPC, int MINB, bool GSM>
 __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     using LS = LuSmem<N, T>;
     constexpr int RT = LS::RT, NC = LS::NC, G = LS::G;
@@ -448,13 +448,14 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     constexpr int TCN = N % T, CN = N / T;                // owner lane / tile column of the rhs
     static_assert(T <= 32 && 32 % T == 0, "a row group must sit inside one warp");
     extern __shared__ double2 sm[];
-    double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
+    // Gamma(w): staged in shared memory (GSM), or read through L1/L2 when N x N does not fit
+    const double2* Gsm = GSM ? sm : a.Gamma + (size_t)blockIdx.y * N * N;   // Gamma[j + N*i] at i*N + j
     const int tid = threadIdx.x;
     const int g = tid / G, t = tid - g * G;
     const int tr = t / T, tc = t - (t / T) * T;
     const int lane = tid & 31;
         const int bar = g + 1;
-    char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * LS::bytes;
+    char* gs = reinterpret_cast<char*>(sm + (GSM ? N * N : 0)) + g * LS::bytes;
     double2* rowbuf = reinterpret_cast<double2*>(gs);     // [2][RW]
     double2* colbuf = rowbuf + 2 * LS::RW;                // [2][CW]
     double2* pinv = colbuf + 2 * LS::CW;                  // [N] 1/b_kk
@@ -465,9 +466,9 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     const int w = blockIdx.y;
     const int q0 = blockIdx.x * a.qchunk;
     const int q1 = min(a.nq, q0 + a.qchunk);
-    {
+    if (GSM) {
         const double2* Gw = a.Gamma + (size_t)w * N * N;
-        for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+        for (int e = tid; e < N * N; e += blockDim.x) sm[e] = Gw[e];
     }
     __syncthreads();
 
@@ -674,7 +675,7 @@ struct Lu32Smem {
                                     2 * N * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
 };
 
-template <int N, int T, int MPC, int MINB>
+template <int N, int T, int MPC, int MINB, bool GSM>
 __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu32(const BseArgs a) {
     using LS = Lu32Smem<N, T>;
     constexpr int RT = LS::RT, CT = LS::CT, G = LS::G;
@@ -683,13 +684,14 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu32(const BseArgs a)
     static_assert(T <= 32 && 32 % T == 0, "a row group must sit inside one warp");
     static_assert((N * N * sizeof(double2)) % 16 == 0, "16-byte alignment of the group buffers");
     extern __shared__ double2 sm[];
-    double2* Gsm = sm;                                    // [N*N] Gamma(w), Gamma[j + N*i] at i*N + j
+    // Gamma(w): staged in shared memory (GSM), or read through L1/L2 when N x N does not fit
+    const double2* Gsm = GSM ? sm : a.Gamma + (size_t)blockIdx.y * N * N;   // Gamma[j + N*i] at i*N + j
     const int tid = threadIdx.x;
     const int g = tid / G, t = tid - g * G;
     const int tr = t / T, tc = t - (t / T) * T;
     const int lane = tid & 31;
     const int bar = g + 1;
-    char* gs = reinterpret_cast<char*>(Gsm + N * N) + g * LS::bytes;
+    char* gs = reinterpret_cast<char*>(sm + (GSM ? N * N : 0)) + g * LS::bytes;
     float4* rowbuf = reinterpret_cast<float4*>(gs);       // [2][RW]
     float4* colbuf = rowbuf + 2 * LS::RW;                 // [2][CW]
     float2* pinv = reinterpret_cast<float2*>(colbuf + 2 * LS::CW);   // [N] 1/b_kk (FP32)
@@ -701,9 +703,9 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu32(const BseArgs a)
     const int w = blockIdx.y;
     const int q0 = blockIdx.x * a.qchunk;
     const int q1 = min(a.nq, q0 + a.qchunk);
-    {
+    if (GSM) {
         const double2* Gw = a.Gamma + (size_t)w * N * N;
-        for (int e = tid; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+        for (int e = tid; e < N * N; e += blockDim.x) sm[e] = Gw[e];
     }
     __syncthreads();
     const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
@@ -1257,13 +1259,15 @@ __device__ __forceinline__ double block_sum_det(double v, double* red) {
 // Fallback: partial-pivoting FP64 LU of B = A^T (one matrix per CTA, shared memory), used for flagged
 // matrices and for box sizes without a tiled instantiation.  list == nullptr: all (q, w);
 // count_dev (may be null) holds the number of list entries (written earlier on the stream).
+// gscratch (may be null): LDGA_PIVOT_GRID matrices in HBM, used when [N][N+1] exceeds shared memory.
 __global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int32_t* list, int count,
-                                                       const int32_t* count_dev) {
+                                                       const int32_t* count_dev, double2* gscratch) {
     extern __shared__ double2 sm[];
     const int N = a.nnu;
-    double2* B = sm;                 // [N][N+1] row-major, last column = rhs
-    double* red = reinterpret_cast<double*>(B + N * (N + 1));
-    int* piv_s = reinterpret_cast<int*>(red + 64);
+    double* red = reinterpret_cast<double*>(sm);                      // [64]
+    int* piv_s = reinterpret_cast<int*>(red + 64);                    // [4]
+    double2* B = gscratch ? gscratch + (size_t)blockIdx.x * N * (N + 1)   // [N][N+1] row-major, rhs last
+                          : reinterpret_cast<double2*>(piv_s + 4);
     const int ld = N + 1;
     if (count_dev) count = count_dev[0];
     for (int item = blockIdx.x; item < count; item += gridDim.x) {
@@ -1370,12 +1374,12 @@ int run_tile(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
-template <int N, int T, int MPC, int MINB>
+template <int N, int T, int MPC, int MINB, bool GSM = true>
 int run_lu(ldga_ctx* ctx, const BseArgs& a0) {
     BseArgs a = a0;
     const int threads = T * T * MPC;
-    const size_t sm = (size_t)N * N * sizeof(double2) + MPC * LuSmem<N, T>::bytes;
-    auto kern = k_bse_lu<N, T, MPC, MINB>;
+    const size_t sm = (GSM ? (size_t)N * N * sizeof(double2) : 0) + MPC * LuSmem<N, T>::bytes;
+    auto kern = k_bse_lu<N, T, MPC, MINB, GSM>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     int chunk = 4 * MPC;
     while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
@@ -1387,12 +1391,12 @@ int run_lu(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
-template <int N, int T, int MPC, int MINB>
+template <int N, int T, int MPC, int MINB, bool GSM = true>
 int run_lu32(ldga_ctx* ctx, const BseArgs& a0) {
     BseArgs a = a0;
     const int threads = T * T * MPC;
-    const size_t sm = (size_t)N * N * sizeof(double2) + MPC * Lu32Smem<N, T>::bytes;
-    auto kern = k_bse_lu32<N, T, MPC, MINB>;
+    const size_t sm = (GSM ? (size_t)N * N * sizeof(double2) : 0) + MPC * Lu32Smem<N, T>::bytes;
+    auto kern = k_bse_lu32<N, T, MPC, MINB, GSM>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     int chunk = 4 * MPC;
     while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
@@ -1438,10 +1442,12 @@ int run_mode(ldga_ctx* ctx, const BseArgs& a) {
 
 bool bse_has_fast_path(int nnu) {
     switch (nnu) {
-        case 4: case 6: case 8: case 10: case 12: case 16: case 20: case 30: case 40: case 60: return true;
+        case 4: case 6: case 8: case 10: case 12: case 16: case 20: case 30: case 40: case 60: case 120: return true;
         default: return false;
     }
 }
+
+size_t bse_pivot_smem(int nnu) { return (size_t)nnu * (nnu + 1) * sizeof(double2) + 64 * sizeof(double) + 16; }
 
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     BseArgs a;
@@ -1467,15 +1473,21 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
         case 30: st = run_mode<30, 8, 8, 2, 2>(ctx, a); break;
         case 40: st = run_mode<40, 8, 8, 2, 2, 3, 3>(ctx, a); break;
         case 60: st = run_mode<60, 16, 16, 1, 1>(ctx, a); break;
+        case 120:   // Gamma(w) (230 KB) exceeds shared memory: read through L1/L2; FP64_INV solves by LU too
+            st = ctx->prec == LDGA_PREC_MIXED ? run_lu32<120, 16, 1, 1, false>(ctx, a)
+                                              : run_lu<120, 16, 1, 1, false>(ctx, a);
+            break;
         default: generic = true; break;
     }
     if (st != LDGA_OK) return st;
-    const size_t smp = (size_t)ctx->Nnu * (ctx->Nnu + 1) * sizeof(double2) + 64 * sizeof(double) + 16;
-    if (smp > 220 * 1024) return ctx_fail(ctx, LDGA_ERR_ARG, "fermionic box too large for the BSE kernels");
+    const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;
+    if (in_hbm && !ctx->d_pivot_scratch) return ctx_fail(ctx, LDGA_ERR_ARG, "pivoted BSE scratch missing");
+    const size_t smp = in_hbm ? 64 * sizeof(double) + 16 : bse_pivot_smem(ctx->Nnu);
+    double2* gscr = in_hbm ? ctx->d_pivot_scratch : nullptr;
     LDGA_CUDA(ctx, set_smem(ctx, k_bse_lu_pivot, smp));
     if (generic) {
         StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
-        k_bse_lu_pivot<<<4 * 148, 256, smp, ctx->stream>>>(a, nullptr, n, nullptr);
+        k_bse_lu_pivot<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(a, nullptr, n, nullptr, gscr);
         LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
     } else {
         // flagged matrices: compacted on the device, re-solved by a grid-stride pivoted kernel that reads
@@ -1484,7 +1496,7 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
         k_compact_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, ctx->d_list, ctx->d_count);
         LDGA_LAUNCHED(ctx, "k_compact_flags");
         StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
-        k_bse_lu_pivot<<<2 * 148, 256, smp, ctx->stream>>>(a, ctx->d_list, 0, ctx->d_count);
+        k_bse_lu_pivot<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(a, ctx->d_list, 0, ctx->d_count, gscr);
         LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
     }
     // matrices that stayed non-finite after the pivoted solve, accumulated into *d_fail

@@ -105,6 +105,7 @@ struct ldga_ctx {
     int32_t* d_flags = nullptr;    // BSE fallback flags [Nq*Nw]
     int32_t* d_list = nullptr;     // compacted fallback list
     int32_t* d_count = nullptr;
+    double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
 
     cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
     bool capturing = false;              // a CUDA graph of the chain is being captured
@@ -161,6 +162,10 @@ inline cudaError_t set_smem(ldga_ctx* c, F* f, size_t sm) {
 }
 
 bool bse_has_fast_path(int nnu);
+// shared memory of one pivoted-fallback matrix [N][N+1] (complex FP64) plus its reduction scratch
+size_t bse_pivot_smem(int nnu);
+constexpr size_t LDGA_PIVOT_SMEM_MAX = 220 * 1024;
+constexpr int LDGA_PIVOT_GRID = 2 * 148;
 
 // Records CUDA events around one stage when the handle is profiling (no-op otherwise).
 struct StageTimer {

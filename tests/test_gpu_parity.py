@@ -256,3 +256,49 @@ def test_parallel_api_matches_single_call_api(case):
     s_ref = R.calc_Sigma(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], r.chiloc_m_sum, ref["lambda0"],
                          r.grhat, r.kG, r.mP, r.sP, numax=numax, lam_m=0.1)
     assert rel(s_par, s_ref) < RTOL
+
+
+@pytest.mark.parametrize("n_iv", [60, 62])
+@pytest.mark.parametrize("prec", [L.PREC_FP64_INV, L.PREC_FP64, L.PREC_MIXED])
+def test_bse_large_box(n_iv, prec, require_gpu):
+    """Nν = 120 (the β = 40 points of the uneven batch): Γ(ω) no longer fits shared memory and is read
+    through the caches; Nν = 124 has no tiled kernel and runs the pivoted solve with its matrices
+    in HBM.  Both against the oracle at the parity tolerance."""
+    inp = S.make_input(dim=2, ns=4, beta=40.0, U=1.0, n_iv=n_iv, n_iw=2, seed=90 + n_iv)
+    ref = R.run_chain(inp, lambda_type=None)
+    g = gpu_chain(inp, prec)
+    assert rel(g["chi0"].data, ref["chi0"]) < RTOL
+    for r in ("m", "d"):
+        assert g[f"chi_{r}"].n_fallback == 0 or n_iv == 62
+        assert rel(g[f"chi_{r}"].data, ref[f"chi_{r}"].data) < RTOL, (n_iv, prec, r)
+        assert rel(g[f"gamma_{r}"].data, ref[f"gamma_{r}"]) < RTOL, (n_iv, prec, r)
+    assert rel(np.asarray(g["lambda0"]), ref["lambda0"]) < RTOL
+
+
+def test_batch_chain_uneven_points(require_gpu):
+    """ldga_batch_chain_m over points of different Nν (4, 16, 30) and U: each point equals the
+    single-point λm chain and, within the parity tolerance, the oracle."""
+    pts = [dict(dim=2, ns=8, beta=4.0, U=0.8, n_iv=2, n_iw=2, seed=301),
+           dict(dim=2, ns=8, beta=6.0, U=1.1, n_iv=8, n_iw=8, seed=302),
+           dict(dim=2, ns=6, beta=10.0, U=0.9, n_iv=15, n_iw=15, seed=303)]
+    inps = [S.make_input(**p) for p in pts]
+    hs = [L.setup_synthetic(i) for i in inps]
+    batch = L.λm_chain_batch(hs)
+    for inp, h, b in zip(inps, hs, batch):
+        chi0 = L.calc_bubble(h)
+        xm, gm = L.calc_χγ("m", h, chi0)
+        xd, gd = L.calc_χγ("d", h, chi0)
+        l0 = L.calc_λ0(chi0, h)
+        assert rel(b.χ_m, xm.data) < 1e-14 and rel(b.χ_d, xd.data) < 1e-14
+        one = L.λ_correction("m", xm, gm, xd, gd, l0, h)
+        assert abs(b.λm - one.λm) <= 1e-12 * max(1.0, abs(one.λm))
+        assert rel(b.Σ_ladder, one.Σ_ladder) < 1e-12
+        ref = R.run_chain(inp, lambda_type="m")["result"]
+        if ref.converged and one.converged:
+            assert abs(b.λm - ref.lam_m) < ATOL_LAMBDA
+            assert rel(b.Σ_ladder, ref.Sigma_ladder) < RTOL
+            assert abs(b.μ - ref.mu) < ATOL_LAMBDA
+    # a second call on the same handles (graphs off) reproduces the first bitwise
+    again = L.λm_chain_batch(hs)
+    for a, b in zip(batch, again):
+        assert a.λm == b.λm and np.array_equal(a.Σ_ladder, b.Σ_ladder)
