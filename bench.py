@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ns", type=int, default=None, help="smaller k-grid (points per axis) for profiling captures")
     ap.add_argument("--out", default=None, help="also write the JSON line to this file")
+    ap.add_argument("--workload", default="chain", choices=["chain", "batch"],
+                    help="chain: the 3D 32^3 point (default); batch: the uneven 64-point (U, beta) scan on 2D 32^2")
+    ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
     return ap.parse_args()
 
 
@@ -179,7 +182,7 @@ def run_reference(args):
 class Chain:
     """The device chain for one parameter point, driven through the C ABI."""
 
-    def __init__(self, inp, prec: int, device: int):
+    def __init__(self, inp, prec: int, device: int, stream=None):
         import torch
         import ladderdga_b200 as L
         self.L, self.torch = L, torch
@@ -187,7 +190,7 @@ class Chain:
         self.h = L.setup_synthetic(inp, precision=prec, device=device)
         self.ctx = self.h.ctx
         self.lib = self.ctx.lib
-        self.stream = torch.cuda.current_stream(device)
+        self.stream = stream if stream is not None else torch.cuda.current_stream(device)
         self.ctx.call("ldga_set_stream", C.c_void_p(self.stream.cuda_stream))
         h = self.h
         dev = torch.device("cuda", device)
@@ -210,6 +213,15 @@ class Chain:
         self.out_chi_d = torch.empty(nq * nw, dtype=torch.float64).pin_memory()
         self.d2h_bytes = (self.out_sigma.numel() + self.out_chi_m.numel() + self.out_chi_d.numel()) * 8 + 5 * 8
         self.points = nq * nw
+
+    def io(self, src: dict, outputs: bool, sc):
+        """This point's ldga_chain_io (ldga_batch_chain_m)."""
+        from ladderdga_b200 import _lib
+        p = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+        return _lib.ChainIO(p(src["sigma_loc"]), self.n_sigma, p(src["gamma_m"]), p(src["gamma_d"]),
+                            p(src["chi_loc_m"]), p(src["gimp"]), self.n_gimp, self.h.imp_density, self.h.χloc_m_sum,
+                            p(self.out_sigma) if outputs else None, p(self.out_chi_m) if outputs else None,
+                            p(self.out_chi_d) if outputs else None, C.addressof(sc))
 
     def step(self, src: dict, outputs: bool, graph: bool = True):
         """One parameter point through ldga_chain_m (captured once in a CUDA graph, then replayed)."""
@@ -367,10 +379,109 @@ def run_ours(args):
     return 0
 
 
+BATCH_NAME = ("uneven batch: {n} points of 2D sc Nk=32^2 (153 irreducible q), U ~ U[0.5,3], beta in {{5,10,20,40}}, "
+              "Nnu = Nw - 1 = 2 round(1.5 beta) in {{16,30,60,120}}, lambda_m, all points in one ldga_batch_chain_m call")
+
+
+def run_batch(args):
+    """The uneven (U, beta) scan: every point's chain in flight together (one stream per point)."""
+    import torch
+    import ladderdga_b200 as L
+    from ladderdga_b200 import _lib
+    from ladderdga_b200 import synthetic as S
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pts = S.batch_points(args.points, ns=args.ns or 32)
+    chains = []
+    for p in pts:
+        chains.append(Chain(S.make_input(**p), PREC_NAMES[args.prec], local, stream=torch.cuda.Stream(local)))
+    n = len(chains)
+    main = torch.cuda.current_stream(local)
+    scs = [(C.c_double * 8)() for _ in chains]
+    handles = (C.c_void_p * n)(*[c.ctx.h.value for c in chains])
+    status = (C.c_int32 * n)()
+    ios = {}
+    for key, outputs in (("dev", False), ("pin", True)):
+        arr = (_lib.ChainIO * n)()
+        for i, c in enumerate(chains):
+            arr[i] = c.io(c.dev if key == "dev" else c.pin, outputs, scs[i])
+        ios[key] = arr
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lib = chains[0].lib
+    for c in chains:
+        c.ctx.call("ldga_profile", 1)
+
+    def timed(key):
+        times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(main)
+            for c in chains:
+                c.stream.wait_event(a)
+            st = lib.ldga_batch_chain_m(n, handles, ios[key], 1, status)
+            if st != 0:
+                raise RuntimeError(f"ldga_batch_chain_m failed: {[lib.ldga_last_error(c.ctx.h).decode() for c in chains]}")
+            for c in chains:
+                e = torch.cuda.Event()
+                e.record(c.stream)
+                main.wait_event(e)
+            b.record(main)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        return times
+
+    for key in ("dev", "pin"):
+        for _ in range(max(args.warmup, 3)):
+            lib.ldga_batch_chain_m(n, handles, ios[key], 1, status)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    cnt0 = []
+    for c in chains:
+        v = C.c_int64()
+        c.ctx.call("ldga_launch_count", C.byref(v))
+        cnt0.append(v.value)
+    t_dev = timed("dev")
+    cnt1 = []
+    for c in chains:
+        v = C.c_int64()
+        c.ctx.call("ldga_launch_count", C.byref(v))
+        cnt1.append(v.value)
+    t_e2e = timed("pin")
+    clk = clocks.stop()
+    points = sum(c.points for c in chains)
+    ms, ms_e2e = float(np.mean(t_dev)), float(np.mean(t_e2e))
+    from ladderdga_b200 import parallel as P
+    ms, ms_e2e = P.max_over_ranks(ms), P.max_over_ranks(ms_e2e)
+    nnu = sorted({c.ctx.Nnu for c in chains})
+    line = {"metric": METRIC, "value": world * points / (ms / 1e3), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
+            "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
+            "config": {"workload": BATCH_NAME.format(n=n), "global_batch": n * world, "nnu_set": nnu,
+                       "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
+                       "points_per_step_per_gpu": points},
+            "e2e": {"value": world * points / (ms_e2e / 1e3), "unit": METRIC,
+                    "h2d_bytes_per_step": sum(c.h2d_bytes for c in chains),
+                    "d2h_bytes_per_step": sum(c.d2h_bytes for c in chains), "ms_per_step": ms_e2e,
+                    "path": "C ABI (ldga_batch_chain_m) from pinned host buffers"},
+            "gpu_launches": int(sum(cnt1) - sum(cnt0)),
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+        if args.out:
+            open(args.out, "w").write(json.dumps(line) + "\n")
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -1159,8 +1159,67 @@ def λ_correction(type_, χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHe
         return λdm_correction(χm, γm, χd, γd, λ0, h, νmax=νmax, λ_min_δ=λ_min_δ, λ_val_only=λ_val_only,
                               validate_threshold=validate_threshold, verbose=verbose)
     if t in ("sc", "sc_m"):
-        raise NotImplementedError("self-consistent ladder (run_sc) is not built")
+        # conditions_new.jl:76-79: :sc -> run_sc with its defaults (type :fix, λ = 0), :sc_m -> type :m.
+        # The reference omits run_sc's positional μ there; the model's μ is used.
+        μ = kw.get("μ", h.mP.μ)
+        return run_sc(χm, γm, χd, γd, λ0, μ, h, type=("fix" if t == "sc" else "m"),
+                      **{k: v for k, v in kw.items() if k in ("maxit", "mixing", "conv_abs", "trace")})
     raise RuntimeError(f"λ-correction type '{type_}' not recognized!")
+
+
+def run_sc(χm: χT, γm: γT, χd: χT, γd: γT, λ0, μ: float, h: lDΓAHelper, par: bool = False,
+           λ_min_δ: float = 0.0001, νmax: int = -1, maxit: int = 100, mixing: float = 0.2, conv_abs: float = 1e-8,
+           trace: bool = False, verbose: bool = False, update_χ_tail: bool = False, fit_μ: bool = True,
+           tc: bool = True, type="fix", λm: float = 0.0, λd: float = 0.0) -> λ_result:
+    """``run_sc`` (conditions_new.jl:342-407) with its loop ``run_sc!`` (:409-556) on the device.
+
+    type: ``:fix`` (the given λm, λd), ``:m`` / ``:dm`` (the given λ, then :dm re-solves λdm in every
+    iteration), ``:pre_m`` / ``:pre_dm`` (λ from λm_correction / λdm_correction first).  The EoM,
+    μ fit, energies and the transform of G_ladder for the next EoM all run on the GPU handle;
+    the handle's own G is restored afterwards, as the reference iterates on a deepcopy.
+    """
+    t = str(type).lstrip(":")
+    if not fit_μ:
+        warnings.warn("Not fitting μ can lead to unphysical results!")
+    if update_χ_tail:
+        raise NotImplementedError("run_sc: update_χ_tail = true (the χ tail update loop) is not built")
+    if not tc:
+        raise NotImplementedError("run_sc: the EoM of the loop uses the tail correction (tc = true)")
+    if t not in ("fix", "m", "dm", "pre_m", "pre_dm"):
+        warnings.warn(f"Unrecognized type = {type} in run_sc")
+        λm, λd = 0.0, 0.0
+    if t == "pre_m":
+        rhs = λm_rhs(χm, χd, h)
+        λm, validation = λm_correction(χm, rhs, h)
+        λd = 0.0
+    elif t == "pre_dm":
+        λm, λd, validation = λdm_correction(χm, γm, χd, γd, λ0, h, νmax=νmax, λ_min_δ=λ_min_δ, λ_val_only=True,
+                                            validate_threshold=conv_abs, verbose=verbose)
+    else:
+        validation = True
+    if not (validation and math.isfinite(λm) and math.isfinite(λd)):
+        return λ_result(float("nan"), float("nan"), t, False, False, float("nan"), float("nan"), float("nan"),
+                        float("nan"), float("nan"), [], None, None, float("nan"), float("nan"))
+    _prepare_eom(h, χm, γm, χd, γd, λ0)
+    χm._device_λ()
+    χd._device_λ()
+    ctx = h.ctx
+    nu_auto = min(h.sP.n_iν, math.floor(3 * len(usable_ωindices(h.sP, χm, χd)) / 8))
+    nu = nu_auto if νmax < 1 else min(nu_auto, νmax)
+    out = np.zeros(12)
+    S = _lib.cplx_out((ctx.Nq, max(nu, 1)))
+    G = _lib.cplx_out((ctx.Nq, ctx.Nf))
+    ctx.call("ldga_run_sc", float(λm), float(λd), int(t in ("dm", "pre_dm")), float(μ), h.χloc_m_sum, int(νmax),
+             int(maxit), float(mixing), float(conv_abs), int(bool(fit_μ)), float(λ_min_δ), ptr(out), ptr(S), ptr(G))
+    lm, ld, rhs_c1, lhs_c1, ep1, ep2, ek, n, μr, scc = out[:10]
+    if t == "fix":
+        lm, ld = 0.0, 0.0   # run_sc! reports its loop-local λ, which :fix never sets (conditions_new.jl:426-446)
+    sc_converged = bool(scc)
+    converged = (sc_converged and math.isfinite(lhs_c1) and math.isfinite(ep2) and abs(rhs_c1 - lhs_c1) <= conv_abs
+                 and abs(ep1 - ep2) <= conv_abs)
+    # λ_result(λm, λd, type, sc_converged, converged, ...) in the reference's positional order (:404-405)
+    return λ_result(float(lm), float(ld), t, sc_converged, converged, float(ek), float(ep1), float(ep2),
+                    float(rhs_c1), float(lhs_c1), [], G, S[:, :nu], float(μr), float(n))
 
 
 # =============================================================================================

@@ -868,6 +868,7 @@ struct DmState {
     ldga_ctx* ctx;
     double chiloc_m_sum;
     int numax;
+    int fix_n = 1;
     double mu;
     double rhs_c1;
     int evals = 0;
@@ -881,7 +882,7 @@ bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
     s.evals++;
     if (lm > 1e5 || ld > 1e5) { F[0] = F[1] = NAN; return true; }
     int st = eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum);
-    if (!st) st = launch_g_ladder(ctx, s.numax, 1, s.mu, ctx->d_red + 24);
+    if (!st) st = launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, ctx->d_red + 24);
     if (!st) st = launch_sum_kw(ctx, LDGA_CH_M, lm, 0, ctx->d_red + 32);
     if (!st) st = launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33);
     double r[10];
@@ -903,6 +904,55 @@ bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
 double fd_step(double x) {
     const double r = std::sqrt(2.220446049250313e-16);
     return std::max(r * std::fabs(x), r);
+}
+
+// newton_right, N-D (LambdaCorrection/helpers.jl:165-208) on the λdm residual; false on a CUDA or
+// argument error (s.status), *failed when the back-off resets are exhausted.
+bool dm_newton(DmState& s, const double start[2], const double xmin[2], double atol, int nsteps, double xi[2],
+               int* iters, bool* failed_out) {
+    xi[0] = start[0]; xi[1] = start[1];
+    int i = 1, reset_i = 1;
+    bool bis_fail = false, failed = false;
+    const int max_reset = 5;
+    const double reset_backoff = 1.0;
+    while (true) {
+        double fi[2], f0[2], f1[2], J[2][2];
+        if (!dm_residual(s, xi[0], xi[1], fi)) return false;
+        // forward-difference Jacobian; FiniteDiff evaluates f(x) again
+        if (!dm_residual(s, xi[0], xi[1], f0)) return false;
+        for (int j = 0; j < 2; ++j) {
+            double x1[2] = {xi[0], xi[1]};
+            const double e = fd_step(xi[j]);
+            x1[j] += e;
+            if (!dm_residual(s, x1[0], x1[1], f1)) return false;
+            J[0][j] = (f1[0] - f0[0]) / e;
+            J[1][j] = (f1[1] - f0[1]) / e;
+        }
+        const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        const double inv[2][2] = {{J[1][1] / det, -J[0][1] / det}, {-J[1][0] / det, J[0][0] / det}};
+        const double last[2] = {xi[0], xi[1]};
+        xi[0] = xi[0] - (inv[0][0] * fi[0] + inv[0][1] * fi[1]);
+        xi[1] = xi[1] - (inv[1][0] * fi[0] + inv[1][1] * fi[1]);
+        for (int l = 0; l < 2; ++l) {
+            if (xi[l] < xmin[l]) {
+                xi[l] = xmin[l] + std::fabs(last[l] - xmin[l]) / 2.0;
+                if (std::fabs(last[l] - xmin[l]) / 2.0 < 1e-8) bis_fail = true;
+            }
+        }
+        if (bis_fail || !std::isfinite(fi[0]) || !std::isfinite(fi[1])) {
+            bis_fail = false;
+            if (reset_i >= max_reset) { failed = true; break; }
+            reset_i += 1;
+            xi[0] = start[0] + reset_i * reset_backoff * std::fabs(xmin[0]);
+            xi[1] = start[1] + reset_i * reset_backoff * std::fabs(xmin[1]);
+        }
+        if (std::fabs(std::sqrt(fi[0] * fi[0] + fi[1] * fi[1])) < atol) break;
+        if (i >= nsteps) break;
+        i += 1;
+    }
+    *iters = i;
+    *failed_out = failed;
+    return true;
 }
 
 }  // namespace
@@ -930,48 +980,11 @@ int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam
     TRY(copy(ctx, lmin, ctx->d_red + 40, 2 * sizeof(double)));
     TRY(sync(ctx));
     const double xmin[2] = {lmin[0] + lam_min_delta * std::fabs(lmin[0]), lmin[1] + lam_min_delta * std::fabs(lmin[1])};
-    // newton_right, N-D (LambdaCorrection/helpers.jl:165-208)
     const double start[2] = {0.0, 0.0};
-    double xi[2] = {start[0], start[1]};
-    int i = 1, reset_i = 1;
-    bool bis_fail = false, failed = false;
-    const int max_reset = 5;
-    const double reset_backoff = 1.0;
-    while (true) {
-        double fi[2], f0[2], f1[2], J[2][2];
-        if (!dm_residual(s, xi[0], xi[1], fi)) return s.status;
-        // forward-difference Jacobian; FiniteDiff evaluates f(x) again
-        if (!dm_residual(s, xi[0], xi[1], f0)) return s.status;
-        for (int j = 0; j < 2; ++j) {
-            double x1[2] = {xi[0], xi[1]};
-            const double e = fd_step(xi[j]);
-            x1[j] += e;
-            if (!dm_residual(s, x1[0], x1[1], f1)) return s.status;
-            J[0][j] = (f1[0] - f0[0]) / e;
-            J[1][j] = (f1[1] - f0[1]) / e;
-        }
-        const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-        const double inv[2][2] = {{J[1][1] / det, -J[0][1] / det}, {-J[1][0] / det, J[0][0] / det}};
-        const double last[2] = {xi[0], xi[1]};
-        xi[0] = xi[0] - (inv[0][0] * fi[0] + inv[0][1] * fi[1]);
-        xi[1] = xi[1] - (inv[1][0] * fi[0] + inv[1][1] * fi[1]);
-        for (int l = 0; l < 2; ++l) {
-            if (xi[l] < xmin[l]) {
-                xi[l] = xmin[l] + std::fabs(last[l] - xmin[l]) / 2.0;
-                if (std::fabs(last[l] - xmin[l]) / 2.0 < 1e-8) bis_fail = true;
-            }
-        }
-        if (bis_fail || !std::isfinite(fi[0]) || !std::isfinite(fi[1])) {
-            bis_fail = false;
-            if (reset_i >= max_reset) { failed = true; break; }
-            reset_i += 1;
-            xi[0] = start[0] + reset_i * reset_backoff * std::fabs(xmin[0]);
-            xi[1] = start[1] + reset_i * reset_backoff * std::fabs(xmin[1]);
-        }
-        if (std::fabs(std::sqrt(fi[0] * fi[0] + fi[1] * fi[1])) < atol) break;
-        if (i >= nsteps) break;
-        i += 1;
-    }
+    double xi[2];
+    int i = 0;
+    bool failed = false;
+    if (!dm_newton(s, start, xmin, atol, nsteps, xi, &i, &failed)) return s.status;
     ctx->lambda_dm_evals = s.evals;
     if (failed || !std::isfinite(xi[0]) || !std::isfinite(xi[1])) {
         *lam_m = NAN; *lam_d = NAN;
@@ -993,6 +1006,131 @@ int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam
         TRY(copy(ctx, G_out, ctx->d_gladder, (size_t)ctx->Nq * ctx->Nf * sizeof(double2)));
     }
     return sync(ctx);
+}
+
+// ------------------------------------------------------------------------------- run_sc ----
+namespace {
+// Sigma <- (1 - a) Sigma + a Sigma_old  (run_sc!, conditions_new.jl:469)
+__global__ void k_sigma_mix(double2* sigma, const double2* old, size_t n, double a) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const double2 x = sigma[e], y = old[e];
+        sigma[e] = make_double2((1.0 - a) * x.x + a * y.x, (1.0 - a) * x.y + a * y.y);
+    }
+}
+
+// Device buffers of one run_sc call, freed on every exit path.
+struct ScBuffers {
+    double2 *sigma_old = nullptr, *ghat_save = nullptr, *gloc_save = nullptr;
+    ~ScBuffers() {
+        if (sigma_old) cudaFree(sigma_old);
+        if (ghat_save) cudaFree(ghat_save);
+        if (gloc_save) cudaFree(gloc_save);
+    }
+};
+}  // namespace
+
+int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t redo_dm, double mu, double chiloc_m_sum,
+                int32_t numax, int32_t maxit, double mixing, double conv_abs, int32_t fit_mu, double lam_min_delta,
+                double* out, double* sigma_out, double* G_out) {
+    if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(eom_inputs_ready(ctx));
+    NEED(ctx, ctx->d_sigma_loc != nullptr, "run_sc: Sigma_loc missing (call ldga_gloc)");
+    NEED(ctx, ctx->have_ghat, "run_sc: G missing (call ldga_gloc or ldga_set_gloc)");
+    if (!std::isfinite(lam_m) || !std::isfinite(lam_d)) return ctx_fail(ctx, LDGA_ERR_ARG, "λ must be finite");
+    if (maxit < 1) return ctx_fail(ctx, LDGA_ERR_ARG, "maxit must be >= 1");
+    DeviceGuard g(ctx->device);
+    int nu = std::min(ctx->sp.n_iv, (int)std::floor(3.0 * ctx->Nw / 8.0));   // gen_νω_indices νGrid
+    if (numax >= 1) nu = std::min(nu, (int)numax);
+    if (nu < 1) return ctx_fail(ctx, LDGA_ERR_ARG, "run_sc: no fermionic frequencies for the EoM");
+    const size_t nsig = (size_t)ctx->Nq * nu, ngf = (size_t)ctx->Nq * ctx->Nf;
+    ScBuffers b;
+    TRY(dev_alloc(ctx, &b.sigma_old, nsig));
+    TRY(dev_alloc(ctx, &b.ghat_save, ngf));
+    TRY(dev_alloc(ctx, &b.gloc_save, ngf));
+    // the reference works on deepcopy(h.gLoc_rfft): the handle's G and its transform are restored at the end
+    TRY(copy(ctx, b.ghat_save, ctx->d_ghat, ngf * sizeof(double2)));
+    TRY(copy(ctx, b.gloc_save, ctx->d_gloc, ngf * sizeof(double2)));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_sigma, 0, nsig * sizeof(double2), ctx->stream));
+
+    const double U = ctx->mp.U, nn = ctx->mp.n;
+    const double rhs_c1 = nn / 2.0 * (1.0 - nn / 2.0);
+    double lm = lam_m, ld = lam_d;
+    auto sums = [&](double* lhs, double* ep2) -> int {
+        double r[2];
+        TRY(launch_sum_kw(ctx, LDGA_CH_M, lm, 0, ctx->d_red + 32));
+        TRY(launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33));
+        TRY(copy(ctx, r, ctx->d_red + 32, 2 * sizeof(double)));
+        TRY(sync(ctx));
+        *lhs = (r[1] + r[0]) / 2.0;
+        *ep2 = (U / 2.0) * (r[1] - r[0]) + U * (nn / 2.0 * nn / 2.0);
+        return LDGA_OK;
+    };
+    double lhs_c1 = 0.0, E_pot_2 = 0.0, E_pot_1 = INFINITY, E_kin = INFINITY, n_fill = NAN;
+    TRY(sums(&lhs_c1, &E_pot_2));
+    bool converged = false;
+    int it = 1, iters = 0;
+    double r[4] = {mu, NAN, NAN, NAN};
+    while (true) {
+        if (it > 1 && redo_dm) {
+            // λdm_correction on the current G transform, from the previous root (conditions_new.jl:431-436)
+            DmState s;
+            s.ctx = ctx; s.chiloc_m_sum = chiloc_m_sum; s.numax = nu; s.mu = mu; s.fix_n = fit_mu ? 1 : 0;
+            s.rhs_c1 = rhs_c1;
+            double lmin[2];
+            TRY(launch_lambda_min(ctx, LDGA_CH_M, ctx->d_red + 40));
+            TRY(launch_lambda_min(ctx, LDGA_CH_D, ctx->d_red + 41));
+            TRY(copy(ctx, lmin, ctx->d_red + 40, 2 * sizeof(double)));
+            TRY(sync(ctx));
+            const double xmin[2] = {lmin[0] + lam_min_delta * std::fabs(lmin[0]), lmin[1] + lam_min_delta * std::fabs(lmin[1])};
+            const double start[2] = {lm, ld};
+            double xi[2];
+            int ni = 0;
+            bool failed = false;
+            if (!dm_newton(s, start, xmin, 1e-8, 500, xi, &ni, &failed)) return s.status;
+            // a failed root ends the loop with NaN λ and μ; a found one always counts as valid there
+            // (the inner λ_result's `converged` field is true for every root, conditions_new.jl:314)
+            if (failed || !std::isfinite(xi[0]) || !std::isfinite(xi[1])) { lm = NAN; ld = NAN; mu = NAN; break; }
+            double F[2];
+            if (!dm_residual(s, xi[0], xi[1], F)) return s.status;
+            lm = xi[0]; ld = xi[1]; mu = s.mu;
+        }
+        TRY(copy(ctx, b.sigma_old, ctx->d_sigma, nsig * sizeof(double2)));
+        TRY(eom_device(ctx, lm, ld, nu, 1, chiloc_m_sum));
+        if (mixing != 0.0 && it > 1) {
+            k_sigma_mix<<<2 * 148, 256, 0, ctx->stream>>>(ctx->d_sigma, b.sigma_old, nsig, mixing);
+            LDGA_LAUNCHED(ctx, "k_sigma_mix");
+        }
+        // G_from_Σladder! (μ fit), calc_E, filling_pos, then the G transform for the next EoM
+        TRY(launch_g_ladder(ctx, nu, fit_mu ? 1 : 0, mu, ctx->d_red + 24));
+        TRY(launch_g_ladder_full(ctx, nu, ctx->d_red + 24));
+        TRY(copy(ctx, r, ctx->d_red + 24, 4 * sizeof(double)));
+        TRY(sync(ctx));
+        iters = it;
+        if (std::isnan(r[0])) break;
+        mu = r[0];
+        const double E_pot_1_old = E_pot_1, E_pot_2_old = E_pot_2;
+        E_kin = r[1]; E_pot_1 = r[2]; n_fill = r[3];
+        TRY(copy(ctx, ctx->d_gloc, ctx->d_gladder, ngf * sizeof(double2)));
+        TRY(launch_gloc_transform(ctx, false));
+        TRY(sums(&lhs_c1, &E_pot_2));
+        if (std::fabs(E_pot_1 - E_pot_1_old) < conv_abs && std::fabs(E_pot_2 - E_pot_2_old) < conv_abs) {
+            converged = true;
+            break;
+        }
+        if (it >= maxit) break;
+        it += 1;
+    }
+    if (sigma_out) TRY(copy(ctx, sigma_out, ctx->d_sigma, nsig * sizeof(double2)));
+    if (G_out) TRY(copy(ctx, G_out, ctx->d_gladder, ngf * sizeof(double2)));
+    TRY(copy(ctx, ctx->d_ghat, b.ghat_save, ngf * sizeof(double2)));
+    TRY(copy(ctx, ctx->d_gloc, b.gloc_save, ngf * sizeof(double2)));
+    TRY(sync(ctx));
+    ctx->sigma_numax = nu;
+    // out: λm, λd, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n, μ, sc_converged, iterations, νmax
+    const double vals[12] = {lm, ld, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n_fill, mu, converged ? 1.0 : 0.0,
+                             (double)iters, (double)nu};
+    for (int k = 0; k < 12; ++k) out[k] = vals[k];
+    return LDGA_OK;
 }
 
 int ldga_lambda_dm_evals(const ldga_ctx* ctx, int32_t* n_evals) {

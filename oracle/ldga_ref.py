@@ -985,15 +985,16 @@ def lambda_dm_residual(lam, chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0,
 
 def lambda_dm_correction(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, h: Helper,
                          numax: int = -1, lam_min_delta: float = 1e-4, validate_threshold: float = 1e-8,
-                         lam_init=(0.0, 0.0), atol: float = 1e-8, nsteps: int = 500):
-    """``λdm_correction`` (conditions_new.jl:219-324), plain (non-sc) branch -> LambdaResult."""
+                         lam_init=(0.0, 0.0), atol: float = 1e-8, nsteps: int = 500, mu0: float | None = None):
+    """``λdm_correction`` (conditions_new.jl:219-324), plain (non-sc) branch -> LambdaResult.
+    ``mu0``: starting μ of the μ fits (the reference's keyword μ, default mP.μ)."""
     if chi_m.lam != 0 or chi_d.lam != 0:
         raise RuntimeError("λ parameter already set. Aborting λdm calculation")
     mP = h.mP
     wind, nu_auto = gen_nu_w_indices(chi_m, chi_d, mP, h.sP)
     numax = nu_auto if numax < 1 else min(nu_auto, numax)
     rhs_c1 = mP.n / 2 * (1 - mP.n / 2)
-    state = {"mu": mP.mu}
+    state = {"mu": mP.mu if mu0 is None else mu0}
 
     def residual_f(lam):
         r = lambda_dm_residual(lam, chi_m, gamma_m, chi_d, gamma_d, lambda0, h, numax, state)
@@ -1014,6 +1015,86 @@ def lambda_dm_correction(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, h:
                             G, S, mu, n)
     return LambdaResult(float(root[0]), float(root[1]), "dm", True, False, *(float("nan"),) * 5,
                         None, None, float("nan"), float("nan"))
+
+
+def run_sc(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, mu: float, h: Helper, type: str = "fix",
+           lam_m: float = 0.0, lam_d: float = 0.0, numax: int = -1, maxit: int = 100, mixing: float = 0.2,
+           conv_abs: float = 1e-8, fit_mu: bool = True, lam_min_delta: float = 1e-4) -> LambdaResult:
+    """``run_sc`` (conditions_new.jl:342-407) and its loop ``run_sc!`` (:409-556), update_χ_tail = false,
+    tc = true.  Returns the reference's λ_result (its positional order: converged <- sc_converged)."""
+    import dataclasses
+    mP, kG, sP = h.mP, h.kG, h.sP
+    wind, nu_auto = gen_nu_w_indices(chi_m, chi_d, mP, sP)
+    numax = nu_auto if numax < 1 else min(nu_auto, numax)
+    if type == "pre_m":
+        rhs = lambda_m_rhs(h.imp_density, chi_m, chi_d, kG, mP, sP)
+        lam_m, valid = lambda_m_correction(chi_m, rhs, kG, mP, sP)
+        lam_d = 0.0
+    elif type == "pre_dm":
+        r = lambda_dm_correction(chi_m, gamma_m, chi_d, gamma_d, lambda0, h, numax=numax,
+                                 lam_min_delta=lam_min_delta, validate_threshold=conv_abs)
+        lam_m, lam_d, valid = r.lam_m, r.lam_d, r.sc_converged
+    else:
+        valid = True
+    nan = float("nan")
+    if not (valid and np.isfinite(lam_m) and np.isfinite(lam_d)):
+        return LambdaResult(nan, nan, type, False, False, nan, nan, nan, nan, nan, None, None, nan, nan)
+    redo_dm = type in ("dm", "pre_dm")
+    off = -sP.fft_range[0]
+    grhat = h.grhat
+    S = np.zeros((kG.Nq, numax), dtype=np.complex128)
+    G = None
+    rhs_c1 = mP.n / 2 * (1 - mP.n / 2)
+
+    def sums(lm, ld):
+        cm, cd = chi_m.copy(), chi_d.copy()
+        chi_lambda_inplace(cm, lm)
+        chi_lambda_inplace(cd, ld)
+        xm, xd = sum_kw(kG, cm), sum_kw(kG, cd)
+        return (xd + xm) / 2, (mP.U / 2) * (xd - xm) + mP.U * (mP.n / 2 * mP.n / 2)
+
+    lm, ld = lam_m, lam_d
+    lhs_c1, E_pot_2 = sums(lm, ld)
+    E_pot_1, E_kin, n = np.inf, np.inf, nan
+    converged = False
+    it = 1
+    while True:
+        if it > 1 and redo_dm:
+            hc = dataclasses.replace(h, grhat=grhat)
+            r = lambda_dm_correction(chi_m, gamma_m, chi_d, gamma_d, lambda0, hc, numax=numax,
+                                     lam_min_delta=1e-4, lam_init=(lm, ld), mu0=mu)
+            lm, ld, mu = r.lam_m, r.lam_d, r.mu
+            if not (np.isfinite(lm) and np.isfinite(ld)):
+                break
+        S_work = S.copy()
+        cm, cd = chi_m.copy(), chi_d.copy()
+        chi_lambda_inplace(cm, lm)
+        chi_lambda_inplace(cd, ld)
+        S = calc_Sigma_inner(cm, gamma_m, cd, gamma_d, h.chiloc_m_sum, lambda0, grhat, kG, mP, sP, numax, True)
+        if mixing != 0 and it > 1:
+            S = (1 - mixing) * S + mixing * S_work
+        mu, G = G_from_Sigma_ladder(S, h.sigma_loc, kG, mP, sP.fft_range, fix_n=fit_mu, mu=mu)
+        if np.isnan(mu):
+            break
+        E_pot_1_old, E_pot_2_old = E_pot_1, E_pot_2
+        E_kin, E_pot_1 = calc_E(G[:, off:off + numax], S, mu, kG, mP)
+        n = filling_pos(kG.kintegrate(G[:, off:off + numax], 0), mP.U, mu, mP.beta)
+        _, grhat = G_fft(kG, G)
+        lhs_c1, E_pot_2 = sums(lm, ld)
+        if abs(E_pot_1 - E_pot_1_old) < conv_abs and abs(E_pot_2 - E_pot_2_old) < conv_abs:
+            converged = True
+            break
+        if it >= maxit:
+            break
+        it += 1
+    if type == "fix":
+        lm, ld = 0.0, 0.0      # run_sc! returns its loop-local λ, never set for :fix
+    conv = (converged and np.isfinite(lhs_c1) and np.isfinite(E_pot_2) and abs(rhs_c1 - lhs_c1) <= conv_abs
+            and abs(E_pot_1 - E_pot_2) <= conv_abs)
+    res = LambdaResult(float(lm), float(ld), type, converged, conv, float(E_kin), float(E_pot_1), float(E_pot_2),
+                       rhs_c1, float(lhs_c1), G, S, float(mu), float(n))
+    res.iterations = it
+    return res
 
 
 # =============================================================================================

@@ -302,3 +302,33 @@ def test_batch_chain_uneven_points(require_gpu):
     again = L.λm_chain_batch(hs)
     for a, b in zip(batch, again):
         assert a.λm == b.λm and np.array_equal(a.Σ_ladder, b.Σ_ladder)
+
+
+@pytest.mark.parametrize("sc_type", ["fix", "pre_m", "pre_dm"])
+def test_run_sc(sc_type, require_gpu):
+    """run_sc / run_sc! (conditions_new.jl:342-556): the self-consistent ladder loop on the device
+    (EoM -> mixing -> μ fit -> energies -> transform of G_ladder) against the oracle's loop."""
+    inp = S.make_input(dim=2, ns=8, beta=5.0, U=1.0, n_iv=4, n_iw=4, seed=401)
+    ref = R.run_chain(inp, lambda_type=None)
+    r = ref["h"]
+    g = gpu_chain(inp)
+    h = g["h"]
+    kw = dict(maxit=25, mixing=0.2, conv_abs=1e-8)
+    lam = dict(λm=0.2, λd=0.1) if sc_type == "fix" else {}
+    res = L.run_sc(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], h.mP.μ, h, type=sc_type, **lam, **kw)
+    o = R.run_sc(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"], r.mP.mu, r, type=sc_type,
+                 lam_m=lam.get("λm", 0.0), lam_d=lam.get("λd", 0.0), **kw)
+    assert res.converged == o.converged and res.sc_converged == o.sc_converged
+    if not math.isfinite(o.mu):
+        assert not math.isfinite(res.μ)
+        return
+    assert abs(res.λm - o.lam_m) < 1e-8 and abs(res.λd - o.lam_d) < 1e-8
+    assert abs(res.μ - o.mu) < 1e-8
+    assert rel(res.Σ_ladder, o.Sigma_ladder) < 1e-8
+    for a, b in ((res.EPot_p1, o.EPot_p1), (res.EKin, o.EKin), (res.n, o.n)):
+        assert abs(a - b) <= 1e-8 * max(1.0, abs(b))
+    # the handle's own G transform is restored: the single-shot EoM is unchanged afterwards
+    s1 = L.calc_Σ(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], h, λm=0.2)
+    s0 = R.calc_Sigma(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], r.chiloc_m_sum, ref["lambda0"], r.grhat,
+                      r.kG, r.mP, r.sP, numax=h.sP.n_iν, lam_m=0.2)
+    assert rel(s1, s0) < RTOL
