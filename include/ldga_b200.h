@@ -146,6 +146,17 @@ int ldga_set_chi0(ldga_ctx* ctx, const double* chi0);
 int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* chi_out,
              double* gam_out, int32_t* n_fallback);
 
+/* Vector-Jacobian product of ldga_bse for one channel (the adjoint the reference differentiates
+ * through zgetri in inv!, LapackWrapper.jl:64-72, for calc_χγ, BSETools.jl:192-248): given upstream
+ * gradients of a real loss with respect to that channel's last chi_r [Nq, Nw] (real) and
+ * gamma_r [Nq, Nnu, Nw] (complex, dL/dRe + i dL/dIm), either may be NULL for zero, returns
+ *   Gamma_bar [Nnu, Nnu, Nw] = dL/dGamma_r   and   chi0_bar [Nq, Nnu, Nw] = dL/dchi0
+ * in the same convention (either output may be NULL).  One FP64 adjoint solve per (q, w) with the
+ * untransposed vertex, verified by its backward error; n_flagged (may be NULL) counts solves
+ * above 1e-12.  The forward solution is rebuilt from gamma_r and chi_r, not recomputed. */
+int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const double* gam_bar,
+                 double* Gamma_bar, double* chi0_bar, int32_t* n_flagged);
+
 /* Copy a device-resident array of the handle to `out` (host or device) without recomputing it.
  * No reference counterpart: the reference's arrays live in Julia memory; here they stay in HBM
  * until asked for.  what: one of LDGA_GET_*; channel only for chi and gamma. */

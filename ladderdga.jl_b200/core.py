@@ -917,6 +917,23 @@ def calc_χγ(type_, h_or_Γ, χ0: χ0T, *args):
     return χ, γ
 
 
+def calc_χγ_vjp(type_, h: lDΓAHelper, χ̄=None, γ̄=None):
+    """Vector-Jacobian product of ``calc_χγ(type, h, χ0)`` (BSETools.jl:192-248) at its last call on
+    the GPU handle: upstream gradients of a real loss with respect to χ_r.data [Nq, Nω] and
+    γ_r.data [Nq, Nν, Nω] (complex: ∂L/∂Re + i ∂L/∂Im; None = 0) -> (Γ̄_r [Nν, Nν, Nω], χ̄₀ [Nq, Nν, Nω])."""
+    ch = _channel(type_)
+    ctx = h.ctx
+    xb = None if χ̄ is None else np.asfortranarray(np.asarray(χ̄, dtype=np.float64))
+    gb = None if γ̄ is None else as_fc(γ̄)
+    Gb = _lib.cplx_out((ctx.Nnu, ctx.Nnu, ctx.Nw))
+    c0b = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+    nf = _lib.C.c_int32()
+    ctx.call("ldga_bse_vjp", ch, ptr(xb), ptr(gb), ptr(Gb), ptr(c0b), _lib.C.byref(nf))
+    if nf.value:
+        warnings.warn(f"calc_χγ_vjp: {nf.value} adjoint solves above the backward-error threshold")
+    return Gb, c0b
+
+
 def _log_q0_χ_check(ctx: Context, χ: χT, type_) -> None:
     """``log_q0_χ_check`` (helpers.jl:114-121), kept as a returned value instead of a log line."""
     q0 = 0
@@ -1434,3 +1451,4 @@ F_from_chi = F_from_χ
 calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_χγ_par, collect_χ0, collect_χ, collect_γ
 calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_part
 lambda_m_chain_batch = λm_chain_batch
+calc_chi_gamma_vjp = calc_χγ_vjp

@@ -170,6 +170,19 @@ void free_all(ldga_ctx* c) {
         if (p) cudaFree(p);
 }
 
+// device scratch of one call (e.g. an adjoint), freed on every exit path
+struct DevScratch {
+    std::vector<void*> p;
+    template <typename T>
+    int get(ldga_ctx* ctx, T** out, size_t n) {
+        *out = nullptr;
+        TRY(dev_alloc(ctx, out, n));
+        p.push_back(*out);
+        return LDGA_OK;
+    }
+    ~DevScratch() { for (void* x : p) cudaFree(x); }
+};
+
 int set_sigma_loc(ldga_ctx* ctx, const double* sigma_loc, int n_sigma) {
     const int L = std::max(std::abs(ctx->sp.fft_lo), std::abs(ctx->sp.fft_hi));
     if (n_sigma <= L)
@@ -389,6 +402,35 @@ int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* c
     if (chi_out) TRY(copy(ctx, chi_out, ctx->d_chi[channel], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
     if (gam_out) TRY(copy(ctx, gam_out, ctx->d_gam[channel], (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
     return sync(ctx);
+}
+
+int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const double* gam_bar, double* Gamma_bar,
+                 double* chi0_bar, int32_t* n_flagged) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi0 && ctx->have_Gamma[channel] && ctx->have_chi[channel] && ctx->have_gam[channel],
+         "calc_χγ adjoint: run ldga_bse for this channel first");
+    DeviceGuard g(ctx->device);
+    const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw, qw = (size_t)ctx->Nq * ctx->Nw;
+    const size_t vvw = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw;
+    DevScratch sc;
+    double* d_xb = nullptr;
+    double2 *d_gb = nullptr, *d_c0b = nullptr, *d_y = nullptr, *d_z = nullptr, *d_Gb = nullptr;
+    if (chi_bar) { TRY(sc.get(ctx, &d_xb, qw)); TRY(copy(ctx, d_xb, chi_bar, qw * sizeof(double))); }
+    if (gam_bar) { TRY(sc.get(ctx, &d_gb, qvw)); TRY(copy(ctx, d_gb, gam_bar, qvw * sizeof(double2))); }
+    TRY(sc.get(ctx, &d_c0b, qvw));
+    TRY(sc.get(ctx, &d_y, qvw));
+    TRY(sc.get(ctx, &d_z, qvw));
+    TRY(sc.get(ctx, &d_Gb, vvw));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    TRY(launch_bse_adj(ctx, channel, d_xb, d_gb, d_c0b, d_y, d_z, d_Gb, ctx->d_count + 1));
+    int32_t cnt[2] = {0, 0};
+    TRY(copy(ctx, cnt, ctx->d_count, 2 * sizeof(int32_t)));
+    if (Gamma_bar) TRY(copy(ctx, Gamma_bar, d_Gb, vvw * sizeof(double2)));
+    if (chi0_bar) TRY(copy(ctx, chi0_bar, d_c0b, qvw * sizeof(double2)));
+    TRY(sync(ctx));
+    if (n_flagged) *n_flagged = cnt[1];
+    return LDGA_OK;
 }
 
 int ldga_get(ldga_ctx* ctx, int32_t what, int32_t channel, double* out) {

@@ -1244,6 +1244,278 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Adjoint (vector-Jacobian product) of the BSE step.  For a real loss L with upstream gradients
+// chi_bar (real) and gamma_bar (complex, dL/dRe + i dL/dIm) per (q, w):
+//   forward: B = Gamma(w)^T + diag(d), d = 1/chi0, y = B^-1 1, chi = Re sum y / beta^2,
+//            gamma = y d rf, rf = 1/(1 + s U chi)
+//   y from the forward outputs: y = gamma chi0 / rf (no forward solve is repeated)
+//   chi_bar_tot = chi_bar - s U rf^2 sum_i Re(conj(gamma_bar_i) y_i d_i)
+//   y_bar_i = conj(d_i rf) gamma_bar_i + chi_bar_tot / beta^2
+//   z = B^-H y_bar  <=>  (Gamma(w) + diag(d)) conj(z) = conj(y_bar): the same LU kernel on the
+//       untransposed vertex (one FP64 solve per matrix, verified by its backward error)
+//   B_bar = -z y^H  ->  Gamma_bar(w)[a, b] = -sum_q conj(y_a) z_b  (k_bse_gamma_grad)
+//   chi0_bar_i = -conj(d_i^2) (conj(y_i rf) gamma_bar_i - z_i conj(y_i))
+// This is the chi-bar contraction of the inverse, chi^T chi_bar chi^T, restricted to the single
+// right-hand side the forward pass used.
+struct BseAdjArgs {
+    int nq, nnu, nw, qchunk;
+    double beta, U;
+    int s;
+    const double2* Gamma;     // [N, N, Nw]
+    const double2* chi0;      // [Nq, N, Nw]
+    const double* chi;        // [Nq, Nw]      forward chi_r
+    const double2* gam;       // [Nq, N, Nw]   forward gamma_r
+    const double* chi_bar;    // [Nq, Nw]      (may be null: zero)
+    const double2* gam_bar;   // [Nq, N, Nw]   (may be null: zero)
+    double2* chi0_bar;        // [Nq, N, Nw]   out
+    double2* ybuf;            // [Nq, N, Nw]   out: y
+    double2* zbuf;            // [Nq, N, Nw]   out: z
+    int32_t* flags;           // [Nq, Nw]      1: backward error above 1e-12
+};
+
+template <int N, int T, int MINB>
+__global__ void __launch_bounds__(T * T, MINB) k_bse_adj(const BseAdjArgs a) {
+    using LS = LuSmem<N, T>;
+    constexpr int RT = LS::RT, G = LS::G;
+    constexpr int CT = (N + 1 + T - 1) / T;
+    constexpr int TCN = N % T, CN = N / T;
+    static_assert(T <= 32 && 32 % T == 0, "a row group must sit inside one warp");
+    extern __shared__ double2 sm[];
+    double2* Gsm = sm;                                    // Gamma[j + N*i] at i*N + j
+    const int t = threadIdx.x;
+    const int tr = t / T, tc = t - (t / T) * T;
+    const int lane = t & 31;
+    const int bar = 1;
+    double2* rowbuf = Gsm + N * N;                        // [2][RW]
+    double2* colbuf = rowbuf + 2 * LS::RW;                // [2][CW]
+    double2* pinv = colbuf + 2 * LS::CW;                  // [N]
+    double2* dinv = pinv + N;                             // [N]
+    double2* xsm = dinv + N;                              // [N] solution of (Gamma + D) x = rhs
+    double* red = reinterpret_cast<double*>(xsm + N);     // [8 * G/32]
+    double2* rhs = reinterpret_cast<double2*>(red + 8 * (G / 32) + 2);   // [N] conj(y_bar)
+    double2* yfw = rhs + N;                               // [N] forward y
+
+    const int w = blockIdx.y;
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    {
+        const double2* Gw = a.Gamma + (size_t)w * N * N;
+        for (int e = t; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
+    }
+    __syncthreads();
+    const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
+
+    for (int q = q0; q < q1; ++q) {
+        const size_t cq = (size_t)q + (size_t)a.nq * w;
+        const double chi = a.chi[cq];
+        const double f = 1.0 + a.s * a.U * chi, rf = 1.0 / f;
+        // ---- y from the forward outputs, and y_bar
+        double s1 = 0.0;
+        for (int i = t; i < N; i += G) {
+            const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+            const double2 c0 = a.chi0[ci];
+            const double2 d = cinv(c0);
+            const double2 y = cscale(cmul(a.gam[ci], c0), f);
+            dinv[i] = d;
+            yfw[i] = y;
+            if (a.gam_bar) {
+                const double2 gb = a.gam_bar[ci], yd = cmul(y, d);
+                s1 += gb.x * yd.x + gb.y * yd.y;   // Re(conj(gb) y d)
+            }
+        }
+        {
+            double v[1] = {s1};
+            const int op[1] = {0};
+            group_reduce<1, G>(v, op, red, bar, t);   // its barriers also publish dinv / yfw
+            s1 = v[0];
+        }
+        const double xbar = (a.chi_bar ? a.chi_bar[cq] : 0.0) - a.s * a.U * rf * rf * s1;
+        for (int i = t; i < N; i += G) {
+            const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+            double2 yb = make_double2(xbar / (a.beta * a.beta), 0.0);
+            if (a.gam_bar) yb = cadd(yb, cmul(cconj(cscale(dinv[i], rf)), a.gam_bar[ci]));
+            rhs[i] = cconj(yb);
+        }
+        named_barrier(bar, G);
+        // ---- tile of [A | conj(y_bar)], A_ij = Gamma[i, j] + delta_ij d_i (the untransposed vertex)
+        double2 b[RT][CT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+#pragma unroll
+            for (int c = 0; c < CT; ++c) {
+                const int j = tc + T * c;
+                double2 v = dmk(0.0, 0.0);
+                if (i < N) {
+                    if (j < N) {
+                        v = Gsm[j * N + i];
+                        if (c == ra && tr == tc) v = cadd(v, dinv[i]);
+                    } else if (j == N) {
+                        v = rhs[i];
+                    }
+                }
+                b[ra][c] = v;
+            }
+        }
+        // ---- forward elimination and block back substitution (as k_bse_lu)
+#pragma unroll
+        for (int kc = 0; kc < RT; ++kc) {
+            const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+#pragma unroll 1
+            for (int ktc = 0; ktc < kend; ++ktc) {
+                const int k = ktc + T * kc;
+                double2* rb = rowbuf + (k & 1) * LS::RW;
+                double2* cb = colbuf + (k & 1) * LS::CW;
+                if (tr == ktc) {
+                    double2 p;
+                    p.x = __shfl_sync(gmask, b[kc][kc].x, ktc, T);
+                    p.y = __shfl_sync(gmask, b[kc][kc].y, ktc, T);
+                    const double2 inv = vinv(p);
+                    if (tc == ktc) pinv[k] = inv;
+#pragma unroll
+                    for (int c = kc; c < CT; ++c) rb[tc + T * c] = vmul<double2>(b[kc][c], inv);
+                }
+                if (tc == ktc) {
+#pragma unroll
+                    for (int ra = kc; ra < RT; ++ra) cb[tr + T * ra] = b[ra][kc];
+                }
+                named_barrier(bar, G);
+                double2 u[CT];
+#pragma unroll
+                for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
+#pragma unroll
+                for (int ra = kc; ra < RT; ++ra) {
+                    if (ra > kc || tr != ktc) {
+                        const double2 m = cb[tr + T * ra];
+#pragma unroll
+                        for (int c = kc; c < CT; ++c) {
+                            if (c > kc || tc > ktc) vfnms<double2>(b[ra][c], m, u[c]);
+                        }
+                    }
+                }
+            }
+        }
+        double2 acc[RT];
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) acc[ra] = dmk(0.0, 0.0);
+#pragma unroll
+        for (int r = RT - 1; r >= 0; --r) {
+            const int nb = (N - T * r) < T ? (N - T * r) : T;
+            double2 sv = acc[r];
+#pragma unroll
+            for (int o = 1; o < T; o <<= 1) {
+                sv.x += __shfl_xor_sync(0xffffffffu, sv.x, o);
+                sv.y += __shfl_xor_sync(0xffffffffu, sv.y, o);
+            }
+            if (tc == TCN && tr < nb) xsm[T * r + tr] = cmul(csub(b[r][CN], sv), pinv[T * r + tr]);
+            named_barrier(bar, G);
+            if (r > 0 && T * r + tc < N) {
+                const double2 xj = xsm[T * r + tc];
+#pragma unroll
+                for (int ra = 0; ra < r; ++ra) acc[ra] = cadd(acc[ra], cmul(b[ra][r], xj));
+            }
+        }
+        // ---- FP64 backward error |rhs - A x| / (|A| |x| + |rhs|)
+        double st[4] = {0.0, 0.0, 0.0, 0.0};
+        const int op[4] = {1, 1, 1, 1};
+#pragma unroll
+        for (int ra = 0; ra < RT; ++ra) {
+            const int i = tr + T * ra;
+            double2 accr = dmk(0.0, 0.0);
+            double rown = 0.0;
+            if (i < N) {
+#pragma unroll
+                for (int c = 0; c < CT; ++c) {
+                    const int j = tc + T * c;
+                    if (j < N) {
+                        double2 gv = Gsm[j * N + i];
+                        if (c == ra && tr == tc) gv = cadd(gv, dinv[i]);
+                        accr = cadd(accr, cmul(gv, xsm[j]));
+                        rown += fabs(gv.x) + fabs(gv.y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < T; o <<= 1) {
+                accr.x += __shfl_xor_sync(0xffffffffu, accr.x, o);
+                accr.y += __shfl_xor_sync(0xffffffffu, accr.y, o);
+                rown += __shfl_xor_sync(0xffffffffu, rown, o);
+            }
+            if (i < N && tc == 0) {
+                const double2 r = csub(rhs[i], accr), xv = xsm[i];
+                st[0] = fmax(st[0], fabs(r.x) + fabs(r.y));
+                st[1] = fmax(st[1], fabs(xv.x) + fabs(xv.y));
+                st[2] = fmax(st[2], rown);
+                st[3] = fmax(st[3], fabs(rhs[i].x) + fabs(rhs[i].y));
+            }
+        }
+        group_reduce<4, G>(st, op, red, bar, t);
+        const double berr = st[0] / (st[2] * st[1] + st[3] + 1e-300);
+        if (t == 0) a.flags[cq] = (isfinite(berr) && berr <= 1e-12) ? 0 : 1;
+        // ---- z = conj(x); chi0_bar; y and z for the vertex gradient
+        for (int i = t; i < N; i += G) {
+            const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)N * w);
+            const double2 z = cconj(xsm[i]), y = yfw[i], d = dinv[i];
+            double2 db = cscale(cmul(z, cconj(y)), -1.0);                        // from B
+            if (a.gam_bar) db = cadd(db, cmul(cconj(cscale(y, rf)), a.gam_bar[ci]));   // from gamma
+            a.chi0_bar[ci] = cscale(cmul(cconj(cmul(d, d)), db), -1.0);
+            a.ybuf[ci] = y;
+            a.zbuf[ci] = z;
+        }
+        named_barrier(bar, G);
+    }
+}
+
+// Gamma_bar(w)[a, b] = -sum_q conj(y[q, a, w]) z[q, b, w], one CTA per (w, 32 x 32 output tile);
+// q is staged through shared memory in chunks, summed in a fixed order.
+__global__ void __launch_bounds__(256) k_bse_gamma_grad(int nq, int n, const double2* __restrict__ y,
+                                                        const double2* __restrict__ z, double2* __restrict__ gbar) {
+    constexpr int TQ = 16;
+    __shared__ double2 ys[TQ][32], zs[TQ][32];
+    const int w = blockIdx.z;
+    const int a0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+    const int ta = threadIdx.x & 31, tb = threadIdx.x >> 5;   // 32 x 8 threads, 4 outputs each
+    double2 acc[4] = {dmk(0, 0), dmk(0, 0), dmk(0, 0), dmk(0, 0)};
+    for (int qc = 0; qc < nq; qc += TQ) {
+        for (int e = threadIdx.x; e < TQ * 32; e += blockDim.x) {
+            const int qq = e / 32, jj = e % 32;
+            const int qi = qc + qq;
+            const bool ok = qi < nq;
+            ys[qq][jj] = (ok && a0 + jj < n) ? y[(size_t)qi + (size_t)nq * (a0 + jj + (size_t)n * w)] : dmk(0, 0);
+            zs[qq][jj] = (ok && b0 + jj < n) ? z[(size_t)qi + (size_t)nq * (b0 + jj + (size_t)n * w)] : dmk(0, 0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int qq = 0; qq < TQ; ++qq) {
+            const double2 ya = cconj(ys[qq][ta]);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[r] = cadd(acc[r], cmul(ya, zs[qq][tb + 8 * r]));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int aa = a0 + ta, bb = b0 + tb + 8 * r;
+        if (aa < n && bb < n) gbar[(size_t)aa + (size_t)n * (bb + (size_t)n * w)] = cscale(acc[r], -1.0);
+    }
+}
+
+template <int N, int T, int MINB>
+int run_bse_adj(ldga_ctx* ctx, const BseAdjArgs& a0) {
+    BseAdjArgs a = a0;
+    const size_t sm = (size_t)N * N * sizeof(double2) + LuSmem<N, T>::bytes + 2 * N * sizeof(double2) + 16;
+    auto kern = k_bse_adj<N, T, MINB>;
+    LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+    int chunk = 4;
+    while (chunk > 1 && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) --chunk;
+    a.qchunk = chunk;
+    dim3 grid((a.nq + chunk - 1) / chunk, a.nw);
+    kern<<<grid, T * T, sm, ctx->stream>>>(a);
+    LDGA_LAUNCHED(ctx, "k_bse_adj");
+    return LDGA_OK;
+}
+
 __device__ __forceinline__ double block_sum_det(double v, double* red) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -1501,6 +1773,44 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     }
     // matrices that stayed non-finite after the pivoted solve, accumulated into *d_fail
     k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, d_fail);
+    LDGA_LAUNCHED(ctx, "k_count_flags");
+    return LDGA_OK;
+}
+
+int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const double2* gam_bar, double2* chi0_bar,
+                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail) {
+    BseAdjArgs a;
+    a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
+    a.beta = ctx->mp.beta; a.U = ctx->mp.U;
+    a.s = channel == LDGA_CH_D ? -1 : 1;
+    a.Gamma = ctx->d_Gamma[channel];
+    a.chi0 = ctx->d_chi0;
+    a.chi = ctx->d_chi[channel];
+    a.gam = ctx->d_gam[channel];
+    a.chi_bar = chi_bar; a.gam_bar = gam_bar;
+    a.chi0_bar = chi0_bar; a.ybuf = ybuf; a.zbuf = zbuf;
+    a.flags = ctx->d_flags;
+    int st = LDGA_OK;
+    switch (ctx->Nnu) {
+        case 4: st = run_bse_adj<4, 8, 4>(ctx, a); break;
+        case 6: st = run_bse_adj<6, 8, 4>(ctx, a); break;
+        case 8: st = run_bse_adj<8, 8, 4>(ctx, a); break;
+        case 10: st = run_bse_adj<10, 8, 4>(ctx, a); break;
+        case 12: st = run_bse_adj<12, 8, 4>(ctx, a); break;
+        case 16: st = run_bse_adj<16, 8, 4>(ctx, a); break;
+        case 20: st = run_bse_adj<20, 8, 4>(ctx, a); break;
+        case 30: st = run_bse_adj<30, 8, 4>(ctx, a); break;
+        case 40: st = run_bse_adj<40, 8, 6>(ctx, a); break;
+        case 60: st = run_bse_adj<60, 16, 1>(ctx, a); break;
+        default: return ctx_fail(ctx, LDGA_ERR_ARG, "BSE adjoint: fermionic box " + std::to_string(ctx->Nnu) +
+                                                        " not built (4..60 even sizes of the tiled kernels)");
+    }
+    if (st != LDGA_OK) return st;
+    const int n = ctx->Nnu;
+    dim3 g2((n + 31) / 32, (n + 31) / 32, ctx->Nw);
+    k_bse_gamma_grad<<<g2, 256, 0, ctx->stream>>>(ctx->Nq, n, ybuf, zbuf, gamma_bar);
+    LDGA_LAUNCHED(ctx, "k_bse_gamma_grad");
+    k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, ctx->Nq * ctx->Nw, d_fail);
     LDGA_LAUNCHED(ctx, "k_count_flags");
     return LDGA_OK;
 }

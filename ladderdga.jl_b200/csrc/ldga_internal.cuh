@@ -182,6 +182,10 @@ int launch_bubble(ldga_ctx* ctx);
 // BSE for one channel; enqueues the fallback for flagged matrices on the device (no host sync).
 // d_fail (device int32) receives the number of matrices that stayed unsolved.
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail);
+// Adjoint of one BSE channel: chi0_bar, y and z buffers [Nq, Nnu, Nw], Gamma_bar [Nnu, Nnu, Nw]; d_fail
+// receives the number of adjoint solves above the backward-error threshold.
+int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const double2* gam_bar, double2* chi0_bar,
+                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail);
 int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp);
 int launch_lambda0(ldga_ctx* ctx);
 // EoM forward + inverse.  lam_*_dev (may be null) are device scalars added to lam_m / lam_d.

@@ -415,6 +415,43 @@ def calc_chi_gamma(rtype: str, Gamma: np.ndarray, chi0: np.ndarray, mP: ModelPar
     return chi, gam
 
 
+def calc_chi_gamma_vjp(rtype: str, Gamma: np.ndarray, chi0: np.ndarray, mP: ModelParameters,
+                       chi_bar=None, gamma_bar=None):
+    """Adjoint of ``calc_chi_gamma`` (the reference's calc_χγ with inv!, BSETools.jl:192-248) for a real
+    loss: upstream chi_bar [Nq, Nw] (real) and gamma_bar [Nq, Nnu, Nw] (dL/dRe + i dL/dIm) ->
+    (Gamma_bar [Nnu, Nnu, Nw], chi0_bar [Nq, Nnu, Nw]) in the same convention.  Written from the
+    forward's matrix calculus with numpy's dense solver: the FP64 reference gradient of the adjoint.
+    With A = Gamma + diag(1/chi0) (the reference's matrix), X = A^-1, u = X^T 1 (the column sums):
+    chi = Re sum u / beta^2, gamma = u / (chi0 (1 + s U chi)), and dX = -X dA X."""
+    s = -1 if rtype == "d" else 1
+    Nq, nnu, nw = chi0.shape
+    beta, U = mP.beta, mP.U
+    xb = np.zeros((Nq, nw)) if chi_bar is None else np.asarray(chi_bar, dtype=np.float64)
+    gb = np.zeros((Nq, nnu, nw), dtype=np.complex128) if gamma_bar is None else np.asarray(gamma_bar)
+    Gbar = np.zeros_like(Gamma, dtype=np.complex128)
+    c0bar = np.zeros((Nq, nnu, nw), dtype=np.complex128)
+    idx = np.arange(nnu)
+    one = np.ones(nnu)
+    for wi in range(nw):
+        A = np.broadcast_to(Gamma[:, :, wi], (Nq, nnu, nnu)).copy()
+        d = 1.0 / chi0[:, :, wi]
+        A[:, idx, idx] += d
+        u = np.linalg.solve(np.transpose(A, (0, 2, 1)), np.broadcast_to(one, (Nq, nnu))[..., None])[..., 0]
+        chi = np.real(u.sum(axis=1)) / beta**2
+        rf = 1.0 / (1.0 + s * U * chi)
+        g = gb[:, :, wi]
+        s1 = np.sum(np.real(np.conj(g) * u * d), axis=1)
+        xbt = xb[:, wi] - s * U * rf**2 * s1
+        ubar = np.conj(d * rf[:, None]) * g + (xbt / beta**2)[:, None]
+        # u = A^-T 1: dL = Re <ubar, du>, du = -A^-T dA^T u  ->  Abar = -conj(u) z^T with A^* z = ubar
+        z = np.linalg.solve(np.conj(A), ubar[..., None])[..., 0]
+        Abar = -np.einsum("qa,qb->qab", np.conj(u), z)
+        Gbar[:, :, wi] = Abar.sum(axis=0)
+        dbar = Abar[:, idx, idx] + np.conj(u * rf[:, None]) * g
+        c0bar[:, :, wi] = -np.conj(d * d) * dbar
+    return Gbar, c0bar
+
+
 def calc_lambda0(chi0: np.ndarray, F: np.ndarray, mP: ModelParameters, sP: SimulationParameters):
     """``calc_λ0`` plain branch (BSETools.jl:129-141): lambda0[q,nu',w] = chi0 * sum_nu F / beta^2."""
     sh = sP.n_iv_shell
