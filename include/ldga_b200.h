@@ -157,6 +157,16 @@ int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* c
 int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const double* gam_bar,
                  double* Gamma_bar, double* chi0_bar, int32_t* n_flagged);
 
+/* Vector-Jacobian product of ldga_eom (calc_Σ, ladderDGATools_singleCore.jl:49-136) at (lam_m,
+ * lam_d, numax, tc) on the handle's current chi, gamma, lambda_0 and G transform: given the
+ * upstream gradient of a real loss with respect to Sigma_ladder [Nq, numax] (complex, dL/dRe +
+ * i dL/dIm), returns dL/d chi_m, dL/d chi_d [Nq, Nw] (real; through the λ correction and the tail
+ * term's sum_kω) and dL/d gamma_m, dL/d gamma_d, dL/d lambda_0 [Nq, Nnu, Nw] (complex; zero at the
+ * ν the EoM does not read).  Any output may be NULL.  Each (ν_n, ω) term is one transform-product-
+ * transform pass, the adjoint of the forward's convolution. */
+int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, const double* sigma_bar,
+                 double* chi_m_bar, double* gam_m_bar, double* chi_d_bar, double* gam_d_bar, double* lambda0_bar);
+
 /* Copy a device-resident array of the handle to `out` (host or device) without recomputing it.
  * No reference counterpart: the reference's arrays live in Julia memory; here they stay in HBM
  * until asked for.  what: one of LDGA_GET_*; channel only for chi and gamma. */

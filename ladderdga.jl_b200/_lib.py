@@ -26,7 +26,7 @@ EXPORTS = [
     "ldga_set_lambda0", "ldga_sum_kw", "ldga_sum_wk", "ldga_lambda_min", "ldga_eom", "ldga_eom_parts",
     "ldga_lambda_m", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
     "ldga_lambda_dm_evals", "ldga_set_stream", "ldga_profile", "ldga_stage_times", "ldga_launch_count",
-    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp",
+    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp", "ldga_eom_vjp",
 ]
 GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
 STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
@@ -117,6 +117,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_chain_m": (C.c_int, [P, P, I32, P, P, P, P, I32, D, D, I32, P, P, P, P]),
         "ldga_batch_chain_m": (C.c_int, [I32, P, P, I32, PI32]),
         "ldga_bse_vjp": (C.c_int, [P, I32, P, P, P, P, PI32]),
+        "ldga_eom_vjp": (C.c_int, [P, D, D, I32, I32, P, P, P, P, P, P]),
         "ldga_run_sc": (C.c_int, [P, D, D, I32, D, D, I32, I32, D, D, I32, D, P, P, P]),
         "ldga_set_sigma": (C.c_int, [P, P, I32]),
         "ldga_calc_E": (C.c_int, [P, P, P, I32, D, PD, PD]),
@@ -136,9 +137,15 @@ def ptr(a) -> C.c_void_p | None:
     if isinstance(a, np.ndarray):
         if not (a.flags.f_contiguous or a.flags.c_contiguous):
             raise ValueError("array must be contiguous")
-        return C.c_void_p(a.ctypes.data)
+        v = C.c_void_p(a.ctypes.data)
+        # the pointer owns a reference: `ptr(as_fc(x))` passes a temporary copy, which would
+        # otherwise be freed (and its first bytes reused by the allocator) before the C call reads it
+        v._owner = a
+        return v
     if hasattr(a, "data_ptr"):
-        return C.c_void_p(a.data_ptr())
+        v = C.c_void_p(a.data_ptr())
+        v._owner = a
+        return v
     raise TypeError(f"unsupported buffer type {type(a)}")
 
 

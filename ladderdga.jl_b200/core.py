@@ -997,6 +997,25 @@ def calc_Σ(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, νmax: 
     return out
 
 
+def calc_Σ_vjp(Σ̄, χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, νmax: int | None = None, λm: float = 0.0,
+               λd: float = 0.0, tc: bool = True):
+    """Vector-Jacobian product of ``calc_Σ`` (ladderDGATools_singleCore.jl:108-136) on the GPU handle:
+    the upstream gradient of a real loss with respect to Σ_ladder [Nq, νmax] (∂L/∂Re + i ∂L/∂Im)
+    -> (χ̄m, γ̄m, χ̄d, γ̄d, λ̄₀) with respect to the arrays calc_Σ reads (χ before the λ correction)."""
+    S = as_fc(Σ̄)
+    νmax = S.shape[1] if νmax is None else νmax
+    _prepare_eom(h, χm, γm, χd, γd, λ0)
+    ctx = h.ctx
+    xmb = np.empty((ctx.Nq, ctx.Nw), order="F")
+    xdb = np.empty((ctx.Nq, ctx.Nw), order="F")
+    gmb = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+    gdb = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+    l0b = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+    ctx.call("ldga_eom_vjp", χm._device_λ(λm), χd._device_λ(λd), νmax, int(bool(tc)), ptr(S), ptr(xmb), ptr(gmb),
+             ptr(xdb), ptr(gdb), ptr(l0b))
+    return xmb, gmb, xdb, gdb, l0b
+
+
 def calc_Σ_parts(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, tc: bool = True, λm: float = 0.0,
                  λd: float = 0.0) -> np.ndarray:
     """``calc_Σ_parts`` (ladderDGATools_singleCore.jl:149-189) -> [q, ν_n, 7]."""
@@ -1451,4 +1470,4 @@ F_from_chi = F_from_χ
 calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_χγ_par, collect_χ0, collect_χ, collect_γ
 calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_part
 lambda_m_chain_batch = λm_chain_batch
-calc_chi_gamma_vjp = calc_χγ_vjp
+calc_chi_gamma_vjp, calc_Sigma_vjp = calc_χγ_vjp, calc_Σ_vjp

@@ -594,6 +594,38 @@ int ldga_eom(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t t
     return sync(ctx);
 }
 
+int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, const double* sigma_bar,
+                 double* chi_m_bar, double* gam_m_bar, double* chi_d_bar, double* gam_d_bar, double* lambda0_bar) {
+    if (!ctx || !sigma_bar) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(eom_inputs_ready(ctx));
+    if (!std::isfinite(lam_m) || !std::isfinite(lam_d)) return ctx_fail(ctx, LDGA_ERR_ARG, "λ must be finite");
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
+    DeviceGuard g(ctx->device);
+    const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw, qw = (size_t)ctx->Nq * ctx->Nw;
+    const size_t nsb = (size_t)ctx->Nq * numax;
+    DevScratch sc;
+    double2 *d_sb = nullptr, *d_shat = nullptr, *d_gm = nullptr, *d_gd = nullptr, *d_l0 = nullptr;
+    double *d_xm = nullptr, *d_xd = nullptr, *d_cm = nullptr, *d_cd = nullptr;
+    TRY(sc.get(ctx, &d_sb, nsb));
+    TRY(copy(ctx, d_sb, sigma_bar, nsb * sizeof(double2)));
+    TRY(sc.get(ctx, &d_shat, nsb));
+    TRY(sc.get(ctx, &d_cm, nsb * ctx->Nw));
+    TRY(sc.get(ctx, &d_cd, nsb * ctx->Nw));
+    if (gam_m_bar) { TRY(sc.get(ctx, &d_gm, qvw)); LDGA_CUDA(ctx, cudaMemsetAsync(d_gm, 0, qvw * sizeof(double2), ctx->stream)); }
+    if (gam_d_bar) { TRY(sc.get(ctx, &d_gd, qvw)); LDGA_CUDA(ctx, cudaMemsetAsync(d_gd, 0, qvw * sizeof(double2), ctx->stream)); }
+    if (lambda0_bar) { TRY(sc.get(ctx, &d_l0, qvw)); LDGA_CUDA(ctx, cudaMemsetAsync(d_l0, 0, qvw * sizeof(double2), ctx->stream)); }
+    if (chi_m_bar) TRY(sc.get(ctx, &d_xm, qw));
+    if (chi_d_bar) TRY(sc.get(ctx, &d_xd, qw));
+    TRY(launch_eom_vjp(ctx, numax, lam_m, lam_d, tc, d_sb, d_gm, d_gd, d_l0, d_xm, d_xd, d_shat, d_cm, d_cd));
+    if (gam_m_bar) TRY(copy(ctx, gam_m_bar, d_gm, qvw * sizeof(double2)));
+    if (gam_d_bar) TRY(copy(ctx, gam_d_bar, d_gd, qvw * sizeof(double2)));
+    if (lambda0_bar) TRY(copy(ctx, lambda0_bar, d_l0, qvw * sizeof(double2)));
+    if (chi_m_bar) TRY(copy(ctx, chi_m_bar, d_xm, qw * sizeof(double)));
+    if (chi_d_bar) TRY(copy(ctx, chi_d_bar, d_xd, qw * sizeof(double)));
+    return sync(ctx);
+}
+
 int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum, double* parts_out) {
     if (!ctx || !parts_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
     TRY(eom_inputs_ready(ctx));

@@ -248,6 +248,141 @@ __global__ void __launch_bounds__(kThreads) k_eom_inverse(
 }
 
 // ---------------------------------------------------------------------------------------------
+// Adjoint of the EoM (calc_Σ, ladderDGATools_singleCore.jl:49-136) for a real loss with upstream
+// Sbar[q, n] = dL/dRe Σ + i dL/dIm Σ over the stored (irreducible) values.  The forward is
+//   Σ(q, n) = (1/(β N_k²)) S( Σ_ω S(K(·, n, ω)) Ĝ(ν_n + ω) )(q) + tail(n) + Hartree,
+// and on symmetric functions the transform satisfies Sᵀ = kMult S kMult⁻¹, so
+//   K̄(q, n, ω) = kMult(q)/(β N_k²) S( conj(Ĝ(ν_n + ω)) · S(Sbar(·, n)/kMult) )(q),
+// the same transform-product-transform shape as the bubble.  From K = eom(γm, γd, χm^λ, χd^λ, λ₀):
+//   γ̄m = 1.5 U (1 + U χm^λ) K̄,  γ̄d = -0.5 U (1 - U χd^λ) K̄,  λ̄₀ = U K̄,
+//   χ̄m^λ += Σ_n Re(conj(K̄) 1.5 U² γm),  χ̄d^λ += Σ_n Re(conj(K̄) 0.5 U² γd),
+// plus, with the tail correction, χ̄m^λ(q, ω) += s̄ kMult(q)/(β N_k) with s̄ = U Σ Im(Sbar)/ν_n
+// (the tail is -U(sum_kω χm^λ - χloc_m_sum)/(iν_n)), and finally χ̄ = χ̄^λ/(λχ + 1)².
+// ---------------------------------------------------------------------------------------------
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_vjp_sbar(const TMat<M> T, int numax, const double* __restrict__ kmult,
+                                                       const double2* __restrict__ sbar, double2* __restrict__ shat) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, numax - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        bufA[p * NQ + q] = cscale(sbar[(size_t)(p0 + p) * NQ + q], 1.0 / kmult[q]);
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        shat[(size_t)(p0 + p) * NQ + q] = v;
+    });
+}
+
+struct EomVjpArgs {
+    int nnu, nw, n_iv, n_iw, shift, fft_lo, numax;
+    double U, lam_m, lam_d, scale;   // scale = 1/(beta N_k^2)
+};
+
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_eom_vjp(
+    const TMat<M> T, const EomVjpArgs a, const double* __restrict__ kmult, const double2* __restrict__ ghat,
+    const double2* __restrict__ shat, const double* __restrict__ chi_m, const double2* __restrict__ gam_m,
+    const double* __restrict__ chi_d, const double2* __restrict__ gam_d, double2* __restrict__ gm_bar,
+    double2* __restrict__ gd_bar, double2* __restrict__ l0_bar, double* __restrict__ cm, double* __restrict__ cd) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int total = a.numax * a.nw;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, total - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    __shared__ int s_vi[16];
+    if (threadIdx.x < np) {
+        const int pi = p0 + threadIdx.x;
+        const int wi = pi / a.numax, n = pi - wi * a.numax;
+        const int v0 = a.n_iv + a.shift * ((wi - a.n_iw) / 2);          // ν0Index_of_ωIndex - 1
+        const int len = min(a.numax, 2 * a.n_iv - v0);
+        s_vi[threadIdx.x] = (n < len && v0 + n >= 0) ? v0 + n : -1;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int pi = p0 + p;
+        const int wi = pi / a.numax, n = pi - wi * a.numax;
+        const int wn = wi - a.n_iw;
+        double2 v = make_double2(0.0, 0.0);
+        if (s_vi[p] >= 0) v = cmul(shat[(size_t)n * NQ + q], cconj(ghat[(size_t)(n + wn - a.fft_lo) * NQ + q]));
+        bufA[p * NQ + q] = v;
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        const int pi = p0 + p;
+        const int wi = pi / a.numax, n = pi - wi * a.numax;
+        const int vi = s_vi[p];
+        const size_t cslot = (size_t)n * NQ * a.nw + (size_t)q + (size_t)NQ * wi;
+        if (vi < 0) {
+            cm[cslot] = 0.0;
+            cd[cslot] = 0.0;
+            return;
+        }
+        const double2 kb = cscale(v, kmult[q] * a.scale);
+        const size_t iq = (size_t)q + (size_t)NQ * wi;
+        const size_t iv = (size_t)q + (size_t)NQ * (vi + (size_t)a.nnu * wi);
+        const double U = a.U;
+        const double xm = chi_lam(chi_m[iq], a.lam_m), xd = chi_lam(chi_d[iq], a.lam_d);
+        if (gm_bar) gm_bar[iv] = cscale(kb, 1.5 * U * (1.0 + U * xm));
+        if (gd_bar) gd_bar[iv] = cscale(kb, -0.5 * U * (1.0 - U * xd));
+        if (l0_bar) l0_bar[iv] = cscale(kb, U);
+        const double2 gm = gam_m[iv], gd = gam_d[iv];
+        cm[cslot] = 1.5 * U * U * (kb.x * gm.x + kb.y * gm.y);    // Re(conj(kb) gm) 1.5 U^2
+        cd[cslot] = 0.5 * U * U * (kb.x * gd.x + kb.y * gd.y);
+    });
+}
+
+// s̄ = U Σ_{q,n} Im(Sbar(q, n)) / ν_n, one CTA, fixed order
+__global__ void __launch_bounds__(256) k_vjp_tail(int nq, int numax, double beta, double U,
+                                                   const double2* __restrict__ sbar, double* __restrict__ out) {
+    __shared__ double red[8];
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < nq * numax; e += blockDim.x) {
+        const int n = e / nq;
+        acc += sbar[e].y / ((2.0 * n + 1.0) * M_PI / beta);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int i = 0; i < 8; ++i) r += red[i];
+        out[0] = U * r;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_eom_vjp_chi(int nq, int nw, int numax, double lam_m, double lam_d, double tail_w,
+                                                      const double* __restrict__ kmult, const double* __restrict__ sb_dev,
+                                                      const double* __restrict__ chi_m, const double* __restrict__ chi_d,
+                                                      const double* __restrict__ cm, const double* __restrict__ cd,
+                                                      double* __restrict__ xm_bar, double* __restrict__ xd_bar) {
+    const size_t n_qw = (size_t)nq * nw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_qw; e += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(e % nq);
+        double am = 0.0, ad = 0.0;
+        for (int n = 0; n < numax; ++n) {
+            am += cm[(size_t)n * n_qw + e];
+            ad += cd[(size_t)n * n_qw + e];
+        }
+        if (tail_w != 0.0) am += sb_dev[0] * kmult[q] * tail_w;
+        const double fm = lam_m * chi_m[e] + 1.0, fd = lam_d * chi_d[e] + 1.0;
+        if (xm_bar) xm_bar[e] = am / (fm * fm);
+        if (xd_bar) xd_bar[e] = ad / (fd * fd);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host-side dispatch on (DIM, M)
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M>
@@ -335,6 +470,47 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
     return LDGA_OK;
 }
 
+template <int DIM, int M>
+int run_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, const double2* sbar,
+                double2* gm_bar, double2* gd_bar, double2* l0_bar, double* xm_bar, double* xd_bar, double2* shat,
+                double* cm, double* cd) {
+    {   // Ŝbar = S(Sbar / kMult)
+        const int np = pairs_per_cta<DIM, M>(numax);
+        const size_t sm = smem_bytes<DIM, M>(np);
+        auto kern = k_vjp_sbar<DIM, M>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        dim3 grid((numax + np - 1) / np, np);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, ctx->d_kmult, sbar, shat);
+        LDGA_LAUNCHED(ctx, "k_vjp_sbar");
+    }
+    {
+        const int total = numax * ctx->Nw;
+        const int np = pairs_per_cta<DIM, M>(total);
+        const size_t sm = smem_bytes<DIM, M>(np);
+        auto kern = k_eom_vjp<DIM, M>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        EomVjpArgs a;
+        a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
+        a.fft_lo = ctx->fft_lo; a.numax = numax; a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d;
+        a.scale = 1.0 / (ctx->mp.beta * (double)ctx->Nk * (double)ctx->Nk);
+        dim3 grid((total + np - 1) / np, np);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_kmult, ctx->d_ghat, shat, ctx->d_chi[0],
+                                                   ctx->d_gam[0], ctx->d_chi[1], ctx->d_gam[1], gm_bar, gd_bar, l0_bar,
+                                                   cm, cd);
+        LDGA_LAUNCHED(ctx, "k_eom_vjp");
+    }
+    if (tc) {
+        k_vjp_tail<<<1, 256, 0, ctx->stream>>>(ctx->Nq, numax, ctx->mp.beta, ctx->mp.U, sbar, ctx->d_red + 60);
+        LDGA_LAUNCHED(ctx, "k_vjp_tail");
+    }
+    const double tail_w = tc ? 1.0 / (ctx->mp.beta * (double)ctx->Nk) : 0.0;
+    k_eom_vjp_chi<<<2 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nw, numax, lam_m, lam_d, tail_w, ctx->d_kmult,
+                                                    ctx->d_red + 60, ctx->d_chi[0], ctx->d_chi[1], cm, cd, xm_bar,
+                                                    xd_bar);
+    LDGA_LAUNCHED(ctx, "k_eom_vjp_chi");
+    return LDGA_OK;
+}
+
 }  // namespace
 
 #define LDGA_CASE(D, MM)                                  \
@@ -379,3 +555,11 @@ int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const doubl
     return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
 }
 
+int launch_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, const double2* sbar,
+                   double2* gm_bar, double2* gd_bar, double2* l0_bar, double* xm_bar, double* xd_bar, double2* shat,
+                   double* cm, double* cd) {
+#define BODY(D, MM) run_eom_vjp<D, MM>(ctx, numax, lam_m, lam_d, tc, sbar, gm_bar, gd_bar, l0_bar, xm_bar, xd_bar, shat, cm, cd)
+    LDGA_FOR_EACH_GRID(LDGA_CASE)
+#undef BODY
+    return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}

@@ -186,6 +186,12 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail);
 // receives the number of adjoint solves above the backward-error threshold.
 int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const double2* gam_bar, double2* chi0_bar,
                    double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail);
+// Adjoint of the EoM at (lam_m, lam_d): sbar [numax][Nq] -> gm_bar, gd_bar, l0_bar [Nq, Nnu, Nw] (pre-zeroed;
+// any may be null), xm_bar, xd_bar [Nq, Nw] (may be null).  Scratch: shat [numax * Nq] complex,
+// cm, cd [numax * Nq * Nw] real.
+int launch_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, const double2* sbar,
+                   double2* gm_bar, double2* gd_bar, double2* l0_bar, double* xm_bar, double* xd_bar, double2* shat,
+                   double* cm, double* cd);
 int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp);
 int launch_lambda0(ldga_ctx* ctx);
 // EoM forward + inverse.  lam_*_dev (may be null) are device scalars added to lam_m / lam_d.

@@ -775,6 +775,55 @@ def calc_Sigma_w(eomf, chi_m: np.ndarray, gamma_m, chi_d: np.ndarray, gamma_d, l
     return out
 
 
+def calc_Sigma_vjp(Sigma_bar, chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, G_irr, kG: KGrid,
+                   mP: ModelParameters, sP: SimulationParameters, numax: int, lam_m: float = 0.0, lam_d: float = 0.0,
+                   tc: bool = True):
+    """Adjoint of ``calc_Σ`` (ladderDGATools_singleCore.jl:49-136) at (λm, λd) for a real loss:
+    Sigma_bar [Nq, numax] (dL/dRe + i dL/dIm of the stored irreducible values) ->
+    (chi_m_bar, gamma_m_bar, chi_d_bar, gamma_d_bar, lambda0_bar).  The convolution's adjoint is the
+    full-grid correlation with conj(G), evaluated by FFT like the forward (conv_fft):
+    Kbar(p) = kMult(p)/beta (1/N_k) sum_k Sbar_full(k) conj(G(k + p)), Sbar_full = Sbar/kMult expanded."""
+    U, beta = mP.U, mP.beta
+    d = kG.dim
+    cmv = chi_m.data if lam_m == 0.0 else chi_lambda(chi_m.data, lam_m)
+    cdv = chi_d.data if lam_d == 0.0 else chi_lambda(chi_d.data, lam_d)
+    nw = cmv.shape[1]
+    off = -sP.fft_range[0]
+    gmb = np.zeros_like(gamma_m, dtype=np.complex128)
+    gdb = np.zeros_like(gamma_d, dtype=np.complex128)
+    l0b = np.zeros_like(lambda0, dtype=np.complex128)
+    xmb = np.zeros(cmv.shape)
+    xdb = np.zeros(cdv.shape)
+    Sf = kG.expand(np.asarray(Sigma_bar) / kG.kMult[:, None])
+    Shat = sfft.fftn(Sf, axes=tuple(range(d)), workers=_WORKERS)
+    for wi in range(nw):
+        wn = wi - sP.n_iw
+        v0 = nu0_index_of_w_index(wi + 1, sP) - 1
+        vlist = list(range(v0, 2 * sP.n_iv))[:numax]
+        if not vlist:
+            continue
+        vl = np.array(vlist)
+        nii = np.arange(len(vlist))
+        Gc = np.conj(kG.expand(G_irr[:, nii + wn + off]))
+        rev = Gc[(slice(None, None, -1),) * d]
+        grc = sfft.fftn(rev, axes=tuple(range(d)), workers=_WORKERS)
+        Kbar = conv_fft(kG, Shat[..., nii], grc) * kG.kMult[:, None] / beta
+        gm, gd = gamma_m[:, vl, wi], gamma_d[:, vl, wi]
+        gmb[:, vl, wi] = (1.5 * U * (1.0 + U * cmv[:, wi]))[:, None] * Kbar
+        gdb[:, vl, wi] = (-0.5 * U * (1.0 - U * cdv[:, wi]))[:, None] * Kbar
+        l0b[:, vl, wi] = U * Kbar
+        xmb[:, wi] += np.sum(np.real(np.conj(Kbar) * 1.5 * U * U * gm), axis=1)
+        xdb[:, wi] += np.sum(np.real(np.conj(Kbar) * 0.5 * U * U * gd), axis=1)
+    if tc:
+        # tail -U (sum_kω χm^λ - χloc_m_sum)/(iν_n): d/dχm^λ(q, ω) of sum_kω is kMult(q)/(β N_k)
+        wnu = (2 * np.arange(numax) + 1) * math.pi / beta
+        sbar = U * float(np.sum(np.imag(np.asarray(Sigma_bar)) / wnu[None, :]))
+        xmb += sbar * kG.kMult[:, None] / (beta * kG.Nk)
+    xmb /= (lam_m * chi_m.data + 1.0) ** 2
+    xdb /= (lam_d * chi_d.data + 1.0) ** 2
+    return xmb, gmb, xdb, gdb, l0b
+
+
 def calc_Sigma(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, chi_m_sum: float, lambda0, grhat,
                kG: KGrid, mP: ModelParameters, sP: SimulationParameters, numax: int | None = None,
                lam_m: float = 0.0, lam_d: float = 0.0, tc: bool = True) -> np.ndarray:

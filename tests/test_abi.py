@@ -147,3 +147,19 @@ def test_no_closed_copy_calls_in_sources():
     pat = re.compile(r"Memcpy(3D)?Batch")
     for f in list(PKG.rglob("*.cu")) + list(PKG.rglob("*.cuh")) + list(PKG.rglob("*.py")) + [ROOT / "bench.py"]:
         assert not pat.search(f.read_text()), f
+
+
+def test_ptr_keeps_temporaries_alive():
+    """ptr(as_fc(x)) of a C-ordered array makes a temporary Fortran copy; the returned pointer must
+    keep it alive until the C call has read it (CPython frees unreferenced temporaries at once)."""
+    import gc
+    import numpy as np
+    from ladderdga_b200 import _lib
+    x = np.arange(24, dtype=np.complex128).reshape(2, 3, 4)       # C order: as_fc copies
+    p = _lib.ptr(_lib.as_fc(x))
+    gc.collect()
+    junk = [np.full(24, -1.0 + 0j) for _ in range(64)]            # reuse freed blocks if any
+    import ctypes as C
+    got = np.ctypeslib.as_array((C.c_double * 48).from_address(p.value)).view(np.complex128)
+    assert np.array_equal(got, np.asfortranarray(x).reshape(-1, order="F"))
+    del junk

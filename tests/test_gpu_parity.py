@@ -387,3 +387,45 @@ def test_bse_vjp(case, prec):
         an = float(np.sum(np.real(np.conj(c0b) * dc)))
         assert abs(fd - an) <= 1e-6 * max(abs(an), 1e-8 * np.sum(np.abs(c0b) * np.abs(dc))), (name, t, fd, an)
         h.ctx.call("ldga_set_chi0", L._lib.ptr(L._lib.as_fc(c00)))
+
+
+def test_eom_vjp(case):
+    """Adjoint of calc_Σ at (λm, λd): against the oracle's FFT-correlation gradient and against
+    central finite differences of the GPU EoM along random directions of γm, χm, λ₀ and γd."""
+    name, inp, ref = case
+    rng = np.random.default_rng(12)
+    g = gpu_chain(inp)
+    h, r = g["h"], ref["h"]
+    numax, lm, ld = h.sP.n_iν, 0.1, 0.05
+    Sb = _cgauss(rng, (h.ctx.Nq, numax))
+    xmb, gmb, xdb, gdb, l0b = L.calc_Σ_vjp(Sb, g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], h,
+                                           νmax=numax, λm=lm, λd=ld)
+    o = R.calc_Sigma_vjp(Sb, ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"], r.G_irr, r.kG,
+                         r.mP, r.sP, numax, lam_m=lm, lam_d=ld)
+    for a, b, what in zip((xmb, gmb, xdb, gdb, l0b), o, ("chi_m", "gamma_m", "chi_d", "gamma_d", "lambda0")):
+        assert rel(a, b) < 1e-9, (name, what)
+    ctx = h.ctx
+    base = {"chi_m": np.array(g["chi_m"].data), "chi_d": np.array(g["chi_d"].data),
+            "gamma_m": np.array(g["gamma_m"].data), "gamma_d": np.array(g["gamma_d"].data),
+            "lambda0": np.array(np.asarray(g["lambda0"]))}
+
+    def loss(arrs):
+        ctx.call("ldga_set_chi", L.CH_M, L._lib.ptr(np.asfortranarray(arrs["chi_m"])))
+        ctx.call("ldga_set_chi", L.CH_D, L._lib.ptr(np.asfortranarray(arrs["chi_d"])))
+        ctx.call("ldga_set_gamma", L.CH_M, L._lib.ptr(L._lib.as_fc(arrs["gamma_m"])))
+        ctx.call("ldga_set_gamma", L.CH_D, L._lib.ptr(L._lib.as_fc(arrs["gamma_d"])))
+        ctx.call("ldga_set_lambda0", L._lib.ptr(L._lib.as_fc(arrs["lambda0"])))
+        S_ = L._lib.cplx_out((ctx.Nq, numax))
+        ctx.call("ldga_eom", lm, ld, numax, 1, h.χloc_m_sum, L._lib.ptr(S_))
+        return float(np.sum(np.real(np.conj(Sb) * S_)))
+
+    grads = {"chi_m": xmb, "gamma_m": gmb, "chi_d": xdb, "gamma_d": gdb, "lambda0": l0b}
+    for k in ("gamma_m", "chi_m", "lambda0", "gamma_d", "chi_d"):
+        d = rng.standard_normal(base[k].shape) if k.startswith("chi") else _cgauss(rng, base[k].shape)
+        eps = 1e-6 * np.max(np.abs(base[k])) / np.max(np.abs(d))
+        plus = dict(base); plus[k] = base[k] + eps * d
+        minus = dict(base); minus[k] = base[k] - eps * d
+        fd = (loss(plus) - loss(minus)) / (2 * eps)
+        an = float(np.sum(np.real(np.conj(grads[k]) * d)))
+        assert abs(fd - an) <= 1e-6 * np.sum(np.abs(grads[k]) * np.abs(d)), (name, k, fd, an)
+    loss(base)
