@@ -1016,6 +1016,19 @@ def calc_Σ_vjp(Σ̄, χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelpe
     return xmb, gmb, xdb, gdb, l0b
 
 
+def chain_vjp_Γ(h: lDΓAHelper, Σ̄, χm: χT, γm: γT, χd: χT, γd: γT, λ0, νmax: int | None = None, λm: float = 0.0,
+                λd: float = 0.0, tc: bool = True) -> dict:
+    """Adjoint of the ladder chain's BSE → EoM part at fixed λ: for a real loss L(Σ_ladder) with
+    Σ̄ = ∂L/∂Σ_ladder [Nq, νmax], the gradients with respect to the local vertices Γ_m, Γ_d
+    [Nν, Nν, Nω], the bubble χ₀ (both channels' BSE) and λ₀, all computed on the GPU handle.
+    χm, γm, χd, γd must be the outputs of the handle's last ``calc_χγ`` calls (the BSE adjoint
+    rebuilds its forward solution from them)."""
+    xmb, gmb, xdb, gdb, l0b = calc_Σ_vjp(Σ̄, χm, γm, χd, γd, λ0, h, νmax=νmax, λm=λm, λd=λd, tc=tc)
+    Gmb, c0m = calc_χγ_vjp("m", h, xmb, gmb)
+    Gdb, c0d = calc_χγ_vjp("d", h, xdb, gdb)
+    return {"Γ_m": Gmb, "Γ_d": Gdb, "χ0": c0m + c0d, "λ0": l0b}
+
+
 def calc_Σ_parts(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, tc: bool = True, λm: float = 0.0,
                  λd: float = 0.0) -> np.ndarray:
     """``calc_Σ_parts`` (ladderDGATools_singleCore.jl:149-189) -> [q, ν_n, 7]."""
@@ -1470,4 +1483,4 @@ F_from_chi = F_from_χ
 calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_χγ_par, collect_χ0, collect_χ, collect_γ
 calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_part
 lambda_m_chain_batch = λm_chain_batch
-calc_chi_gamma_vjp, calc_Sigma_vjp = calc_χγ_vjp, calc_Σ_vjp
+calc_chi_gamma_vjp, calc_Sigma_vjp, chain_vjp_Gamma = calc_χγ_vjp, calc_Σ_vjp, chain_vjp_Γ
