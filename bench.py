@@ -34,6 +34,12 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(cfg=3, dim=3, ns=32, beta=20.0, U=1.5, n_iv=20, n_iw=20)
 WORKLOAD_NAME = "3D sc Nk=32^3 (969 irreducible q), beta=20, U=1.5, Nnu=40, Nw=41, lambda_m"
+# the other single-point configurations, selectable with --cfg (the chain is the lambda_m chain for all)
+CFG_NAMES = {
+    1: "2D sq Nk=16^2 (45 irreducible q), beta=10, U=1, Nnu=20, Nw=21, lambda_m",
+    2: "2D sq Nk=64^2 (561 irreducible q), beta=30, U=2, Nnu=60, Nw=61, lambda_m chain",
+    3: WORKLOAD_NAME,
+}
 METRIC = "(q,w)-points/s"
 PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
 REF_BUDGET_S = 120.0
@@ -63,6 +69,8 @@ def parse():
     ap.add_argument("--workload", default="chain", choices=["chain", "batch"],
                     help="chain: the 3D 32^3 point (default); batch: the uneven 64-point (U, beta) scan on 2D 32^2")
     ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
+    ap.add_argument("--cfg", type=int, default=3, choices=[1, 2, 3],
+                    help="single-point configuration of the chain workload (3: the headline 3D 32^3 point)")
     return ap.parse_args()
 
 
@@ -147,8 +155,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     from ladderdga_b200 import synthetic as S
-    inp = S.config_input(WORKLOAD["cfg"])
-    points = 969 * (2 * WORKLOAD["n_iw"] + 1)
+    inp = S.config_input(args.cfg)
+    from oracle import ldga_ref as R
+    points = R.gen_kGrid(inp.kgrid_kind, inp.ns).Nq * (2 * inp.n_iw + 1)
     # one step is a whole chain (about 10 s on 8 cores): the warm-up is capped at one chain and the
     # timed steps stop once REF_BUDGET_S seconds are spent, so the arm ends within a few minutes
     for _ in range(min(args.warmup, 1)):
@@ -166,7 +175,7 @@ def run_reference(args):
             "steps_requested": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD_NAME, "global_batch": 1, "l2": "inputs resident in host memory"},
+            "config": {"workload": CFG_NAMES[args.cfg], "global_batch": 1, "l2": "inputs resident in host memory"},
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -295,7 +304,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from ladderdga_b200 import synthetic as S
     over = {"ns": args.ns} if args.ns else {}
-    inp = S.config_input(WORKLOAD["cfg"], point=rank, **over)
+    inp = S.config_input(args.cfg, point=rank, **over)
     chain = Chain(inp, PREC_NAMES[args.prec], local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = {}
@@ -355,7 +364,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
                 "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
-                "config": {"workload": WORKLOAD_NAME, "global_batch": world, "seq_len": None,
+                "config": {"workload": CFG_NAMES[args.cfg], "global_batch": world, "seq_len": None,
                            "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
                            "points_per_step_per_gpu": chain.points},
                 "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": chain.h2d_bytes,
