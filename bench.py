@@ -243,6 +243,18 @@ class Chain:
         return list(sc)
 
 
+def tune(chain) -> str:
+    """Untimed: run the bubble, let the autotuner pick the BSE configuration for this box size and
+    precision mode (both channels' inputs), and return its name."""
+    ctx = chain.ctx
+    ctx.call("ldga_bubble", None)
+    import ladderdga_b200 as L
+    for t in ("m", "d"):
+        L.autotune_bse(chain.h, t, reps=3)
+    name = chain.lib.ldga_bse_config_name(ctx.Nnu, ctx.precision, -1)
+    return name.decode() if name else "pivoted"
+
+
 def stage_times(chain):
     from ladderdga_b200._lib import STAGES
     ms = (C.c_double * 10)()
@@ -306,6 +318,7 @@ def run_ours(args):
     over = {"ns": args.ns} if args.ns else {}
     inp = S.config_input(args.cfg, point=rank, **over)
     chain = Chain(inp, PREC_NAMES[args.prec], local)
+    bse_config = tune(chain)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = {}
     try:
@@ -366,7 +379,7 @@ def run_ours(args):
                 "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
                 "config": {"workload": CFG_NAMES[args.cfg], "global_batch": world, "seq_len": None,
                            "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
-                           "points_per_step_per_gpu": chain.points},
+                           "points_per_step_per_gpu": chain.points, "bse_config": bse_config},
                 "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": chain.h2d_bytes,
                         "d2h_bytes_per_step": chain.d2h_bytes, "ms_per_step": ms_e2e,
                         "path": "C ABI (ldga_*) from pinned host buffers"},
@@ -405,6 +418,10 @@ def run_batch(args):
     for p in pts:
         chains.append(Chain(S.make_input(**p), PREC_NAMES[args.prec], local, stream=torch.cuda.Stream(local)))
     n = len(chains)
+    tuned = {}
+    for c in chains:                                   # one autotuning run per box size
+        if c.ctx.Nnu not in tuned:
+            tuned[c.ctx.Nnu] = tune(c)
     main = torch.cuda.current_stream(local)
     scs = [(C.c_double * 8)() for _ in chains]
     handles = (C.c_void_p * n)(*[c.ctx.h.value for c in chains])
@@ -470,6 +487,7 @@ def run_batch(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
             "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
             "config": {"workload": BATCH_NAME.format(n=n), "global_batch": n * world, "nnu_set": nnu,
+                       "bse_config": {str(k): v for k, v in sorted(tuned.items())},
                        "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
                        "points_per_step_per_gpu": points},
             "e2e": {"value": world * points / (ms_e2e / 1e3), "unit": METRIC,

@@ -167,6 +167,23 @@ int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const do
 int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, const double* sigma_bar,
                  double* chi_m_bar, double* gam_m_bar, double* chi_d_bar, double* gam_d_bar, double* lambda0_bar);
 
+/* Tile-shape autotuning of the BSE kernel (no reference counterpart; the reference has one LAPACK
+ * path).  Every fast-path box size has a few compiled configurations per precision mode (threads
+ * per matrix, CTAs per SM the register allocation allows); this times each one `reps` times on the
+ * channel's current chi0 and Gamma_r, records the fastest for (Nnu, precision mode) in the process,
+ * and leaves that channel's chi and gamma as ldga_bse would.  variant / ms (may be NULL): the chosen
+ * index (0 = the default) and its time per launch (-1 when there was only one configuration).
+ * Later launches -- including graphs captured afterwards -- use the choice. */
+int ldga_autotune_bse(ldga_ctx* ctx, int32_t channel, int32_t reps, int32_t* variant, double* ms);
+/* Save / load the recorded choices as text lines "bse <Nnu> <precision> <configuration name>";
+ * unknown names are ignored on load. */
+int ldga_tune_save(const char* path);
+int ldga_tune_load(const char* path);
+/* Name of BSE configuration `index` for (nnu, precision) -- index < 0: the one in use -- or NULL. */
+const char* ldga_bse_config_name(int32_t nnu, int32_t precision, int32_t index);
+/* Forget every recorded choice: all box sizes use their default configuration again. */
+int ldga_tune_reset(void);
+
 /* Copy a device-resident array of the handle to `out` (host or device) without recomputing it.
  * No reference counterpart: the reference's arrays live in Julia memory; here they stay in HBM
  * until asked for.  what: one of LDGA_GET_*; channel only for chi and gamma. */

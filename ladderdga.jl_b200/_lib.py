@@ -26,7 +26,9 @@ EXPORTS = [
     "ldga_set_lambda0", "ldga_sum_kw", "ldga_sum_wk", "ldga_lambda_min", "ldga_eom", "ldga_eom_parts",
     "ldga_lambda_m", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
     "ldga_lambda_dm_evals", "ldga_set_stream", "ldga_profile", "ldga_stage_times", "ldga_launch_count",
-    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp", "ldga_eom_vjp",
+    "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp",
+    "ldga_eom_vjp", "ldga_autotune_bse", "ldga_tune_save", "ldga_tune_load",
+    "ldga_tune_reset", "ldga_bse_config_name",
 ]
 GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
 STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
@@ -118,6 +120,11 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_batch_chain_m": (C.c_int, [I32, P, P, I32, PI32]),
         "ldga_bse_vjp": (C.c_int, [P, I32, P, P, P, P, PI32]),
         "ldga_eom_vjp": (C.c_int, [P, D, D, I32, I32, P, P, P, P, P, P]),
+        "ldga_autotune_bse": (C.c_int, [P, I32, I32, PI32, PD]),
+        "ldga_tune_save": (C.c_int, [C.c_char_p]),
+        "ldga_tune_load": (C.c_int, [C.c_char_p]),
+        "ldga_tune_reset": (C.c_int, []),
+        "ldga_bse_config_name": (C.c_char_p, [I32, I32, I32]),
         "ldga_run_sc": (C.c_int, [P, D, D, I32, D, D, I32, I32, D, D, I32, D, P, P, P]),
         "ldga_set_sigma": (C.c_int, [P, P, I32]),
         "ldga_calc_E": (C.c_int, [P, P, P, I32, D, PD, PD]),

@@ -934,6 +934,38 @@ def calc_χγ_vjp(type_, h: lDΓAHelper, χ̄=None, γ̄=None):
     return Gb, c0b
 
 
+def autotune_bse(h: lDΓAHelper, type_="m", reps: int = 3) -> tuple[int, float]:
+    """Time the compiled BSE configurations for this handle's box size and precision mode on its
+    current χ₀ and Γ_r, and use the fastest from now on (``ldga_autotune_bse``).  The channel's χ
+    and γ are left as ``calc_χγ`` would leave them.  Returns (configuration index, ms per launch)."""
+    ctx = h.ctx
+    ch = _channel(type_)
+    Γ = h.Γ_m if ch == CH_M else h.Γ_d
+    ctx.call("ldga_bse", ch, ptr(as_fc(Γ)), None, None, None)
+    v, ms = _lib.C.c_int32(), _lib.C.c_double()
+    ctx.call("ldga_autotune_bse", ch, int(reps), _lib.C.byref(v), _lib.C.byref(ms))
+    return v.value, ms.value
+
+
+def tune_save(path) -> None:
+    """Write the recorded BSE configuration choices (``ldga_tune_save``)."""
+    lib = _lib.load()
+    if lib.ldga_tune_save(str(path).encode()) != _lib.LDGA_OK:
+        raise OSError(lib.ldga_last_error(None).decode())
+
+
+def tune_load(path) -> None:
+    """Read BSE configuration choices written by ``tune_save`` (``ldga_tune_load``)."""
+    lib = _lib.load()
+    if lib.ldga_tune_load(str(path).encode()) != _lib.LDGA_OK:
+        raise OSError(lib.ldga_last_error(None).decode())
+
+
+def tune_reset() -> None:
+    """Forget the recorded BSE configuration choices (``ldga_tune_reset``)."""
+    _lib.load().ldga_tune_reset()
+
+
 def _log_q0_χ_check(ctx: Context, χ: χT, type_) -> None:
     """``log_q0_χ_check`` (helpers.jl:114-121), kept as a returned value instead of a log line."""
     q0 = 0

@@ -433,6 +433,91 @@ int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const do
     return LDGA_OK;
 }
 
+int ldga_autotune_bse(ldga_ctx* ctx, int32_t channel, int32_t reps, int32_t* variant, double* ms) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
+    NEED(ctx, ctx->have_chi0 && ctx->have_Gamma[channel], "autotune: run ldga_bubble and load Gamma_r first");
+    if (reps < 1) reps = 1;
+    DeviceGuard g(ctx->device);
+    const int nv = bse_variant_count(ctx->Nnu, ctx->prec);
+    int best = 0;
+    double best_ms = -1.0;
+    if (nv > 1) {
+        cudaEvent_t e0, e1;
+        LDGA_CUDA(ctx, cudaEventCreate(&e0));
+        LDGA_CUDA(ctx, cudaEventCreate(&e1));
+        const bool prof = ctx->profiling;
+        ctx->profiling = false;   // the trial launches stay out of the stage timers
+        int st = LDGA_OK;
+        for (int i = 0; i < nv && st == LDGA_OK; ++i) {
+            st = bse_run_variant(ctx, channel, i);                       // warm-up (and smem opt-in)
+            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventRecord(e0, ctx->stream), "cudaEventRecord");
+            for (int r = 0; r < reps && st == LDGA_OK; ++r) st = bse_run_variant(ctx, channel, i);
+            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventRecord(e1, ctx->stream), "cudaEventRecord");
+            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float t = 0.f;
+            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+            const double per = (double)t / reps;
+            if (st == LDGA_OK && (best_ms < 0.0 || per < best_ms)) { best_ms = per; best = i; }
+        }
+        ctx->profiling = prof;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st != LDGA_OK) return st;
+        bse_set_variant(ctx->Nnu, ctx->prec, best);
+    }
+    // leave the channel's outputs as a regular ldga_bse would (fallback for flagged matrices included)
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    TRY(launch_bse(ctx, channel, ctx->d_count + 1));
+    TRY(sync(ctx));
+    ctx->have_chi[channel] = ctx->have_gam[channel] = true;
+    if (variant) *variant = best;
+    if (ms) *ms = best_ms;
+    return LDGA_OK;
+}
+
+int ldga_tune_save(const char* path) {
+    if (!path) return ctx_fail(nullptr, LDGA_ERR_ARG, "null path");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return ctx_fail(nullptr, LDGA_ERR_ARG, std::string("cannot write ") + path);
+    std::fprintf(f, "# libldga_b200 BSE kernel choices: bse <Nnu> <precision mode> <configuration>\n");
+    for (int nnu = 1; nnu <= LDGA_MAX_NNU; ++nnu)
+        for (int prec = LDGA_PREC_FP64_INV; prec <= LDGA_PREC_MIXED; ++prec) {
+            const int n = bse_variant_count(nnu, prec);
+            const int i = bse_tuned_variant(nnu, prec);
+            if (n > 1 && i > 0 && i < n) std::fprintf(f, "bse %d %d %s\n", nnu, prec, bse_variant_name(nnu, prec, i));
+        }
+    std::fclose(f);
+    return LDGA_OK;
+}
+
+const char* ldga_bse_config_name(int32_t nnu, int32_t precision, int32_t index) {
+    if (index < 0) index = bse_tuned_variant(nnu, precision);
+    return bse_variant_name(nnu, precision, index);
+}
+
+int ldga_tune_reset(void) {
+    bse_reset_variants();
+    return LDGA_OK;
+}
+
+int ldga_tune_load(const char* path) {
+    if (!path) return ctx_fail(nullptr, LDGA_ERR_ARG, "null path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) return ctx_fail(nullptr, LDGA_ERR_ARG, std::string("cannot read ") + path);
+    char line[256];
+    while (std::fgets(line, sizeof line, f)) {
+        int nnu = 0, prec = 0;
+        char name[64] = {0};
+        if (std::sscanf(line, "bse %d %d %63s", &nnu, &prec, name) != 3) continue;   // comments, other lines
+        const int n = bse_variant_count(nnu, prec);
+        for (int i = 0; i < n; ++i)
+            if (std::strcmp(bse_variant_name(nnu, prec, i), name) == 0) bse_set_variant(nnu, prec, i);
+    }
+    std::fclose(f);
+    return LDGA_OK;
+}
+
 int ldga_get(ldga_ctx* ctx, int32_t what, int32_t channel, double* out) {
     if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
     DeviceGuard g(ctx->device);

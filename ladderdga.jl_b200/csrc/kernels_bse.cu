@@ -31,8 +31,14 @@
 // and re-solved by a partial-pivoting FP64 LU kernel, which is also the path for box sizes that
 // have no tiled instantiation.
 #include <cmath>
+#include <map>
+#include <mutex>
 
 #include "ldga_internal.cuh"
+
+#ifndef LDGA_LU_LOOKAHEAD
+#define LDGA_LU_LOOKAHEAD true
+#endif
 
 namespace {
 
@@ -440,7 +446,7 @@ struct LuSmem {
         (2 * RW + 2 * CW + N + N + N) * sizeof(double2) + 8 * (G / 32) * sizeof(double) + 16;
 };
 
-template <int N, int T, int MPC, int MINB, bool GSM>
+template <int N, int T, int MPC, int MINB, bool GSM, bool LA>
 __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
     using LS = LuSmem<N, T>;
     constexpr int RT = LS::RT, NC = LS::NC, G = LS::G;
@@ -502,39 +508,116 @@ __global__ void __launch_bounds__(T * T * MPC, MINB) k_bse_lu(const BseArgs a) {
         // of the tile hold zeros and stay zero (their published values are zero), so no step needs
         // a bounds predicate; entries at or left of the pivot are published but never read.
         const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
+        if constexpr (LA) {
+            // Lookahead: in step k every thread first updates its part of the tile row and tile
+            // column that hold row k+1 and column k+1, the owners then publish step k+1 into the other
+            // buffer pair, and only then is the rest of the tile updated, so the pivot shuffle, the
+            // reciprocal and the stores of step k+1 overlap the bulk of step k.  Writing buffer
+            // (k+1)&1 after barrier k is safe: its last readers (step k-1) finished before barrier k.
+            // publish(kp, ktp): step kp = ktp + T kp (kp a compile-time tile index)
+#define LDGA_LU_PUBLISH(KP, KTP)                                                                  \
+            {                                                                                   \
+                const int kk_ = (KTP) + T * (KP);                                                \
+                double2* rb_ = rowbuf + (kk_ & 1) * LS::RW;                                      \
+                double2* cb_ = colbuf + (kk_ & 1) * LS::CW;                                      \
+                if (tr == (KTP)) {                                                               \
+                    double2 p_;                                                                  \
+                    p_.x = __shfl_sync(gmask, b[KP][KP].x, (KTP), T);                            \
+                    p_.y = __shfl_sync(gmask, b[KP][KP].y, (KTP), T);                            \
+                    const double2 inv_ = vinv(p_);                                               \
+                    if (tc == (KTP)) pinv[kk_] = inv_;                                           \
+                    _Pragma("unroll") for (int c_ = (KP); c_ < CT; ++c_)                         \
+                        rb_[tc + T * c_] = vmul<double2>(b[KP][c_], inv_);                       \
+                }                                                                                \
+                if (tc == (KTP)) {                                                               \
+                    _Pragma("unroll") for (int r_ = (KP); r_ < RT; ++r_) cb_[tr + T * r_] = b[r_][KP]; \
+                }                                                                                \
+            }
+            // update of step k (tile index KC, lane ktc) restricted to the elements with COND(ra, c)
+#define LDGA_LU_UPDATE(KC, COND)                                                                  \
+            _Pragma("unroll") for (int ra = (KC); ra < RT; ++ra) {                               \
+                if (ra > (KC) || tr != ktc) {                                                    \
+                    const double2 m = cb[tr + T * ra];                                           \
+                    _Pragma("unroll") for (int c = (KC); c < CT; ++c) {                          \
+                        if ((COND) && (c > (KC) || tc > ktc)) vfnms<double2>(b[ra][c], m, u[c]); \
+                    }                                                                            \
+                }                                                                                \
+            }
+            LDGA_LU_PUBLISH(0, 0)
+            named_barrier(bar, G);
 #pragma unroll
-        for (int kc = 0; kc < RT; ++kc) {
-            const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+            for (int kc = 0; kc < RT; ++kc) {
+                const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+                // steps whose successor lies in the same diagonal block (cross = tile row/column kc)
 #pragma unroll 1
-            for (int ktc = 0; ktc < kend; ++ktc) {
-                const int k = ktc + T * kc;
-                double2* rb = rowbuf + (k & 1) * LS::RW;
-                double2* cb = colbuf + (k & 1) * LS::CW;
-                if (tr == ktc) {
-                    // the row group of row k scales its row by 1/b_kk (pivot shuffled from lane ktc)
-                    double2 p;
-                    p.x = __shfl_sync(gmask, b[kc][kc].x, ktc, T);
-                    p.y = __shfl_sync(gmask, b[kc][kc].y, ktc, T);
-                    const double2 inv = vinv(p);
-                    if (tc == ktc) pinv[k] = inv;
+                for (int ktc = 0; ktc < kend - 1; ++ktc) {
+                    const int k = ktc + T * kc;
+                    const double2* rb = rowbuf + (k & 1) * LS::RW;
+                    const double2* cb = colbuf + (k & 1) * LS::CW;
+                    double2 u[CT];
 #pragma unroll
-                    for (int c = kc; c < CT; ++c) rb[tc + T * c] = vmul<double2>(b[kc][c], inv);
+                    for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
+                    LDGA_LU_UPDATE(kc, (ra == kc || c == kc))
+                    LDGA_LU_PUBLISH(kc, ktc + 1)
+                    LDGA_LU_UPDATE(kc, (ra != kc && c != kc))
+                    named_barrier(bar, G);
                 }
-                if (tc == ktc) {
+                // the last step of the block: the next pivot opens block kc + 1
+                {
+                    const int ktc = kend - 1;
+                    const int k = ktc + T * kc;
+                    const double2* rb = rowbuf + (k & 1) * LS::RW;
+                    const double2* cb = colbuf + (k & 1) * LS::CW;
+                    double2 u[CT];
 #pragma unroll
-                    for (int ra = kc; ra < RT; ++ra) cb[tr + T * ra] = b[ra][kc];
+                    for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
+                    if (kc + 1 < RT) {
+                        LDGA_LU_UPDATE(kc, (ra == kc + 1 || c == kc + 1))
+                        LDGA_LU_PUBLISH(kc + 1, 0)
+                        LDGA_LU_UPDATE(kc, (ra != kc + 1 && c != kc + 1))
+                        named_barrier(bar, G);
+                    } else {
+                        LDGA_LU_UPDATE(kc, true)
+                    }
                 }
-                named_barrier(bar, G);
-                double2 u[CT];
-#pragma unroll
-                for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
-#pragma unroll
-                for (int ra = kc; ra < RT; ++ra) {
-                    if (ra > kc || tr != ktc) {
-                        const double2 m = cb[tr + T * ra];
-#pragma unroll
-                        for (int c = kc; c < CT; ++c) {
-                            if (c > kc || tc > ktc) vfnms<double2>(b[ra][c], m, u[c]);
+            }
+#undef LDGA_LU_PUBLISH
+#undef LDGA_LU_UPDATE
+        } else {
+    #pragma unroll
+            for (int kc = 0; kc < RT; ++kc) {
+                const int kend = (N - T * kc) < T ? (N - T * kc) : T;
+    #pragma unroll 1
+                for (int ktc = 0; ktc < kend; ++ktc) {
+                    const int k = ktc + T * kc;
+                    double2* rb = rowbuf + (k & 1) * LS::RW;
+                    double2* cb = colbuf + (k & 1) * LS::CW;
+                    if (tr == ktc) {
+                        // the row group of row k scales its row by 1/b_kk (pivot shuffled from lane ktc)
+                        double2 p;
+                        p.x = __shfl_sync(gmask, b[kc][kc].x, ktc, T);
+                        p.y = __shfl_sync(gmask, b[kc][kc].y, ktc, T);
+                        const double2 inv = vinv(p);
+                        if (tc == ktc) pinv[k] = inv;
+    #pragma unroll
+                        for (int c = kc; c < CT; ++c) rb[tc + T * c] = vmul<double2>(b[kc][c], inv);
+                    }
+                    if (tc == ktc) {
+    #pragma unroll
+                        for (int ra = kc; ra < RT; ++ra) cb[tr + T * ra] = b[ra][kc];
+                    }
+                    named_barrier(bar, G);
+                    double2 u[CT];
+    #pragma unroll
+                    for (int c = kc; c < CT; ++c) u[c] = rb[tc + T * c];
+    #pragma unroll
+                    for (int ra = kc; ra < RT; ++ra) {
+                        if (ra > kc || tr != ktc) {
+                            const double2 m = cb[tr + T * ra];
+    #pragma unroll
+                            for (int c = kc; c < CT; ++c) {
+                                if (c > kc || tc > ktc) vfnms<double2>(b[ra][c], m, u[c]);
+                            }
                         }
                     }
                 }
@@ -1646,12 +1729,12 @@ int run_tile(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
-template <int N, int T, int MPC, int MINB, bool GSM = true>
+template <int N, int T, int MPC, int MINB, bool GSM = true, bool LA = LDGA_LU_LOOKAHEAD>
 int run_lu(ldga_ctx* ctx, const BseArgs& a0) {
     BseArgs a = a0;
     const int threads = T * T * MPC;
     const size_t sm = (GSM ? (size_t)N * N * sizeof(double2) : 0) + MPC * LuSmem<N, T>::bytes;
-    auto kern = k_bse_lu<N, T, MPC, MINB, GSM>;
+    auto kern = k_bse_lu<N, T, MPC, MINB, GSM, LA>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     int chunk = 4 * MPC;
     while (chunk > MPC && (long)((a.nq + chunk - 1) / chunk) * a.nw < 8 * 148) chunk -= MPC;
@@ -1697,17 +1780,81 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
-// TR x TC thread grid per matrix (TC lanes of a row group inside one warp); MPC matrices per CTA
-// MINB of the FP64 elimination (the register-heaviest variant that still spills little when capped)
-template <int N, int TR, int TC, int MPC64, int MPC32, int MINB64 = 1, int MINB32 = 1>
-int run_mode(ldga_ctx* ctx, const BseArgs& a) {
-    switch (ctx->prec) {
-        case LDGA_PREC_FP64_INV: return run_tile<N, TR, TC, MPC64, 1, double, LDGA_PREC_FP64_INV>(ctx, a);
-        case LDGA_PREC_FP64: return run_lu<N, TC, 1, MINB64 * MPC64>(ctx, a);   // one matrix per CTA
-        default:
-            if constexpr (N <= 40) return run_warp32<N, 8, 4, 4, MINB32>(ctx, a);   // one matrix per warp
-            else return run_lu32<N, TC, MPC32, MINB32>(ctx, a);
+// ------------------------------------------------------------------------------------------------
+// Configurations per box size and precision mode (threads per matrix, matrices per CTA, resident
+// CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
+// autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
+using BseRun = int (*)(ldga_ctx*, const BseArgs&);
+struct BseVariant {
+    BseRun run;
+    const char* name;
+};
+
+#define LDGA_SMALL_BOX(N)                                                                              \
+    const BseVariant fp64_##N[] = {{&run_lu<N, 8, 1, 2>, "lu8:2"}, {&run_lu<N, 8, 1, 4>, "lu8:4"},     \
+                                   {&run_lu<N, 8, 1, 8>, "lu8:8"}};                                     \
+    const BseVariant mixed_##N[] = {{&run_warp32<N, 8, 4, 4, 1>, "warp:1"},                            \
+                                    {&run_warp32<N, 8, 4, 4, 3>, "warp:3"}};                           \
+    const BseVariant inv_##N[] = {{&run_tile<N, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
+LDGA_SMALL_BOX(4)
+LDGA_SMALL_BOX(6)
+LDGA_SMALL_BOX(8)
+LDGA_SMALL_BOX(10)
+LDGA_SMALL_BOX(12)
+LDGA_SMALL_BOX(16)
+LDGA_SMALL_BOX(20)
+LDGA_SMALL_BOX(30)
+#undef LDGA_SMALL_BOX
+const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
+                              {&run_lu<40, 8, 1, 5>, "lu8:5"}};
+const BseVariant mixed_40[] = {{&run_warp32<40, 8, 4, 4, 3>, "warp:3"}, {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}};
+const BseVariant inv_40[] = {{&run_tile<40, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
+const BseVariant fp64_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu<60, 16, 1, 1>, "lu16:1"},
+                              {&run_lu<60, 16, 1, 3>, "lu16:3"}};
+const BseVariant mixed_60[] = {{&run_lu32<60, 16, 1, 3>, "lu32x16:3"}, {&run_lu32<60, 16, 1, 2>, "lu32x16:2"}};
+const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64_INV>, "gj16x1"}};
+// Nν = 120: Gamma(w) (230 KB) exceeds shared memory and is read through L1/L2; FP64_INV solves by LU
+const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};
+const BseVariant mixed_120[] = {{&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
+
+int variants_of(int nnu, int prec, const BseVariant** out) {
+#define LDGA_BOX(N)                                                                                      \
+    case N:                                                                                             \
+        if (prec == LDGA_PREC_FP64) { *out = fp64_##N; return (int)(sizeof(fp64_##N) / sizeof(BseVariant)); }     \
+        if (prec == LDGA_PREC_MIXED) { *out = mixed_##N; return (int)(sizeof(mixed_##N) / sizeof(BseVariant)); }  \
+        *out = inv_##N; return (int)(sizeof(inv_##N) / sizeof(BseVariant));
+    switch (nnu) {
+        LDGA_BOX(4) LDGA_BOX(6) LDGA_BOX(8) LDGA_BOX(10) LDGA_BOX(12) LDGA_BOX(16) LDGA_BOX(20) LDGA_BOX(30)
+        LDGA_BOX(40) LDGA_BOX(60)
+        case 120:
+            if (prec == LDGA_PREC_MIXED) { *out = mixed_120; return 1; }
+            *out = fp64_120; return 1;
+        default: *out = nullptr; return 0;
     }
+#undef LDGA_BOX
+}
+
+// chosen variant per (Nν, precision mode); absent = 0
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int> g_tune;
+
+int tuned_index(int nnu, int prec) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({nnu, prec});
+    return it == g_tune.end() ? 0 : it->second;
+}
+
+BseArgs bse_args(ldga_ctx* ctx, int channel) {
+    BseArgs a;
+    a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
+    a.beta = ctx->mp.beta; a.U = ctx->mp.U;
+    a.s = channel == LDGA_CH_D ? -1 : 1;
+    a.Gamma = ctx->d_Gamma[channel];
+    a.chi0 = ctx->d_chi0;
+    a.chi = ctx->d_chi[channel];
+    a.gam = ctx->d_gam[channel];
+    a.flags = ctx->d_flags;
+    return a;
 }
 
 }  // namespace
@@ -1721,35 +1868,51 @@ bool bse_has_fast_path(int nnu) {
 
 size_t bse_pivot_smem(int nnu) { return (size_t)nnu * (nnu + 1) * sizeof(double2) + 64 * sizeof(double) + 16; }
 
+int bse_variant_count(int nnu, int prec) {
+    const BseVariant* v = nullptr;
+    return variants_of(nnu, prec, &v);
+}
+
+const char* bse_variant_name(int nnu, int prec, int i) {
+    const BseVariant* v = nullptr;
+    const int n = variants_of(nnu, prec, &v);
+    return (i >= 0 && i < n) ? v[i].name : nullptr;
+}
+
+int bse_tuned_variant(int nnu, int prec) { return tuned_index(nnu, prec); }
+
+void bse_set_variant(int nnu, int prec, int i) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{nnu, prec}] = i;
+}
+
+void bse_reset_variants() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+}
+
+int bse_run_variant(ldga_ctx* ctx, int channel, int i) {
+    const BseVariant* v = nullptr;
+    const int n = variants_of(ctx->Nnu, ctx->prec, &v);
+    if (i < 0 || i >= n) return ctx_fail(ctx, LDGA_ERR_ARG, "BSE variant index out of range");
+    return v[i].run(ctx, bse_args(ctx, channel));
+}
+
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
-    BseArgs a;
-    a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
-    a.beta = ctx->mp.beta; a.U = ctx->mp.U;
-    a.s = channel == LDGA_CH_D ? -1 : 1;
-    a.Gamma = ctx->d_Gamma[channel];
-    a.chi0 = ctx->d_chi0;
-    a.chi = ctx->d_chi[channel];
-    a.gam = ctx->d_gam[channel];
-    a.flags = ctx->d_flags;
+    const BseArgs a = bse_args(ctx, channel);
     const int n = ctx->Nq * ctx->Nw;
     int st = LDGA_OK;
     bool generic = false;
-    switch (ctx->Nnu) {       // T x T thread grid: tiles of ceil(N/T) x ceil((N+1)/T) per thread
-        case 4: st = run_mode<4, 8, 8, 2, 2>(ctx, a); break;
-        case 6: st = run_mode<6, 8, 8, 2, 2>(ctx, a); break;
-        case 8: st = run_mode<8, 8, 8, 2, 2>(ctx, a); break;
-        case 10: st = run_mode<10, 8, 8, 2, 2>(ctx, a); break;
-        case 12: st = run_mode<12, 8, 8, 2, 2>(ctx, a); break;
-        case 16: st = run_mode<16, 8, 8, 2, 4>(ctx, a); break;
-        case 20: st = run_mode<20, 8, 8, 2, 4>(ctx, a); break;
-        case 30: st = run_mode<30, 8, 8, 2, 2>(ctx, a); break;
-        case 40: st = run_mode<40, 8, 8, 2, 2, 3, 3>(ctx, a); break;
-        case 60: st = run_mode<60, 16, 16, 1, 1>(ctx, a); break;
-        case 120:   // Gamma(w) (230 KB) exceeds shared memory: read through L1/L2; FP64_INV solves by LU too
-            st = ctx->prec == LDGA_PREC_MIXED ? run_lu32<120, 16, 1, 1, false>(ctx, a)
-                                              : run_lu<120, 16, 1, 1, false>(ctx, a);
-            break;
-        default: generic = true; break;
+    {
+        const BseVariant* v = nullptr;
+        const int nv = variants_of(ctx->Nnu, ctx->prec, &v);
+        if (nv > 0) {
+            int i = tuned_index(ctx->Nnu, ctx->prec);
+            if (i >= nv) i = 0;
+            st = v[i].run(ctx, a);
+        } else {
+            generic = true;
+        }
     }
     if (st != LDGA_OK) return st;
     const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;
@@ -1801,7 +1964,7 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
         case 20: st = run_bse_adj<20, 8, 4>(ctx, a); break;
         case 30: st = run_bse_adj<30, 8, 4>(ctx, a); break;
         case 40: st = run_bse_adj<40, 8, 6>(ctx, a); break;
-        case 60: st = run_bse_adj<60, 16, 1>(ctx, a); break;
+        case 60: st = run_bse_adj<60, 16, 2>(ctx, a); break;
         default: return ctx_fail(ctx, LDGA_ERR_ARG, "BSE adjoint: fermionic box " + std::to_string(ctx->Nnu) +
                                                         " not built (4..60 even sizes of the tiled kernels)");
     }

@@ -162,6 +162,14 @@ inline cudaError_t set_smem(ldga_ctx* c, F* f, size_t sm) {
 }
 
 bool bse_has_fast_path(int nnu);
+// BSE kernel configurations (autotuning): count and name per (Nν, precision), the chosen index,
+// and one uncompacted launch of configuration i on the channel's current inputs.
+int bse_variant_count(int nnu, int prec);
+const char* bse_variant_name(int nnu, int prec, int i);
+int bse_tuned_variant(int nnu, int prec);
+void bse_set_variant(int nnu, int prec, int i);
+void bse_reset_variants();
+int bse_run_variant(ldga_ctx* ctx, int channel, int i);
 // shared memory of one pivoted-fallback matrix [N][N+1] (complex FP64) plus its reduction scratch
 size_t bse_pivot_smem(int nnu);
 constexpr size_t LDGA_PIVOT_SMEM_MAX = 220 * 1024;

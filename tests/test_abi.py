@@ -163,3 +163,21 @@ def test_ptr_keeps_temporaries_alive():
     got = np.ctypeslib.as_array((C.c_double * 48).from_address(p.value)).view(np.complex128)
     assert np.array_equal(got, np.asfortranarray(x).reshape(-1, order="F"))
     del junk
+
+
+def test_tune_cache_roundtrip(tmp_path):
+    """BSE configuration choices: a cache file is read by name (unknown lines and names ignored) and
+    written back with the same entries; no GPU is needed for the registry."""
+    import ladderdga_b200 as L
+    src = tmp_path / "tune.txt"
+    src.write_text("# comment\nbse 40 1 lu8:5\nbse 60 2 lu32x16:2\nbse 40 2 no-such-config\ngarbage line\n")
+    L.tune_load(src)
+    out = tmp_path / "out.txt"
+    L.tune_save(out)
+    lines = [l for l in out.read_text().splitlines() if not l.startswith("#")]
+    assert "bse 40 1 lu8:5" in lines and "bse 60 2 lu32x16:2" in lines
+    assert not any("no-such-config" in l for l in lines)
+    # back to the defaults for the rest of the session
+    L.tune_reset()
+    L.tune_save(out)
+    assert [l for l in out.read_text().splitlines() if not l.startswith("#")] == []

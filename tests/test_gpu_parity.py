@@ -470,3 +470,20 @@ def test_chain_vjp_gamma(case):
             fd = (loss(Gm0, G0 + eps * d) - loss(Gm0, G0 - eps * d)) / (2 * eps)
         an = float(np.sum(np.real(np.conj(grad[key]) * d)))
         assert abs(fd - an) <= 1e-6 * np.sum(np.abs(grad[key]) * np.abs(d)), (name, key, fd, an)
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_MIXED, L.PREC_FP64_INV])
+def test_autotune_bse(case, prec):
+    """The autotuner times the compiled configurations and keeps the fastest; every configuration
+    gives the oracle's χ and γ, before and after the choice."""
+    name, inp, ref = case
+    g = gpu_chain(inp, prec)
+    h = g["h"]
+    try:
+        for t in ("m", "d"):
+            v, ms = L.autotune_bse(h, t, reps=2)
+            assert v >= 0 and (ms > 0 or ms == -1.0)
+            x, gm = L.calc_χγ(t, h, g["chi0"])
+            assert rel(x.data, ref[f"chi_{t}"].data) < RTOL and rel(gm.data, ref[f"gamma_{t}"]) < RTOL, (name, t)
+    finally:
+        L.tune_reset()
