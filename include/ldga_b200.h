@@ -167,6 +167,18 @@ int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const do
 int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, const double* sigma_bar,
                  double* chi_m_bar, double* gam_m_bar, double* chi_d_bar, double* gam_d_bar, double* lambda0_bar);
 
+/* Vector-Jacobian product of the lattice G (the setup loop runHelpers.jl:113-130 with the bubble,
+ * BSETools.jl:157-172, and the EoM's G(k, ν+ω), ladderDGATools_singleCore.jl:49-81) for a real loss:
+ *   chi0_bar [Nq, Nnu, Nw] = dL/dchi0 (e.g. from ldga_bse_vjp of both channels),
+ *   lambda0_bar [Nq, Nnu, Nw] = dL/dlambda_0 (through lambda_0 = chi0 sum_nu F / beta^2, F fixed),
+ *   sigma_bar [Nq, numax] = dL/dSigma_ladder with the EoM at (lam_m, lam_d) -- its direct use of G,
+ * any of them may be NULL, all complex (dL/dRe + i dL/dIm) ->
+ *   sigma_loc_bar [n_sigma] = dL/dSigma_loc(nu_n), n = 0..n_sigma-1 (negative nu by conjugation), and
+ *   gloc_bar [Nq, Nf] = dL/dG(q, nu) on the wedge over fft_range (either output may be NULL).
+ * mu, G_imp, F_m and the local vertices are held fixed. */
+int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_bar, const double* sigma_bar,
+                  double lam_m, double lam_d, int32_t numax, int32_t n_sigma, double* sigma_loc_bar, double* gloc_bar);
+
 /* Tile-shape autotuning of the BSE kernel (no reference counterpart; the reference has one LAPACK
  * path).  Every fast-path box size has a few compiled configurations per precision mode (threads
  * per matrix, CTAs per SM the register allocation allows); this times each one `reps` times on the

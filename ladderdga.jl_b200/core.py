@@ -1061,6 +1061,33 @@ def chain_vjp_Î“(h: lDÎ“AHelper, Î£Ì„, Ï‡m: Ï‡T, Î³m: Î³T, Ï‡d: Ï‡T, Î³d: Î³T, Î
     return {"Î“_m": Gmb, "Î“_d": Gdb, "Ï‡0": c0m + c0d, "Î»0": l0b}
 
 
+def gloc_vjp(h: lDÎ“AHelper, Ï‡Ì„0=None, Î»Ì„0=None, Î£Ì„=None, Î»m: float = 0.0, Î»d: float = 0.0, Î½max: int | None = None):
+    """Vector-Jacobian product of the lattice G(k, Î½) = 1/(iÎ½ + Î¼ - Îµ_k - Î£_loc(Î½)) through the bubble
+    (Ï‡Ì„â‚€), Î»â‚€ = Ï‡â‚€ Î£_Î½ F / Î²Â² (Î»Ì„â‚€, F fixed) and the EoM's direct use of G (Î£Ì„ at Î»m, Î»d)
+    -> (Î£Ì„_loc [len(Î£_loc)], á¸  [Nq, Nf]); Î¼, G_imp and the local vertices are held fixed."""
+    ctx = h.ctx
+    c0 = None if Ï‡Ì„0 is None else as_fc(Ï‡Ì„0)
+    l0 = None if Î»Ì„0 is None else as_fc(Î»Ì„0)
+    S = None if Î£Ì„ is None else as_fc(Î£Ì„)
+    nu = 0 if S is None else (S.shape[1] if Î½max is None else Î½max)
+    ns = len(h.Î£_loc)
+    slb = np.empty(ns, dtype=np.complex128)
+    gb = _lib.cplx_out((ctx.Nq, ctx.Nf))
+    ctx.call("ldga_gloc_vjp", ptr(c0), ptr(l0), ptr(S), float(Î»m), float(Î»d), int(nu), int(ns), ptr(slb), ptr(gb))
+    return slb, gb
+
+
+def chain_vjp_Î£loc(h: lDÎ“AHelper, Î£Ì„, Ï‡m: Ï‡T, Î³m: Î³T, Ï‡d: Ï‡T, Î³d: Î³T, Î»0, Î½max: int | None = None, Î»m: float = 0.0,
+                   Î»d: float = 0.0, tc: bool = True) -> dict:
+    """``chain_vjp_Î“`` continued to the lattice self-energy: the gradient of a real loss L(Î£_ladder)
+    at fixed Î» with respect to Î£_loc (through G, the bubble, both BSE channels, Î»â‚€ and the EoM),
+    plus the vertex gradients.  G_imp, F_m and the local vertices are held fixed."""
+    out = chain_vjp_Î“(h, Î£Ì„, Ï‡m, Î³m, Ï‡d, Î³d, Î»0, Î½max=Î½max, Î»m=Î»m, Î»d=Î»d, tc=tc)
+    slb, gb = gloc_vjp(h, out["Ï‡0"], out["Î»0"], Î£Ì„, Î»m=Î»m, Î»d=Î»d, Î½max=Î½max)
+    out["Î£_loc"], out["G"] = slb, gb
+    return out
+
+
 def calc_Î£_parts(Ï‡m: Ï‡T, Î³m: Î³T, Ï‡d: Ï‡T, Î³d: Î³T, Î»0, h: lDÎ“AHelper, tc: bool = True, Î»m: float = 0.0,
                  Î»d: float = 0.0) -> np.ndarray:
     """``calc_Î£_parts`` (ladderDGATools_singleCore.jl:149-189) -> [q, Î½_n, 7]."""
@@ -1516,3 +1543,4 @@ calc_chi_gamma_par, collect_chi0, collect_chi, collect_gamma = calc_Ï‡Î³_par, co
 calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Î£_par, calc_Î£_par_, gen_Ï‰_part
 lambda_m_chain_batch = Î»m_chain_batch
 calc_chi_gamma_vjp, calc_Sigma_vjp, chain_vjp_Gamma = calc_Ï‡Î³_vjp, calc_Î£_vjp, chain_vjp_Î“
+chain_vjp_Sigma_loc = chain_vjp_Î£loc

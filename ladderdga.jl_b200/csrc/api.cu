@@ -449,14 +449,15 @@ int ldga_autotune_bse(ldga_ctx* ctx, int32_t channel, int32_t reps, int32_t* var
         const bool prof = ctx->profiling;
         ctx->profiling = false;   // the trial launches stay out of the stage timers
         int st = LDGA_OK;
+        auto cu = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? LDGA_OK : ctx_cuda(ctx, e, what); };
         for (int i = 0; i < nv && st == LDGA_OK; ++i) {
             st = bse_run_variant(ctx, channel, i);                       // warm-up (and smem opt-in)
-            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventRecord(e0, ctx->stream), "cudaEventRecord");
+            if (st == LDGA_OK) st = cu(cudaEventRecord(e0, ctx->stream), "cudaEventRecord");
             for (int r = 0; r < reps && st == LDGA_OK; ++r) st = bse_run_variant(ctx, channel, i);
-            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventRecord(e1, ctx->stream), "cudaEventRecord");
-            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventSynchronize(e1), "cudaEventSynchronize");
+            if (st == LDGA_OK) st = cu(cudaEventRecord(e1, ctx->stream), "cudaEventRecord");
+            if (st == LDGA_OK) st = cu(cudaEventSynchronize(e1), "cudaEventSynchronize");
             float t = 0.f;
-            if (st == LDGA_OK) st = ctx_cuda(ctx, cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+            if (st == LDGA_OK) st = cu(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
             const double per = (double)t / reps;
             if (st == LDGA_OK && (best_ms < 0.0 || per < best_ms)) { best_ms = per; best = i; }
         }
@@ -709,6 +710,80 @@ int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32
     if (chi_m_bar) TRY(copy(ctx, chi_m_bar, d_xm, qw * sizeof(double)));
     if (chi_d_bar) TRY(copy(ctx, chi_d_bar, d_xd, qw * sizeof(double)));
     return sync(ctx);
+}
+
+int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_bar, const double* sigma_bar,
+                  double lam_m, double lam_d, int32_t numax, int32_t n_sigma, double* sigma_loc_bar, double* gloc_bar) {
+    if (!ctx) return LDGA_ERR_ARG;
+    NEED(ctx, ctx->have_ghat, "G adjoint: call ldga_gloc first");
+    if (lambda0_bar) NEED(ctx, ctx->have_F, "G adjoint: F_m missing (call ldga_F_from_chi)");
+    if (sigma_bar) {
+        TRY(eom_inputs_ready(ctx));
+        if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+        if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
+    } else {
+        numax = 0;
+    }
+    if (sigma_loc_bar && n_sigma < 1) return ctx_fail(ctx, LDGA_ERR_ARG, "n_sigma must be >= 1");
+    DeviceGuard g(ctx->device);
+    const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw, nfq = (size_t)ctx->Nf * ctx->Nq;
+    const bool bub = chi0_bar || lambda0_bar;
+    const int nbub = bub ? ctx->Nnu * ctx->Nw : 0, neom = numax * ctx->Nw;
+    // CSR: rows contributing to each fft_range frequency, in increasing row order
+    std::vector<std::vector<int32_t>> lists(ctx->Nf);
+    for (int wi = 0; wi < ctx->Nw && bub; ++wi)
+        for (int vi = 0; vi < ctx->Nnu; ++vi) {
+            const int pi = vi + ctx->Nnu * wi, wn = wi - ctx->sp.n_iw;
+            const int vn = (vi - ctx->sp.n_iv) - ctx->sp.shift * (wn / 2);
+            lists[vn - ctx->fft_lo].push_back(2 * pi);
+            lists[vn + wn - ctx->fft_lo].push_back(2 * pi + 1);
+        }
+    for (int wi = 0; wi < ctx->Nw && numax > 0; ++wi)
+        for (int n = 0; n < numax; ++n) {
+            const int wn = wi - ctx->sp.n_iw;
+            lists[n + wn - ctx->fft_lo].push_back(2 * nbub + n + numax * wi);
+        }
+    for (auto& l : lists) std::sort(l.begin(), l.end());
+    std::vector<int32_t> start(ctx->Nf + 1, 0), idx;
+    for (int f = 0; f < ctx->Nf; ++f) {
+        start[f + 1] = start[f] + (int)lists[f].size();
+        idx.insert(idx.end(), lists[f].begin(), lists[f].end());
+    }
+    DevScratch sc;
+    double2 *d_c0b = nullptr, *d_l0b = nullptr, *d_sb = nullptr, *d_shat = nullptr, *d_rows = nullptr;
+    double2 *d_ghb = nullptr, *d_gb = nullptr, *d_slb = nullptr;
+    int32_t *d_start = nullptr, *d_idx = nullptr;
+    if (bub) {
+        TRY(sc.get(ctx, &d_c0b, qvw));
+        if (chi0_bar) TRY(copy(ctx, d_c0b, chi0_bar, qvw * sizeof(double2)));
+        else LDGA_CUDA(ctx, cudaMemsetAsync(d_c0b, 0, qvw * sizeof(double2), ctx->stream));
+        if (lambda0_bar) {
+            TRY(sc.get(ctx, &d_l0b, qvw));
+            TRY(copy(ctx, d_l0b, lambda0_bar, qvw * sizeof(double2)));
+            TRY(launch_lambda0_vjp(ctx, d_l0b, d_c0b));
+        }
+    }
+    if (numax > 0) {
+        TRY(sc.get(ctx, &d_sb, (size_t)ctx->Nq * numax));
+        TRY(copy(ctx, d_sb, sigma_bar, (size_t)ctx->Nq * numax * sizeof(double2)));
+        TRY(sc.get(ctx, &d_shat, (size_t)ctx->Nq * numax));
+    }
+    TRY(sc.get(ctx, &d_rows, (size_t)(2 * nbub + neom + 1) * ctx->Nq));
+    TRY(sc.get(ctx, &d_start, start.size()));
+    TRY(sc.get(ctx, &d_idx, std::max<size_t>(idx.size(), 1)));
+    TRY(copy(ctx, d_start, start.data(), start.size() * sizeof(int32_t)));
+    if (!idx.empty()) TRY(copy(ctx, d_idx, idx.data(), idx.size() * sizeof(int32_t)));
+    TRY(sc.get(ctx, &d_ghb, nfq));
+    TRY(sc.get(ctx, &d_gb, nfq));
+    TRY(launch_gloc_vjp(ctx, bub ? d_c0b : nullptr, numax > 0 ? d_sb : nullptr, numax, lam_m, lam_d, d_shat, d_rows,
+                        d_start, d_idx, d_ghb, d_gb));
+    if (sigma_loc_bar) {
+        TRY(sc.get(ctx, &d_slb, (size_t)n_sigma));
+        TRY(launch_sigma_loc_grad(ctx, d_gb, n_sigma, d_slb));
+        TRY(copy(ctx, sigma_loc_bar, d_slb, (size_t)n_sigma * sizeof(double2)));
+    }
+    if (gloc_bar) TRY(copy(ctx, gloc_bar, d_gb, nfq * sizeof(double2)));
+    return sync(ctx);   // host vectors (start, idx) outlive the asynchronous copies
 }
 
 int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum, double* parts_out) {

@@ -383,6 +383,161 @@ __global__ void __launch_bounds__(256) k_eom_vjp_chi(int nq, int nw, int numax, 
 }
 
 // ---------------------------------------------------------------------------------------------
+// Adjoint of the lattice G (setup + bubble + the EoM's direct use of Ĝ) -> dL/dΣ_loc.
+//   bubble: χ₀(ν, ω) = s_b S(Ĝ(ν) Ĝ(ν+ω)), s_b = -β/N_k²  ->  P̄ = s_b kMult S(χ̄₀/kMult),
+//           Ĝ̄(ν) += conj(Ĝ(ν+ω)) P̄,  Ĝ̄(ν+ω) += conj(Ĝ(ν)) P̄          (k_bubble_vjp)
+//   EoM:    Σ(n) = c S(Σ_ω K̂(n,ω) Ĝ(ν_n+ω)), K̂ = S(K), c = 1/(β N_k²)
+//           ->  Ĝ̄(ν_n+ω) += c kMult Ŝ̄(n) conj(K̂(n,ω)),  Ŝ̄ = S(Σ̄/kMult)   (k_eom_gvjp)
+// Each (ν, ω) term writes its contribution to its own scratch row; k_ghat_gather sums, per
+// frequency of fft_range, the rows that touch it in a fixed (host-computed) order.  Then
+// Ḡ = kMult S(Ĝ̄/kMult) (k_vjp_transform) and, from G = 1/(iν + μ - ε - Σ_loc),
+//   Σ̄_loc(m) = Σ_q conj(G²) Ḡ over ν_m,  + Σ_q conj(Ḡ) G² over ν_{-m-1}   (k_sigma_loc_grad).
+// ---------------------------------------------------------------------------------------------
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_bubble_vjp(
+    const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double sb,
+    const double* __restrict__ kmult, const double2* __restrict__ ghat, const double2* __restrict__ chi0_bar,
+    double2* __restrict__ rows) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int total = nnu * nw;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, total - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        bufA[p * NQ + q] = cscale(chi0_bar[(size_t)(p0 + p) * NQ + q], 1.0 / kmult[q]);
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        const int pi = p0 + p;
+        const int wi = pi / nnu, vi = pi - wi * nnu;
+        const int wn = wi - n_iw;
+        const int vn = (vi - n_iv) - shift * (wn / 2);
+        const double2 pb = cscale(v, sb * kmult[q]);
+        const double2 g1 = ghat[(size_t)(vn - fft_lo) * NQ + q], g2 = ghat[(size_t)(vn + wn - fft_lo) * NQ + q];
+        rows[(size_t)(2 * pi) * NQ + q] = cmul(cconj(g2), pb);       // -> frequency vn
+        rows[(size_t)(2 * pi + 1) * NQ + q] = cmul(cconj(g1), pb);   // -> frequency vn + wn
+    });
+}
+
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_eom_gvjp(
+    const TMat<M> T, const EomArgs a, double c, const double* __restrict__ kmult, const double2* __restrict__ shat,
+    const double* __restrict__ chi_m, const double2* __restrict__ gam_m, const double* __restrict__ chi_d,
+    const double2* __restrict__ gam_d, const double2* __restrict__ lambda0, double2* __restrict__ rows) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int total = a.numax * a.nw;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, total - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    __shared__ int s_vi[16];
+    if (threadIdx.x < np) {
+        const int pi = p0 + threadIdx.x;
+        const int wi = pi / a.numax, n = pi - wi * a.numax;
+        const int v0 = a.n_iv + a.shift * ((wi - a.n_iw) / 2);
+        const int len = min(a.numax, 2 * a.n_iv - v0);
+        s_vi[threadIdx.x] = (n < len && v0 + n >= 0) ? v0 + n : -1;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        const int wi = (p0 + p) / a.numax;
+        const int vi = s_vi[p];
+        double2 K = make_double2(0.0, 0.0);
+        if (vi >= 0) {
+            const size_t iq = (size_t)q + (size_t)NQ * wi;
+            const size_t iv = (size_t)q + (size_t)NQ * (vi + (size_t)a.nnu * wi);
+            K = eom_value(a, gam_m[iv], gam_d[iv], chi_lam(chi_m[iq], a.lam_m), chi_lam(chi_d[iq], a.lam_d), lambda0[iv]);
+        }
+        bufA[p * NQ + q] = K;
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        const int pi = p0 + p;
+        const int n = pi - (pi / a.numax) * a.numax;
+        double2 r = make_double2(0.0, 0.0);
+        if (s_vi[p] >= 0) r = cmul(cscale(shat[(size_t)n * NQ + q], c * kmult[q]), cconj(v));
+        rows[(size_t)pi * NQ + q] = r;
+    });
+}
+
+// out(f) = (mul_kmult ? kMult : 1) S(in(f) / kMult) for nf vectors of the wedge
+template <int DIM, int M>
+__global__ void __launch_bounds__(kThreads) k_vjp_transform(const TMat<M> T, int nf, int mul_kmult,
+                                                            const double* __restrict__ kmult,
+                                                            const double2* __restrict__ in, double2* __restrict__ out) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int NQ = S::NQ;
+    extern __shared__ double2 smem[];
+    const int np_max = (int)gridDim.y;
+    const int p0 = blockIdx.x * np_max;
+    const int np = min(np_max, nf - p0);
+    double2* bufA = smem;
+    double2* bufB = smem + np_max * S::BUF_A;
+    for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
+        const int p = it / NQ, q = it - p * NQ;
+        bufA[p * NQ + q] = cscale(in[(size_t)(p0 + p) * NQ + q], 1.0 / kmult[q]);
+    }
+    __syncthreads();
+    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+        out[(size_t)(p0 + p) * NQ + q] = mul_kmult ? cscale(v, kmult[q]) : v;
+    });
+}
+
+// Ĝ̄[f][q] = Σ_{j in list(f)} rows[idx[j]][q], CSR over the fft_range frequencies, fixed order
+__global__ void __launch_bounds__(256) k_ghat_gather(int nf, int nq, const int32_t* __restrict__ start,
+                                                      const int32_t* __restrict__ idx, const double2* __restrict__ rows,
+                                                      double2* __restrict__ gbar) {
+    const size_t n = (size_t)nf * nq;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int f = (int)(e / nq), q = (int)(e % nq);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int j = start[f]; j < start[f + 1]; ++j) acc = cadd(acc, rows[(size_t)idx[j] * nq + q]);
+        gbar[e] = acc;
+    }
+}
+
+// Σ̄_loc(m), m = 0..n_sigma-1: one CTA per m, fixed-order block reduction over q
+__global__ void __launch_bounds__(256) k_sigma_loc_grad(int nq, int nf, int fft_lo, int n_sigma,
+                                                         const double2* __restrict__ gloc, const double2* __restrict__ gbar,
+                                                         double2* __restrict__ out) {
+    __shared__ double2 red[8];
+    const int m = blockIdx.x;
+    if (m >= n_sigma) return;
+    double2 acc = make_double2(0.0, 0.0);
+    const int fp = m - fft_lo, fn = -m - 1 - fft_lo;   // columns of ν_m and ν_{-m-1}
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        if (fp >= 0 && fp < nf) {
+            const double2 g = gloc[(size_t)fp * nq + q];
+            acc = cadd(acc, cmul(cconj(cmul(g, g)), gbar[(size_t)fp * nq + q]));
+        }
+        if (fn >= 0 && fn < nf) {
+            const double2 g = gloc[(size_t)fn * nq + q];
+            acc = cadd(acc, cmul(cconj(gbar[(size_t)fn * nq + q]), cmul(g, g)));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 r = make_double2(0.0, 0.0);
+        for (int i = 0; i < 8; ++i) r = cadd(r, red[i]);
+        out[m] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host-side dispatch on (DIM, M)
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M>
@@ -467,6 +622,64 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
                                                hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,
                                                add_hartree);
     LDGA_LAUNCHED(ctx, "k_eom_inverse");
+    return LDGA_OK;
+}
+
+template <int DIM, int M>
+int run_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, int numax, double lam_m, double lam_d,
+                 double2* shat, double2* rows, const int32_t* start, const int32_t* idx, double2* gbar_hat,
+                 double2* gbar) {
+    const int nbub = chi0_bar ? ctx->Nnu * ctx->Nw : 0;
+    if (chi0_bar) {
+        const int np = pairs_per_cta<DIM, M>(nbub);
+        const size_t sm = smem_bytes<DIM, M>(np);
+        auto kern = k_bubble_vjp<DIM, M>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        dim3 grid((nbub + np - 1) / np, np);
+        const double sb = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
+                                                   ctx->sp.shift, ctx->fft_lo, sb, ctx->d_kmult, ctx->d_ghat, chi0_bar,
+                                                   rows);
+        LDGA_LAUNCHED(ctx, "k_bubble_vjp");
+    }
+    if (sbar) {
+        {
+            const int np = pairs_per_cta<DIM, M>(numax);
+            const size_t sm = smem_bytes<DIM, M>(np);
+            auto kern = k_vjp_transform<DIM, M>;
+            LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+            dim3 grid((numax + np - 1) / np, np);
+            kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, 0, ctx->d_kmult, sbar, shat);
+            LDGA_LAUNCHED(ctx, "k_vjp_transform");
+        }
+        const int total = numax * ctx->Nw;
+        const int np = pairs_per_cta<DIM, M>(total);
+        const size_t sm = smem_bytes<DIM, M>(np);
+        auto kern = k_eom_gvjp<DIM, M>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        EomArgs a;
+        a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
+        a.fft_lo = ctx->fft_lo; a.numax = numax; a.w_per_chunk = 1;
+        a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = -1;
+        a.lam_m_dev = nullptr; a.lam_d_dev = nullptr;
+        dim3 grid((total + np - 1) / np, np);
+        const double c = 1.0 / (ctx->mp.beta * (double)ctx->Nk * (double)ctx->Nk);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, c, ctx->d_kmult, shat, ctx->d_chi[0], ctx->d_gam[0],
+                                                   ctx->d_chi[1], ctx->d_gam[1], ctx->d_lambda0,
+                                                   rows + (size_t)2 * nbub * ctx->Nq);
+        LDGA_LAUNCHED(ctx, "k_eom_gvjp");
+    }
+    k_ghat_gather<<<2 * 148, 256, 0, ctx->stream>>>(ctx->Nf, ctx->Nq, start, idx, rows, gbar_hat);
+    LDGA_LAUNCHED(ctx, "k_ghat_gather");
+    {
+        const int np = pairs_per_cta<DIM, M>(ctx->Nf);
+        const size_t sm = smem_bytes<DIM, M>(np);
+        auto kern = k_vjp_transform<DIM, M>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        dim3 grid((ctx->Nf + np - 1) / np, np);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, 1, ctx->d_kmult, gbar_hat, gbar);
+        LDGA_LAUNCHED(ctx, "k_vjp_transform");
+    }
     return LDGA_OK;
 }
 
@@ -562,4 +775,19 @@ int launch_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc,
     LDGA_FOR_EACH_GRID(LDGA_CASE)
 #undef BODY
     return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}
+
+int launch_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, int numax, double lam_m,
+                    double lam_d, double2* shat, double2* rows, const int32_t* start, const int32_t* idx,
+                    double2* gbar_hat, double2* gbar) {
+#define BODY(D, MM) run_gloc_vjp<D, MM>(ctx, chi0_bar, sbar, numax, lam_m, lam_d, shat, rows, start, idx, gbar_hat, gbar)
+    LDGA_FOR_EACH_GRID(LDGA_CASE)
+#undef BODY
+    return ctx_fail(ctx, LDGA_ERR_ARG, "unsupported k-grid size");
+}
+
+int launch_sigma_loc_grad(ldga_ctx* ctx, const double2* gbar, int n_sigma, double2* out) {
+    k_sigma_loc_grad<<<n_sigma, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nf, ctx->fft_lo, n_sigma, ctx->d_gloc, gbar, out);
+    LDGA_LAUNCHED(ctx, "k_sigma_loc_grad");
+    return LDGA_OK;
 }

@@ -162,6 +162,16 @@ __global__ void k_lambda0(int nq, int nnu, int nw, double inv_beta2, const doubl
     }
 }
 
+// adjoint of k_lambda0 with respect to chi0: chi0_bar += lambda0_bar conj(colF) / beta^2
+__global__ void k_lambda0_vjp(int nq, int nnu, int nw, double inv_beta2, const double2* __restrict__ colF,
+                              const double2* __restrict__ l0_bar, double2* __restrict__ chi0_bar) {
+    const size_t total = (size_t)nq * nnu * nw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t vw = e / nq;
+        chi0_bar[e] = cadd(chi0_bar[e], cscale(cmul(l0_bar[e], cconj(colF[vw])), inv_beta2));
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // sum_kω (DataTypes.jl:230-249):  (sum_w [ sum_q kMult f(chi)/N_k - c2/(i w)^2 ] - beta^2 c2/12)/beta
 // ---------------------------------------------------------------------------------------------
@@ -511,6 +521,16 @@ int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_
     k_F_from_chi<<<256, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw, ctx->sp.shift,
                                               ctx->mp.beta, d_chi_loc, d_gimp, ctx->d_F);
     LDGA_LAUNCHED(ctx, "k_F_from_chi");
+    return LDGA_OK;
+}
+
+int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar) {
+    double2* colF = reinterpret_cast<double2*>(ctx->d_red + 64);
+    k_colsum_F<<<64, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
+    LDGA_LAUNCHED(ctx, "k_colsum_F");
+    k_lambda0_vjp<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, ctx->Nw, 1.0 / (ctx->mp.beta * ctx->mp.beta),
+                                                    colF, l0_bar, chi0_bar);
+    LDGA_LAUNCHED(ctx, "k_lambda0_vjp");
     return LDGA_OK;
 }
 

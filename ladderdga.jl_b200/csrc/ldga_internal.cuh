@@ -200,8 +200,18 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
 int launch_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, const double2* sbar,
                    double2* gm_bar, double2* gd_bar, double2* l0_bar, double* xm_bar, double* xd_bar, double2* shat,
                    double* cm, double* cd);
+// Adjoint of the lattice G: bubble part (chi0_bar [Nq, Nnu, Nw], may be null) and the EoM's direct
+// use of Ghat (sbar [numax][Nq], may be null) -> rows (scratch, one per term), gathered by the CSR
+// lists start/idx per fft_range frequency into gbar_hat [Nf][Nq]; gbar = kMult S(gbar_hat/kMult).
+int launch_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, int numax, double lam_m,
+                    double lam_d, double2* shat, double2* rows, const int32_t* start, const int32_t* idx,
+                    double2* gbar_hat, double2* gbar);
+// Sigma_loc_bar(m), m < n_sigma, from gbar [Nf][Nq] and the handle's G (d_gloc)
+int launch_sigma_loc_grad(ldga_ctx* ctx, const double2* gbar, int n_sigma, double2* out);
 int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_gimp, int n_gimp);
 int launch_lambda0(ldga_ctx* ctx);
+// chi0_bar += lambda0_bar conj(sum_nu F) / beta^2 (adjoint of launch_lambda0 with F fixed)
+int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar);
 // EoM forward + inverse.  lam_*_dev (may be null) are device scalars added to lam_m / lam_d.
 int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lam_m_dev,
                const double* lam_d_dev, int part, const double* d_tail, int tc, double chiloc_m_sum,

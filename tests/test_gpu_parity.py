@@ -487,3 +487,57 @@ def test_autotune_bse(case, prec):
             assert rel(x.data, ref[f"chi_{t}"].data) < RTOL and rel(gm.data, ref[f"gamma_{t}"]) < RTOL, (name, t)
     finally:
         L.tune_reset()
+
+
+def _oracle_sigma_loss(ref, sigma_loc, numax, lm, ld):
+    """L = Σ_k,ν |Σ_ladder|² of the oracle chain at fixed λ with the lattice Σ_loc replaced
+    (G_imp, F_m and Γ_r held fixed): G -> bubble -> BSE (m, d) -> λ₀ -> EoM."""
+    r = ref["h"]
+    G_irr = R.lattice_G(r.kG, sigma_loc, r.mP, r.sP.fft_range)
+    ghat, grhat = R.G_fft(r.kG, G_irr)
+    chi0 = R.calc_bubble(ghat, grhat, r.kG, r.mP, r.sP)
+    xm, gm = R.calc_chi_gamma("m", r.Gamma_m, chi0, r.mP, r.sP)
+    xd, gd = R.calc_chi_gamma("d", r.Gamma_d, chi0, r.mP, r.sP)
+    cm = R.ChiT(xm, r.mP.beta, tail_c=[0, 0, r.mP.Ekin_DMFT])
+    cd = R.ChiT(xd, r.mP.beta, tail_c=[0, 0, r.mP.Ekin_DMFT])
+    l0 = R.calc_lambda0(chi0, R.F_m_of(r), r.mP, r.sP)
+    S_ = R.calc_Sigma(cm, gm, cd, gd, r.chiloc_m_sum, l0, grhat, r.kG, r.mP, r.sP, numax=numax, lam_m=lm, lam_d=ld)
+    return float(np.sum(r.kG.kMult[:, None] * np.abs(S_) ** 2))
+
+
+@pytest.mark.parametrize("cname", ["2d16", "3d8", "2d6_shift"])
+def test_chain_vjp_sigma_loc(cname, require_gpu):
+    """Gradient of L = Σ_k,ν |Σ_ladder|² (fixed λ) with respect to the lattice Σ_loc through G, the
+    bubble, both BSE channels, λ₀ and the EoM: against central differences of the GPU chain and of
+    the oracle's FP64 chain (the reference path's gradient along the same direction)."""
+    inp = S.make_input(**CASES[cname])
+    ref = R.run_chain(inp, lambda_type=None)
+    rng = np.random.default_rng(14)
+    g = gpu_chain(inp)
+    h = g["h"]
+    numax, lm, ld = h.sP.n_iν, 0.1, 0.05
+    ctx = h.ctx
+    kmult = ctx.kmult
+    sig0 = np.array(h.Σ_loc)
+
+    def gpu_loss(sig):
+        ctx.call("ldga_gloc", L._lib.ptr(np.ascontiguousarray(sig)), len(sig), None)
+        chi0 = L.calc_bubble(h)
+        xm, gm = L.calc_χγ("m", h, chi0)
+        xd, gd = L.calc_χγ("d", h, chi0)
+        l0 = L.calc_λ0(chi0, h)
+        S_ = L.calc_Σ(xm, gm, xd, gd, l0, h, νmax=numax, λm=lm, λd=ld)
+        return float(np.sum(kmult[:, None] * np.abs(S_) ** 2)), (xm, gm, xd, gd, l0, S_)
+
+    L0, (xm, gm, xd, gd, l0, S0) = gpu_loss(sig0)
+    grad = L.chain_vjp_Σloc(h, 2.0 * kmult[:, None] * S0, xm, gm, xd, gd, l0, νmax=numax, λm=lm, λd=ld)
+    d = _cgauss(rng, sig0.shape)
+    eps = 1e-6 * np.max(np.abs(sig0)) / np.max(np.abs(d))
+    fd_gpu = (gpu_loss(sig0 + eps * d)[0] - gpu_loss(sig0 - eps * d)[0]) / (2 * eps)
+    fd_ref = (_oracle_sigma_loss(ref, sig0 + eps * d, numax, lm, ld)
+              - _oracle_sigma_loss(ref, sig0 - eps * d, numax, lm, ld)) / (2 * eps)
+    an = float(np.sum(np.real(np.conj(grad["Σ_loc"]) * d)))
+    scale = np.sum(np.abs(grad["Σ_loc"]) * np.abs(d))
+    assert abs(fd_gpu - an) <= 1e-6 * scale, (cname, fd_gpu, an)
+    assert abs(fd_ref - an) <= 1e-6 * scale, (cname, fd_ref, an)
+    gpu_loss(sig0)
