@@ -156,6 +156,29 @@ int alloc_all(ldga_ctx* c) {
     TRY(dev_alloc(c, &c->d_count, 4));
     if (bse_pivot_smem((int)nnu) > LDGA_PIVOT_SMEM_MAX)
         TRY(dev_alloc(c, &c->d_pivot_scratch, (size_t)LDGA_PIVOT_GRID * nnu * (nnu + 1)));
+    {   // bubble representatives: pair (vi, wi) and its conjugate partner nu'' = -nu - w - 1 in the box
+        std::vector<int2> pairs;
+        std::vector<char> done(nnu * nw, 0);
+        for (int wi = 0; wi < (int)nw; ++wi)
+            for (int vi = 0; vi < (int)nnu; ++vi) {
+                const int pi = vi + (int)nnu * wi;
+                if (done[pi]) continue;
+                const int wn = wi - c->sp.n_iw, sh = c->sp.shift * (wn / 2);
+                const int vn = (vi - c->sp.n_iv) - sh;
+                const int vi2 = (-vn - wn - 1) + c->sp.n_iv + sh;
+                int pj = -1;
+                if (vi2 >= 0 && vi2 < (int)nnu && vi2 != vi) {
+                    pj = vi2 + (int)nnu * wi;
+                    done[pj] = 1;
+                }
+                done[pi] = 1;
+                pairs.push_back(make_int2(pi, pj));
+            }
+        c->n_bub_pairs = (int)pairs.size();
+        TRY(dev_alloc(c, &c->d_bub_pairs, pairs.size()));
+        TRY(copy(c, c->d_bub_pairs, pairs.data(), pairs.size() * sizeof(int2)));
+        TRY(sync(c));   // the host vector goes out of scope
+    }
     TRY(copy(c, c->d_kmult, c->kmult.data(), nq * sizeof(double)));
     TRY(copy(c, c->d_eps, c->eps.data(), nq * sizeof(double)));
     return sync(c);
@@ -165,7 +188,7 @@ void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
                     c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
-                    c->d_pivot_scratch};
+                    c->d_pivot_scratch, c->d_bub_pairs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

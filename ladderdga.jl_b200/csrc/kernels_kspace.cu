@@ -75,23 +75,26 @@ __global__ void __launch_bounds__(kThreads) k_gloc_transform(
 
 // ---------------------------------------------------------------------------------------------
 // a2: chi0[q, nu, w] = -beta/N_k^2 S(Ghat(nu) Ghat(nu+w))(q)
+// G(k, -nu) = conj(G(k, nu)) (nu_n -> nu_{-n-1}) and G is even in k, so
+//   chi0(q, nu'', w) = conj(chi0(q, nu, w)),  nu'' = -nu - w - 1,
+// and a pair whose partner lies in the box is computed once: `pairs` lists the representatives
+// (pair index vi + Nnu wi, partner's index or -1), built on the host with the handle.
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_bubble(
     const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double scale,
-    const double2* __restrict__ ghat, double2* __restrict__ chi0) {
+    const double2* __restrict__ ghat, const int2* __restrict__ pairs, int total, double2* __restrict__ chi0) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
     const int np_max = (int)gridDim.y;
-    const int total = nnu * nw;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, total - p0);
     double2* bufA = smem;
     double2* bufB = smem + np_max * S::BUF_A;
     for (int it = threadIdx.x; it < np * NQ; it += blockDim.x) {
         const int p = it / NQ, q = it - p * NQ;
-        const int pi = p0 + p;
+        const int pi = pairs[p0 + p].x;
         const int wi = pi / nnu, vi = pi - wi * nnu;
         const int wn = wi - n_iw;
         const int vn = (vi - n_iv) - shift * (wn / 2);    // C division truncates like trunc(Int, .)
@@ -101,7 +104,10 @@ __global__ void __launch_bounds__(kThreads) k_bubble(
     }
     __syncthreads();
     sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
-        chi0[(size_t)(p0 + p) * NQ + q] = cscale(v, scale);
+        const int2 pp = pairs[p0 + p];
+        const double2 c = cscale(v, scale);
+        chi0[(size_t)pp.x * NQ + q] = c;
+        if (pp.y >= 0) chi0[(size_t)pp.y * NQ + q] = cconj(c);
     });
 }
 
@@ -557,7 +563,7 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
 
 template <int DIM, int M>
 int run_bubble(ldga_ctx* ctx) {
-    const int total = ctx->Nnu * ctx->Nw;
+    const int total = ctx->n_bub_pairs;
     const int np = pairs_per_cta<DIM, M>(total);
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_bubble<DIM, M>;
@@ -566,7 +572,8 @@ int run_bubble(ldga_ctx* ctx) {
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
     StageTimer st_(ctx, LDGA_STAGE_BUBBLE);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
-                                               ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_chi0);
+                                               ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_bub_pairs, total,
+                                               ctx->d_chi0);
     LDGA_LAUNCHED(ctx, "k_bubble");
     return LDGA_OK;
 }

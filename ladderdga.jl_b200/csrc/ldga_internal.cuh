@@ -106,6 +106,8 @@ struct ldga_ctx {
     int32_t* d_list = nullptr;     // compacted fallback list
     int32_t* d_count = nullptr;
     double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
+    int2* d_bub_pairs = nullptr;          // bubble pairs computed directly (pair, conjugate partner or -1)
+    int n_bub_pairs = 0;
 
     cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
     bool capturing = false;              // a CUDA graph of the chain is being captured
