@@ -179,6 +179,12 @@ int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32
 int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_bar, const double* sigma_bar,
                   double lam_m, double lam_d, int32_t numax, int32_t n_sigma, double* sigma_loc_bar, double* gloc_bar);
 
+/* Gradient of E_pot,1 (calc_E, thermodynamics.jl:142-168, on G_from_Σladder!, GFTools.jl:154-186)
+ * with respect to Sigma_ladder [Nq, numax] (complex, dE/dRe + i dE/dIm), μ following the filling
+ * condition the μ fit solves (μ = the fitted value).  The piece of the λdm implicit derivative
+ * that goes through the energies. */
+int ldga_epot_vjp(ldga_ctx* ctx, int32_t numax, double mu, const double* sigma, double* sigma_bar);
+
 /* Tile-shape autotuning of the BSE kernel (no reference counterpart; the reference has one LAPACK
  * path).  Every fast-path box size has a few compiled configurations per precision mode (threads
  * per matrix, CTAs per SM the register allocation allows); this times each one `reps` times on the

@@ -1088,6 +1088,56 @@ def chain_vjp_Σloc(h: lDΓAHelper, Σ̄, χm: χT, γm: γT, χd: χT, γd: γT
     return out
 
 
+def epot_vjp(h: lDΓAHelper, Σ, μ: float) -> np.ndarray:
+    """∂E_pot,1/∂Σ_ladder [Nq, νmax] (complex gradient) of ``calc_E`` on ``G_from_Σladder!`` with μ
+    following the filling condition (``ldga_epot_vjp``)."""
+    S = as_fc(Σ)
+    out = _lib.cplx_out(S.shape)
+    h.ctx.call("ldga_epot_vjp", S.shape[1], float(μ), ptr(S), ptr(out))
+    return out
+
+
+def λdm_vjp(h: lDΓAHelper, χm: χT, γm: γT, χd: χT, γd: γT, λ0, res: "λ_result", Σ̄=None, Ē: float = 0.0) -> dict:
+    """Gradient of L = f(Σ_ladder) + Ē·E_pot,1 evaluated at the λdm root (``λdm_correction``,
+    conditions_new.jl:207-324) with respect to Γ_m, Γ_d, Σ_loc, χ₀ and λ₀, including the implicit
+    dependence of (λm, λd) on them: with F(λ) = [PP_2 - n/2(1-n/2), E_pot,1 - E_pot,2] = 0,
+        dL/dθ = ∂L/∂θ + wᵀ ∂F/∂θ,   Jᵀ w = -∂L/∂λ,   J = ∂F/∂λ (analytic, 2 x 2).
+    Σ̄ = ∂f/∂Σ_ladder [Nq, νmax] at the root (None = 0).  ``res`` is the λ_result of the λdm call on
+    this handle; χm, χd are the unshifted (λ = 0) susceptibilities it was computed from."""
+    if χm.λ != 0 or χd.λ != 0:
+        raise RuntimeError("λdm_vjp: χ must be unshifted (λ = 0), as for λdm_correction")
+    ctx = h.ctx
+    S = as_fc(res.Σ_ladder)
+    nu = S.shape[1]
+    lm, ld, mu = float(res.λm), float(res.λd), float(res.μ)
+    U, β = h.mP.U, h.mP.β
+    kmult = np.asarray(ctx.kmult)
+    SE = epot_vjp(h, S, mu)
+    SL = (np.zeros_like(SE) if Σ̄ is None else as_fc(Σ̄)) + Ē * SE
+    oL = calc_Σ_vjp(SL, χm, γm, χd, γd, λ0, h, νmax=nu, λm=lm, λd=ld)
+    oE = calc_Σ_vjp(SE, χm, γm, χd, γd, λ0, h, νmax=nu, λm=lm, λd=ld)
+    xm, xd = np.asarray(χm.data), np.asarray(χd.data)
+    dL = np.array([-np.sum(oL[0] * xm**2), -np.sum(oL[2] * xd**2)])
+    dE1 = np.array([-np.sum(oE[0] * xm**2), -np.sum(oE[2] * xd**2)])
+    dsm, dsd = _lib.C.c_double(), _lib.C.c_double()
+    ctx.call("ldga_sum_kw", CH_M, lm, 1, _lib.C.byref(dsm))
+    ctx.call("ldga_sum_kw", CH_D, ld, 1, _lib.C.byref(dsd))
+    J = np.array([[0.5 * dsm.value, 0.5 * dsd.value],
+                  [dE1[0] + 0.5 * U * dsm.value, dE1[1] - 0.5 * U * dsd.value]])
+    w = np.linalg.solve(J.T, -dL)
+    # ∂s/∂χ(q, ω) of sum_kω at λ for the unshifted χ
+    nk = float(np.sum(kmult))
+    dsm_dx = (kmult[:, None] / (β * nk)) / (lm * xm + 1.0) ** 2
+    dsd_dx = (kmult[:, None] / (β * nk)) / (ld * xd + 1.0) ** 2
+    xmb = oL[0] + w[1] * oE[0] + (0.5 * w[0] + 0.5 * U * w[1]) * dsm_dx
+    xdb = oL[2] + w[1] * oE[2] + (0.5 * w[0] - 0.5 * U * w[1]) * dsd_dx
+    gmb, gdb, l0b = oL[1] + w[1] * oE[1], oL[3] + w[1] * oE[3], oL[4] + w[1] * oE[4]
+    Gmb, c0m = calc_χγ_vjp("m", h, xmb, gmb)
+    Gdb, c0d = calc_χγ_vjp("d", h, xdb, gdb)
+    slb, gb = gloc_vjp(h, c0m + c0d, l0b, SL + w[1] * SE, λm=lm, λd=ld, νmax=nu)
+    return {"Γ_m": Gmb, "Γ_d": Gdb, "Σ_loc": slb, "χ0": c0m + c0d, "λ0": l0b, "w": w, "J": J, "∂L/∂λ": dL}
+
+
 def calc_Σ_parts(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, tc: bool = True, λm: float = 0.0,
                  λd: float = 0.0) -> np.ndarray:
     """``calc_Σ_parts`` (ladderDGATools_singleCore.jl:149-189) -> [q, ν_n, 7]."""
@@ -1544,3 +1594,4 @@ calc_Sigma_par, calc_Sigma_par_, gen_w_part = calc_Σ_par, calc_Σ_par_, gen_ω_
 lambda_m_chain_batch = λm_chain_batch
 calc_chi_gamma_vjp, calc_Sigma_vjp, chain_vjp_Gamma = calc_χγ_vjp, calc_Σ_vjp, chain_vjp_Γ
 chain_vjp_Sigma_loc = chain_vjp_Σloc
+lambda_dm_vjp = λdm_vjp

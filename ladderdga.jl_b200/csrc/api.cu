@@ -456,6 +456,22 @@ int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const do
     return LDGA_OK;
 }
 
+int ldga_epot_vjp(ldga_ctx* ctx, int32_t numax, double mu, const double* sigma, double* sigma_bar) {
+    if (!ctx || !sigma || !sigma_bar) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    if (!std::isfinite(mu)) return ctx_fail(ctx, LDGA_ERR_ARG, "μ must be finite");
+    DeviceGuard g(ctx->device);
+    const size_t n = (size_t)ctx->Nq * numax;
+    DevScratch sc;
+    double2 *d_s = nullptr, *d_o = nullptr;
+    TRY(sc.get(ctx, &d_s, n));
+    TRY(sc.get(ctx, &d_o, n));
+    TRY(copy(ctx, d_s, sigma, n * sizeof(double2)));
+    TRY(launch_epot_vjp(ctx, numax, mu, d_s, d_o));
+    TRY(copy(ctx, sigma_bar, d_o, n * sizeof(double2)));
+    return sync(ctx);
+}
+
 int ldga_autotune_bse(ldga_ctx* ctx, int32_t channel, int32_t reps, int32_t* variant, double* ms) {
     if (!ctx) return LDGA_ERR_ARG;
     if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");

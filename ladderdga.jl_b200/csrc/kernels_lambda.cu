@@ -524,6 +524,66 @@ int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_
     return LDGA_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Gradient of E_pot,1 = calc_E(G_ladder(Σ, μ(Σ)), Σ, μ) with respect to Σ_ladder [Nq, numax]
+// (thermodynamics.jl:142-168, GFTools.jl:154-186), μ following the filling condition
+// f(μ, Σ) = 2(2 Re Σ_n G_k(n)/β + 1/2 + μ s)/(1 + U s) - n = 0 (s = G_shell_sum):
+//   G = 1/(iν_n + μ - ε - Σ),  A = (2/(β N_k)) kMult conj(G (1 + Σ G))          (∂E/∂Σ at fixed μ)
+//   ∂E/∂μ = (1/(β N_k)) Σ_q kMult [2 Σ_n (Re(-G² Σ) - U n/2 / ν_n²) + β² U n/8]
+//   ∂f/∂μ = 2 (2 Re Σ_n (1/N_k) Σ_q kMult (-G²)/β + s)/(1 + U s),
+//   B = 4/(β (1 + U s)) kMult/N_k conj(G²)                                      (∂f/∂Σ)
+//   out = A - (∂E/∂μ / ∂f/∂μ) B.   One CTA: two fixed-order reductions, then the elementwise pass.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_epot_vjp(int nq, int numax, double beta, double U, double nfill, double mu,
+                                                   double shell, double inv_nk, const double* __restrict__ kmult,
+                                                   const double* __restrict__ eps, const double2* __restrict__ sigma,
+                                                   double2* __restrict__ out) {
+    __shared__ double red[2][32];
+    const double hartree = nfill * U / 2.0;
+    double dEdmu = 0.0, dfdmu = 0.0;
+    const int total = nq * numax;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int q = e % nq, n = e / nq;
+        const double vn = (2.0 * n + 1.0) * M_PI / beta;
+        const double2 s = sigma[e];
+        const double2 g = cinv(make_double2(mu - eps[q] - s.x, vn - s.y));
+        const double2 g2 = cmul(g, g);
+        const double2 g2s = cmul(g2, s);
+        dEdmu += kmult[q] * (2.0 * (-g2s.x - hartree / (vn * vn)));
+        dfdmu += kmult[q] * (-g2.x);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dEdmu += __shfl_down_sync(0xffffffffu, dEdmu, o);
+        dfdmu += __shfl_down_sync(0xffffffffu, dfdmu, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = dEdmu; red[1][threadIdx.x >> 5] = dfdmu; }
+    __syncthreads();
+    double sE = 0.0, sf = 0.0, km = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { sE += red[0][i]; sf += red[1][i]; }
+    for (int q = 0; q < nq; ++q) km += kmult[q];                                // N_k
+    // the tail constant β² U n/8 per k point, weighted by kMult: Σ_q kMult = N_k
+    const double dE = (sE + km * beta * beta * hartree / 4.0) * inv_nk / beta;
+    const double df = 2.0 * (2.0 * sf * inv_nk / beta + shell) / (1.0 + U * shell);
+    const double r = dE / df;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int q = e % nq, n = e / nq;
+        const double vn = (2.0 * n + 1.0) * M_PI / beta;
+        const double2 s = sigma[e];
+        const double2 g = cinv(make_double2(mu - eps[q] - s.x, vn - s.y));
+        const double2 a = cscale(cconj(cmul(g, cadd(make_double2(1.0, 0.0), cmul(s, g)))), 2.0 * kmult[q] * inv_nk / beta);
+        const double2 b = cscale(cconj(cmul(g, g)), 4.0 / (beta * (1.0 + U * shell)) * kmult[q] * inv_nk);
+        out[e] = make_double2(a.x - r * b.x, a.y - r * b.y);
+    }
+}
+
+int launch_epot_vjp(ldga_ctx* ctx, int numax, double mu, const double2* sigma, double2* out) {
+    k_epot_vjp<<<1, 1024, 0, ctx->stream>>>(ctx->Nq, numax, ctx->mp.beta, ctx->mp.U, ctx->mp.n, mu,
+                                            host_G_shell_sum(numax + 1, ctx->mp.beta), 1.0 / (double)ctx->Nk,
+                                            ctx->d_kmult, ctx->d_eps, sigma, out);
+    LDGA_LAUNCHED(ctx, "k_epot_vjp");
+    return LDGA_OK;
+}
+
 int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar) {
     double2* colF = reinterpret_cast<double2*>(ctx->d_red + 64);
     k_colsum_F<<<64, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);

@@ -214,6 +214,8 @@ int launch_F_from_chi(ldga_ctx* ctx, const double2* d_chi_loc, const double2* d_
 int launch_lambda0(ldga_ctx* ctx);
 // chi0_bar += lambda0_bar conj(sum_nu F) / beta^2 (adjoint of launch_lambda0 with F fixed)
 int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar);
+// dE_pot,1/dΣ_ladder [Nq, numax] with μ following the filling condition (calc_E after G_from_Σladder!)
+int launch_epot_vjp(ldga_ctx* ctx, int numax, double mu, const double2* sigma, double2* out);
 // EoM forward + inverse.  lam_*_dev (may be null) are device scalars added to lam_m / lam_d.
 int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* lam_m_dev,
                const double* lam_d_dev, int part, const double* d_tail, int tc, double chiloc_m_sum,

@@ -541,3 +541,40 @@ def test_chain_vjp_sigma_loc(cname, require_gpu):
     assert abs(fd_gpu - an) <= 1e-6 * scale, (cname, fd_gpu, an)
     assert abs(fd_ref - an) <= 1e-6 * scale, (cname, fd_ref, an)
     gpu_loss(sig0)
+
+
+def test_lambda_dm_vjp(require_gpu):
+    """North-star configuration 4's loss L = Σ_k,ν |Σ_ladder|² + E_pot,1 after the λdm correction:
+    its gradient with respect to Γ_m and the lattice Σ_loc, through the implicit dependence of
+    (λm, λd) on them, against central differences of the GPU chain re-solved at every point (λdm to
+    a residual of 1e-12)."""
+    inp = S.make_input(dim=3, ns=8, beta=5.0, U=1.2, n_iv=4, n_iw=4, seed=77)
+    rng = np.random.default_rng(15)
+    h = L.setup_synthetic(inp)
+    ctx = h.ctx
+    kmult = ctx.kmult
+    Gm0, sig0 = np.array(h.Γ_m), np.array(h.Σ_loc)
+
+    def forward(Gm, sig):
+        ctx.call("ldga_gloc", L._lib.ptr(np.ascontiguousarray(sig)), len(sig), None)
+        chi0 = L.calc_bubble(h)
+        xm, gm = L.calc_χγ("m", Gm, chi0, h.kG, h.mP, h.sP)
+        xd, gd = L.calc_χγ("d", h, chi0)
+        l0 = L.calc_λ0(chi0, h)
+        res = L.λdm_correction(xm, gm, xd, gd, l0, h, atol=1e-12, nsteps=500)
+        loss = float(np.sum(kmult[:, None] * np.abs(res.Σ_ladder) ** 2) + res.EPot_p1)
+        return loss, (xm, gm, xd, gd, l0, res)
+
+    L0, (xm, gm, xd, gd, l0, res) = forward(Gm0, sig0)
+    assert res.sc_converged, "λdm did not converge on this point"
+    grad = L.λdm_vjp(h, xm, gm, xd, gd, l0, res, Σ̄=2.0 * kmult[:, None] * res.Σ_ladder, Ē=1.0)
+    for key, base in (("Γ_m", Gm0), ("Σ_loc", sig0)):
+        d = _cgauss(rng, base.shape)
+        eps = 1e-6 * np.max(np.abs(base)) / np.max(np.abs(d))
+        if key == "Γ_m":
+            fd = (forward(Gm0 + eps * d, sig0)[0] - forward(Gm0 - eps * d, sig0)[0]) / (2 * eps)
+        else:
+            fd = (forward(Gm0, sig0 + eps * d)[0] - forward(Gm0, sig0 - eps * d)[0]) / (2 * eps)
+        an = float(np.sum(np.real(np.conj(grad[key]) * d)))
+        assert abs(fd - an) <= 1e-5 * np.sum(np.abs(grad[key]) * np.abs(d)), (key, fd, an)
+    forward(Gm0, sig0)
