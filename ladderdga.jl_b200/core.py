@@ -1119,14 +1119,15 @@ def λdm_vjp(h: lDΓAHelper, χm: χT, γm: γT, χd: χT, γd: γT, λ0, res: "
     xm, xd = np.asarray(χm.data), np.asarray(χd.data)
     dL = np.array([-np.sum(oL[0] * xm**2), -np.sum(oL[2] * xd**2)])
     dE1 = np.array([-np.sum(oE[0] * xm**2), -np.sum(oE[2] * xd**2)])
-    dsm, dsd = _lib.C.c_double(), _lib.C.c_double()
-    ctx.call("ldga_sum_kw", CH_M, lm, 1, _lib.C.byref(dsm))
-    ctx.call("ldga_sum_kw", CH_D, ld, 1, _lib.C.byref(dsd))
-    J = np.array([[0.5 * dsm.value, 0.5 * dsd.value],
-                  [dE1[0] + 0.5 * U * dsm.value, dE1[1] - 0.5 * U * dsd.value]])
+    # d sum_kω(χ^λ)/dλ = -(1/β) Σ_ω ⟨(χ^λ)²⟩_q exactly.  (The reference's λm Newton, which the
+    # library mirrors in ldga_sum_kw's derivative mode, also subtracts the χ tail constants there;
+    # the implicit derivative needs the true one.)
+    nk = float(np.sum(kmult))
+    dsm = -float(np.sum(kmult[:, None] * (xm / (lm * xm + 1.0)) ** 2)) / (β * nk)
+    dsd = -float(np.sum(kmult[:, None] * (xd / (ld * xd + 1.0)) ** 2)) / (β * nk)
+    J = np.array([[0.5 * dsm, 0.5 * dsd], [dE1[0] + 0.5 * U * dsm, dE1[1] - 0.5 * U * dsd]])
     w = np.linalg.solve(J.T, -dL)
     # ∂s/∂χ(q, ω) of sum_kω at λ for the unshifted χ
-    nk = float(np.sum(kmult))
     dsm_dx = (kmult[:, None] / (β * nk)) / (lm * xm + 1.0) ** 2
     dsd_dx = (kmult[:, None] / (β * nk)) / (ld * xd + 1.0) ** 2
     xmb = oL[0] + w[1] * oE[0] + (0.5 * w[0] + 0.5 * U * w[1]) * dsm_dx
