@@ -71,7 +71,27 @@ def parse():
     ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
     ap.add_argument("--cfg", type=int, default=3, choices=[1, 2, 3],
                     help="single-point configuration of the chain workload (3: the headline 3D 32^3 point)")
+    ap.add_argument("--input", default=None,
+                    help="a readConfig TOML file: run the chain workload on that DMFT impurity input "
+                         "(e.g. tests/golden/b1u2_plain.toml) instead of a synthetic configuration")
     return ap.parse_args()
+
+
+def workload_input(args, rank: int = 0):
+    """(input, workload name, data label) of the chain workload."""
+    if args.input:
+        import ladderdga_b200 as L
+        from ladderdga_b200 import inputs as I
+        _, mP, sP, env, kgs = L.readConfig(args.input)
+        inp = I.load_impurity_input(env.inputVars, kgs[0], mP, sP)
+        nq = L.gen_kGrid(*kgs[0]).kMult.size
+        name = (f"DMFT input {os.path.basename(env.inputVars)}: {inp.dim}D sc Nk={inp.ns}^{inp.dim} "
+                f"({nq} irreducible q), beta={inp.beta:g}, U={inp.U:g}, Nnu={2 * inp.n_iv}, "
+                f"Nw={2 * inp.n_iw + 1}, shift={inp.shift}, lambda_m")
+        return inp, name, f"DMFT impurity file {os.path.basename(env.inputVars)} (read by readConfig)"
+    from ladderdga_b200 import synthetic as S
+    over = {"ns": args.ns} if args.ns else {}
+    return S.config_input(args.cfg, point=rank, **over), CFG_NAMES[args.cfg], "synthetic"
 
 
 def dist_env():
@@ -154,8 +174,7 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from ladderdga_b200 import synthetic as S
-    inp = S.config_input(args.cfg)
+    inp, wname, data = workload_input(args)
     from oracle import ldga_ref as R
     points = R.gen_kGrid(inp.kgrid_kind, inp.ns).Nq * (2 * inp.n_iw + 1)
     # one step is a whole chain (about 10 s on 8 cores): the warm-up is capped at one chain and the
@@ -173,9 +192,9 @@ def run_reference(args):
               "algorithm (oracle/ldga_ref.py), scipy.fft workers and OpenBLAS threads = all cores")
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": len(ts),
             "steps_requested": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": data,
             "impl": "reference",
-            "config": {"workload": CFG_NAMES[args.cfg], "global_batch": 1, "l2": "inputs resident in host memory"},
+            "config": {"workload": wname, "global_batch": 1, "l2": "inputs resident in host memory"},
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -289,9 +308,10 @@ def roofline(stages: dict, chain, peaks: dict) -> dict:
                 "executed": {"tflops": exe, "frac": exe / peak,
                              "work": "flops of the LU solve of [B | 1], its back substitution and the "
                                      "backward-error check (one pass; refinement sweeps not counted)"},
-                "traffic": BSE_DRAM_BYTES_PER_MATRIX * nq * nw,
-                "traffic_source": "ncu dram__bytes_read+write of one FP64 launch on 3D 16^3 (6765 matrices, "
-                                  "802 B each), scaled by the matrix count",
+                "traffic": BSE_DRAM_BYTES_PER_MATRIX * nq * nw if nnu == 40 else None,
+                "traffic_source": ("ncu dram__bytes_read+write of one FP64 launch on 3D 16^3 (6765 matrices, "
+                                   "802 B each), scaled by the matrix count" if nnu == 40 else
+                                   "no capture at this Nnu"),
                 "peak_source": f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz "
                                "(no FP64 figure is measured; the CUDA-core pipe, not HBM or tensor cores, "
                                "bounds this kernel)"}
@@ -314,9 +334,7 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from ladderdga_b200 import synthetic as S
-    over = {"ns": args.ns} if args.ns else {}
-    inp = S.config_input(args.cfg, point=rank, **over)
+    inp, wname, data = workload_input(args, rank)
     chain = Chain(inp, PREC_NAMES[args.prec], local)
     bse_config = tune(chain)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -376,8 +394,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
-                "data": "synthetic", "impl": "ours", "precision_mode": args.prec,
-                "config": {"workload": CFG_NAMES[args.cfg], "global_batch": world, "seq_len": None,
+                "data": data, "impl": "ours", "precision_mode": args.prec,
+                "config": {"workload": wname, "global_batch": world, "seq_len": None,
                            "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step",
                            "points_per_step_per_gpu": chain.points, "bse_config": bse_config},
                 "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": chain.h2d_bytes,

@@ -781,14 +781,19 @@ def setup_LDGA(kGridStr, mP: ModelParameters, sP: SimulationParameters, inputs, 
                device: int = 0, silent: bool = True) -> lDΓAHelper:
     """``setup_LDGA`` (runHelpers.jl:85-201).
 
-    ``inputs`` replaces the JLD2 impurity file: any object with ``sigma_loc`` (Σ_loc(n), n >= 0),
-    ``gimp`` (G_imp(n), n >= 0), ``chi_loc_m``/``chi_loc_d`` and ``gamma_m``/``gamma_d``
-    ([Nν, Nν, Nω] complex), e.g. ``synthetic.make_input``.
+    ``inputs``: the ``EnvironmentVars`` of ``readConfig`` (the impurity file ``env.inputVars`` is
+    read as the reference does, ``inputs.load_impurity_input``), or any object with ``sigma_loc``
+    (Σ_loc(n), n >= 0), ``gimp`` (G_imp(n), n >= 0), ``chi_loc_m``/``chi_loc_d`` and
+    ``gamma_m``/``gamma_d`` ([Nν, Nν, Nω] complex), e.g. ``synthetic.make_input``.
     """
+    from .inputs import EnvironmentVars, load_impurity_input
     kind, ns = kGridStr
     kG = gen_kGrid(kind, ns)
     if sP.χ_helper is not None or sP.n_iν_shell != 0:
-        raise NotImplementedError("only the plain path (χ_helper = nothing, n_iν_shell = 0) is built")
+        raise NotImplementedError("only the plain path (χ_helper = nothing, n_iν_shell = 0) is built; "
+                                  "the χ asymptotics helpers come from BSE_SC.jl")
+    if isinstance(inputs, EnvironmentVars):
+        inputs = load_impurity_input(inputs.inputVars, kGridStr, mP, sP)
     fr = sP.fft_range
     rm = max(abs(fr[0]), abs(fr[-1]))
     Σ_loc = np.ascontiguousarray(np.asarray(inputs.sigma_loc, dtype=np.complex128))

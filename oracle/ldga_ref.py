@@ -11,7 +11,10 @@ Parity status
   ``filling`` on the 2x2 grid = 1.1706318843228878 (test/GFTools.jl:33), chi_lambda and
   ``newton_right`` roots (test/LambdaCorrection/helpers.jl:1-24), the Matsubara-sum identities
   (test/DataTypes.jl:47-67), ``find_usable_chi_interval`` cases (test/GFFit.jl:39-55),
-  ``reduce_range`` (test/helpers.jl:1-11), frequency index maps (test/helpers.jl:13-22).
+  ``reduce_range`` (test/helpers.jl:1-11), frequency index maps (test/helpers.jl:13-22),
+  ``calc_E_ED`` on the reference's DMFT fixture (test/thermodynamics.jl:1-5: E_kin ≈ -0.10448 and
+  E_pot ≈ 0.28354, atol 1e-3; the fixture is read by ``ladderdga_b200.jld2`` and frozen as
+  tests/golden/b1u2_dmft.npz).
 * UNPINNED for the bubble / BSE / EoM / lambda chain: the reference ships no golden vectors for
   them (test/ladderDGATools.jl is empty, test/full_run.jl asserts properties only) and Julia is
   not installed, so it cannot be run.  Those functions are restated from the source lines cited
@@ -894,6 +897,24 @@ def calc_E(G_nu: np.ndarray, Sigma: np.ndarray, mu: float, kG: KGrid, mP: ModelP
     E_kin = kG.kintegrate(4 * ekin_full.sum(axis=1) + ekin_tail_inv) / mP.beta
     E_pot = kG.kintegrate(2 * epot_full.sum(axis=1) + epot_tail_inv) / mP.beta
     return float(E_kin), float(E_pot)
+
+
+def calc_E_ED(eps_k, V_k, gimp, U: float, n: float, mu: float, beta: float):
+    """``calc_E_ED`` (thermodynamics.jl:46-64): Anderson-impurity energies from the bath and G_imp.
+    Delta(nu) = sum_k V_k^2 / (i nu - eps_k), Sigma = i nu - Delta - 1/G + mu, with the 1/nu^2
+    tails (sum V_k^2 and U^2/2 n(1-n/2) - Sigma_H (Sigma_H - mu)) summed analytically."""
+    eps_k = np.asarray(eps_k, dtype=np.float64)
+    V_k = np.asarray(V_k, dtype=np.float64)
+    gimp = np.asarray(gimp, dtype=np.complex128)
+    vk = float(np.sum(V_k**2))
+    s_h = n * U / 2
+    epot_tail = U**2 / 2 * n * (1 - n / 2) - s_h * (s_h - mu)
+    ivn = iv_array(beta, range(len(gimp)))
+    delta = np.array([np.sum(V_k * V_k / (iv - eps_k)) for iv in ivn])
+    sigma = ivn - delta - 1.0 / gimp + mu
+    e_kin = float(np.sum(2 * np.real(gimp * delta - vk / ivn**2)))
+    e_pot = float(np.sum(2 * np.real(gimp * sigma - epot_tail / ivn**2)))
+    return e_kin * (2 / beta) - (beta / 2) * vk, e_pot / beta + 0.5 * s_h - (beta / 4) * epot_tail
 
 
 # =============================================================================================
