@@ -66,8 +66,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ns", type=int, default=None, help="smaller k-grid (points per axis) for profiling captures")
     ap.add_argument("--out", default=None, help="also write the JSON line to this file")
-    ap.add_argument("--workload", default="chain", choices=["chain", "batch"],
-                    help="chain: the 3D 32^3 point (default); batch: the uneven 64-point (U, beta) scan on 2D 32^2")
+    ap.add_argument("--workload", default="chain", choices=["chain", "batch", "adjoint"],
+                    help="chain: the 3D 32^3 point (default); batch: the uneven 64-point (U, beta) scan on 2D 32^2; "
+                         "adjoint: the chain's vector-Jacobian product (ldga_chain_vjp) against its forward "
+                         "(ldga_chain_m) on 2D 48^2, Nnu=40, Nw=41")
     ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
     ap.add_argument("--cfg", type=int, default=3, choices=[1, 2, 3],
                     help="single-point configuration of the chain workload (3: the headline 3D 32^3 point)")
@@ -419,6 +421,89 @@ def run_ours(args):
     return 0
 
 
+ADJ_NAME = ("2D sq Nk=48^2 (325 irreducible q), beta=20, U=1.5, Nnu=40, Nw=41: forward = the lambda_m chain "
+            "(ldga_chain_m), adjoint = dL/dGamma_m, dL/dGamma_d, dL/dSigma_loc of L = sum |Sigma_ladder|^2 at the "
+            "chain's lambda_m (ldga_chain_vjp)")
+
+
+def run_adjoint(args):
+    """The adjoint's cost against the forward chain on the same point (time ratio, lower is better)."""
+    import torch
+    from ladderdga_b200 import synthetic as S
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    inp = S.config_input(4)
+    chain = Chain(inp, PREC_NAMES[args.prec], local)
+    bse_config = tune(chain)
+    ctx, stream = chain.ctx, chain.stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 3)):
+        scal = chain.step(chain.dev, True)
+    torch.cuda.synchronize()
+    lam_m = scal[0]
+    nq, nnu, nw, numax = ctx.Nq, ctx.Nnu, ctx.Nw, chain.numax
+    dev = torch.device("cuda", local)
+    sig = chain.out_sigma.to(dev)                                   # Sigma_ladder [Nq, numax] (re, im)
+    sbar = 2.0 * sig                                                # dL/dSigma for L = sum |Sigma|^2
+    n_sigma = chain.n_sigma
+    gm_bar = torch.empty(nnu * nnu * nw * 2, dtype=torch.float64, device=dev)
+    gd_bar = torch.empty_like(gm_bar)
+    sl_bar = torch.empty(n_sigma * 2, dtype=torch.float64, device=dev)
+    nf = C.c_int32()
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def adjoint():
+        ctx.call("ldga_chain_vjp", p(sbar), lam_m, 0.0, numax, 1, p(gm_bar), p(gd_bar), n_sigma, p(sl_bar), None,
+                 C.byref(nf))
+
+    def timed(fn):
+        times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        return times
+
+    for _ in range(max(args.warmup, 3)):
+        adjoint()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    n0 = C.c_int64()
+    ctx.call("ldga_launch_count", C.byref(n0))
+    t_fwd = timed(lambda: chain.step(chain.dev, False))
+    n1 = C.c_int64()
+    ctx.call("ldga_launch_count", C.byref(n1))
+    t_adj = timed(adjoint)
+    n2 = C.c_int64()
+    ctx.call("ldga_launch_count", C.byref(n2))
+    clk = clocks.stop()
+    fwd, adj = float(np.mean(t_fwd)), float(np.mean(t_adj))
+    line = {"metric": "adjoint / forward time", "value": adj / fwd, "unit": "ratio", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": adj, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
+            "precision_mode": args.prec,
+            "config": {"workload": ADJ_NAME, "global_batch": 1, "l2": "flushed (256 MiB write) before each step",
+                       "points_per_step_per_gpu": chain.points, "bse_config": bse_config},
+            "forward_ms": fwd, "adjoint_ms": adj,
+            "forward_points_per_s": chain.points / (fwd / 1e3), "adjoint_points_per_s": chain.points / (adj / 1e3),
+            "adjoint_flagged_solves": nf.value,
+            "gpu_launches": {"forward": int(n1.value - n0.value) // args.steps,
+                             "adjoint": int(n2.value - n1.value) // args.steps, "unit": "per step"},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    if args.out:
+        open(args.out, "w").write(json.dumps(line) + "\n")
+    return 0
+
+
 BATCH_NAME = ("uneven batch: {n} points of 2D sc Nk=32^2 (153 irreducible q), U ~ U[0.5,3], beta in {{5,10,20,40}}, "
               "Nnu = Nw - 1 = 2 round(1.5 beta) in {{16,30,60,120}}, lambda_m, all points in one ldga_batch_chain_m call")
 
@@ -527,6 +612,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -179,6 +179,19 @@ int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32
 int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_bar, const double* sigma_bar,
                   double lam_m, double lam_d, int32_t numax, int32_t n_sigma, double* sigma_loc_bar, double* gloc_bar);
 
+/* The whole ladder chain's vector-Jacobian product at fixed λ in one call, every intermediate on
+ * the device: ldga_eom_vjp, then ldga_bse_vjp of both channels (their chi0_bar summed), the
+ * λ_0 term and ldga_gloc_vjp -- what a ChainRulesCore rrule of calc_bubble → calc_χγ(:m, :d) →
+ * calc_λ0 → calc_Σ (BSETools.jl:157-248, ladderDGATools_singleCore.jl:49-136) would pull back.
+ * Input sigma_bar [Nq, numax] = dL/dSigma_ladder (complex) for the EoM at (lam_m, lam_d, tc) on the
+ * handle's current chi, gamma, lambda_0 (e.g. right after ldga_chain_m).  Outputs (any may be NULL):
+ * Gamma_m_bar, Gamma_d_bar [Nnu, Nnu, Nw], sigma_loc_bar [n_sigma] = dL/dSigma_loc(nu_n) through the
+ * lattice G, chi0_bar [Nq, Nnu, Nw] = the total dL/dchi0.  Pointers may be host or device memory.
+ * n_flagged (may be NULL): adjoint solves of both channels above the backward-error threshold. */
+int ldga_chain_vjp(ldga_ctx* ctx, const double* sigma_bar, double lam_m, double lam_d, int32_t numax, int32_t tc,
+                   double* Gamma_m_bar, double* Gamma_d_bar, int32_t n_sigma, double* sigma_loc_bar,
+                   double* chi0_bar, int32_t* n_flagged);
+
 /* Gradient of E_pot,1 (calc_E, thermodynamics.jl:142-168, on G_from_Σladder!, GFTools.jl:154-186)
  * with respect to Sigma_ladder [Nq, numax] (complex, dE/dRe + i dE/dIm), μ following the filling
  * condition the μ fit solves (μ = the fitted value).  The piece of the λdm implicit derivative

@@ -1093,6 +1093,28 @@ def chain_vjp_Σloc(h: lDΓAHelper, Σ̄, χm: χT, γm: γT, χd: χT, γd: γT
     return out
 
 
+def chain_vjp(h: lDΓAHelper, Σ̄, χm: χT, γm: γT, χd: χT, γd: γT, λ0, νmax: int | None = None, λm: float = 0.0,
+              λd: float = 0.0, tc: bool = True) -> dict:
+    """``chain_vjp_Σloc`` in one device call (``ldga_chain_vjp``): every intermediate gradient stays
+    on the GPU.  Returns Γ_m, Γ_d [Nν, Nν, Nω], Σ_loc [len(Σ_loc)] and χ0 [Nq, Nν, Nω], the total
+    gradient with respect to the bubble (both BSE channels and λ₀), plus the count of adjoint solves
+    above the backward-error threshold."""
+    S = as_fc(Σ̄)
+    νmax = S.shape[1] if νmax is None else νmax
+    _prepare_eom(h, χm, γm, χd, γd, λ0)
+    ctx = h.ctx
+    Gm = _lib.cplx_out((ctx.Nnu, ctx.Nnu, ctx.Nw))
+    Gd = _lib.cplx_out((ctx.Nnu, ctx.Nnu, ctx.Nw))
+    c0 = _lib.cplx_out((ctx.Nq, ctx.Nnu, ctx.Nw))
+    slb = np.empty(len(h.Σ_loc), dtype=np.complex128)
+    nf = _lib.C.c_int32()
+    ctx.call("ldga_chain_vjp", ptr(S), χm._device_λ(λm), χd._device_λ(λd), νmax, int(bool(tc)), ptr(Gm), ptr(Gd),
+             len(slb), ptr(slb), ptr(c0), _lib.C.byref(nf))
+    if nf.value:
+        warnings.warn(f"chain_vjp: {nf.value} adjoint solves above the backward-error threshold")
+    return {"Γ_m": Gm, "Γ_d": Gd, "Σ_loc": slb, "χ0": c0, "n_flagged": nf.value}
+
+
 def epot_vjp(h: lDΓAHelper, Σ, μ: float) -> np.ndarray:
     """∂E_pot,1/∂Σ_ladder [Nq, νmax] (complex gradient) of ``calc_E`` on ``G_from_Σladder!`` with μ
     following the filling condition (``ldga_epot_vjp``)."""

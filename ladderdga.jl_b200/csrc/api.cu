@@ -188,23 +188,105 @@ void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
                     c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
-                    c->d_pivot_scratch, c->d_bub_pairs};
+                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
 
-// device scratch of one call (e.g. an adjoint), freed on every exit path
+// device scratch of one call (e.g. an adjoint), released on every exit path.  Buffers are carved
+// from the handle's arena (256-byte aligned); what does not fit is cudaMalloc'ed and freed at the
+// end, and the arena is regrown to the call's total demand when the next call opens its scratch
+// (every entry point synchronises its stream before returning, so no kernel still uses it).
 struct DevScratch {
-    std::vector<void*> p;
+    ldga_ctx* c = nullptr;
+    size_t mark = 0, demand = 0;
+    std::vector<void*> own;
+    int open(ldga_ctx* ctx) {
+        c = ctx;
+        mark = ctx->arena_used;
+        if (mark == 0 && ctx->arena_want > ctx->arena_cap) {
+            if (ctx->d_arena) cudaFree(ctx->d_arena);
+            ctx->d_arena = nullptr;
+            ctx->arena_cap = 0;
+            cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ctx->d_arena), ctx->arena_want);
+            if (e != cudaSuccess) {
+                ctx->d_arena = nullptr;
+                return ctx_cuda(ctx, e, "cudaMalloc (adjoint scratch)");
+            }
+            ctx->arena_cap = ctx->arena_want;
+        }
+        return LDGA_OK;
+    }
     template <typename T>
     int get(ldga_ctx* ctx, T** out, size_t n) {
         *out = nullptr;
+        if (!c) TRY(open(ctx));
+        const size_t bytes = (std::max<size_t>(n, 1) * sizeof(T) + 255) & ~size_t(255);
+        demand += bytes;
+        ctx->arena_want = std::max(ctx->arena_want, mark + demand);
+        if (ctx->arena_used + bytes <= ctx->arena_cap) {
+            *out = reinterpret_cast<T*>(ctx->d_arena + ctx->arena_used);
+            ctx->arena_used += bytes;
+            return LDGA_OK;
+        }
         TRY(dev_alloc(ctx, out, n));
-        p.push_back(*out);
+        own.push_back(*out);
         return LDGA_OK;
     }
-    ~DevScratch() { for (void* x : p) cudaFree(x); }
+    ~DevScratch() {
+        for (void* x : own) cudaFree(x);
+        if (c) c->arena_used = mark;
+    }
 };
+
+// The lattice-G adjoint on device buffers: chi0_bar (bubble, may be null) and sbar [numax][Nq] (the
+// EoM's direct use of G, numax = 0: none) -> G_bar [Nf, Nq] (*gb) and, for n_sigma > 0,
+// Sigma_loc_bar [n_sigma] (*slb).  The CSR lists of rows per fft_range frequency are built here
+// in increasing row order; start and idx must outlive the stream's copies (the caller syncs).
+int gloc_vjp_device(ldga_ctx* ctx, DevScratch& sc, const double2* d_c0b, const double2* d_sb, int numax, double lam_m,
+                    double lam_d, int n_sigma, std::vector<int32_t>& start, std::vector<int32_t>& idx,
+                    double2** slb, double2** gb) {
+    const size_t nfq = (size_t)ctx->Nf * ctx->Nq;
+    const bool bub = d_c0b != nullptr;
+    const int nbub = bub ? ctx->Nnu * ctx->Nw : 0, neom = numax * ctx->Nw;
+    std::vector<std::vector<int32_t>> lists(ctx->Nf);
+    for (int wi = 0; wi < ctx->Nw && bub; ++wi)
+        for (int vi = 0; vi < ctx->Nnu; ++vi) {
+            const int pi = vi + ctx->Nnu * wi, wn = wi - ctx->sp.n_iw;
+            const int vn = (vi - ctx->sp.n_iv) - ctx->sp.shift * (wn / 2);
+            lists[vn - ctx->fft_lo].push_back(2 * pi);
+            lists[vn + wn - ctx->fft_lo].push_back(2 * pi + 1);
+        }
+    for (int wi = 0; wi < ctx->Nw && numax > 0; ++wi)
+        for (int n = 0; n < numax; ++n) {
+            const int wn = wi - ctx->sp.n_iw;
+            lists[n + wn - ctx->fft_lo].push_back(2 * nbub + n + numax * wi);
+        }
+    for (auto& l : lists) std::sort(l.begin(), l.end());
+    start.assign(ctx->Nf + 1, 0);
+    idx.clear();
+    for (int f = 0; f < ctx->Nf; ++f) {
+        start[f + 1] = start[f] + (int)lists[f].size();
+        idx.insert(idx.end(), lists[f].begin(), lists[f].end());
+    }
+    double2 *d_shat = nullptr, *d_rows = nullptr, *d_ghb = nullptr;
+    int32_t *d_start = nullptr, *d_idx = nullptr;
+    if (numax > 0) TRY(sc.get(ctx, &d_shat, (size_t)ctx->Nq * numax));
+    TRY(sc.get(ctx, &d_rows, (size_t)(2 * nbub + neom + 1) * ctx->Nq));
+    TRY(sc.get(ctx, &d_start, start.size()));
+    TRY(sc.get(ctx, &d_idx, std::max<size_t>(idx.size(), 1)));
+    TRY(copy(ctx, d_start, start.data(), start.size() * sizeof(int32_t)));
+    if (!idx.empty()) TRY(copy(ctx, d_idx, idx.data(), idx.size() * sizeof(int32_t)));
+    TRY(sc.get(ctx, &d_ghb, nfq));
+    TRY(sc.get(ctx, gb, nfq));
+    TRY(launch_gloc_vjp(ctx, d_c0b, numax > 0 ? d_sb : nullptr, numax, lam_m, lam_d, d_shat, d_rows, d_start, d_idx,
+                        d_ghb, *gb));
+    if (n_sigma > 0) {
+        TRY(sc.get(ctx, slb, (size_t)n_sigma));
+        TRY(launch_sigma_loc_grad(ctx, *gb, n_sigma, *slb));
+    }
+    return LDGA_OK;
+}
 
 int set_sigma_loc(ldga_ctx* ctx, const double* sigma_loc, int n_sigma) {
     const int L = std::max(std::abs(ctx->sp.fft_lo), std::abs(ctx->sp.fft_hi));
@@ -767,31 +849,8 @@ int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_b
     DeviceGuard g(ctx->device);
     const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw, nfq = (size_t)ctx->Nf * ctx->Nq;
     const bool bub = chi0_bar || lambda0_bar;
-    const int nbub = bub ? ctx->Nnu * ctx->Nw : 0, neom = numax * ctx->Nw;
-    // CSR: rows contributing to each fft_range frequency, in increasing row order
-    std::vector<std::vector<int32_t>> lists(ctx->Nf);
-    for (int wi = 0; wi < ctx->Nw && bub; ++wi)
-        for (int vi = 0; vi < ctx->Nnu; ++vi) {
-            const int pi = vi + ctx->Nnu * wi, wn = wi - ctx->sp.n_iw;
-            const int vn = (vi - ctx->sp.n_iv) - ctx->sp.shift * (wn / 2);
-            lists[vn - ctx->fft_lo].push_back(2 * pi);
-            lists[vn + wn - ctx->fft_lo].push_back(2 * pi + 1);
-        }
-    for (int wi = 0; wi < ctx->Nw && numax > 0; ++wi)
-        for (int n = 0; n < numax; ++n) {
-            const int wn = wi - ctx->sp.n_iw;
-            lists[n + wn - ctx->fft_lo].push_back(2 * nbub + n + numax * wi);
-        }
-    for (auto& l : lists) std::sort(l.begin(), l.end());
-    std::vector<int32_t> start(ctx->Nf + 1, 0), idx;
-    for (int f = 0; f < ctx->Nf; ++f) {
-        start[f + 1] = start[f] + (int)lists[f].size();
-        idx.insert(idx.end(), lists[f].begin(), lists[f].end());
-    }
     DevScratch sc;
-    double2 *d_c0b = nullptr, *d_l0b = nullptr, *d_sb = nullptr, *d_shat = nullptr, *d_rows = nullptr;
-    double2 *d_ghb = nullptr, *d_gb = nullptr, *d_slb = nullptr;
-    int32_t *d_start = nullptr, *d_idx = nullptr;
+    double2 *d_c0b = nullptr, *d_l0b = nullptr, *d_sb = nullptr, *d_slb = nullptr, *d_gb = nullptr;
     if (bub) {
         TRY(sc.get(ctx, &d_c0b, qvw));
         if (chi0_bar) TRY(copy(ctx, d_c0b, chi0_bar, qvw * sizeof(double2)));
@@ -805,24 +864,73 @@ int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_b
     if (numax > 0) {
         TRY(sc.get(ctx, &d_sb, (size_t)ctx->Nq * numax));
         TRY(copy(ctx, d_sb, sigma_bar, (size_t)ctx->Nq * numax * sizeof(double2)));
-        TRY(sc.get(ctx, &d_shat, (size_t)ctx->Nq * numax));
     }
-    TRY(sc.get(ctx, &d_rows, (size_t)(2 * nbub + neom + 1) * ctx->Nq));
-    TRY(sc.get(ctx, &d_start, start.size()));
-    TRY(sc.get(ctx, &d_idx, std::max<size_t>(idx.size(), 1)));
-    TRY(copy(ctx, d_start, start.data(), start.size() * sizeof(int32_t)));
-    if (!idx.empty()) TRY(copy(ctx, d_idx, idx.data(), idx.size() * sizeof(int32_t)));
-    TRY(sc.get(ctx, &d_ghb, nfq));
-    TRY(sc.get(ctx, &d_gb, nfq));
-    TRY(launch_gloc_vjp(ctx, bub ? d_c0b : nullptr, numax > 0 ? d_sb : nullptr, numax, lam_m, lam_d, d_shat, d_rows,
-                        d_start, d_idx, d_ghb, d_gb));
-    if (sigma_loc_bar) {
-        TRY(sc.get(ctx, &d_slb, (size_t)n_sigma));
-        TRY(launch_sigma_loc_grad(ctx, d_gb, n_sigma, d_slb));
-        TRY(copy(ctx, sigma_loc_bar, d_slb, (size_t)n_sigma * sizeof(double2)));
-    }
+    std::vector<int32_t> start, idx;
+    TRY(gloc_vjp_device(ctx, sc, d_c0b, d_sb, numax, lam_m, lam_d, sigma_loc_bar ? n_sigma : 0, start, idx, &d_slb,
+                        &d_gb));
+    if (sigma_loc_bar) TRY(copy(ctx, sigma_loc_bar, d_slb, (size_t)n_sigma * sizeof(double2)));
     if (gloc_bar) TRY(copy(ctx, gloc_bar, d_gb, nfq * sizeof(double2)));
     return sync(ctx);   // host vectors (start, idx) outlive the asynchronous copies
+}
+
+int ldga_chain_vjp(ldga_ctx* ctx, const double* sigma_bar, double lam_m, double lam_d, int32_t numax, int32_t tc,
+                   double* Gamma_m_bar, double* Gamma_d_bar, int32_t n_sigma, double* sigma_loc_bar,
+                   double* chi0_bar, int32_t* n_flagged) {
+    if (!ctx || !sigma_bar) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(eom_inputs_ready(ctx));
+    NEED(ctx, ctx->have_chi0 && ctx->have_Gamma[0] && ctx->have_Gamma[1],
+         "chain adjoint: run the bubble and both BSE channels first");
+    NEED(ctx, ctx->have_F, "chain adjoint: F_m missing (call ldga_F_from_chi)");
+    if (!std::isfinite(lam_m) || !std::isfinite(lam_d)) return ctx_fail(ctx, LDGA_ERR_ARG, "λ must be finite");
+    if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
+    if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
+    if (sigma_loc_bar && n_sigma < 1) return ctx_fail(ctx, LDGA_ERR_ARG, "n_sigma must be >= 1");
+    DeviceGuard g(ctx->device);
+    const size_t qvw = (size_t)ctx->Nq * ctx->Nnu * ctx->Nw, qw = (size_t)ctx->Nq * ctx->Nw;
+    const size_t vvw = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw, nsb = (size_t)ctx->Nq * numax;
+    DevScratch sc;
+    double2 *d_sb = nullptr, *d_shat = nullptr, *d_gm = nullptr, *d_gd = nullptr, *d_l0 = nullptr;
+    double *d_xm = nullptr, *d_xd = nullptr, *d_cm = nullptr, *d_cd = nullptr;
+    double2 *d_c0b = nullptr, *d_y = nullptr, *d_z = nullptr, *d_Gm = nullptr, *d_Gd = nullptr;
+    double2 *d_slb = nullptr, *d_gb = nullptr;
+    // 1. EoM: Sigma_bar -> gamma_m_bar, gamma_d_bar, lambda0_bar, chi_m_bar, chi_d_bar
+    TRY(sc.get(ctx, &d_sb, nsb));
+    TRY(copy(ctx, d_sb, sigma_bar, nsb * sizeof(double2)));
+    TRY(sc.get(ctx, &d_shat, nsb));
+    TRY(sc.get(ctx, &d_cm, nsb * ctx->Nw));
+    TRY(sc.get(ctx, &d_cd, nsb * ctx->Nw));
+    TRY(sc.get(ctx, &d_gm, qvw));
+    TRY(sc.get(ctx, &d_gd, qvw));
+    TRY(sc.get(ctx, &d_l0, qvw));
+    TRY(sc.get(ctx, &d_xm, qw));
+    TRY(sc.get(ctx, &d_xd, qw));
+    LDGA_CUDA(ctx, cudaMemsetAsync(d_gm, 0, qvw * sizeof(double2), ctx->stream));
+    LDGA_CUDA(ctx, cudaMemsetAsync(d_gd, 0, qvw * sizeof(double2), ctx->stream));
+    LDGA_CUDA(ctx, cudaMemsetAsync(d_l0, 0, qvw * sizeof(double2), ctx->stream));
+    TRY(launch_eom_vjp(ctx, numax, lam_m, lam_d, tc, d_sb, d_gm, d_gd, d_l0, d_xm, d_xd, d_shat, d_cm, d_cd));
+    // 2. both BSE channels -> Gamma_bar_r, chi0_bar (summed), then lambda0 -> chi0_bar
+    TRY(sc.get(ctx, &d_c0b, qvw));
+    TRY(sc.get(ctx, &d_y, qvw));
+    TRY(sc.get(ctx, &d_z, qvw));
+    TRY(sc.get(ctx, &d_Gm, vvw));
+    TRY(sc.get(ctx, &d_Gd, vvw));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    TRY(launch_bse_adj(ctx, LDGA_CH_M, d_xm, d_gm, d_c0b, d_y, d_z, d_Gm, ctx->d_count + 1, false));
+    TRY(launch_bse_adj(ctx, LDGA_CH_D, d_xd, d_gd, d_c0b, d_y, d_z, d_Gd, ctx->d_count + 1, true));
+    TRY(launch_lambda0_vjp(ctx, d_l0, d_c0b));
+    // 3. lattice G: bubble (chi0_bar) and the EoM's G (Sigma_bar) -> G_bar -> Sigma_loc_bar
+    std::vector<int32_t> start, idx;
+    if (sigma_loc_bar)
+        TRY(gloc_vjp_device(ctx, sc, d_c0b, d_sb, numax, lam_m, lam_d, n_sigma, start, idx, &d_slb, &d_gb));
+    int32_t cnt[2] = {0, 0};
+    TRY(copy(ctx, cnt, ctx->d_count, 2 * sizeof(int32_t)));
+    if (Gamma_m_bar) TRY(copy(ctx, Gamma_m_bar, d_Gm, vvw * sizeof(double2)));
+    if (Gamma_d_bar) TRY(copy(ctx, Gamma_d_bar, d_Gd, vvw * sizeof(double2)));
+    if (chi0_bar) TRY(copy(ctx, chi0_bar, d_c0b, qvw * sizeof(double2)));
+    if (sigma_loc_bar) TRY(copy(ctx, sigma_loc_bar, d_slb, (size_t)n_sigma * sizeof(double2)));
+    TRY(sync(ctx));
+    if (n_flagged) *n_flagged = cnt[1];
+    return LDGA_OK;
 }
 
 int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum, double* parts_out) {

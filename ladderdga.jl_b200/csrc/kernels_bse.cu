@@ -1351,7 +1351,8 @@ struct BseAdjArgs {
     const double2* gam;       // [Nq, N, Nw]   forward gamma_r
     const double* chi_bar;    // [Nq, Nw]      (may be null: zero)
     const double2* gam_bar;   // [Nq, N, Nw]   (may be null: zero)
-    double2* chi0_bar;        // [Nq, N, Nw]   out
+    double2* chi0_bar;        // [Nq, N, Nw]   out (added to when accumulate)
+    int accumulate;
     double2* ybuf;            // [Nq, N, Nw]   out: y
     double2* zbuf;            // [Nq, N, Nw]   out: z
     int32_t* flags;           // [Nq, Nw]      1: backward error above 1e-12
@@ -1542,7 +1543,8 @@ __global__ void __launch_bounds__(T * T, MINB) k_bse_adj(const BseAdjArgs a) {
             const double2 z = cconj(xsm[i]), y = yfw[i], d = dinv[i];
             double2 db = cscale(cmul(z, cconj(y)), -1.0);                        // from B
             if (a.gam_bar) db = cadd(db, cmul(cconj(cscale(y, rf)), a.gam_bar[ci]));   // from gamma
-            a.chi0_bar[ci] = cscale(cmul(cconj(cmul(d, d)), db), -1.0);
+            const double2 c0b = cscale(cmul(cconj(cmul(d, d)), db), -1.0);
+            a.chi0_bar[ci] = a.accumulate ? cadd(a.chi0_bar[ci], c0b) : c0b;
             a.ybuf[ci] = y;
             a.zbuf[ci] = z;
         }
@@ -1941,7 +1943,7 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
 }
 
 int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const double2* gam_bar, double2* chi0_bar,
-                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail) {
+                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail, bool accumulate) {
     BseAdjArgs a;
     a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
     a.beta = ctx->mp.beta; a.U = ctx->mp.U;
@@ -1952,6 +1954,7 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
     a.gam = ctx->d_gam[channel];
     a.chi_bar = chi_bar; a.gam_bar = gam_bar;
     a.chi0_bar = chi0_bar; a.ybuf = ybuf; a.zbuf = zbuf;
+    a.accumulate = accumulate ? 1 : 0;
     a.flags = ctx->d_flags;
     int st = LDGA_OK;
     switch (ctx->Nnu) {

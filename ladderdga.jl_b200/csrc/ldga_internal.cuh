@@ -107,6 +107,11 @@ struct ldga_ctx {
     int32_t* d_count = nullptr;
     double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
     int2* d_bub_pairs = nullptr;          // bubble pairs computed directly (pair, conjugate partner or -1)
+    // scratch arena of the adjoint entry points: bump-allocated within a call, reused by later
+    // calls; a call that needs more takes extra cudaMalloc blocks and the arena grows to the
+    // recorded demand at the start of the next call
+    char* d_arena = nullptr;
+    size_t arena_cap = 0, arena_used = 0, arena_want = 0;
     int n_bub_pairs = 0;
 
     cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
@@ -192,10 +197,11 @@ int launch_bubble(ldga_ctx* ctx);
 // BSE for one channel; enqueues the fallback for flagged matrices on the device (no host sync).
 // d_fail (device int32) receives the number of matrices that stayed unsolved.
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail);
-// Adjoint of one BSE channel: chi0_bar, y and z buffers [Nq, Nnu, Nw], Gamma_bar [Nnu, Nnu, Nw]; d_fail
-// receives the number of adjoint solves above the backward-error threshold.
+// Adjoint of one BSE channel: chi0_bar (written, or added to when accumulate), y and z buffers
+// [Nq, Nnu, Nw], Gamma_bar [Nnu, Nnu, Nw]; the number of adjoint solves above the backward-error
+// threshold is added to d_fail.
 int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const double2* gam_bar, double2* chi0_bar,
-                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail);
+                   double2* ybuf, double2* zbuf, double2* gamma_bar, int32_t* d_fail, bool accumulate = false);
 // Adjoint of the EoM at (lam_m, lam_d): sbar [numax][Nq] -> gm_bar, gd_bar, l0_bar [Nq, Nnu, Nw] (pre-zeroed;
 // any may be null), xm_bar, xd_bar [Nq, Nw] (may be null).  Scratch: shat [numax * Nq] complex,
 // cm, cd [numax * Nq * Nw] real.

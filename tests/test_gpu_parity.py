@@ -543,6 +543,34 @@ def test_chain_vjp_sigma_loc(cname, require_gpu):
     gpu_loss(sig0)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("cname", ["3d8", "2d6_shift"])
+def test_chain_vjp_fused_matches_composed(cname, require_gpu):
+    """ldga_chain_vjp (one call, intermediates on the device) against the composition of the
+    single-stage adjoints (EoM → BSE m, d → λ₀ → lattice G) through host arrays, twice in a row
+    (the second call reuses the handle's scratch arena)."""
+    inp = S.make_input(**CASES[cname])
+    g = gpu_chain(inp)
+    h = g["h"]
+    numax, lm, ld = h.sP.n_iν, 0.1, 0.05
+    chi0 = L.calc_bubble(h)
+    xm, gm = L.calc_χγ("m", h, chi0)
+    xd, gd = L.calc_χγ("d", h, chi0)
+    l0 = L.calc_λ0(chi0, h)
+    S_ = L.calc_Σ(xm, gm, xd, gd, l0, h, νmax=numax, λm=lm, λd=ld)
+    Sb = 2.0 * h.ctx.kmult[:, None] * S_
+    comp = L.chain_vjp_Σloc(h, Sb, xm, gm, xd, gd, l0, νmax=numax, λm=lm, λd=ld)
+    F = L.F_from_χ("m", h)
+    colF = F.sum(axis=0)                                   # [Nν', Nω]
+    c0_total = comp["χ0"] + comp["λ0"] * np.conj(colF)[None] / h.mP.β ** 2
+    for _ in range(2):
+        fused = L.chain_vjp(h, Sb, xm, gm, xd, gd, l0, νmax=numax, λm=lm, λd=ld)
+        assert fused["n_flagged"] == 0
+        for k in ("Γ_m", "Γ_d", "Σ_loc"):
+            assert rel(fused[k], comp[k]) < 1e-13, k
+        assert rel(fused["χ0"], c0_total) < 1e-13
+
+
 def test_lambda_dm_vjp(require_gpu):
     """North-star configuration 4's loss L = Σ_k,ν |Σ_ladder|² + E_pot,1 after the λdm correction:
     its gradient with respect to Γ_m and the lattice Σ_loc, through the implicit dependence of
