@@ -509,15 +509,29 @@ def dχ_λ(χ, λ: float):
     return -χ_λ(χ, λ) ** 2
 
 
-def χ_λ_(χ: χT, λ: float) -> None:
-    """``χ_λ!`` (LambdaCorrection/helpers.jl:38-53): in place, accumulates χ.λ."""
-    if λ == 0.0:
-        return
-    if not math.isfinite(λ):
-        print(f"WARNING. SKIPPING λ correction because {λ} is not finite!")
-        return
-    χ._data[:, :] = χ._data / (λ * χ._data + 1)
-    χ.λ = χ.λ + λ
+def χ_λ_(*args) -> None:
+    """``χ_λ!`` (LambdaCorrection/helpers.jl:38-53): ``χ_λ_(χ, λ)`` in place, accumulating χ.λ;
+    ``χ_λ_(χ_new, χ, λ)`` writes χ's corrected values into χ_new (χ_new.λ = χ.λ + λ); both also for
+    plain arrays (``χ_λ_(res, χ, λ)``).  λ = 0 leaves the data untouched."""
+    if len(args) == 2:
+        χ_new, χ, λ = args[0], args[0], args[1]
+    elif len(args) == 3:
+        χ_new, χ, λ = args
+    else:
+        raise TypeError("χ_λ_(χ, λ) or χ_λ_(χ_new, χ, λ)")
+    if isinstance(χ_new, χT) != isinstance(χ, χT):
+        raise TypeError("χ_λ_: both arguments χT, or both arrays")
+    src = χ._data if isinstance(χ, χT) else χ
+    dst = χ_new._data if isinstance(χ_new, χT) else χ_new
+    if λ != 0.0:
+        if not math.isfinite(λ):
+            print(f"WARNING. SKIPPING λ correction because {λ} is not finite!")
+            return
+        dst[...] = src / (λ * src + 1)
+    if isinstance(χ_new, χT):
+        χ_new.λ = χ.λ + λ
+        if χ_new is not χ and χ_new._ctx is not None:
+            χ_new._dirty = True      # its device copy holds other data: upload before the next use
 
 
 def reset_(χ: χT) -> None:
@@ -1591,6 +1605,18 @@ def gen_ω_part(sP: SimulationParameters, N: int):
     """``gen_ω_part`` (parallelization_helpers.jl:49-53); see ``parallel``."""
     from . import parallel
     return parallel.gen_ω_part(sP, N)
+
+
+def gen_ν_part(νGrid, sP: SimulationParameters, N: int):
+    """``gen_ν_part`` (parallelization_helpers.jl:62-68); see ``parallel``."""
+    from . import parallel
+    return parallel.gen_ν_part(νGrid, sP, N)
+
+
+def gen_ν_part_slices(data, index_list):
+    """``gen_ν_part_slices`` (parallelization_helpers.jl:81-102); see ``parallel``."""
+    from . import parallel
+    return parallel.gen_ν_part_slices(data, index_list)
 
 
 def par_partition(set_, N: int):

@@ -50,6 +50,46 @@ def gen_νω_part(sP, N: int):
     return rng, par_partition(rng, N)
 
 
+def gen_ν_part(νGrid, sP, N: int) -> list[list[tuple[int, int, int, int]]]:
+    """``gen_ν_part`` (parallelization_helpers.jl:62-68): ``νGrid`` (the EoM's νn, e.g.
+    ``range(0, n_iν)``) split into ``N`` segments; each segment's list of (ωi, ωn, νi, νn) over the
+    box whose νn lies in the segment, sorted by νn (stable, so ω ascends within one νn).  νn is the
+    shifted frequency νn − ⌊shift·ωn/2⌋ (trunc); ωi and νi are 0-based here."""
+    grid = list(νGrid)
+    parts = par_partition(grid, N)
+    cells = []
+    for vi, j in enumerate(range(-sP.n_iν, sP.n_iν)):          # Julia's comprehension: ω fastest
+        for wi, wn in enumerate(range(-sP.n_iω, sP.n_iω + 1)):
+            cells.append((wi, wn, vi, j - int(sP.shift * wn / 2)))
+    out = []
+    for seg in parts:
+        keep = set(grid[i] for i in seg)
+        out.append(sorted((c for c in cells if c[3] in keep), key=lambda c: c[3]))
+    return out
+
+
+def gen_ν_part_slices(data, index_list):
+    """``gen_ν_part_slices`` (parallelization_helpers.jl:81-102): ``data`` [Nq, Nν, Nω] rearranged
+    for one segment of ``gen_ν_part`` -> (res [Nq, Nω, len(νn_list)] with zeros where a (ω, νn) is
+    not in the box, νn_list, ωn_ranges)."""
+    import numpy as np
+    data = np.asarray(data)
+    νn = [c[3] for c in index_list]
+    νn_list = list(dict.fromkeys(νn))                            # unique, first-seen order
+    res = np.zeros((data.shape[0], data.shape[2], len(νn_list)), dtype=data.dtype, order="F")
+    ωn_ranges = []
+    for v in νn_list:
+        sl = [c[1] for c in index_list if c[3] == v]
+        ωn_ranges.append(range(sl[0], sl[-1] + 1))
+    k, cur = 0, index_list[0][3]
+    for wi, _, vi, vn in index_list:
+        if vn != cur:
+            cur = vn
+            k += 1
+        res[:, wi, k] = data[:, vi, wi]
+    return res, νn_list, ωn_ranges
+
+
 def point_weight(n_nu: int, n_q: int, n_w: int) -> float:
     """Relative cost of one parameter point: the two BSE channels, N_q N_ω matrices of Nν³."""
     return float(n_q) * float(n_w) * float(n_nu) ** 3

@@ -235,3 +235,20 @@ def test_kgrid_wedge(kind, ns, nq):
     assert np.array_equal(p.wedge, o.wedge) and np.array_equal(p.kMult, o.kMult)
     assert np.allclose(p.ϵkGrid, o.eps, atol=1e-15)
     assert np.all(p.wedge[0] == 0)
+
+
+def test_chi_lambda_three_argument_form():
+    """test/LambdaCorrection/helpers.jl:9-12: χ_λ!(χ, χ, λ) equals χ_λ(χ, λ); reset! restores."""
+    c = L.χT([[1.0, 2.0, 1.0]], 1.0)
+    t = L.χ_λ(c, 1.1)
+    L.χ_λ_(c, c, 1.1)
+    assert np.allclose(c.data, t.data) and c.λ == 1.1
+    L.reset_(c)
+    assert np.allclose(c.data, [[1.0, 2.0, 1.0]]) and c.λ == 0.0
+    d = L.χT([[0.0, 0.0, 0.0]], 1.0)
+    L.χ_λ_(d, c, 0.5)                                      # into another χT: d.λ = c.λ + λ
+    assert np.allclose(d.data, np.array([[1.0, 2.0, 1.0]]) / (0.5 * np.array([[1.0, 2.0, 1.0]]) + 1))
+    assert d.λ == 0.5 and c.λ == 0.0
+    arr = np.zeros(3)
+    L.χ_λ_(arr, np.array([1.0, 2.0, 1.0]), 1.0)
+    assert arr.tolist() == [0.5, 2.0 / 3.0, 0.5]

@@ -135,3 +135,24 @@ def test_two_rank_gloo_batch():
     # the Nν = 120 point outweighs all others together: its rank takes nothing else
     heavy = 0 if 3 in outs[0][2] else 1
     assert outs[heavy][2] == [3]
+
+
+def test_gen_nu_part_reference_case():
+    """test/parallelization_helpers.jl:5-12 (sP_grid_s1 = SimulationParameters(4, 5, 2, true, ...)):
+    three segments; the first holds νn = 0, 1 over the whole ω grid -4:4."""
+    sp = _SP(n_iω=4, n_iν=5, shift=True)
+    t = P.gen_ν_part(range(0, sp.n_iν), sp, 3)
+    assert len(t) == 3
+    data = np.random.default_rng(5).standard_normal((3, 2 * sp.n_iν, 2 * sp.n_iω + 1)) + 0j
+    res, νn, ωn = P.gen_ν_part_slices(data, t[0])
+    assert νn == [0, 1]
+    assert ωn[0] == range(-4, 5)
+    assert res.shape == (3, 9, 2)
+    # every (ω, νn) cell of the segment carries the box value at its shifted ν index
+    for wi, wn, vi, vn in t[0]:
+        assert res[:, wi, νn.index(vn)].tolist() == data[:, vi, wi].tolist()
+        assert vn == (vi - sp.n_iν) - int(sp.shift * wn / 2)
+    # the segments cover the requested νn exactly once per (ω, νn) in the box
+    seen = [(c[0], c[3]) for seg in t for c in seg]
+    assert len(seen) == len(set(seen))
+    assert {c[3] for seg in t for c in seg} == set(range(0, sp.n_iν))
