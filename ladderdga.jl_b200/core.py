@@ -132,6 +132,18 @@ class KGrid:
     def eps(self) -> np.ndarray:
         return self.ϵkGrid
 
+    def full_to_irr(self) -> np.ndarray:
+        """Wedge index of every point of the full grid (``expandKArr``'s map), shape gridshape."""
+        if getattr(self, "_f2i", None) is None:
+            widx = {tuple(int(v) for v in w): i for i, w in enumerate(self.wedge)}
+            ns = self.Ns
+            fold = np.minimum(np.arange(ns), (ns - np.arange(ns)) % ns)
+            out = np.empty((ns,) * self.dim, dtype=np.int64)
+            for idx in np.ndindex(*out.shape):
+                out[idx] = widx[tuple(sorted((int(fold[i]) for i in idx), reverse=True))]
+            self._f2i = out
+        return self._f2i
+
     def gridshape(self):
         return (self.Ns,) * self.dim
 
@@ -233,6 +245,9 @@ class χ0T:
     """``χ0T`` (DataTypes.jl:52-69): bubble with axes (q, ν, ω).  ``asym`` is not built (plain path)."""
 
     def __init__(self, data, β: float, ωnGrid, n_iν: int, shift: bool, ν_shell_size: int = 0, ctx=None):
+        ωs = list(ωnGrid)
+        if len(ωs) == 0 or ωs[-1] < ωs[0]:
+            raise ValueError("Cannot construct χ₀ array with empty frequency mesh!")   # DataTypes.jl:92-94
         self._dev = data if isinstance(data, DeviceArray) else None
         self._data = None if self._dev is not None else as_fc(data)
         self.β = β
@@ -256,6 +271,23 @@ class χ0T:
 
     def __getitem__(self, idx):
         return self.data[idx]
+
+
+def χ0Asym_coeffs(kG: KGrid, local_tail: bool, mP: ModelParameters):
+    """``χ₀Asym_coeffs`` (DataTypes.jl:110-124): tail coefficients (c1, c2[q], c3) of the bubble's
+    asymptotics.  Local: c1 = Un/2 − μ, c2 = [c1²], c3 = c1² + sVk + U² n/2 (1 − n/2).  Lattice, with
+    t1(k) = ε_k + Un/2 − μ: c1 = ⟨t1⟩_k, c2(q) = (1/N_k) Σ_k t1(k) t1(k+q), c3 = ⟨t1²⟩_k + U² n/2 (1 − n/2).
+    The asymptotic array itself (χ₀Asym) needs BSE_SC.jl's shell sums and is not built."""
+    t2 = mP.U ** 2 * (mP.n / 2) * (1 - mP.n / 2)
+    if local_tail:
+        c1 = mP.U * mP.n / 2 - mP.μ
+        return c1, [c1 * c1], c1 * c1 + mP.sVk + t2
+    t1 = np.asarray(kG.ϵkGrid, dtype=np.float64) + mP.U * mP.n / 2 - mP.μ
+    full = t1[kG.full_to_irr()]
+    F = np.fft.fftn(full)
+    corr = np.fft.ifftn(np.conj(F) * F).real / kG.Nk
+    c2 = corr[tuple(kG.wedge[:, d] for d in range(kG.dim))]
+    return float(kintegrate(kG, t1)), c2, float(kintegrate(kG, t1 ** 2)) + t2
 
 
 def core(χ0: χ0T) -> np.ndarray:
@@ -1649,3 +1681,5 @@ lambda_m_chain_batch = λm_chain_batch
 calc_chi_gamma_vjp, calc_Sigma_vjp, chain_vjp_Gamma = calc_χγ_vjp, calc_Σ_vjp, chain_vjp_Γ
 chain_vjp_Sigma_loc = chain_vjp_Σloc
 lambda_dm_vjp = λdm_vjp
+chi0Asym_coeffs = χ0Asym_coeffs
+gen_nu_part, gen_nu_part_slices = gen_ν_part, gen_ν_part_slices

@@ -899,6 +899,18 @@ def calc_E(G_nu: np.ndarray, Sigma: np.ndarray, mu: float, kG: KGrid, mP: ModelP
     return float(E_kin), float(E_pot)
 
 
+def chi0_asym_coeffs(kG: KGrid, local_tail: bool, mP: ModelParameters):
+    """``χ₀Asym_coeffs`` (DataTypes.jl:110-124) -> (c1, c2[q], c3); the lattice c2 is the
+    convolution (1/N_k) sum_k t1(k) t1(k+q) of t1 = eps_k + Un/2 - mu (Dispersions ``conv_noPlan``)."""
+    t2 = mP.U**2 * (mP.n / 2) * (1 - mP.n / 2)
+    if local_tail:
+        c1 = mP.U * mP.n / 2 - mP.mu
+        return c1, [c1 * c1], c1 * c1 + mP.sVk + t2
+    t1 = kG.eps + mP.U * mP.n / 2 - mP.mu
+    c2 = np.real(conv_direct(kG, t1.astype(np.complex128), t1.astype(np.complex128)))
+    return float(kG.kintegrate(t1)), c2, float(kG.kintegrate(t1**2)) + t2
+
+
 def calc_E_ED(eps_k, V_k, gimp, U: float, n: float, mu: float, beta: float):
     """``calc_E_ED`` (thermodynamics.jl:46-64): Anderson-impurity energies from the bath and G_imp.
     Delta(nu) = sum_k V_k^2 / (i nu - eps_k), Sigma = i nu - Delta - 1/G + mu, with the 1/nu^2

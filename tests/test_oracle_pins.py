@@ -252,3 +252,34 @@ def test_chi_lambda_three_argument_form():
     arr = np.zeros(3)
     L.χ_λ_(arr, np.array([1.0, 2.0, 1.0]), 1.0)
     assert arr.tolist() == [0.5, 2.0 / 3.0, 0.5]
+
+
+def test_chi0_asym_coeffs_known_answer():
+    """test/DataTypes.jl:16-27 with mP_1 = ModelParameters(1.1, 1.2, 1.3, 1.4, 1.5, 1.6, 1.7): the local
+    tail coefficients, and the empty ω mesh that χ₀T refuses (ArgumentError)."""
+    U, mu, beta, n, sVk = 1.1, 1.2, 1.3, 1.4, 1.5
+    c1_ref = U * n / 2 - mu
+    c3_ref = c1_ref * c1_ref + sVk + U**2 * (n / 2) * (1 - n / 2)
+    mP = L.ModelParameters(U, mu, beta, n, sVk, 1.6, 1.7)
+    kG = L.gen_kGrid("2Dsc-1.0", 2)
+    c1, c2, c3 = L.χ0Asym_coeffs(kG, True, mP)
+    assert c1 == pytest.approx(c1_ref) and c2[0] == pytest.approx(c1 ** 2) and c3 == pytest.approx(c3_ref)
+    o1, o2, o3 = R.chi0_asym_coeffs(R.gen_kGrid("2Dsc-1.0", 2), True, R.ModelParameters(U, mu, beta, n, sVk, 1.6, 1.7))
+    assert (o1, o2[0], o3) == pytest.approx((c1, c2[0], c3))
+    td = (np.arange(1, 25).reshape(3, 2, 4, order="F")).astype(np.complex128)
+    t = L.χ0T(td, beta, range(1, 5), 1, True)
+    assert np.array_equal(t.data, td)
+    with pytest.raises(ValueError):
+        L.χ0T(td, beta, range(1, -1), 1, True)
+
+
+@pytest.mark.parametrize("kind,ns", [("2Dsc-1.0", 6), ("3Dsc-0.7", 4), ("2Dsc-1.0-0.2-0.05", 8)])
+def test_chi0_asym_coeffs_lattice(kind, ns):
+    """Lattice tail coefficients: the package's FFT correlation against the oracle's O(N_k²) sum."""
+    mP = L.ModelParameters(1.3, 0.4, 7.0, 0.9, 0.2, 0.0, 0.0)
+    c1, c2, c3 = L.χ0Asym_coeffs(L.gen_kGrid(kind, ns), False, mP)
+    o1, o2, o3 = R.chi0_asym_coeffs(R.gen_kGrid(kind, ns), False, R.ModelParameters(1.3, 0.4, 7.0, 0.9, 0.2, 0.0, 0.0))
+    assert c1 == pytest.approx(o1, abs=1e-14) and c3 == pytest.approx(o3, rel=1e-14)
+    assert np.allclose(c2, o2, rtol=1e-13, atol=1e-14)
+    # q = 0 is the k-mean of t1²: c2[q0] = c3 - U² n/2 (1 - n/2)
+    assert c2[0] == pytest.approx(c3 - 1.3**2 * 0.45 * 0.55, rel=1e-13)
