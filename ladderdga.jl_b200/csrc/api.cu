@@ -154,6 +154,7 @@ int alloc_all(ldga_ctx* c) {
     TRY(dev_alloc(c, &c->d_flags, nq * nw));
     TRY(dev_alloc(c, &c->d_list, nq * nw));
     TRY(dev_alloc(c, &c->d_count, 4));
+    TRY(dev_alloc(c, &c->d_qperm, nq * nw));
     if (bse_pivot_smem((int)nnu) > LDGA_PIVOT_SMEM_MAX)
         TRY(dev_alloc(c, &c->d_pivot_scratch, (size_t)LDGA_PIVOT_GRID * nnu * (nnu + 1)));
     {   // bubble representatives: pair (vi, wi) and its conjugate partner nu'' = -nu - w - 1 in the box
@@ -188,7 +189,7 @@ void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
                     c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
-                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena};
+                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

@@ -1328,6 +1328,329 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 }
 
 // ------------------------------------------------------------------------------------------------
+// MIXED, q-shared preconditioner ("iter").  All q of one w share Gamma(w); their matrices differ only
+// by the diagonal 1/chi0(q, :, w).  k_bse_qorder sorts the q of every w by Re 1/chi0(q, N/2, w);
+// a CTA of k_bse_iter takes 32 consecutive q of that order and forms, in FP32, the in-place
+// Gauss-Jordan inverse C of B_bar = Gamma(w)^T + diag(mean over its q of 1/chi0).  Every q of the
+// group then iterates (Richardson refinement with the approximate inverse C)
+//     r = 1 - B_q x   (FP64, one N^2 product),   x += C r   (FP32 product, FP64 update)
+// from x = C 1 until the FP64 backward error of x -- the measure of the LU kernels -- is at most
+// 1e-14, or kIterMax sweeps; a q above 1e-12 at the end is flagged for the pivoted FP64 solve.  The
+// sweep count is set by how far B_q is from B_bar (about 7 on the 3D 32^3 matrices), so the FP64
+// work per matrix is ~7 N^2 instead of the elimination's N^3 / 3 plus its latency-bound steps.
+// Layout: LPQ adjacent lanes per q; lane h of a q owns rows [h RPL, (h+1) RPL) of x, r and of the
+// products.  x_k and r_k of the other rows come from the q's lanes by shuffles (column
+// k = s RPL + j sits in lane s of the q, register j); Gamma^T and C rows are shared-memory reads
+// that the LPQ distinct rows of a warp fetch in one wavefront (row stride N + 1).  Warps iterate
+// independently (no CTA barrier in the loop) until all q of the warp have converged.
+constexpr int kIterQ = 32;      // q per CTA: one preconditioner
+constexpr int kIterMax = 40;    // sweeps before a q is handed to the pivoted solve
+constexpr double kIterTol = 1e-14;
+
+template <int N>
+struct IterSmem {
+    static constexpr int LD = N + 1;
+    static constexpr size_t off_D = (size_t)N * LD * sizeof(double2);              // Gt [N][LD] double2
+    static constexpr size_t off_C = off_D + (size_t)kIterQ * N * sizeof(double2);  // D [32][N] double2
+    static constexpr size_t off_rowabs = off_C + (((size_t)N * LD * sizeof(float2) + 15) & ~size_t(15));
+    static constexpr size_t off_dbar = off_rowabs + (((size_t)N * sizeof(double) + 15) & ~size_t(15));
+    static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);       // [2][column, row]
+    static constexpr size_t bytes = off_pc + 4 * (size_t)N * sizeof(float2);
+};
+
+// perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order.  One CTA per w,
+// bitonic sort of the next power of two >= nq (<= 4096) in shared memory; non-finite keys sort as 0.
+__global__ void __launch_bounds__(1024) k_bse_qorder(int nq, int nnu, const double2* __restrict__ chi0,
+                                                     int32_t* __restrict__ perm) {
+    extern __shared__ __align__(16) unsigned char qo_raw[];
+    int P = 1;
+    while (P < nq) P <<= 1;
+    double* key = reinterpret_cast<double*>(qo_raw);
+    int* idx = reinterpret_cast<int*>(key + P);
+    const int w = blockIdx.x, vc = nnu / 2;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        if (i < nq) {
+            const double2 z = chi0[(size_t)i + (size_t)nq * (vc + (size_t)nnu * w)];
+            double k = z.x / (z.x * z.x + z.y * z.y);
+            if (!isfinite(k)) k = 0.0;
+            key[i] = k;
+        } else {
+            key[i] = INFINITY;
+        }
+        idx[i] = i;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const bool gt = key[i] > key[l] || (key[i] == key[l] && idx[i] > idx[l]);
+                    if (gt == up) {
+                        const double tk = key[i]; key[i] = key[l]; key[l] = tk;
+                        const int ti = idx[i]; idx[i] = idx[l]; idx[l] = ti;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < nq; i += blockDim.x) perm[(size_t)w * nq + i] = idx[i];
+}
+
+// identity order (boxes with more than 4096 q)
+__global__ void k_bse_qorder_id(int nq, int nw, int32_t* __restrict__ perm) {
+    const size_t total = (size_t)nq * nw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+        perm[e] = (int32_t)(e % nq);
+}
+
+__device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
+    acc.x = fmaf(c.x, r.x, acc.x);
+    acc.x = fmaf(-c.y, r.y, acc.x);
+    acc.y = fmaf(c.x, r.y, acc.y);
+    acc.y = fmaf(c.y, r.x, acc.y);
+    return acc;
+}
+
+template <int N, int LPQ, int MINB>
+__global__ void __launch_bounds__(kIterQ * LPQ, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
+    using S = IterSmem<N>;
+    constexpr int LD = S::LD;
+    constexpr int RPL = (N + LPQ - 1) / LPQ;
+    constexpr int NT = kIterQ * LPQ;
+    static_assert(32 % LPQ == 0, "the lanes of one q sit in one warp");
+    extern __shared__ __align__(16) unsigned char it_raw[];
+    double2* Gt = reinterpret_cast<double2*>(it_raw);
+    double2* Dq = reinterpret_cast<double2*>(it_raw + S::off_D);
+    float2* C = reinterpret_cast<float2*>(it_raw + S::off_C);
+    double* rowabs = reinterpret_cast<double*>(it_raw + S::off_rowabs);
+    double2* dbar = reinterpret_cast<double2*>(it_raw + S::off_dbar);
+    float2* pc = reinterpret_cast<float2*>(it_raw + S::off_pc);
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int w = blockIdx.y, g0 = blockIdx.x * kIterQ;
+    const int ql = tid / LPQ, h = tid % LPQ, gbase = lane - h;
+    const int nvalid = min(kIterQ, a.nq - g0);
+    const bool active = ql < nvalid;
+    const int32_t* pw = perm + (size_t)w * a.nq + g0;
+    const int q = active ? pw[ql] : 0;
+
+    // ---- B rows: B_ij = Gamma[w][i N + j] + delta_ij D_i;  D = 1/chi0 of the CTA's q
+    const double2* Gw = a.Gamma + (size_t)w * N * N;
+    for (int e = tid; e < N * N; e += NT) {
+        const int i = e / N, j = e - (e / N) * N;
+        Gt[i * LD + j] = Gw[e];
+    }
+    for (int e = tid; e < kIterQ * N; e += NT) {
+        const int qq = e / N, v = e - (e / N) * N;
+        double2 d = dmk(0.0, 0.0);
+        if (qq < nvalid) d = cinv(a.chi0[(size_t)pw[qq] + (size_t)a.nq * (v + (size_t)N * w)]);
+        Dq[qq * N + v] = d;
+    }
+    __syncthreads();
+    // |row|_1 of Gamma^T (lanes over columns) and the group's mean diagonal (lanes over q), one row
+    // per warp at a time, fixed-order butterfly sums
+    {
+        constexpr int NWARP = NT / 32;
+        for (int i = tid >> 5; i < N; i += NWARP) {
+            double sacc = 0.0;
+            for (int j = lane; j < N; j += 32) sacc += fabs(Gt[i * LD + j].x) + fabs(Gt[i * LD + j].y);
+            double2 m = lane < nvalid ? Dq[lane * N + i] : dmk(0.0, 0.0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+                m.x += __shfl_xor_sync(0xffffffffu, m.x, o);
+                m.y += __shfl_xor_sync(0xffffffffu, m.y, o);
+            }
+            if (lane == 0) {
+                rowabs[i] = sacc;
+                dbar[i] = cscale(m, 1.0 / (double)max(nvalid, 1));
+            }
+        }
+    }
+    __syncthreads();
+    // ---- C = B_bar^-1: in-place Gauss-Jordan in FP32 without pivoting (a poor C only costs sweeps).
+    // Every thread keeps its elements e = tid + NT jj in registers; the owners of column k and row k
+    // publish them to a double-buffered pair of shared vectors, so one barrier per step suffices
+    // (buffer k & 1 was last read in step k - 2, before barrier k - 1).
+    {
+        constexpr int NE = (N * N + NT - 1) / NT;
+        float2 ce[NE];
+#pragma unroll
+        for (int jj = 0; jj < NE; ++jj) {
+            const int e = tid + NT * jj;
+            ce[jj] = make_float2(0.f, 0.f);
+            if (e < N * N) {
+                const int i = e / N, j = e - (e / N) * N;
+                double2 v = Gt[i * LD + j];
+                if (i == j) v = cadd(v, dbar[i]);
+                ce[jj] = make_float2((float)v.x, (float)v.y);
+            }
+        }
+        for (int k = 0; k < N; ++k) {
+            float2* pcol = pc + (k & 1) * 2 * N;   // [N] column k, then [N] row k
+            float2* prow = pcol + N;
+#pragma unroll
+            for (int jj = 0; jj < NE; ++jj) {
+                const int e = tid + NT * jj;
+                if (e < N * N) {
+                    const int i = e / N, j = e - (e / N) * N;
+                    if (j == k) pcol[i] = ce[jj];
+                    if (i == k) prow[j] = ce[jj];
+                }
+            }
+            __syncthreads();
+            const float2 p = vinv(pcol[k]);
+#pragma unroll
+            for (int jj = 0; jj < NE; ++jj) {
+                const int e = tid + NT * jj;
+                if (e < N * N) {
+                    const int i = e / N, j = e - (e / N) * N;
+                    float2 v;
+                    if (i == k && j == k) {
+                        v = p;
+                    } else if (i == k) {
+                        v = fmul(ce[jj], p);
+                    } else if (j == k) {
+                        const float2 t = fmul(ce[jj], p);
+                        v = make_float2(-t.x, -t.y);
+                    } else {
+                        const float2 m = fmul(pcol[i], p), u = prow[j];
+                        v = ce[jj];
+                        v.x = fmaf(-m.x, u.x, v.x);
+                        v.x = fmaf(m.y, u.y, v.x);
+                        v.y = fmaf(-m.x, u.y, v.y);
+                        v.y = fmaf(-m.y, u.x, v.y);
+                    }
+                    ce[jj] = v;
+                }
+            }
+        }
+#pragma unroll
+        for (int jj = 0; jj < NE; ++jj) {
+            const int e = tid + NT * jj;
+            if (e < N * N) C[(e / N) * LD + (e - (e / N) * N)] = ce[jj];
+        }
+    }
+    __syncthreads();
+
+    // ---- per q: norm of B_q's rows, x = C 1
+    double rown = 0.0;
+    double2 x[RPL];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+        const int i = h * RPL + r;
+        x[r] = dmk(0.0, 0.0);
+        if (N % LPQ == 0 || i < N) {
+            const double2 d = Dq[ql * N + i], g = Gt[i * LD + i];
+            const double rn = rowabs[i] - (fabs(g.x) + fabs(g.y)) + fabs(g.x + d.x) + fabs(g.y + d.y);
+            rown = fmax(rown, rn);
+            float2 sacc = make_float2(0.f, 0.f);
+            for (int j = 0; j < N; ++j) sacc = fadd(sacc, C[i * LD + j]);
+            x[r] = dmk((double)sacc.x, (double)sacc.y);
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < LPQ; o <<= 1) rown = fmax(rown, __shfl_xor_sync(0xffffffffu, rown, o));
+
+    bool conv = !active;
+    double berr = 0.0;
+    for (int it = 0;; ++it) {
+        // residual r = 1 - B_q x (FP64); the source-lane loop stays rolled (code size)
+        double2 acc[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) acc[r] = dmk(0.0, 0.0);
+#pragma unroll 1
+        for (int s = 0; s < LPQ; ++s) {
+            const double2* grow = Gt + (size_t)(h * RPL) * LD + s * RPL;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) {
+                const double2 xk = shfl_v(x[j], gbase + s);
+                if (N % LPQ != 0 && s * RPL + j >= N) continue;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) {
+                    if (N % LPQ == 0 || h * RPL + r < N) {
+                        const double2 g = grow[r * LD + j];
+                        acc[r].x = fma(g.x, xk.x, acc[r].x);
+                        acc[r].x = fma(-g.y, xk.y, acc[r].x);
+                        acc[r].y = fma(g.x, xk.y, acc[r].y);
+                        acc[r].y = fma(g.y, xk.x, acc[r].y);
+                    }
+                }
+            }
+        }
+        double res = 0.0, xn = 0.0;
+        float2 rr[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+            const int i = h * RPL + r;
+            rr[r] = make_float2(0.f, 0.f);
+            if (N % LPQ == 0 || i < N) {
+                const double2 t = cadd(acc[r], cmul(Dq[ql * N + i], x[r]));
+                const double rx = 1.0 - t.x, ry = -t.y;
+                res = fmax(res, fabs(rx) + fabs(ry));
+                xn = fmax(xn, fabs(x[r].x) + fabs(x[r].y));
+                rr[r] = make_float2((float)rx, (float)ry);
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < LPQ; o <<= 1) {
+            res = fmax(res, __shfl_xor_sync(0xffffffffu, res, o));
+            xn = fmax(xn, __shfl_xor_sync(0xffffffffu, xn, o));
+        }
+        if (!conv) berr = res / (rown * xn + 1.0);
+        conv = conv || berr <= kIterTol;
+        if (__all_sync(0xffffffffu, conv) || it >= kIterMax) break;
+        // correction x += C r (FP32 product)
+        float2 dx[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) dx[r] = make_float2(0.f, 0.f);
+#pragma unroll 1
+        for (int s = 0; s < LPQ; ++s) {
+            const float2* crow = C + (size_t)(h * RPL) * LD + s * RPL;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) {
+                const float2 rk = shfl_v(rr[j], gbase + s);
+                if (N % LPQ != 0 && s * RPL + j >= N) continue;
+#pragma unroll
+                for (int r = 0; r < RPL; ++r)
+                    if (N % LPQ == 0 || h * RPL + r < N) dx[r] = f2_fma(crow[r * LD + j], rk, dx[r]);
+            }
+        }
+        if (!conv) {
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                x[r].x += (double)dx[r].x;
+                x[r].y += (double)dx[r].y;
+            }
+        }
+    }
+
+    // ---- chi, gamma = x / (chi0 (1 + s U chi)), flag
+    double sx = 0.0;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r)
+        if (N % LPQ == 0 || h * RPL + r < N) sx += x[r].x;
+#pragma unroll
+    for (int o = 1; o < LPQ; o <<= 1) sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    if (!active) return;
+    const double chi = sx / (a.beta * a.beta);
+    const bool ok = isfinite(berr) && berr <= 1e-12;
+    if (h == 0) {
+        a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+        a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+    }
+    const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+        const int i = h * RPL + r;
+        if (N % LPQ == 0 || i < N)
+            a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)N * w)] = cscale(cmul(x[r], Dq[ql * N + i]), rf);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // Adjoint (vector-Jacobian product) of the BSE step.  For a real loss L with upstream gradients
 // chi_bar (real) and gamma_bar (complex, dL/dRe + i dL/dIm) per (q, w):
 //   forward: B = Gamma(w)^T + diag(d), d = 1/chi0, y = B^-1 1, chi = Re sum y / beta^2,
@@ -1787,6 +2110,30 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
+template <int N, int LPQ, int MINB>
+int run_iter(ldga_ctx* ctx, const BseArgs& a) {
+    if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
+    using S = IterSmem<N>;
+    auto kern = k_bse_iter<N, LPQ, MINB>;
+    LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
+    StageTimer st_(ctx, LDGA_STAGE_BSE);
+    if (a.nq <= 4096) {
+        int P = 1;
+        while (P < a.nq) P <<= 1;
+        const size_t smq = (size_t)P * (sizeof(double) + sizeof(int));
+        LDGA_CUDA(ctx, set_smem(ctx, k_bse_qorder, smq));
+        k_bse_qorder<<<a.nw, 1024, smq, ctx->stream>>>(a.nq, N, a.chi0, ctx->d_qperm);
+        LDGA_LAUNCHED(ctx, "k_bse_qorder");
+    } else {
+        k_bse_qorder_id<<<148, 256, 0, ctx->stream>>>(a.nq, a.nw, ctx->d_qperm);
+        LDGA_LAUNCHED(ctx, "k_bse_qorder_id");
+    }
+    dim3 grid((a.nq + kIterQ - 1) / kIterQ, a.nw);
+    kern<<<grid, kIterQ * LPQ, S::bytes, ctx->stream>>>(a, ctx->d_qperm);
+    LDGA_LAUNCHED(ctx, "k_bse_iter");
+    return LDGA_OK;
+}
+
 struct BseVariant {
     BseRun run;
     const char* name;
@@ -1803,17 +2150,28 @@ LDGA_SMALL_BOX(6)
 LDGA_SMALL_BOX(8)
 LDGA_SMALL_BOX(10)
 LDGA_SMALL_BOX(12)
-LDGA_SMALL_BOX(16)
-LDGA_SMALL_BOX(20)
-LDGA_SMALL_BOX(30)
 #undef LDGA_SMALL_BOX
+// Nν = 16..30: the warp LU stays the MIXED default (its N^3 is small); the q-shared preconditioned
+// iteration is a configuration the autotuner may pick
+#define LDGA_ITER_BOX(N, LPQ, MINB)                                                                     \
+    const BseVariant fp64_##N[] = {{&run_lu<N, 8, 1, 2>, "lu8:2"}, {&run_lu<N, 8, 1, 4>, "lu8:4"},     \
+                                   {&run_lu<N, 8, 1, 8>, "lu8:8"}};                                     \
+    const BseVariant mixed_##N[] = {{&run_warp32<N, 8, 4, 4, 1>, "warp:1"}, {&run_warp32<N, 8, 4, 4, 3>, "warp:3"}, \
+                                    {&run_iter<N, LPQ, MINB>, "iter"}};                                \
+    const BseVariant inv_##N[] = {{&run_tile<N, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
+LDGA_ITER_BOX(16, 4, 4)
+LDGA_ITER_BOX(20, 4, 4)
+LDGA_ITER_BOX(30, 4, 3)
+#undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_warp32<40, 8, 4, 4, 3>, "warp:3"}, {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}};
+const BseVariant mixed_40[] = {{&run_iter<40, 4, 3>, "iter"}, {&run_warp32<40, 8, 4, 4, 3>, "warp:3"},
+                               {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}, {&run_iter<40, 8, 2>, "iter8:2"}};
 const BseVariant inv_40[] = {{&run_tile<40, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
 const BseVariant fp64_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu<60, 16, 1, 1>, "lu16:1"},
                               {&run_lu<60, 16, 1, 3>, "lu16:3"}};
-const BseVariant mixed_60[] = {{&run_lu32<60, 16, 1, 3>, "lu32x16:3"}, {&run_lu32<60, 16, 1, 2>, "lu32x16:2"}};
+const BseVariant mixed_60[] = {{&run_lu32<60, 16, 1, 3>, "lu32x16:3"}, {&run_lu32<60, 16, 1, 2>, "lu32x16:2"},
+                               {&run_iter<60, 8, 1>, "iter"}};
 const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64_INV>, "gj16x1"}};
 // Nν = 120: Gamma(w) (230 KB) exceeds shared memory and is read through L1/L2; FP64_INV solves by LU
 const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};

@@ -258,6 +258,38 @@ def test_parallel_api_matches_single_call_api(case):
     assert rel(s_par, s_ref) < RTOL
 
 
+@pytest.mark.parametrize("n_iv,dim,ns", [(20, 2, 24), (30, 2, 20), (15, 2, 20), (10, 2, 24), (8, 3, 12)])
+def test_bse_preconditioned_iteration(n_iv, dim, ns, require_gpu):
+    """MIXED's q-shared preconditioned iteration ("iter": FP32 inverse of each 32-q group's mean
+    matrix, FP64 residuals) against the oracle at the parity tolerance, for every box size it is
+    built for; matrices it leaves above the backward-error threshold go to the pivoted FP64 solve."""
+    import os
+    import tempfile
+    nnu = 2 * n_iv
+    inp = S.make_input(dim=dim, ns=ns, beta=12.0, U=1.2, n_iv=n_iv, n_iw=3, seed=300 + n_iv)
+    ref = R.run_chain(inp, lambda_type=None)
+    lib = L._lib.load()
+    names = []
+    while lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)):
+        names.append(lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)).decode())
+    assert "iter" in names, names
+    fd, path = tempfile.mkstemp()
+    os.write(fd, f"bse {nnu} {L.PREC_MIXED} iter\n".encode())
+    os.close(fd)
+    try:
+        L.tune_reset()
+        L.tune_load(path)
+        assert lib.ldga_bse_config_name(nnu, L.PREC_MIXED, -1).decode() == "iter"
+        g = gpu_chain(inp, L.PREC_MIXED)
+        for r in ("m", "d"):
+            assert rel(g[f"chi_{r}"].data, ref[f"chi_{r}"].data) < RTOL, (nnu, r)
+            assert rel(g[f"gamma_{r}"].data, ref[f"gamma_{r}"]) < RTOL, (nnu, r)
+            assert g[f"chi_{r}"].n_fallback <= 0.02 * g["h"].ctx.Nq * g["h"].ctx.Nw
+    finally:
+        os.unlink(path)
+        L.tune_reset()
+
+
 @pytest.mark.parametrize("n_iv", [60, 62])
 @pytest.mark.parametrize("prec", [L.PREC_FP64_INV, L.PREC_FP64, L.PREC_MIXED])
 def test_bse_large_box(n_iv, prec, require_gpu):
