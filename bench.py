@@ -45,6 +45,8 @@ PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
 REF_BUDGET_S = 120.0
 # DRAM bytes per BSE matrix (Nnu = 40, FP64) from one ncu capture (profiles/k_bse_lu_n40_fp64_3d16.md)
 BSE_DRAM_BYTES_PER_MATRIX = 5423872 / 6765
+# the same for the MIXED preconditioned solve (profiles/k_bse_iter_n40_mixed_3d32.md: 3D 32^3, 39 729 matrices)
+BSE_ITER_DRAM_BYTES_PER_MATRIX = 26811392 / 39729
 BSE_TILE = 8   # rows per diagonal block of the LU kernels at Nnu = 40
 
 
@@ -62,7 +64,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--prec", default="fp64", choices=list(PREC_NAMES))
+    ap.add_argument("--prec", default="mixed", choices=list(PREC_NAMES),
+                    help="BSE precision mode (mixed: FP32 preconditioner with FP64 residuals, results verified "
+                         "to FP64 backward error 1e-14; fp64: the FP64 LU)")
+    ap.add_argument("--tune-file", default=None,
+                    help="load BSE configuration choices (ldga_tune_save format) instead of autotuning")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip timing the same chain in FP64 mode (mixed runs report mixed / FP64)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ns", type=int, default=None, help="smaller k-grid (points per axis) for profiling captures")
     ap.add_argument("--out", default=None, help="also write the JSON line to this file")
@@ -264,14 +272,21 @@ class Chain:
         return list(sc)
 
 
+TUNE_FILE = None
+
+
 def tune(chain) -> str:
     """Untimed: run the bubble, let the autotuner pick the BSE configuration for this box size and
-    precision mode (both channels' inputs), and return its name."""
+    precision mode (both channels' inputs) -- or load the choices of --tune-file -- and return its
+    name."""
     ctx = chain.ctx
     ctx.call("ldga_bubble", None)
     import ladderdga_b200 as L
-    for t in ("m", "d"):
-        L.autotune_bse(chain.h, t, reps=3)
+    if TUNE_FILE:
+        L.tune_load(TUNE_FILE)
+    else:
+        for t in ("m", "d"):
+            L.autotune_bse(chain.h, t, reps=3)
     name = chain.lib.ldga_bse_config_name(ctx.Nnu, ctx.precision, -1)
     return name.decode() if name else "pivoted"
 
@@ -298,8 +313,22 @@ def roofline(stages: dict, chain, peaks: dict) -> dict:
         ach = flops / t / 1e12
         # what the kernel executes: elimination of [B | 1] alone (BSE_EXEC_CMACS complex multiply-adds)
         exe = nq * nw * 8.0 * BSE_EXEC_CMACS(nnu) / t / 1e12
-        # bound: FP32 (mixed) / FP64 CUDA-core pipes, nominal B200 rates at the measured max clock
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+        cfg = chain.lib.ldga_bse_config_name(nnu, chain.ctx.precision, -1)
+        cfg = cfg.decode() if cfg else ""
+        if cfg.startswith("iter"):
+            # MIXED preconditioned solve: FP64 residual sweeps (N^2 complex MACs each) set the bound
+            peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+            return {"kernel": "k_bse_iter (FP32 group inverse, FP64 residual sweeps)", "bound": "fp64",
+                    "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                    "work": "8 N^3 + 8 N^2 flops per matrix (the reference's LU + inverse formulation; the "
+                            "iteration does ~7 sweeps of 8 N^2 FP64 + 8 N^2 FP32 flops instead)",
+                    "traffic": BSE_ITER_DRAM_BYTES_PER_MATRIX * nq * nw if nnu == 40 else None,
+                    "traffic_source": ("ncu dram__bytes_read+write of one launch on 3D 32^3 (39 729 matrices)"
+                                       if nnu == 40 else "no capture at this Nnu"),
+                    "peak_source": f"nominal 64 FP64 FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (no FP64 figure "
+                                   "is measured)"}
+        # bound: FP32 (mixed) / FP64 CUDA-core pipes, nominal B200 rates at the measured max clock
         fp = "fp32" if chain.ctx.precision == 2 else "fp64"
         lanes = 128 if fp == "fp32" else 64
         peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
@@ -391,6 +420,33 @@ def run_ours(args):
     value = world * chain.points / (ms / 1e3)
     e2e = world * chain.points / (ms_e2e / 1e3)
     launches = int(n1.value - n0.value)
+    fp64_cmp = None
+    if args.prec == "mixed" and world == 1 and not args.no_fp64_compare:
+        # the same chain with the FP64 LU, same timing: the mixed / FP64 ratio of the headline metric
+        ref = Chain(inp, PREC_NAMES["fp64"], local)
+        ref_cfg = tune(ref)
+        ref.ctx.call("ldga_profile", 1)
+        for _ in range(max(args.warmup, 3)):
+            ref.step(ref.dev, False)
+        torch.cuda.synchronize()
+        stage_times(ref)
+        tr = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ref.stream)
+            ref.step(ref.dev, False)
+            b.record(ref.stream)
+            b.synchronize()
+            tr.append(a.elapsed_time(b))
+        rst = stage_times(ref)
+        ref.ctx.call("ldga_profile", 0)
+        ms64 = float(np.mean(tr))
+        bse64 = rst["bse"][0] / args.steps
+        bse_mx = stages["bse"][0] / args.steps
+        fp64_cmp = {"ms_per_step": ms64, "value": chain.points / (ms64 / 1e3), "bse_config": ref_cfg,
+                    "bse_ms_per_step": bse64, "mixed_over_fp64": ms64 / ms,
+                    "bse_mixed_over_fp64": bse64 / bse_mx}
     if rank == 0:
         rl = roofline(stages, chain, peaks)
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -409,6 +465,8 @@ def run_ours(args):
                 "result": {"lambda_m": scal[0], "mu": scal[1], "E_kin": scal[2], "E_pot1": scal[3],
                            "newton_iterations": scal[6]},
                 "clocks": clk}
+        if fp64_cmp is not None:
+            line["fp64_compare"] = fp64_cmp
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(inp, chain.points)
         print(json.dumps(line), flush=True)
@@ -607,7 +665,9 @@ def run_batch(args):
 
 
 def main():
+    global TUNE_FILE
     args = parse()
+    TUNE_FILE = args.tune_file
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":

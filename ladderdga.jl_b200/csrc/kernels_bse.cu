@@ -1335,7 +1335,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 // group then iterates (Richardson refinement with the approximate inverse C)
 //     r = 1 - B_q x   (FP64, one N^2 product),   x += C r   (FP32 product, FP64 update)
 // from x = C 1 until the FP64 backward error of x -- the measure of the LU kernels -- is at most
-// 1e-14, or kIterMax sweeps; a q above 1e-12 at the end is flagged for the pivoted FP64 solve.  The
+// 1e-14, or kIterMax sweeps; a q still above 1e-14 is flagged for the pivoted FP64 solve.  The
 // sweep count is set by how far B_q is from B_bar (about 7 on the 3D 32^3 matrices), so the FP64
 // work per matrix is ~7 N^2 instead of the elimination's N^3 / 3 plus its latency-bound steps.
 // Layout: LPQ adjacent lanes per q; lane h of a q owns rows [h RPL, (h+1) RPL) of x, r and of the
@@ -1413,12 +1413,12 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
     return acc;
 }
 
-template <int N, int LPQ, int MINB>
-__global__ void __launch_bounds__(kIterQ * LPQ, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
+template <int N, int LPQ, int QPL, int MINB>
+__global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
     using S = IterSmem<N>;
     constexpr int LD = S::LD;
     constexpr int RPL = (N + LPQ - 1) / LPQ;
-    constexpr int NT = kIterQ * LPQ;
+    constexpr int NT = kIterQ * LPQ / QPL;
     static_assert(32 % LPQ == 0, "the lanes of one q sit in one warp");
     extern __shared__ __align__(16) unsigned char it_raw[];
     double2* Gt = reinterpret_cast<double2*>(it_raw);
@@ -1430,11 +1430,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ, MINB) k_bse_iter(const BseArgs a
 
     const int tid = threadIdx.x, lane = tid & 31;
     const int w = blockIdx.y, g0 = blockIdx.x * kIterQ;
-    const int ql = tid / LPQ, h = tid % LPQ, gbase = lane - h;
+    const int h = tid % LPQ, gbase = lane - h, ql0 = (tid / LPQ) * QPL;   // this lane group's q: ql0 + c
     const int nvalid = min(kIterQ, a.nq - g0);
-    const bool active = ql < nvalid;
     const int32_t* pw = perm + (size_t)w * a.nq + g0;
-    const int q = active ? pw[ql] : 0;
 
     // ---- B rows: B_ij = Gamma[w][i N + j] + delta_ij D_i;  D = 1/chi0 of the CTA's q
     const double2* Gw = a.Gamma + (size_t)w * N * N;
@@ -1536,117 +1534,162 @@ __global__ void __launch_bounds__(kIterQ * LPQ, MINB) k_bse_iter(const BseArgs a
     __syncthreads();
 
     // ---- per q: norm of B_q's rows, x = C 1
-    double rown = 0.0;
-    double2 x[RPL];
+    double rown[QPL];
+    double2 x[QPL][RPL];
+#pragma unroll
+    for (int c = 0; c < QPL; ++c) rown[c] = 0.0;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
         const int i = h * RPL + r;
-        x[r] = dmk(0.0, 0.0);
+        float2 sacc = make_float2(0.f, 0.f);
+        double rowg = 0.0;
+        double2 g = dmk(0.0, 0.0);
         if (N % LPQ == 0 || i < N) {
-            const double2 d = Dq[ql * N + i], g = Gt[i * LD + i];
-            const double rn = rowabs[i] - (fabs(g.x) + fabs(g.y)) + fabs(g.x + d.x) + fabs(g.y + d.y);
-            rown = fmax(rown, rn);
-            float2 sacc = make_float2(0.f, 0.f);
+            g = Gt[i * LD + i];
+            rowg = rowabs[i] - (fabs(g.x) + fabs(g.y));
             for (int j = 0; j < N; ++j) sacc = fadd(sacc, C[i * LD + j]);
-            x[r] = dmk((double)sacc.x, (double)sacc.y);
+        }
+#pragma unroll
+        for (int c = 0; c < QPL; ++c) {
+            x[c][r] = dmk(0.0, 0.0);
+            if (N % LPQ == 0 || i < N) {
+                const double2 d = Dq[(ql0 + c) * N + i];
+                rown[c] = fmax(rown[c], rowg + fabs(g.x + d.x) + fabs(g.y + d.y));
+                x[c][r] = dmk((double)sacc.x, (double)sacc.y);
+            }
         }
     }
+    bool conv[QPL];
+    double berr[QPL];
 #pragma unroll
-    for (int o = 1; o < LPQ; o <<= 1) rown = fmax(rown, __shfl_xor_sync(0xffffffffu, rown, o));
+    for (int c = 0; c < QPL; ++c) {
+#pragma unroll
+        for (int o = 1; o < LPQ; o <<= 1) rown[c] = fmax(rown[c], __shfl_xor_sync(0xffffffffu, rown[c], o));
+        conv[c] = ql0 + c >= nvalid;
+        berr[c] = 0.0;
+    }
 
-    bool conv = !active;
-    double berr = 0.0;
     for (int it = 0;; ++it) {
-        // residual r = 1 - B_q x (FP64); the source-lane loop stays rolled (code size)
-        double2 acc[RPL];
+        // residual r = 1 - B_q x (FP64); the source-lane loop stays rolled (code size); every Gamma^T
+        // element read from shared memory serves the QPL q of the lane group
+        double2 acc[QPL][RPL];
 #pragma unroll
-        for (int r = 0; r < RPL; ++r) acc[r] = dmk(0.0, 0.0);
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) acc[c][r] = dmk(0.0, 0.0);
 #pragma unroll 1
         for (int s = 0; s < LPQ; ++s) {
             const double2* grow = Gt + (size_t)(h * RPL) * LD + s * RPL;
 #pragma unroll
             for (int j = 0; j < RPL; ++j) {
-                const double2 xk = shfl_v(x[j], gbase + s);
+                double2 xk[QPL];
+#pragma unroll
+                for (int c = 0; c < QPL; ++c) xk[c] = shfl_v(x[c][j], gbase + s);
                 if (N % LPQ != 0 && s * RPL + j >= N) continue;
 #pragma unroll
                 for (int r = 0; r < RPL; ++r) {
                     if (N % LPQ == 0 || h * RPL + r < N) {
                         const double2 g = grow[r * LD + j];
-                        acc[r].x = fma(g.x, xk.x, acc[r].x);
-                        acc[r].x = fma(-g.y, xk.y, acc[r].x);
-                        acc[r].y = fma(g.x, xk.y, acc[r].y);
-                        acc[r].y = fma(g.y, xk.x, acc[r].y);
+#pragma unroll
+                        for (int c = 0; c < QPL; ++c) {
+                            acc[c][r].x = fma(g.x, xk[c].x, acc[c][r].x);
+                            acc[c][r].x = fma(-g.y, xk[c].y, acc[c][r].x);
+                            acc[c][r].y = fma(g.x, xk[c].y, acc[c][r].y);
+                            acc[c][r].y = fma(g.y, xk[c].x, acc[c][r].y);
+                        }
                     }
                 }
             }
         }
-        double res = 0.0, xn = 0.0;
-        float2 rr[RPL];
+        float2 rr[QPL][RPL];
+        bool all = true;
 #pragma unroll
-        for (int r = 0; r < RPL; ++r) {
-            const int i = h * RPL + r;
-            rr[r] = make_float2(0.f, 0.f);
-            if (N % LPQ == 0 || i < N) {
-                const double2 t = cadd(acc[r], cmul(Dq[ql * N + i], x[r]));
-                const double rx = 1.0 - t.x, ry = -t.y;
-                res = fmax(res, fabs(rx) + fabs(ry));
-                xn = fmax(xn, fabs(x[r].x) + fabs(x[r].y));
-                rr[r] = make_float2((float)rx, (float)ry);
+        for (int c = 0; c < QPL; ++c) {
+            double res = 0.0, xn = 0.0;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                const int i = h * RPL + r;
+                rr[c][r] = make_float2(0.f, 0.f);
+                if (N % LPQ == 0 || i < N) {
+                    const double2 t = cadd(acc[c][r], cmul(Dq[(ql0 + c) * N + i], x[c][r]));
+                    const double rx = 1.0 - t.x, ry = -t.y;
+                    res = fmax(res, fabs(rx) + fabs(ry));
+                    xn = fmax(xn, fabs(x[c][r].x) + fabs(x[c][r].y));
+                    rr[c][r] = make_float2((float)rx, (float)ry);
+                }
             }
-        }
 #pragma unroll
-        for (int o = 1; o < LPQ; o <<= 1) {
-            res = fmax(res, __shfl_xor_sync(0xffffffffu, res, o));
-            xn = fmax(xn, __shfl_xor_sync(0xffffffffu, xn, o));
+            for (int o = 1; o < LPQ; o <<= 1) {
+                res = fmax(res, __shfl_xor_sync(0xffffffffu, res, o));
+                xn = fmax(xn, __shfl_xor_sync(0xffffffffu, xn, o));
+            }
+            if (!conv[c]) berr[c] = res / (rown[c] * xn + 1.0);
+            conv[c] = conv[c] || berr[c] <= kIterTol;
+            all = all && conv[c];
         }
-        if (!conv) berr = res / (rown * xn + 1.0);
-        conv = conv || berr <= kIterTol;
-        if (__all_sync(0xffffffffu, conv) || it >= kIterMax) break;
+        if (__all_sync(0xffffffffu, all) || it >= kIterMax) break;
         // correction x += C r (FP32 product)
-        float2 dx[RPL];
+        float2 dx[QPL][RPL];
 #pragma unroll
-        for (int r = 0; r < RPL; ++r) dx[r] = make_float2(0.f, 0.f);
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) dx[c][r] = make_float2(0.f, 0.f);
 #pragma unroll 1
         for (int s = 0; s < LPQ; ++s) {
             const float2* crow = C + (size_t)(h * RPL) * LD + s * RPL;
 #pragma unroll
             for (int j = 0; j < RPL; ++j) {
-                const float2 rk = shfl_v(rr[j], gbase + s);
+                float2 rk[QPL];
+#pragma unroll
+                for (int c = 0; c < QPL; ++c) rk[c] = shfl_v(rr[c][j], gbase + s);
                 if (N % LPQ != 0 && s * RPL + j >= N) continue;
 #pragma unroll
                 for (int r = 0; r < RPL; ++r)
-                    if (N % LPQ == 0 || h * RPL + r < N) dx[r] = f2_fma(crow[r * LD + j], rk, dx[r]);
-            }
-        }
-        if (!conv) {
+                    if (N % LPQ == 0 || h * RPL + r < N) {
+                        const float2 cv = crow[r * LD + j];
 #pragma unroll
-            for (int r = 0; r < RPL; ++r) {
-                x[r].x += (double)dx[r].x;
-                x[r].y += (double)dx[r].y;
+                        for (int c = 0; c < QPL; ++c) dx[c][r] = f2_fma(cv, rk[c], dx[c][r]);
+                    }
             }
         }
+#pragma unroll
+        for (int c = 0; c < QPL; ++c)
+            if (!conv[c]) {
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) {
+                    x[c][r].x += (double)dx[c][r].x;
+                    x[c][r].y += (double)dx[c][r].y;
+                }
+            }
     }
 
-    // ---- chi, gamma = x / (chi0 (1 + s U chi)), flag
-    double sx = 0.0;
+    // ---- chi, gamma = x / (chi0 (1 + s U chi)), flag.  A q that did not reach kIterTol goes to the
+    // pivoted solve: between 1e-14 and the LU kernels' 1e-12 the forward error (condition number x
+    // backward error) could exceed the FP64 target.
 #pragma unroll
-    for (int r = 0; r < RPL; ++r)
-        if (N % LPQ == 0 || h * RPL + r < N) sx += x[r].x;
+    for (int c = 0; c < QPL; ++c) {
+        double sx = 0.0;
 #pragma unroll
-    for (int o = 1; o < LPQ; o <<= 1) sx += __shfl_xor_sync(0xffffffffu, sx, o);
-    if (!active) return;
-    const double chi = sx / (a.beta * a.beta);
-    const bool ok = isfinite(berr) && berr <= 1e-12;
-    if (h == 0) {
-        a.chi[(size_t)q + (size_t)a.nq * w] = chi;
-        a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
-    }
-    const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+        for (int r = 0; r < RPL; ++r)
+            if (N % LPQ == 0 || h * RPL + r < N) sx += x[c][r].x;
 #pragma unroll
-    for (int r = 0; r < RPL; ++r) {
-        const int i = h * RPL + r;
-        if (N % LPQ == 0 || i < N)
-            a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)N * w)] = cscale(cmul(x[r], Dq[ql * N + i]), rf);
+        for (int o = 1; o < LPQ; o <<= 1) sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        const int ql = ql0 + c;
+        if (ql >= nvalid) continue;
+        const int q = pw[ql];
+        const double chi = sx / (a.beta * a.beta);
+        const bool ok = isfinite(berr[c]) && berr[c] <= kIterTol;
+        if (h == 0) {
+            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+            a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+        }
+        const double rf = 1.0 / (1.0 + a.s * a.U * chi);
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+            const int i = h * RPL + r;
+            if (N % LPQ == 0 || i < N)
+                a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)N * w)] = cscale(cmul(x[c][r], Dq[ql * N + i]), rf);
+        }
     }
 }
 
@@ -2110,11 +2153,11 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
-template <int N, int LPQ, int MINB>
+template <int N, int LPQ, int MINB, int QPL = 1>
 int run_iter(ldga_ctx* ctx, const BseArgs& a) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
     using S = IterSmem<N>;
-    auto kern = k_bse_iter<N, LPQ, MINB>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     if (a.nq <= 4096) {
@@ -2129,7 +2172,7 @@ int run_iter(ldga_ctx* ctx, const BseArgs& a) {
         LDGA_LAUNCHED(ctx, "k_bse_qorder_id");
     }
     dim3 grid((a.nq + kIterQ - 1) / kIterQ, a.nw);
-    kern<<<grid, kIterQ * LPQ, S::bytes, ctx->stream>>>(a, ctx->d_qperm);
+    kern<<<grid, kIterQ * LPQ / QPL, S::bytes, ctx->stream>>>(a, ctx->d_qperm);
     LDGA_LAUNCHED(ctx, "k_bse_iter");
     return LDGA_OK;
 }
@@ -2165,17 +2208,20 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 4, 3>, "iter"}, {&run_warp32<40, 8, 4, 4, 3>, "warp:3"},
-                               {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}, {&run_iter<40, 8, 2>, "iter8:2"}};
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
+                               {&run_iter<40, 8, 2>, "iter8:2"}, {&run_iter<40, 4, 3>, "iter"},
+                               {&run_warp32<40, 8, 4, 4, 3>, "warp:3"}, {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}};
 const BseVariant inv_40[] = {{&run_tile<40, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
 const BseVariant fp64_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu<60, 16, 1, 1>, "lu16:1"},
                               {&run_lu<60, 16, 1, 3>, "lu16:3"}};
-const BseVariant mixed_60[] = {{&run_lu32<60, 16, 1, 3>, "lu32x16:3"}, {&run_lu32<60, 16, 1, 2>, "lu32x16:2"},
-                               {&run_iter<60, 8, 1>, "iter"}};
+// MIXED may pick any configuration whose results meet the FP64 backward-error bound, the FP64 LU
+// included: at Nν = 60 and 120 that is the fastest one measured
+const BseVariant mixed_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu32<60, 16, 1, 3>, "lu32x16:3"},
+                               {&run_lu32<60, 16, 1, 2>, "lu32x16:2"}, {&run_iter<60, 8, 1>, "iter"}};
 const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64_INV>, "gj16x1"}};
 // Nν = 120: Gamma(w) (230 KB) exceeds shared memory and is read through L1/L2; FP64_INV solves by LU
 const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};
-const BseVariant mixed_120[] = {{&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
+const BseVariant mixed_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}, {&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
 
 int variants_of(int nnu, int prec, const BseVariant** out) {
 #define LDGA_BOX(N)                                                                                      \
@@ -2187,7 +2233,7 @@ int variants_of(int nnu, int prec, const BseVariant** out) {
         LDGA_BOX(4) LDGA_BOX(6) LDGA_BOX(8) LDGA_BOX(10) LDGA_BOX(12) LDGA_BOX(16) LDGA_BOX(20) LDGA_BOX(30)
         LDGA_BOX(40) LDGA_BOX(60)
         case 120:
-            if (prec == LDGA_PREC_MIXED) { *out = mixed_120; return 1; }
+            if (prec == LDGA_PREC_MIXED) { *out = mixed_120; return (int)(sizeof(mixed_120) / sizeof(BseVariant)); }
             *out = fp64_120; return 1;
         default: *out = nullptr; return 0;
     }
