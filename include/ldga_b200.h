@@ -44,7 +44,10 @@ typedef struct ldga_ctx ldga_ctx;
 /* BSE precision modes (per handle) */
 #define LDGA_PREC_FP64_INV 0 /* full FP64 inverse of every (q, w) matrix: the reference's inv! */
 #define LDGA_PREC_FP64     1 /* FP64 elimination of the single right-hand side that chi/gamma use */
-#define LDGA_PREC_MIXED    2 /* FP32 elimination + FP64 iterative refinement against FP64 residuals */
+#define LDGA_PREC_MIXED    2 /* FP32 work refined against FP64 residuals to backward error 1e-14:
+                                 a q-shared FP32 preconditioner with FP64 Richardson sweeps, or an
+                                 FP32 elimination with FP64 refinement, or the FP64 elimination where
+                                 that is fastest (per box size, autotuned) */
 
 #define LDGA_CH_M 0
 #define LDGA_CH_D 1
