@@ -481,6 +481,7 @@ int ldga_set_chi0(ldga_ctx* ctx, const double* chi0) {
     if (!ctx || !chi0) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
     DeviceGuard g(ctx->device);
     TRY(copy(ctx, ctx->d_chi0, chi0, (size_t)ctx->Nq * ctx->Nnu * ctx->Nw * sizeof(double2)));
+    ++ctx->chi0_gen;
     ctx->have_chi0 = true;
     return sync(ctx);
 }

@@ -1628,7 +1628,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             all = all && conv[c];
         }
         if (__all_sync(0xffffffffu, all) || it >= kIterMax) break;
-        // correction x += C r (FP32 product)
+        // correction x += C r (FP32 product; every C element read serves the QPL q)
         float2 dx[QPL][RPL];
 #pragma unroll
         for (int c = 0; c < QPL; ++c)
@@ -2160,16 +2160,20 @@ int run_iter(ldga_ctx* ctx, const BseArgs& a) {
     auto kern = k_bse_iter<N, LPQ, QPL, MINB>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
-    if (a.nq <= 4096) {
-        int P = 1;
-        while (P < a.nq) P <<= 1;
-        const size_t smq = (size_t)P * (sizeof(double) + sizeof(int));
-        LDGA_CUDA(ctx, set_smem(ctx, k_bse_qorder, smq));
-        k_bse_qorder<<<a.nw, 1024, smq, ctx->stream>>>(a.nq, N, a.chi0, ctx->d_qperm);
-        LDGA_LAUNCHED(ctx, "k_bse_qorder");
-    } else {
-        k_bse_qorder_id<<<148, 256, 0, ctx->stream>>>(a.nq, a.nw, ctx->d_qperm);
-        LDGA_LAUNCHED(ctx, "k_bse_qorder_id");
+    // the q order depends on chi0 only: the second channel of the same bubble reuses it
+    if (ctx->qperm_gen != ctx->chi0_gen) {
+        if (a.nq <= 4096) {
+            int P = 1;
+            while (P < a.nq) P <<= 1;
+            const size_t smq = (size_t)P * (sizeof(double) + sizeof(int));
+            LDGA_CUDA(ctx, set_smem(ctx, k_bse_qorder, smq));
+            k_bse_qorder<<<a.nw, 1024, smq, ctx->stream>>>(a.nq, N, a.chi0, ctx->d_qperm);
+            LDGA_LAUNCHED(ctx, "k_bse_qorder");
+        } else {
+            k_bse_qorder_id<<<148, 256, 0, ctx->stream>>>(a.nq, a.nw, ctx->d_qperm);
+            LDGA_LAUNCHED(ctx, "k_bse_qorder_id");
+        }
+        ctx->qperm_gen = ctx->chi0_gen;
     }
     dim3 grid((a.nq + kIterQ - 1) / kIterQ, a.nw);
     kern<<<grid, kIterQ * LPQ / QPL, S::bytes, ctx->stream>>>(a, ctx->d_qperm);

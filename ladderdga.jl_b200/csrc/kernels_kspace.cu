@@ -744,6 +744,7 @@ int launch_gloc_transform(ldga_ctx* ctx, bool from_sigma) {
 }
 
 int launch_bubble(ldga_ctx* ctx) {
+    ++ctx->chi0_gen;
 #define BODY(D, MM) run_bubble<D, MM>(ctx)
     LDGA_FOR_EACH_GRID(LDGA_CASE)
 #undef BODY
