@@ -1469,66 +1469,68 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     }
     __syncthreads();
     // ---- C = B_bar^-1: in-place Gauss-Jordan in FP32 without pivoting (a poor C only costs sweeps).
-    // Every thread keeps its elements e = tid + NT jj in registers; the owners of column k and row k
-    // publish them to a double-buffered pair of shared vectors, so one barrier per step suffices
-    // (buffer k & 1 was last read in step k - 2, before barrier k - 1).
+    // TPR threads own each row (a contiguous segment of CPT columns each, in registers); the owners
+    // of column k and row k publish them to a double-buffered pair of shared vectors, so one barrier
+    // per step suffices (buffer k & 1 was last read in step k - 2, before barrier k - 1).  Step k:
+    // a_kk <- 1/a_kk, row k <- row k / a_kk, column k <- -column k / a_kk, the rest a_ij -= m_i a_kj
+    // with m_i = a_ik / a_kk formed once per row.
     {
-        constexpr int NE = (N * N + NT - 1) / NT;
-        float2 ce[NE];
+        constexpr int TPR = NT / N > 0 ? NT / N : 1;
+        constexpr int CPT = (N + TPR - 1) / TPR;
+        const int gi = tid / TPR, gp = tid - (tid / TPR) * TPR, j0 = gp * CPT;
+        const bool own = gi < N;
+        float2 ce[CPT];
 #pragma unroll
-        for (int jj = 0; jj < NE; ++jj) {
-            const int e = tid + NT * jj;
-            ce[jj] = make_float2(0.f, 0.f);
-            if (e < N * N) {
-                const int i = e / N, j = e - (e / N) * N;
-                double2 v = Gt[i * LD + j];
-                if (i == j) v = cadd(v, dbar[i]);
-                ce[jj] = make_float2((float)v.x, (float)v.y);
+        for (int c = 0; c < CPT; ++c) {
+            const int jj = j0 + c;
+            ce[c] = make_float2(0.f, 0.f);
+            if (own && jj < N) {
+                double2 v = Gt[gi * LD + jj];
+                if (gi == jj) v = cadd(v, dbar[gi]);
+                ce[c] = make_float2((float)v.x, (float)v.y);
             }
         }
         for (int k = 0; k < N; ++k) {
             float2* pcol = pc + (k & 1) * 2 * N;   // [N] column k, then [N] row k
             float2* prow = pcol + N;
+            if (own) {
 #pragma unroll
-            for (int jj = 0; jj < NE; ++jj) {
-                const int e = tid + NT * jj;
-                if (e < N * N) {
-                    const int i = e / N, j = e - (e / N) * N;
-                    if (j == k) pcol[i] = ce[jj];
-                    if (i == k) prow[j] = ce[jj];
+                for (int c = 0; c < CPT; ++c) {
+                    const int jj = j0 + c;
+                    if (jj == k) pcol[gi] = ce[c];
+                    if (gi == k && jj < N) prow[jj] = ce[c];
                 }
             }
             __syncthreads();
-            const float2 p = vinv(pcol[k]);
+            if (own) {
+                const float2 p = vinv(pcol[k]);
+                if (gi == k) {
 #pragma unroll
-            for (int jj = 0; jj < NE; ++jj) {
-                const int e = tid + NT * jj;
-                if (e < N * N) {
-                    const int i = e / N, j = e - (e / N) * N;
-                    float2 v;
-                    if (i == k && j == k) {
-                        v = p;
-                    } else if (i == k) {
-                        v = fmul(ce[jj], p);
-                    } else if (j == k) {
-                        const float2 t = fmul(ce[jj], p);
-                        v = make_float2(-t.x, -t.y);
-                    } else {
-                        const float2 m = fmul(pcol[i], p), u = prow[j];
-                        v = ce[jj];
-                        v.x = fmaf(-m.x, u.x, v.x);
-                        v.x = fmaf(m.y, u.y, v.x);
-                        v.y = fmaf(-m.x, u.y, v.y);
-                        v.y = fmaf(-m.y, u.x, v.y);
+                    for (int c = 0; c < CPT; ++c) ce[c] = (j0 + c == k) ? p : fmul(ce[c], p);
+                } else {
+                    const float2 m = fmul(pcol[gi], p);
+#pragma unroll
+                    for (int c = 0; c < CPT; ++c) {
+                        const int jj = j0 + c;
+                        if (jj == k) {
+                            ce[c] = make_float2(-m.x, -m.y);
+                        } else if (jj < N) {
+                            const float2 u = prow[jj];
+                            float2 v = ce[c];
+                            v.x = fmaf(-m.x, u.x, v.x);
+                            v.x = fmaf(m.y, u.y, v.x);
+                            v.y = fmaf(-m.x, u.y, v.y);
+                            v.y = fmaf(-m.y, u.x, v.y);
+                            ce[c] = v;
+                        }
                     }
-                    ce[jj] = v;
                 }
             }
         }
+        if (own) {
 #pragma unroll
-        for (int jj = 0; jj < NE; ++jj) {
-            const int e = tid + NT * jj;
-            if (e < N * N) C[(e / N) * LD + (e - (e / N) * N)] = ce[jj];
+            for (int c = 0; c < CPT; ++c)
+                if (j0 + c < N) C[gi * LD + j0 + c] = ce[c];
         }
     }
     __syncthreads();
