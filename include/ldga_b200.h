@@ -215,6 +215,10 @@ int ldga_tune_save(const char* path);
 int ldga_tune_load(const char* path);
 /* Name of BSE configuration `index` for (nnu, precision) -- index < 0: the one in use -- or NULL. */
 const char* ldga_bse_config_name(int32_t nnu, int32_t precision, int32_t index);
+/* Work counters of the MIXED preconditioned BSE since the last call (no reference counterpart:
+ * diagnostics for rooflines): passes = residual evaluations summed over warps (each warp iterates
+ * its q in lockstep), warps = warps that ran.  Both are reset by the call. */
+int ldga_bse_sweeps(ldga_ctx* ctx, int64_t* passes, int64_t* warps);
 /* Forget every recorded choice: all box sizes use their default configuration again. */
 int ldga_tune_reset(void);
 

@@ -29,6 +29,7 @@ EXPORTS = [
     "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp",
     "ldga_eom_vjp", "ldga_autotune_bse", "ldga_tune_save", "ldga_tune_load",
     "ldga_tune_reset", "ldga_bse_config_name", "ldga_gloc_vjp", "ldga_epot_vjp", "ldga_chain_vjp",
+    "ldga_bse_sweeps",
 ]
 GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
 STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
@@ -128,6 +129,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_gloc_vjp": (C.c_int, [P, P, P, P, D, D, I32, I32, P, P]),
         "ldga_epot_vjp": (C.c_int, [P, I32, D, P, P]),
         "ldga_chain_vjp": (C.c_int, [P, P, D, D, I32, I32, P, P, I32, P, P, P]),
+        "ldga_bse_sweeps": (C.c_int, [P, P, P]),
         "ldga_run_sc": (C.c_int, [P, D, D, I32, D, D, I32, I32, D, D, I32, D, P, P, P]),
         "ldga_set_sigma": (C.c_int, [P, P, I32]),
         "ldga_calc_E": (C.c_int, [P, P, P, I32, D, PD, PD]),

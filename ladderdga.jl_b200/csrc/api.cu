@@ -155,6 +155,8 @@ int alloc_all(ldga_ctx* c) {
     TRY(dev_alloc(c, &c->d_list, nq * nw));
     TRY(dev_alloc(c, &c->d_count, 4));
     TRY(dev_alloc(c, &c->d_qperm, nq * nw));
+    TRY(dev_alloc(c, &c->d_iter_stats, 2));
+    LDGA_CUDA(c, cudaMemset(c->d_iter_stats, 0, 2 * sizeof(unsigned long long)));
     if (bse_pivot_smem((int)nnu) > LDGA_PIVOT_SMEM_MAX)
         TRY(dev_alloc(c, &c->d_pivot_scratch, (size_t)LDGA_PIVOT_GRID * nnu * (nnu + 1)));
     {   // bubble representatives: pair (vi, wi) and its conjugate partner nu'' = -nu - w - 1 in the box
@@ -189,7 +191,7 @@ void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
                     c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
-                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm};
+                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -612,6 +614,18 @@ int ldga_tune_save(const char* path) {
             if (n > 1 && i > 0 && i < n) std::fprintf(f, "bse %d %d %s\n", nnu, prec, bse_variant_name(nnu, prec, i));
         }
     std::fclose(f);
+    return LDGA_OK;
+}
+
+int ldga_bse_sweeps(ldga_ctx* ctx, int64_t* passes, int64_t* warps) {
+    if (!ctx) return LDGA_ERR_ARG;
+    DeviceGuard g(ctx->device);
+    unsigned long long v[2] = {0, 0};
+    TRY(copy(ctx, v, ctx->d_iter_stats, sizeof v));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_iter_stats, 0, sizeof v, ctx->stream));
+    TRY(sync(ctx));
+    if (passes) *passes = (int64_t)v[0];
+    if (warps) *warps = (int64_t)v[1];
     return LDGA_OK;
 }
 

@@ -100,6 +100,7 @@ struct BseArgs {
     double* chi;            // [Nq, Nw]
     double2* gam;           // [Nq, Nnu, Nw]
     int32_t* flags;         // [Nq, Nw]
+    unsigned long long* stats = nullptr;   // [2] k_bse_iter: residual passes and warps (may be null)
 };
 
 __device__ __forceinline__ double2 dmk(double r, double i) { return make_double2(r, i); }
@@ -1435,16 +1436,41 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     const int32_t* pw = perm + (size_t)w * a.nq + g0;
 
     // ---- B rows: B_ij = Gamma[w][i N + j] + delta_ij D_i;  D = 1/chi0 of the CTA's q
+    // fixed trip counts, fully unrolled: every global load of a thread is in flight at once
     const double2* Gw = a.Gamma + (size_t)w * N * N;
-    for (int e = tid; e < N * N; e += NT) {
-        const int i = e / N, j = e - (e / N) * N;
-        Gt[i * LD + j] = Gw[e];
+    {
+        constexpr int NG = (N * N + NT - 1) / NT;
+        double2 gv[NG];
+#pragma unroll
+        for (int m = 0; m < NG; ++m) {
+            const int e = tid + NT * m;
+            if (e < N * N) gv[m] = Gw[e];
+        }
+#pragma unroll
+        for (int m = 0; m < NG; ++m) {
+            const int e = tid + NT * m;
+            if (e < N * N) Gt[(e / N) * LD + (e - (e / N) * N)] = gv[m];
+        }
     }
-    for (int e = tid; e < kIterQ * N; e += NT) {
-        const int qq = e / N, v = e - (e / N) * N;
-        double2 d = dmk(0.0, 0.0);
-        if (qq < nvalid) d = cinv(a.chi0[(size_t)pw[qq] + (size_t)a.nq * (v + (size_t)N * w)]);
-        Dq[qq * N + v] = d;
+    {
+        constexpr int ND = (kIterQ * N + NT - 1) / NT;
+        int qg[ND];
+        double2 cv[ND];
+#pragma unroll
+        for (int m = 0; m < ND; ++m) {
+            const int e = tid + NT * m, qq = e / N;
+            qg[m] = (e < kIterQ * N && qq < nvalid) ? pw[qq] : -1;
+        }
+#pragma unroll
+        for (int m = 0; m < ND; ++m) {
+            const int e = tid + NT * m, v = e - (e / N) * N;
+            cv[m] = qg[m] >= 0 ? a.chi0[(size_t)qg[m] + (size_t)a.nq * (v + (size_t)N * w)] : dmk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int m = 0; m < ND; ++m) {
+            const int e = tid + NT * m;
+            if (e < kIterQ * N) Dq[e] = qg[m] >= 0 ? cinv(cv[m]) : dmk(0.0, 0.0);
+        }
     }
     __syncthreads();
     // |row|_1 of Gamma^T (lanes over columns) and the group's mean diagonal (lanes over q), one row
@@ -1549,7 +1575,13 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         if (N % LPQ == 0 || i < N) {
             g = Gt[i * LD + i];
             rowg = rowabs[i] - (fabs(g.x) + fabs(g.y));
-            for (int j = 0; j < N; ++j) sacc = fadd(sacc, C[i * LD + j]);
+            float2 s2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < N; j += 2) {
+                sacc = fadd(sacc, C[i * LD + j]);
+                if (j + 1 < N) s2 = fadd(s2, C[i * LD + j + 1]);
+            }
+            sacc = fadd(sacc, s2);
         }
 #pragma unroll
         for (int c = 0; c < QPL; ++c) {
@@ -1571,6 +1603,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         berr[c] = 0.0;
     }
 
+    int passes = 0;
     for (int it = 0;; ++it) {
         // residual r = 1 - B_q x (FP64); the source-lane loop stays rolled (code size); every Gamma^T
         // element read from shared memory serves the QPL q of the lane group
@@ -1629,6 +1662,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             conv[c] = conv[c] || berr[c] <= kIterTol;
             all = all && conv[c];
         }
+        passes = it + 1;
         if (__all_sync(0xffffffffu, all) || it >= kIterMax) break;
         // correction x += C r (FP32 product; every C element read serves the QPL q)
         float2 dx[QPL][RPL];
@@ -1663,6 +1697,11 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                     x[c][r].y += (double)dx[c][r].y;
                 }
             }
+    }
+
+    if (a.stats && lane == 0) {
+        atomicAdd(&a.stats[0], (unsigned long long)passes);
+        atomicAdd(&a.stats[1], 1ull);
     }
 
     // ---- chi, gamma = x / (chi0 (1 + s U chi)), flag.  A q that did not reach kIterTol goes to the
@@ -2266,6 +2305,7 @@ BseArgs bse_args(ldga_ctx* ctx, int channel) {
     a.chi = ctx->d_chi[channel];
     a.gam = ctx->d_gam[channel];
     a.flags = ctx->d_flags;
+    a.stats = ctx->d_iter_stats;
     return a;
 }
 

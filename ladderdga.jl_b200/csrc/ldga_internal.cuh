@@ -110,6 +110,7 @@ struct ldga_ctx {
     int32_t* d_qperm = nullptr;           // [Nw][Nq] q order of the preconditioned BSE (k_bse_qorder)
     uint64_t chi0_gen = 0;                // bumped whenever chi0 is (re)written on the stream
     uint64_t qperm_gen = ~0ull;           // chi0_gen the q order was computed from (both channels share it)
+    unsigned long long* d_iter_stats = nullptr;   // [2] preconditioned BSE: residual passes, warps
     // scratch arena of the adjoint entry points: bump-allocated within a call, reused by later
     // calls; a call that needs more takes extra cudaMalloc blocks and the arena grows to the
     // recorded demand at the start of the next call
