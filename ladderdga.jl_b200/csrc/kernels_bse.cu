@@ -1329,7 +1329,7 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 }
 
 // ------------------------------------------------------------------------------------------------
-// MIXED, q-shared preconditioner ("iter").  All q of one w share Gamma(w); their matrices differ only
+// MIXED, q-shared preconditioner ("iter"; "tc": its FP32 product on tensor cores).  All q of one w share Gamma(w); their matrices differ only
 // by the diagonal 1/chi0(q, :, w).  k_bse_qorder sorts the q of every w by Re 1/chi0(q, N/2, w);
 // a CTA of k_bse_iter takes 32 consecutive q of that order and forms, in FP32, the in-place
 // Gauss-Jordan inverse C of B_bar = Gamma(w)^T + diag(mean over its q of 1/chi0).  Every q of the
@@ -1348,17 +1348,103 @@ constexpr int kIterQ = 32;      // q per CTA: one preconditioner
 constexpr int kIterMax = 40;    // sweeps before a q is handed to the pivoted solve
 constexpr double kIterTol = 1e-14;
 
-template <int N, bool GSM = true>
+// TC: the FP32 product x += C r runs on tensor cores (mma.sync m16n8k8, TF32 operands, FP32
+// accumulation): C is kept as the A fragments of its real and imaginary parts, MT x KT tiles of
+// 16 x 8 with the rows padded to MT 16, and every warp has an exchange buffer that brings its 8 q's
+// residuals into B-fragment order and the products back to the lanes that own the rows.
+template <int N, bool GSM = true, bool TC = false, int NWARP = 4>
 struct IterSmem {
     static constexpr int LD = N + 1;
+    static constexpr int MT = (N + 15) / 16, KT = N / 8, XS = 2 * N + 4;   // TC tiles, exchange stride
+    static constexpr size_t c_bytes = TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) + (size_t)NWARP * 8 * XS * sizeof(float)
+                                         : (size_t)N * LD * sizeof(float2);
     // Gt [N][LD] double2 (GSM: Gamma staged in shared memory; otherwise read through L1/L2)
     static constexpr size_t off_D = GSM ? (size_t)N * LD * sizeof(double2) : 0;
     static constexpr size_t off_C = off_D + (size_t)kIterQ * N * sizeof(double2);  // D [32][N] double2
-    static constexpr size_t off_rowabs = off_C + (((size_t)N * LD * sizeof(float2) + 15) & ~size_t(15));
+    static constexpr size_t off_X = off_C + (TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) : 0);  // TC exchange
+    static constexpr size_t off_rowabs = off_C + ((c_bytes + 15) & ~size_t(15));
     static constexpr size_t off_dbar = off_rowabs + (((size_t)N * sizeof(double) + 15) & ~size_t(15));
     static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);       // [2][column, row]
     static constexpr size_t bytes = off_pc + 4 * (size_t)N * sizeof(float2);
 };
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+// d += a b, one m16n8k8 TF32 tile (a: 4 A-fragment registers, b: 2 B-fragment registers)
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint4 a, uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+// dx = C r for the warp's 8 q (lane group lane/8 holds q 2 (lane/8) + c, rows h RPL + r) on tensor
+// cores.  fr / fi: A fragments of Re C / Im C, [MT][KT][32 lanes] x 4 tf32; xb: this warp's exchange
+// buffer [8 q][XS] floats, (re, im) per row.  dx_re = Cr r_re - Ci r_im, dx_im = Ci r_re + Cr r_im.
+template <int N, int RPL, int QPL, int LPQ>
+__device__ __forceinline__ void tc_apply(const float2 (&rr)[QPL][RPL], float2 (&dx)[QPL][RPL], const uint4* fr,
+                                         const uint4* fi, float* xb, int lane, int h) {
+    constexpr int MT = (N + 15) / 16, KT = N / 8, XS = 2 * N + 4;
+    static_assert(QPL * 32 / LPQ == 8, "the tensor-core product wants 8 q per warp");
+    static_assert(N % 8 == 0, "the tensor-core product wants whole 8-column tiles");
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < QPL; ++c) {
+        float* xq = xb + ((lane / LPQ) * QPL + c) * XS;
+#pragma unroll
+        for (int r = 0; r < RPL; ++r)
+            if (h * RPL + r < N) *reinterpret_cast<float2*>(xq + 2 * (h * RPL + r)) = rr[c][r];
+    }
+    __syncwarp();
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t bre[KT][2], bim[KT][2], bin[KT][2];
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+        const float2 v0 = *reinterpret_cast<const float2*>(xb + g * XS + 2 * (kt * 8 + t));
+        const float2 v1 = *reinterpret_cast<const float2*>(xb + g * XS + 2 * (kt * 8 + t + 4));
+        bre[kt][0] = to_tf32(v0.x); bre[kt][1] = to_tf32(v1.x);
+        bim[kt][0] = to_tf32(v0.y); bim[kt][1] = to_tf32(v1.y);
+        bin[kt][0] = to_tf32(-v0.y); bin[kt][1] = to_tf32(-v1.y);
+    }
+    float dre[MT][4], dim[MT][4];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) dre[mt][e] = dim[mt][e] = 0.f;
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) {
+            const uint4 ar = fr[(mt * KT + kt) * 32 + lane], ai = fi[(mt * KT + kt) * 32 + lane];
+            mma_tf32(dre[mt], ar, bre[kt][0], bre[kt][1]);
+            mma_tf32(dre[mt], ai, bin[kt][0], bin[kt][1]);
+            mma_tf32(dim[mt], ai, bre[kt][0], bre[kt][1]);
+            mma_tf32(dim[mt], ar, bim[kt][0], bim[kt][1]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+        const int m0 = mt * 16 + g, m1 = m0 + 8;
+        if (m0 < N) {
+            *reinterpret_cast<float2*>(xb + (2 * t) * XS + 2 * m0) = make_float2(dre[mt][0], dim[mt][0]);
+            *reinterpret_cast<float2*>(xb + (2 * t + 1) * XS + 2 * m0) = make_float2(dre[mt][1], dim[mt][1]);
+        }
+        if (m1 < N) {
+            *reinterpret_cast<float2*>(xb + (2 * t) * XS + 2 * m1) = make_float2(dre[mt][2], dim[mt][2]);
+            *reinterpret_cast<float2*>(xb + (2 * t + 1) * XS + 2 * m1) = make_float2(dre[mt][3], dim[mt][3]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < QPL; ++c) {
+        const float* xq = xb + ((lane / LPQ) * QPL + c) * XS;
+#pragma unroll
+        for (int r = 0; r < RPL; ++r)
+            dx[c][r] = h * RPL + r < N ? *reinterpret_cast<const float2*>(xq + 2 * (h * RPL + r)) : make_float2(0.f, 0.f);
+    }
+}
 
 // perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order.  One CTA per w,
 // bitonic sort of the next power of two >= nq (<= 4096) in shared memory; non-finite keys sort as 0.
@@ -1415,9 +1501,9 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
     return acc;
 }
 
-template <int N, int LPQ, int QPL, int MINB, bool GSM>
+template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC>
 __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
-    using S = IterSmem<N, GSM>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32>;
     constexpr int LD = S::LD;
     constexpr int LDG = GSM ? LD : N;   // row stride of Gamma^T where it is read
     constexpr int RPL = (N + LPQ - 1) / LPQ;
@@ -1427,6 +1513,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     double2* Gs = reinterpret_cast<double2*>(it_raw);
     double2* Dq = reinterpret_cast<double2*>(it_raw + S::off_D);
     float2* C = reinterpret_cast<float2*>(it_raw + S::off_C);
+    uint32_t* Cf = reinterpret_cast<uint32_t*>(it_raw + S::off_C);     // TC: [2][MT][KT][32][4] tf32
+    float* Xb = reinterpret_cast<float*>(it_raw + S::off_X);           // TC: [warps][8 q][XS]
     double* rowabs = reinterpret_cast<double*>(it_raw + S::off_rowabs);
     double2* dbar = reinterpret_cast<double2*>(it_raw + S::off_dbar);
     float2* pc = reinterpret_cast<float2*>(it_raw + S::off_pc);
@@ -1556,10 +1644,31 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 }
             }
         }
-        if (own) {
+        if constexpr (TC) {
+            // A fragments: element (m, k) of a 16 x 8 tile sits in lane 4 (m mod 8) + (k mod 4),
+            // register (m / 8) + 2 (k / 4); rows N .. 16 MT - 1 stay zero
+            constexpr int FR = S::MT * S::KT * 32 * 4;
+            __syncthreads();   // the zeroing below must not overtake the last pivot reads
+            for (int e = tid; e < 2 * FR; e += NT) Cf[e] = 0u;
+            __syncthreads();
+            if (own) {
 #pragma unroll
-            for (int c = 0; c < CPT; ++c)
-                if (j0 + c < N) C[gi * LD + j0 + c] = ce[c];
+                for (int c = 0; c < CPT; ++c) {
+                    const int jj = j0 + c;
+                    if (jj < N) {
+                        const int mt = gi >> 4, m16 = gi & 15, kt = jj >> 3, k8 = jj & 7;
+                        const int idx = ((mt * S::KT + kt) * 32 + (m16 & 7) * 4 + (k8 & 3)) * 4 + (m16 >> 3) + 2 * (k8 >> 2);
+                        Cf[idx] = to_tf32(ce[c].x);
+                        Cf[FR + idx] = to_tf32(ce[c].y);
+                    }
+                }
+            }
+        } else {
+            if (own) {
+#pragma unroll
+                for (int c = 0; c < CPT; ++c)
+                    if (j0 + c < N) C[gi * LD + j0 + c] = ce[c];
+            }
         }
     }
     __syncthreads();
@@ -1578,13 +1687,15 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         if (N % LPQ == 0 || i < N) {
             g = Gt[i * LDG + i];
             rowg = rowabs[i] - (fabs(g.x) + fabs(g.y));
-            float2 s2 = make_float2(0.f, 0.f);
+            if constexpr (!TC) {
+                float2 s2 = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int j = 0; j < N; j += 2) {
-                sacc = fadd(sacc, C[i * LD + j]);
-                if (j + 1 < N) s2 = fadd(s2, C[i * LD + j + 1]);
+                for (int j = 0; j < N; j += 2) {
+                    sacc = fadd(sacc, C[i * LD + j]);
+                    if (j + 1 < N) s2 = fadd(s2, C[i * LD + j + 1]);
+                }
+                sacc = fadd(sacc, s2);
             }
-            sacc = fadd(sacc, s2);
         }
 #pragma unroll
         for (int c = 0; c < QPL; ++c) {
@@ -1595,6 +1706,22 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 x[c][r] = dmk((double)sacc.x, (double)sacc.y);
             }
         }
+    }
+    const uint4* Ffr = reinterpret_cast<const uint4*>(Cf);
+    const uint4* Ffi = Ffr + S::MT * S::KT * 32;
+    float* xbw = Xb + (tid >> 5) * 8 * S::XS;
+    if constexpr (TC) {   // x = C 1 through the same tensor-core product
+        float2 one[QPL][RPL], d0[QPL][RPL];
+#pragma unroll
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) one[c][r] = make_float2(1.f, 0.f);
+        tc_apply<N, RPL, QPL, LPQ>(one, d0, Ffr, Ffi, xbw, lane, h);
+#pragma unroll
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+                if (N % LPQ == 0 || h * RPL + r < N) x[c][r] = dmk((double)d0[c][r].x, (double)d0[c][r].y);
     }
     bool conv[QPL];
     double berr[QPL];
@@ -1669,6 +1796,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         if (__all_sync(0xffffffffu, all) || it >= kIterMax) break;
         // correction x += C r (FP32 product; every C element read serves the QPL q)
         float2 dx[QPL][RPL];
+        if constexpr (TC) {
+            tc_apply<N, RPL, QPL, LPQ>(rr, dx, Ffr, Ffi, xbw, lane, h);
+        } else {
 #pragma unroll
         for (int c = 0; c < QPL; ++c)
 #pragma unroll
@@ -1690,6 +1820,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                         for (int c = 0; c < QPL; ++c) dx[c][r] = f2_fma(cv, rk[c], dx[c][r]);
                     }
             }
+        }
         }
 #pragma unroll
         for (int c = 0; c < QPL; ++c)
@@ -2197,11 +2328,11 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
-template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true>
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false>
 int run_iter(ldga_ctx* ctx, const BseArgs& a) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
-    using S = IterSmem<N, GSM>;
-    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
@@ -2256,7 +2387,8 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true>, "iter8x2tc:3"}, {&run_iter<40, 8, 2, 2, true, true>, "iter8x2tc:2"},
+                               {&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
                                {&run_iter<40, 8, 2>, "iter8:2"}, {&run_iter<40, 4, 3>, "iter"},
                                {&run_warp32<40, 8, 4, 4, 3>, "warp:3"}, {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}};
 const BseVariant inv_40[] = {{&run_tile<40, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};

@@ -272,24 +272,25 @@ def test_bse_preconditioned_iteration(n_iv, dim, ns, require_gpu):
     names = []
     while lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)):
         names.append(lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)).decode())
-    it = [n for n in names if n.startswith("iter")]
-    assert it, names
-    fd, path = tempfile.mkstemp()
-    os.write(fd, f"bse {nnu} {L.PREC_MIXED} {it[-1]}\n".encode())
-    os.close(fd)
+    its = [n for n in names if n.startswith("iter")]
+    assert its, names
     try:
-        L.tune_reset()
-        L.tune_load(path)
-        assert lib.ldga_bse_config_name(nnu, L.PREC_MIXED, -1).decode() == it[-1]
-        g = gpu_chain(inp, L.PREC_MIXED)
-        for r in ("m", "d"):
-            assert rel(g[f"chi_{r}"].data, ref[f"chi_{r}"].data) < RTOL, (nnu, r)
-            assert rel(g[f"gamma_{r}"].data, ref[f"gamma_{r}"]) < RTOL, (nnu, r)
-            # these grids have few q per ω (the groups span wide ranges): a few per cent of the
-            # matrices do not converge in the sweep budget and are re-solved by the pivoted path
-            assert g[f"chi_{r}"].n_fallback <= 0.1 * g["h"].ctx.Nq * g["h"].ctx.Nw
+        for it in its:                       # every compiled configuration of the iteration
+            fd, path = tempfile.mkstemp()
+            os.write(fd, f"bse {nnu} {L.PREC_MIXED} {it}\n".encode())
+            os.close(fd)
+            L.tune_reset()
+            L.tune_load(path)
+            os.unlink(path)
+            assert lib.ldga_bse_config_name(nnu, L.PREC_MIXED, -1).decode() == it
+            g = gpu_chain(inp, L.PREC_MIXED)
+            for r in ("m", "d"):
+                assert rel(g[f"chi_{r}"].data, ref[f"chi_{r}"].data) < RTOL, (nnu, it, r)
+                assert rel(g[f"gamma_{r}"].data, ref[f"gamma_{r}"]) < RTOL, (nnu, it, r)
+                # these grids have few q per ω (the groups span wide ranges): a few per cent of the
+                # matrices do not converge in the sweep budget and are re-solved by the pivoted path
+                assert g[f"chi_{r}"].n_fallback <= 0.1 * g["h"].ctx.Nq * g["h"].ctx.Nw, (nnu, it)
     finally:
-        os.unlink(path)
         L.tune_reset()
 
 
