@@ -23,11 +23,14 @@
 //   LDGA_PREC_FP64_INV  in-place FP64 Gauss-Jordan inverse (N^3, the reference's formulation);
 //                       y = row sums of B^-1.
 //   LDGA_PREC_FP64      FP64 elimination of [B | 1].
-//   LDGA_PREC_MIXED     FP32 elimination, then FP64 iterative refinement: r = 1 - B y in FP64
-//                       (Gamma from shared memory), the correction from the stored FP32 multipliers,
-//                       y += delta, until the backward error reaches FP64 resolution.
+//   LDGA_PREC_MIXED     per box size the fastest of: the q-shared preconditioned iteration
+//                       (k_bse_iter: an FP32 inverse per group of 32 q, FP64 residual sweeps, the
+//                       FP32 product on tensor cores at Nν = 40), an FP32 elimination with FP64
+//                       iterative refinement (r = 1 - B y in FP64, the correction from the stored
+//                       FP32 multipliers), or the FP64 elimination.
 // No pivoting is done in the fast path.  Every solution is verified by its FP64 backward error
-// |1 - B y|_inf / (|B|_inf |y|_inf + 1); a matrix above 1e-12 (or with a non-finite y) is flagged
+// |1 - B y|_inf / (|B|_inf |y|_inf + 1); a matrix above 1e-12 (1e-14 for the preconditioned
+// iteration), or with a non-finite y, is flagged
 // and re-solved by a partial-pivoting FP64 LU kernel, which is also the path for box sizes that
 // have no tiled instantiation.
 #include <cmath>
