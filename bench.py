@@ -326,7 +326,9 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
             f64 = passes * qpw * (8.0 * nnu**2 + 8.0 * nnu) / max(cnt, 1)
             f32 = (passes - warps) * qpw * 8.0 * nnu**2 / max(cnt, 1)
             exe = f64 / t / 1e12
-            kname = ("k_bse_iter (FP32 group inverse, FP64 residual passes, FP32 product on tensor cores: "
+            kname = ("k_bse_iter (FP32 group inverse; FP64 residual on the FP64 tensor path, mma.sync m8n8k4; "
+                     "FP32 product on tensor cores, mma.sync TF32)" if "dm" in cfg else
+                     "k_bse_iter (FP32 group inverse, FP64 residual passes, FP32 product on tensor cores: "
                      "mma.sync TF32)" if "tc" in cfg else "k_bse_iter (FP32 group inverse, FP64 residual passes)")
             return {"kernel": kname, "bound": "fp64",
                     "achieved": exe, "peak": peak, "unit": "TFLOP/s", "frac": exe / peak,

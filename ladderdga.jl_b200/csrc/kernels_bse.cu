@@ -24,8 +24,9 @@
 //                       y = row sums of B^-1.
 //   LDGA_PREC_FP64      FP64 elimination of [B | 1].
 //   LDGA_PREC_MIXED     per box size the fastest of: the q-shared preconditioned iteration
-//                       (k_bse_iter: an FP32 inverse per group of 32 q, FP64 residual sweeps, the
-//                       FP32 product on tensor cores at Nν = 40), an FP32 elimination with FP64
+//                       (k_bse_iter: an FP32 inverse per group of 32 q, FP64 residual sweeps; at
+//                       Nν = 40 both products on tensor cores: FP64 mma.sync m8n8k4 for the residual,
+//                       TF32 m16n8k8 for the correction), an FP32 elimination with FP64
 //                       iterative refinement (r = 1 - B y in FP64, the correction from the stored
 //                       FP32 multipliers), or the FP64 elimination.
 // No pivoting is done in the fast path.  Every solution is verified by its FP64 backward error
@@ -1332,7 +1333,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 }
 
 // ------------------------------------------------------------------------------------------------
-// MIXED, q-shared preconditioner ("iter"; "tc": its FP32 product on tensor cores).  All q of one w share Gamma(w); their matrices differ only
+// MIXED, q-shared preconditioner ("iter"; "tc": its FP32 product on tensor cores; "dm": also its
+// FP64 residual product on the FP64 tensor path).  All q of one w share Gamma(w); their matrices differ only
 // by the diagonal 1/chi0(q, :, w).  k_bse_qorder sorts the q of every w by Re 1/chi0(q, N/2, w);
 // a CTA of k_bse_iter takes 32 consecutive q of that order and forms, in FP32, the in-place
 // Gauss-Jordan inverse C of B_bar = Gamma(w)^T + diag(mean over its q of 1/chi0).  Every q of the
@@ -1355,14 +1357,20 @@ constexpr double kIterTol = 1e-14;
 // accumulation): C is kept as the A fragments of its real and imaginary parts, MT x KT tiles of
 // 16 x 8 with the rows padded to MT 16, and every warp has an exchange buffer that brings its 8 q's
 // residuals into B-fragment order and the products back to the lanes that own the rows.
-template <int N, bool GSM = true, bool TC = false, int NWARP = 4>
+// DM: the FP64 residual product runs on the FP64 tensor path (mma.sync m8n8k4 .f64): Gamma^T is kept
+// as the A fragments of its real and imaginary parts (N/8 x N/4 tiles of 8 x 4) instead of row-major.
+template <int N, bool GSM = true, bool TC = false, int NWARP = 4, bool DM = false>
 struct IterSmem {
     static constexpr int LD = N + 1;
     static constexpr int MT = (N + 15) / 16, KT = N / 8, XS = 2 * N + 4;   // TC tiles, exchange stride
-    static constexpr size_t c_bytes = TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) + (size_t)NWARP * 8 * XS * sizeof(float)
+    static constexpr int XD = N + 4;                                       // DM exchange stride (doubles)
+    static constexpr size_t xw_bytes = (size_t)8 * XS * sizeof(float) > (size_t)8 * XD * sizeof(double)
+                                           ? (size_t)8 * XS * sizeof(float) : (size_t)8 * XD * sizeof(double);
+    static constexpr size_t c_bytes = TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) + (size_t)NWARP * xw_bytes
                                          : (size_t)N * LD * sizeof(float2);
-    // Gt [N][LD] double2 (GSM: Gamma staged in shared memory; otherwise read through L1/L2)
-    static constexpr size_t off_D = GSM ? (size_t)N * LD * sizeof(double2) : 0;
+    // Gt [N][LD] double2 (GSM: Gamma staged in shared memory; otherwise read through L1/L2); DM: the
+    // A fragments [2][N/8][N/4][32] doubles
+    static constexpr size_t off_D = DM ? (size_t)N * N * sizeof(double2) : GSM ? (size_t)N * LD * sizeof(double2) : 0;
     static constexpr size_t off_C = off_D + (size_t)kIterQ * N * sizeof(double2);  // D [32][N] double2
     static constexpr size_t off_X = off_C + (TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) : 0);  // TC exchange
     static constexpr size_t off_rowabs = off_C + ((c_bytes + 15) & ~size_t(15));
@@ -1449,6 +1457,69 @@ __device__ __forceinline__ void tc_apply(const float2 (&rr)[QPL][RPL], float2 (&
     }
 }
 
+// d += a b, one m8n8k4 FP64 tile (one A and one B fragment value per lane)
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// acc = B x for the warp's 8 q (the same lane layout as tc_apply) on the FP64 tensor path: gr / gi
+// hold the A fragments of Re and Im of the B rows (Gamma^T without the diagonal), tile (mt, kt) at
+// [(mt KT + kt) 32 + lane]; xb: this warp's exchange buffer [8 q][XD] doubles, used once for the real
+// parts and once for the imaginary parts in each direction.
+template <int N, int RPL, int QPL, int LPQ>
+__device__ __forceinline__ void dm_apply(const double2 (&x)[QPL][RPL], double2 (&acc)[QPL][RPL], const double* gr,
+                                         const double* gi, double* xb, int lane, int h) {
+    constexpr int MT = N / 8, KT = N / 4, XD = N + 4;
+    static_assert(N % 8 == 0 && QPL * 32 / LPQ == 8, "the FP64 tensor product wants 8-row tiles and 8 q per warp");
+    const int g = lane >> 2, t = lane & 3, qb = (lane / LPQ) * QPL;
+    double bre[KT], bim[KT];
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+                if (h * RPL + r < N) xb[(qb + c) * XD + h * RPL + r] = part ? x[c][r].y : x[c][r].x;
+        __syncwarp();
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) (part ? bim : bre)[kt] = xb[g * XD + kt * 4 + t];
+    }
+    double dr[MT][2], di[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+        dr[mt][0] = dr[mt][1] = di[mt][0] = di[mt][1] = 0.0;
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) {
+            const double ar = gr[(mt * KT + kt) * 32 + lane], ai = gi[(mt * KT + kt) * 32 + lane];
+            mma_f64(dr[mt], ar, bre[kt]);
+            mma_f64(dr[mt], -ai, bim[kt]);
+            mma_f64(di[mt], ai, bre[kt]);
+            mma_f64(di[mt], ar, bim[kt]);
+        }
+    }
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+        __syncwarp();
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            xb[(2 * t) * XD + mt * 8 + g] = part ? di[mt][0] : dr[mt][0];
+            xb[(2 * t + 1) * XD + mt * 8 + g] = part ? di[mt][1] : dr[mt][1];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < QPL; ++c)
+#pragma unroll
+            for (int r = 0; r < RPL; ++r)
+                if (h * RPL + r < N) {
+                    const double v = xb[(qb + c) * XD + h * RPL + r];
+                    if (part) acc[c][r].y = v; else acc[c][r].x = v;
+                }
+    }
+}
+
 // perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order.  One CTA per w,
 // bitonic sort of the next power of two >= nq (<= 4096) in shared memory; non-finite keys sort as 0.
 __global__ void __launch_bounds__(1024) k_bse_qorder(int nq, int nnu, const double2* __restrict__ chi0,
@@ -1504,9 +1575,10 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
     return acc;
 }
 
-template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC>
+template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM>
 __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
-    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
+    static_assert(!DM || (GSM && TC), "the FP64 tensor product is built with the tensor-core FP32 product");
     constexpr int LD = S::LD;
     constexpr int LDG = GSM ? LD : N;   // row stride of Gamma^T where it is read
     constexpr int RPL = (N + LPQ - 1) / LPQ;
@@ -1532,6 +1604,17 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     // fixed trip counts, fully unrolled: every global load of a thread is in flight at once
     const double2* Gw = a.Gamma + (size_t)w * N * N;
     const double2* Gt = GSM ? Gs : Gw;
+    double* Gfr = reinterpret_cast<double*>(it_raw);            // DM: A fragments of Re B, then Im B
+    double* Gfi = Gfr + N * N;
+    // element B_ij without the diagonal term, from wherever Gamma^T is kept
+    auto gelt = [&](int i, int j) -> double2 {
+        if constexpr (DM) {
+            const int f = ((i >> 3) * (N / 4) + (j >> 2)) * 32 + (i & 7) * 4 + (j & 3);
+            return dmk(Gfr[f], Gfi[f]);
+        } else {
+            return Gt[i * LDG + j];
+        }
+    };
     if constexpr (GSM) {
         constexpr int NG = (N * N + NT - 1) / NT;
         double2 gv[NG];
@@ -1543,7 +1626,16 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int m = 0; m < NG; ++m) {
             const int e = tid + NT * m;
-            if (e < N * N) Gs[(e / N) * LD + (e - (e / N) * N)] = gv[m];
+            if (e < N * N) {
+                const int i = e / N, j = e - (e / N) * N;
+                if constexpr (DM) {
+                    const int f = ((i >> 3) * (N / 4) + (j >> 2)) * 32 + (i & 7) * 4 + (j & 3);
+                    Gfr[f] = gv[m].x;
+                    Gfi[f] = gv[m].y;
+                } else {
+                    Gs[i * LD + j] = gv[m];
+                }
+            }
         }
     }
     {
@@ -1573,7 +1665,10 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         constexpr int NWARP = NT / 32;
         for (int i = tid >> 5; i < N; i += NWARP) {
             double sacc = 0.0;
-            for (int j = lane; j < N; j += 32) sacc += fabs(Gt[i * LDG + j].x) + fabs(Gt[i * LDG + j].y);
+            for (int j = lane; j < N; j += 32) {
+                const double2 v = gelt(i, j);
+                sacc += fabs(v.x) + fabs(v.y);
+            }
             double2 m = lane < nvalid ? Dq[lane * N + i] : dmk(0.0, 0.0);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -1605,7 +1700,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             const int jj = j0 + c;
             ce[c] = make_float2(0.f, 0.f);
             if (own && jj < N) {
-                double2 v = Gt[gi * LDG + jj];
+                double2 v = gelt(gi, jj);
                 if (gi == jj) v = cadd(v, dbar[gi]);
                 ce[c] = make_float2((float)v.x, (float)v.y);
             }
@@ -1688,7 +1783,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         double rowg = 0.0;
         double2 g = dmk(0.0, 0.0);
         if (N % LPQ == 0 || i < N) {
-            g = Gt[i * LDG + i];
+            g = gelt(i, i);
             rowg = rowabs[i] - (fabs(g.x) + fabs(g.y));
             if constexpr (!TC) {
                 float2 s2 = make_float2(0.f, 0.f);
@@ -1712,7 +1807,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     }
     const uint4* Ffr = reinterpret_cast<const uint4*>(Cf);
     const uint4* Ffi = Ffr + S::MT * S::KT * 32;
-    float* xbw = Xb + (tid >> 5) * 8 * S::XS;
+    float* xbw = reinterpret_cast<float*>(reinterpret_cast<char*>(Xb) + (tid >> 5) * S::xw_bytes);
     if constexpr (TC) {   // x = C 1 through the same tensor-core product
         float2 one[QPL][RPL], d0[QPL][RPL];
 #pragma unroll
@@ -1745,6 +1840,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         for (int c = 0; c < QPL; ++c)
 #pragma unroll
             for (int r = 0; r < RPL; ++r) acc[c][r] = dmk(0.0, 0.0);
+        if constexpr (DM) {
+            dm_apply<N, RPL, QPL, LPQ>(x, acc, Gfr, Gfi, reinterpret_cast<double*>(xbw), lane, h);
+        } else {
 #pragma unroll 1
         for (int s = 0; s < LPQ; ++s) {
             const double2* grow = Gt + (size_t)(h * RPL) * LDG + s * RPL;
@@ -1768,6 +1866,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                     }
                 }
             }
+        }
         }
         float2 rr[QPL][RPL];
         bool all = true;
@@ -2331,11 +2430,11 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
-template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false>
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
 int run_iter(ldga_ctx* ctx, const BseArgs& a) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
-    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32>;
-    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
@@ -2390,7 +2489,8 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true>, "iter8x2tc:3"}, {&run_iter<40, 8, 2, 2, true, true>, "iter8x2tc:2"},
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2"}, {&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3"},
+                               {&run_iter<40, 8, 3, 2, true, true>, "iter8x2tc:3"}, {&run_iter<40, 8, 2, 2, true, true>, "iter8x2tc:2"},
                                {&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
                                {&run_iter<40, 8, 2>, "iter8:2"}, {&run_iter<40, 4, 3>, "iter"},
                                {&run_warp32<40, 8, 4, 4, 3>, "warp:3"}, {&run_warp32<40, 8, 4, 4, 2>, "warp:2"}};
