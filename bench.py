@@ -291,6 +291,22 @@ def tune(chain) -> str:
     return name.decode() if name else "pivoted"
 
 
+def newton_period(chain):
+    """The λm Newton of the last step rerun alone (newton_right's nsteps 100, atol 1e-13): the
+    iterations it reports and where its state began to repeat (iteration, period), from which on
+    whole periods are skipped."""
+    try:
+        chid = C.c_double()
+        chain.ctx.call("ldga_sum_kw", 1, 0.0, 0, C.byref(chid))
+        lam, its, per = C.c_double(), C.c_int32(), (C.c_int32 * 2)()
+        chain.ctx.call("ldga_lambda_m_newton", 2 * chain.h.imp_density - chid.value, 100, 1e-13, C.byref(lam),
+                       C.byref(its), per)
+        return {"lambda_m": lam.value, "iterations": its.value, "repeat_at": per[0], "period": per[1],
+                "executed": per[0] + (its.value - per[0]) % per[1] if per[1] else its.value}
+    except Exception as e:  # reported, not fatal: the bench line stands without it
+        return {"error": str(e)}
+
+
 def stage_times(chain):
     from ladderdga_b200._lib import STAGES
     ms = (C.c_double * 10)()
@@ -427,6 +443,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     chain.ctx.call("ldga_profile", 0)
+    newton = newton_period(chain)
     ms = float(np.mean(t_dev))
     ms_e2e = float(np.mean(t_e2e))
     if world > 1:
@@ -480,7 +497,7 @@ def run_ours(args):
                 "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items() if v[1]},
                 "gpu_launches": launches,
                 "result": {"lambda_m": scal[0], "mu": scal[1], "E_kin": scal[2], "E_pot1": scal[3],
-                           "newton_iterations": scal[6]},
+                           "newton_iterations": scal[6], "newton_rerun": newton},
                 "clocks": clk}
         if fp64_cmp is not None:
             line["fp64_compare"] = fp64_cmp

@@ -297,6 +297,14 @@ int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double
  * conditions_new.jl:144-154), all on the device.  iterations may be NULL. */
 int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iterations);
 
+/* ldga_lambda_m with newton_right's keywords (helpers.jl:133: nsteps >= 1, atol >= 0).  Once the
+ * iteration state (x0, xi) repeats (near the root |f| can stay above atol while xi cycles among a
+ * few values ulps apart), whole periods up to nsteps are skipped; lam_out and iterations are bit
+ * for bit those of the full loop.  period [2] (may be NULL) receives the iteration at which the
+ * repeat was recognised and its period, {0, 0} if nothing was skipped. */
+int ldga_lambda_m_newton(ldga_ctx* ctx, double rhs, int32_t nsteps, double atol, double* lam_out,
+                         int32_t* iterations, int32_t* period);
+
 /* ---------------------------------------------------------------- a15: G_ladder, energies ---- */
 
 /* From the Sigma_ladder of the last ldga_eom: fit mu to the filling n (fix_n != 0; G_from_Σladder!,

@@ -24,7 +24,7 @@ EXPORTS = [
     "ldga_set_model", "ldga_set_precision", "ldga_kgrid", "ldga_gloc", "ldga_set_gloc", "ldga_bubble",
     "ldga_set_chi0", "ldga_bse", "ldga_set_chi", "ldga_set_gamma", "ldga_F_from_chi", "ldga_lambda0",
     "ldga_set_lambda0", "ldga_sum_kw", "ldga_sum_wk", "ldga_lambda_min", "ldga_eom", "ldga_eom_parts",
-    "ldga_lambda_m", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
+    "ldga_lambda_m", "ldga_lambda_m_newton", "ldga_g_ladder", "ldga_set_sigma", "ldga_calc_E", "ldga_lambda_dm",
     "ldga_lambda_dm_evals", "ldga_set_stream", "ldga_profile", "ldga_stage_times", "ldga_launch_count",
     "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp",
     "ldga_eom_vjp", "ldga_autotune_bse", "ldga_tune_save", "ldga_tune_load",
@@ -108,6 +108,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_eom": (C.c_int, [P, D, D, I32, I32, D, P]),
         "ldga_eom_parts": (C.c_int, [P, D, D, I32, D, P]),
         "ldga_lambda_m": (C.c_int, [P, D, PD, PI32]),
+        "ldga_lambda_m_newton": (C.c_int, [P, D, I32, D, PD, PI32, PI32]),
         "ldga_g_ladder": (C.c_int, [P, P, I32, I32, D, PD, P, PD, PD, PD]),
         "ldga_lambda_dm": (C.c_int, [P, D, I32, D, D, I32, PD, PD, PI32, P, PI32, P, P]),
         "ldga_lambda_dm_evals": (C.c_int, [P, PI32]),

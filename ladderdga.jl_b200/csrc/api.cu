@@ -976,17 +976,24 @@ int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double
     return sync(ctx);
 }
 
-int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iterations) {
+int ldga_lambda_m_newton(ldga_ctx* ctx, double rhs, int32_t nsteps, double atol, double* lam_out,
+                         int32_t* iterations, int32_t* period) {
     if (!ctx || !lam_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    if (nsteps < 1 || !(atol >= 0.0)) return ctx_fail(ctx, LDGA_ERR_ARG, "newton_right: nsteps >= 1, atol >= 0");
     NEED(ctx, ctx->have_chi[LDGA_CH_M], "λm_correction: chi_m missing");
     DeviceGuard g(ctx->device);
-    TRY(launch_lambda_m(ctx, rhs, nullptr, ctx->d_red + 16));
-    double r[2];
-    TRY(copy(ctx, r, ctx->d_red + 16, 2 * sizeof(double)));
+    TRY(launch_lambda_m(ctx, rhs, nullptr, ctx->d_red + 16, nsteps, atol));
+    double r[5];
+    TRY(copy(ctx, r, ctx->d_red + 16, 5 * sizeof(double)));
     TRY(sync(ctx));
     *lam_out = r[0];
     if (iterations) *iterations = (int32_t)r[1];
+    if (period) { period[0] = (int32_t)r[3]; period[1] = (int32_t)r[4]; }
     return LDGA_OK;
+}
+
+int ldga_lambda_m(ldga_ctx* ctx, double rhs, double* lam_out, int32_t* iterations) {
+    return ldga_lambda_m_newton(ctx, rhs, 100, 1e-13, lam_out, iterations, nullptr);
 }
 
 int ldga_g_ladder(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, int32_t fix_n, double mu_in,

@@ -246,6 +246,15 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 // K > 0: every thread keeps its K elements of chi and their kMult weights in registers for the whole
 // loop (elements e = tid + j * threads, the order the K = 0 streaming form sums in); the constant
 // tail of sum_kω is formed once.  An iteration is then K divisions, one cluster_sum and the step.
+//
+// Periodic trajectories are shortened exactly.  Near the root |f| often stays above atol (1e-13 is
+// below the rounding noise of the sum), so newton_right runs all nsteps iterations while xi hops
+// among a few values ulps apart.  The state (x0, xi) at the top of an iteration fixes every later
+// iteration (the sums are reduced in a fixed order, so f and df are bitwise reproducible), so once
+// that state equals the one saved at the last power-of-two checkpoint (iterations 1, 2, 4, ...),
+// the trajectory has period p = i - checkpoint and whole periods up to nsteps are skipped; the last
+// < p iterations then run as usual.  xi and i come out bit for bit as from the full loop.
+// out[3], out[4]: the iteration at which the repeat was recognised and p (0, 0: nothing skipped).
 template <int K>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
@@ -269,14 +278,55 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
     }
     double x0 = 0.0, xi = x0;
     int i = 1;
+    long long ck_x0 = __double_as_longlong(x0), ck_xi = __double_as_longlong(xi);
+    int ck_i = 1, skip_at = 0, skip_p = 0;
     while (true) {
         double v[2] = {0.0, 0.0};
         if (K > 0) {
+            // Batch inversion (Montgomery's trick): prefix products of the denominators 1 + xi x,
+            // one division of the total, then every 1/d_j from two products.  The direct form's
+            // K divisions ran one after another, each behind its slow-path branch; these products
+            // overlap.  K > 8 splits into two independent batches (two divisions, shorter chains,
+            // fewer live registers).  A product outside [1e-300, 1e300] (an exact pole, extreme
+            // lambda) takes the direct divisions, so infinities stay confined to their elements.
+            constexpr int NB = K > 8 ? 2 : 1;
+            constexpr int G = (K + NB - 1) / NB;
 #pragma unroll
-            for (int j = 0; j < K; ++j) {
-                const double t = xv[j] / (xi * xv[j] + 1.0);
-                v[0] = fma(kv[j], t, v[0]);
-                v[1] = fma(kv[j], -t * t, v[1]);
+            for (int b = 0; b < NB; ++b) {
+                constexpr int G0 = G > 0 ? G : 1;
+                double d[G0], pre[G0];
+                double prod = 1.0;
+#pragma unroll
+                for (int u = 0; u < G; ++u) {
+                    const int j = b * G + u;
+                    d[u] = j < K ? fma(xi, xv[j < K ? j : 0], 1.0) : 1.0;
+                    pre[u] = prod;
+                    prod *= d[u];
+                }
+                if (fabs(prod) > 1e-300 && fabs(prod) < 1e300) {
+                    double r = 1.0 / prod;
+#pragma unroll
+                    for (int u = G - 1; u >= 0; --u) {
+                        const int j = b * G + u;
+                        const double inv = r * pre[u];
+                        r *= d[u];
+                        if (j < K) {
+                            const double t = xv[j] * inv;
+                            v[0] = fma(kv[j], t, v[0]);
+                            v[1] = fma(kv[j], -t * t, v[1]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < G; ++u) {
+                        const int j = b * G + u;
+                        if (j < K) {
+                            const double t = xv[j] / d[u];
+                            v[0] = fma(kv[j], t, v[0]);
+                            v[1] = fma(kv[j], -t * t, v[1]);
+                        }
+                    }
+                }
             }
         } else {
             for (int e = tid; e < total; e += nth) {
@@ -297,8 +347,24 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
         else x0 = xi;
         if (i >= nsteps) break;
         ++i;
+        // top of iteration i: every thread holds the same (x0, xi), so the branch is uniform
+        const long long bx0 = __double_as_longlong(x0), bxi = __double_as_longlong(xi);
+        if (skip_p == 0 && bx0 == ck_x0 && bxi == ck_xi) {
+            skip_at = i;
+            skip_p = i - ck_i;
+            i += skip_p * ((nsteps - i) / skip_p);
+        } else if (skip_p == 0 && (i & (i - 1)) == 0) {
+            ck_x0 = bx0;
+            ck_xi = bxi;
+            ck_i = i;
+        }
     }
-    if (tid == 0) { out[0] = xi; out[1] = (double)i; }
+    if (tid == 0) {
+        out[0] = xi;
+        out[1] = (double)i;
+        out[3] = (double)skip_at;
+        out[4] = (double)skip_p;
+    }
     cg::this_cluster().sync();
 }
 
@@ -623,8 +689,9 @@ int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
 }
 
 // lambda_m Newton: rhs = rhs_const - *rhs_sub_dev (if given); d_out[0] = lambda, d_out[1] = iterations;
-// d_out[2] receives lambda_min.
-int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out) {
+// d_out[2] receives lambda_min; d_out[3..4] the periodic-trajectory skip (iteration, period).
+int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out, int nsteps,
+                    double atol) {
     int st = launch_lambda_min(ctx, LDGA_CH_M, d_out + 2);
     if (st) return st;
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
@@ -634,7 +701,7 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
               : per <= 8 ? k_lambda_m<8> : per <= 10 ? k_lambda_m<10> : per <= 12 ? k_lambda_m<12>
               : per <= 16 ? k_lambda_m<16> : k_lambda_m<0>;
     kern<<<kCluster, kClThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
-                                                   d_out + 2, 100, 1e-13, d_out);
+                                                   d_out + 2, nsteps, atol, d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");
     return LDGA_OK;
 }

@@ -160,6 +160,76 @@ def test_lambda_m_correction(case):
     assert abs(t_sc - (2 * g["h"].imp_density) / 2) < 1e-9
 
 
+def _lambda_m_newton(xm, rhs, nsteps, atol):
+    lam, its, period = L._lib.C.c_double(), L._lib.C.c_int32(), (L._lib.C.c_int32 * 2)()
+    xm._ctx.call("ldga_lambda_m_newton", rhs, nsteps, atol, L._lib.C.byref(lam), L._lib.C.byref(its), period)
+    return lam.value, its.value, (period[0], period[1])
+
+
+@pytest.mark.parametrize("nsteps,atol", [(100, 1e-13), (500, 0.0)])
+def test_lambda_m_newton_periodic_skip(case, nsteps, atol):
+    """The device newton_right skips whole periods once its state (x0, xi) repeats; the result and
+    the iteration count must be bit for bit those of the full loop.  A run whose nsteps ends before
+    the repeat is recognised executes every iteration, so the skipped run at nsteps must equal the
+    full run at the same phase of the period.  atol = 0 never converges: every case cycles."""
+    name, inp, ref = case
+    g = gpu_chain(inp)
+    xm = g["chi_m"]
+    rhs = 2 * g["h"].imp_density - L.sum_kω(g["h"].kG, g["chi_d"])
+    lam, its, (at, p) = _lambda_m_newton(xm, rhs, nsteps, atol)
+    if atol == 0.0:
+        assert p > 0 and its == nsteps
+    if p > 0:
+        assert its == nsteps
+        s = at - p                                 # the checkpoint the state returned to
+        m = s + (nsteps - s) % p                   # same phase of the period, before the repeat
+        assert m < at
+        lam_full, its_full, per_full = _lambda_m_newton(xm, rhs, m, atol)
+        assert per_full == (0, 0) and its_full == m
+        assert lam == lam_full                     # bitwise
+    lam_default = L._lib.C.c_double()
+    xm._ctx.call("ldga_lambda_m", rhs, L._lib.C.byref(lam_default), None)
+    if nsteps == 100:
+        assert lam_default.value == lam
+    rr = R.lambda_m_correction_full(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"],
+                                    ref["h"])
+    assert abs(lam - rr.lam_m) < ATOL_LAMBDA
+    with pytest.raises(L.LdgaError):
+        _lambda_m_newton(xm, rhs, 0, atol)
+
+
+def test_lambda_m_newton_trajectory_3d32(require_gpu):
+    """The benchmark point (3D sc 32³, β = 20, U = 1.5, Nν = 40, Nω = 41, seed 3000).  Its synthetic
+    χ_m(q, ω) is negative for every q at large |ω|, so f(λ) = sum_kω χ_λ − rhs has poles above
+    λ ≈ 20.9 and several roots between them; newton_right (start 0, df with the tail terms of
+    df_c1) walks right in steps of ~1.4 and then wanders among the poles, where the iterates depend
+    on the rounding of the sums.  Checked: the device iterates equal the oracle's through the smooth
+    phase, and the device's final λ (after nsteps = 100) is a root of the oracle's f.  The oracle
+    itself settles on another root (29.588...); both are valid answers of the same algorithm."""
+    inp = S.config_input(3, point=0)
+    ref = R.run_chain(inp, lambda_type=None)
+    rh, cm = ref["h"], ref["chi_m"]
+    rhs_r = 2 * rh.imp_density - R.sum_kw(rh.kG, ref["chi_d"])
+
+    def f(l):
+        return R.sum_kw(rh.kG, cm, transform=lambda x: R.chi_lambda(x, l)) - rhs_r
+
+    def df(l):
+        return R.sum_kw(rh.kG, cm, transform=lambda x: R.dchi_lambda(x, l))
+
+    g = gpu_chain(inp)
+    rhs = 2 * g["h"].imp_density - L.sum_kω(g["h"].kG, g["chi_d"])
+    assert abs(rhs - rhs_r) < 1e-10 * max(1.0, abs(rhs_r))
+    lmin = R.get_lambda_min(cm.data)
+    for k in (1, 3, 6, 10, 13):                    # f evaluated left of the first pole (20.9)
+        lam_k, its_k, _ = _lambda_m_newton(g["chi_m"], rhs, k, 1e-13)
+        want = R.newton_right(f, df, 0.0, lmin, nsteps=k)
+        assert its_k == k and abs(lam_k - want) <= 1e-9 * max(1.0, abs(want)), (k, lam_k, want)
+    lam, its, _ = _lambda_m_newton(g["chi_m"], rhs, 100, 1e-13)
+    scale = R.sum_kw(rh.kG, cm, transform=lambda x: np.abs(R.chi_lambda(x, lam)))
+    assert its == 100 and lam > 20.0 and abs(f(lam)) <= 1e-9 * max(1.0, scale), (lam, f(lam))
+
+
 def test_lambda_dm_correction(case):
     name, inp, ref = case
     if name != "2d16":
