@@ -1375,8 +1375,8 @@ struct IterSmem {
     static constexpr size_t off_X = off_C + (TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) : 0);  // TC exchange
     static constexpr size_t off_rowabs = off_C + ((c_bytes + 15) & ~size_t(15));
     static constexpr size_t off_dbar = off_rowabs + (((size_t)N * sizeof(double) + 15) & ~size_t(15));
-    static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);       // [2][column, row]
-    static constexpr size_t bytes = off_pc + 4 * (size_t)N * sizeof(float2);
+    static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);  // [2][2 columns, 2 rows]
+    static constexpr size_t bytes = off_pc + 8 * (size_t)N * sizeof(float2);
 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -1659,37 +1659,34 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         }
     }
     __syncthreads();
-    // |row|_1 of Gamma^T (lanes over columns) and the group's mean diagonal (lanes over q), one row
-    // per warp at a time, fixed-order butterfly sums
-    {
-        constexpr int NWARP = NT / 32;
-        for (int i = tid >> 5; i < N; i += NWARP) {
-            double sacc = 0.0;
-            for (int j = lane; j < N; j += 32) {
-                const double2 v = gelt(i, j);
-                sacc += fabs(v.x) + fabs(v.y);
-            }
-            double2 m = lane < nvalid ? Dq[lane * N + i] : dmk(0.0, 0.0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
-                m.x += __shfl_xor_sync(0xffffffffu, m.x, o);
-                m.y += __shfl_xor_sync(0xffffffffu, m.y, o);
-            }
-            if (lane == 0) {
-                rowabs[i] = sacc;
-                dbar[i] = cscale(m, 1.0 / (double)max(nvalid, 1));
-            }
+    // |row|_1 of Gamma^T (one thread per row) and the group's mean diagonal (one thread per nu, in
+    // another warp), each a sequential sum in a fixed order: no shuffle chains on the set-up path
+    static_assert(NT >= 64 + N, "row sums in threads 0..N-1, diagonal means in threads 64..63+N");
+    if (tid < N) {
+        double sacc = 0.0;
+        for (int j = 0; j < N; ++j) {
+            const double2 v = gelt(tid, j);
+            sacc += fabs(v.x) + fabs(v.y);
         }
+        rowabs[tid] = sacc;
+    } else if (tid >= 64 && tid < 64 + N) {
+        const int i = tid - 64;
+        double2 m = dmk(0.0, 0.0);
+        for (int q = 0; q < nvalid; ++q) m = cadd(m, Dq[q * N + i]);
+        dbar[i] = cscale(m, 1.0 / (double)max(nvalid, 1));
     }
     __syncthreads();
-    // ---- C = B_bar^-1: in-place Gauss-Jordan in FP32 without pivoting (a poor C only costs sweeps).
-    // TPR threads own each row (a contiguous segment of CPT columns each, in registers); the owners
-    // of column k and row k publish them to a double-buffered pair of shared vectors, so one barrier
-    // per step suffices (buffer k & 1 was last read in step k - 2, before barrier k - 1).  Step k:
-    // a_kk <- 1/a_kk, row k <- row k / a_kk, column k <- -column k / a_kk, the rest a_ij -= m_i a_kj
-    // with m_i = a_ik / a_kk formed once per row.
+    // ---- C = B_bar^-1: in-place Gauss-Jordan in FP32 without pivoting (a poor C only costs sweeps),
+    // two pivots per step (N is even: N = 2 n_iv).  TPR threads own each row (a contiguous segment of
+    // CPT columns each, in registers).  Step k publishes columns k, k+1 and rows k, k+1 to a
+    // double-buffered shared block, so one barrier per step suffices (buffer (k/2) & 1 was last read
+    // in the step before the previous barrier).  With P the 2 x 2 pivot block, row i outside it takes
+    // a_ij -= (a_i,k:k+1 P^-1) . u_k:k+1,j.  The published rows carry P + I in the pivot columns, so
+    // the same update writes -(a_i,k:k+1 P^-1) into columns k, k+1 (the Gauss-Jordan column entries)
+    // with no per-element branch; the pivot rows become P^-1 u (and P^-1 in the pivot columns, which
+    // is the +I term's product minus the identity).  Mathematically two single-pivot steps.
     {
+        static_assert(N % 2 == 0, "pivot pairs");
         constexpr int TPR = NT / N > 0 ? NT / N : 1;
         constexpr int CPT = (N + TPR - 1) / TPR;
         const int gi = tid / TPR, gp = tid - (tid / TPR) * TPR, j0 = gp * CPT;
@@ -1705,37 +1702,65 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 ce[c] = make_float2((float)v.x, (float)v.y);
             }
         }
-        for (int k = 0; k < N; ++k) {
-            float2* pcol = pc + (k & 1) * 2 * N;   // [N] column k, then [N] row k
-            float2* prow = pcol + N;
+        for (int k = 0; k < N; k += 2) {
+            float2* pb = pc + ((k >> 1) & 1) * 4 * N;   // [N] column k, [N] column k+1, [N] row k, [N] row k+1
             if (own) {
 #pragma unroll
                 for (int c = 0; c < CPT; ++c) {
                     const int jj = j0 + c;
-                    if (jj == k) pcol[gi] = ce[c];
-                    if (gi == k && jj < N) prow[jj] = ce[c];
+                    if (jj == k) pb[gi] = ce[c];
+                    if (jj == k + 1) pb[N + gi] = ce[c];
+                }
+                if (gi == k || gi == k + 1) {
+                    float2* prow = pb + 2 * N + (gi - k) * N;
+#pragma unroll
+                    for (int c = 0; c < CPT; ++c) {
+                        const int jj = j0 + c;
+                        if (jj < N) prow[jj] = jj == gi ? make_float2(ce[c].x + 1.f, ce[c].y) : ce[c];
+                    }
                 }
             }
             __syncthreads();
             if (own) {
-                const float2 p = vinv(pcol[k]);
-                if (gi == k) {
-#pragma unroll
-                    for (int c = 0; c < CPT; ++c) ce[c] = (j0 + c == k) ? p : fmul(ce[c], p);
-                } else {
-                    const float2 m = fmul(pcol[gi], p);
+                const float2* prow0 = pb + 2 * N;
+                const float2* prow1 = pb + 3 * N;
+                const float2 p00 = pb[k], p10 = pb[k + 1], p01 = pb[N + k], p11 = pb[N + k + 1];
+                const float2 pd = fmul(p00, p11), po = fmul(p01, p10);
+                const float2 rdet = vinv(make_float2(pd.x - po.x, pd.y - po.y));
+                const float2 i00 = fmul(p11, rdet), i11 = fmul(p00, rdet);
+                const float2 i01 = fmul(make_float2(-p01.x, -p01.y), rdet);
+                const float2 i10 = fmul(make_float2(-p10.x, -p10.y), rdet);
+                float2 m0, m1;
+                if (gi == k || gi == k + 1) {          // pivot row: P^-1[r, :] u', minus its +1
+                    m0 = gi == k ? i00 : i10;
+                    m1 = gi == k ? i01 : i11;
 #pragma unroll
                     for (int c = 0; c < CPT; ++c) {
                         const int jj = j0 + c;
-                        if (jj == k) {
-                            ce[c] = make_float2(-m.x, -m.y);
-                        } else if (jj < N) {
-                            const float2 u = prow[jj];
+                        if (jj < N) {
+                            float2 v = fadd(fmul(m0, prow0[jj]), fmul(m1, prow1[jj]));
+                            if (jj == gi) v.x -= 1.f;
+                            ce[c] = v;
+                        }
+                    }
+                } else {                                // m = a_i,k:k+1 P^-1; a_ij -= m . u'_j
+                    const float2 a0 = pb[gi], a1 = pb[N + gi];
+                    m0 = fadd(fmul(a0, i00), fmul(a1, i10));
+                    m1 = fadd(fmul(a0, i01), fmul(a1, i11));
+#pragma unroll
+                    for (int c = 0; c < CPT; ++c) {
+                        const int jj = j0 + c;
+                        if (jj < N) {
+                            const float2 u0 = prow0[jj], u1 = prow1[jj];
                             float2 v = ce[c];
-                            v.x = fmaf(-m.x, u.x, v.x);
-                            v.x = fmaf(m.y, u.y, v.x);
-                            v.y = fmaf(-m.x, u.y, v.y);
-                            v.y = fmaf(-m.y, u.x, v.y);
+                            v.x = fmaf(-m0.x, u0.x, v.x);
+                            v.x = fmaf(m0.y, u0.y, v.x);
+                            v.y = fmaf(-m0.x, u0.y, v.y);
+                            v.y = fmaf(-m0.y, u0.x, v.y);
+                            v.x = fmaf(-m1.x, u1.x, v.x);
+                            v.x = fmaf(m1.y, u1.y, v.x);
+                            v.y = fmaf(-m1.x, u1.y, v.y);
+                            v.y = fmaf(-m1.y, u1.x, v.y);
                             ce[c] = v;
                         }
                     }
