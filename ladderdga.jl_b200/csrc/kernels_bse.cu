@@ -1375,8 +1375,13 @@ struct IterSmem {
     static constexpr size_t off_X = off_C + (TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) : 0);  // TC exchange
     static constexpr size_t off_rowabs = off_C + ((c_bytes + 15) & ~size_t(15));
     static constexpr size_t off_dbar = off_rowabs + (((size_t)N * sizeof(double) + 15) & ~size_t(15));
-    static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);  // [2][2 columns, 2 rows]
-    static constexpr size_t bytes = off_pc + 8 * (size_t)N * sizeof(float2);
+    // Gauss-Jordan pivot buffers [2][columns k, k+1: 2 N float2][rows k, k+1 interleaved: RW float4],
+    // RW = the row width the owning threads cover (N rounded up to their segments)
+    static constexpr int TPR = NWARP * 32 / N > 0 ? NWARP * 32 / N : 1;
+    static constexpr int RW = (N + TPR - 1) / TPR * TPR;
+    static constexpr size_t pc_half = 2 * (size_t)N * sizeof(float2) + (size_t)RW * sizeof(float4);
+    static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);
+    static constexpr size_t bytes = off_pc + 2 * pc_half;
 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -1652,10 +1657,33 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             const int e = tid + NT * m, v = e - (e / N) * N;
             cv[m] = qg[m] >= 0 ? a.chi0[(size_t)qg[m] + (size_t)a.nq * (v + (size_t)N * w)] : dmk(0.0, 0.0);
         }
+        // 1/chi0 = conj(chi0) / |chi0|^2 by batch inversion (Montgomery's trick): prefix products of
+        // the ND squared moduli, one division, two products per reciprocal, instead of ND scaled
+        // complex reciprocals (three divisions each) run one after another.  A product outside
+        // [1e-300, 1e300] takes cinv element by element.
+        double nrm[ND], pre[ND];
+        double prod = 1.0;
 #pragma unroll
         for (int m = 0; m < ND; ++m) {
-            const int e = tid + NT * m;
-            if (e < kIterQ * N) Dq[e] = qg[m] >= 0 ? cinv(cv[m]) : dmk(0.0, 0.0);
+            nrm[m] = qg[m] >= 0 ? cv[m].x * cv[m].x + cv[m].y * cv[m].y : 1.0;
+            pre[m] = prod;
+            prod *= nrm[m];
+        }
+        if (prod > 1e-300 && prod < 1e300) {
+            double r = 1.0 / prod;
+#pragma unroll
+            for (int m = ND - 1; m >= 0; --m) {
+                const double inv = r * pre[m];
+                r *= nrm[m];
+                const int e = tid + NT * m;
+                if (e < kIterQ * N) Dq[e] = qg[m] >= 0 ? dmk(cv[m].x * inv, -cv[m].y * inv) : dmk(0.0, 0.0);
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < ND; ++m) {
+                const int e = tid + NT * m;
+                if (e < kIterQ * N) Dq[e] = qg[m] >= 0 ? cinv(cv[m]) : dmk(0.0, 0.0);
+            }
         }
     }
     __syncthreads();
@@ -1702,8 +1730,12 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 ce[c] = make_float2((float)v.x, (float)v.y);
             }
         }
+        static_assert(S::TPR == TPR && S::RW == TPR * CPT, "pivot buffer geometry");
         for (int k = 0; k < N; k += 2) {
-            float2* pb = pc + ((k >> 1) & 1) * 4 * N;   // [N] column k, [N] column k+1, [N] row k, [N] row k+1
+            // [N] column k, [N] column k+1, then [RW] (row k, row k+1) pairs; columns >= N of the
+            // rows are the owners' zero padding, so the updates below need no column bound
+            float2* pb = reinterpret_cast<float2*>(reinterpret_cast<char*>(pc) + ((k >> 1) & 1) * S::pc_half);
+            float2* pr = pb + 2 * N;                    // float2 view of the pairs: [2 j + r]
             if (own) {
 #pragma unroll
                 for (int c = 0; c < CPT; ++c) {
@@ -1712,18 +1744,17 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                     if (jj == k + 1) pb[N + gi] = ce[c];
                 }
                 if (gi == k || gi == k + 1) {
-                    float2* prow = pb + 2 * N + (gi - k) * N;
+                    const int r = gi - k;
 #pragma unroll
                     for (int c = 0; c < CPT; ++c) {
                         const int jj = j0 + c;
-                        if (jj < N) prow[jj] = jj == gi ? make_float2(ce[c].x + 1.f, ce[c].y) : ce[c];
+                        pr[2 * jj + r] = jj == gi ? make_float2(ce[c].x + 1.f, ce[c].y) : ce[c];
                     }
                 }
             }
             __syncthreads();
             if (own) {
-                const float2* prow0 = pb + 2 * N;
-                const float2* prow1 = pb + 3 * N;
+                const float4* pq = reinterpret_cast<const float4*>(pr);
                 const float2 p00 = pb[k], p10 = pb[k + 1], p01 = pb[N + k], p11 = pb[N + k + 1];
                 const float2 pd = fmul(p00, p11), po = fmul(p01, p10);
                 const float2 rdet = vinv(make_float2(pd.x - po.x, pd.y - po.y));
@@ -1737,11 +1768,10 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
                     for (int c = 0; c < CPT; ++c) {
                         const int jj = j0 + c;
-                        if (jj < N) {
-                            float2 v = fadd(fmul(m0, prow0[jj]), fmul(m1, prow1[jj]));
-                            if (jj == gi) v.x -= 1.f;
-                            ce[c] = v;
-                        }
+                        const float4 u = pq[jj];
+                        float2 v = fadd(fmul(m0, make_float2(u.x, u.y)), fmul(m1, make_float2(u.z, u.w)));
+                        if (jj == gi) v.x -= 1.f;
+                        ce[c] = v;
                     }
                 } else {                                // m = a_i,k:k+1 P^-1; a_ij -= m . u'_j
                     const float2 a0 = pb[gi], a1 = pb[N + gi];
@@ -1749,20 +1779,17 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                     m1 = fadd(fmul(a0, i01), fmul(a1, i11));
 #pragma unroll
                     for (int c = 0; c < CPT; ++c) {
-                        const int jj = j0 + c;
-                        if (jj < N) {
-                            const float2 u0 = prow0[jj], u1 = prow1[jj];
-                            float2 v = ce[c];
-                            v.x = fmaf(-m0.x, u0.x, v.x);
-                            v.x = fmaf(m0.y, u0.y, v.x);
-                            v.y = fmaf(-m0.x, u0.y, v.y);
-                            v.y = fmaf(-m0.y, u0.x, v.y);
-                            v.x = fmaf(-m1.x, u1.x, v.x);
-                            v.x = fmaf(m1.y, u1.y, v.x);
-                            v.y = fmaf(-m1.x, u1.y, v.y);
-                            v.y = fmaf(-m1.y, u1.x, v.y);
-                            ce[c] = v;
-                        }
+                        const float4 u = pq[j0 + c];
+                        float2 v = ce[c];
+                        v.x = fmaf(-m0.x, u.x, v.x);
+                        v.x = fmaf(m0.y, u.y, v.x);
+                        v.y = fmaf(-m0.x, u.y, v.y);
+                        v.y = fmaf(-m0.y, u.x, v.y);
+                        v.x = fmaf(-m1.x, u.z, v.x);
+                        v.x = fmaf(m1.y, u.w, v.x);
+                        v.y = fmaf(-m1.x, u.w, v.y);
+                        v.y = fmaf(-m1.y, u.z, v.y);
+                        ce[c] = v;
                     }
                 }
             }
