@@ -1527,42 +1527,84 @@ __device__ __forceinline__ void dm_apply(const double2 (&x)[QPL][RPL], double2 (
 
 // perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order.  One CTA per w,
 // bitonic sort of the next power of two >= nq (<= 4096) in shared memory; non-finite keys sort as 0.
+// Bitonic sort of P = max(2^ceil(log2 nq), 32) keys (padding +inf) under the total order (key,
+// index).  Thread t holds positions t + 1024 r (r < P / 1024) in registers.  A compare-exchange
+// whose partner is fewer than 32 positions away stays inside the warp and runs on shuffles; only
+// the stages with partner distance >= 32 go through shared memory, each behind one barrier
+// (15 of 55 stages at P = 1024).  The sorted order is unique, so any schedule gives the same perm.
+constexpr int kQoMaxR = 4;   // P <= 4096
 __global__ void __launch_bounds__(1024) k_bse_qorder(int nq, int nnu, const double2* __restrict__ chi0,
                                                      int32_t* __restrict__ perm) {
     extern __shared__ __align__(16) unsigned char qo_raw[];
-    int P = 1;
+    int P = 32;
     while (P < nq) P <<= 1;
-    double* key = reinterpret_cast<double*>(qo_raw);
-    int* idx = reinterpret_cast<int*>(key + P);
-    const int w = blockIdx.x, vc = nnu / 2;
-    for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        if (i < nq) {
+    const int R = (P + 1023) / 1024;
+    double* skey = reinterpret_cast<double*>(qo_raw);
+    int* sidx = reinterpret_cast<int*>(skey + P);
+    const int w = blockIdx.x, vc = nnu / 2, tid = threadIdx.x;
+    double key[kQoMaxR];
+    int idx[kQoMaxR];
+#pragma unroll
+    for (int r = 0; r < kQoMaxR; ++r) {
+        const int i = tid + 1024 * r;
+        key[r] = INFINITY;
+        idx[r] = i;
+        if (r < R && i < nq) {
             const double2 z = chi0[(size_t)i + (size_t)nq * (vc + (size_t)nnu * w)];
             double k = z.x / (z.x * z.x + z.y * z.y);
             if (!isfinite(k)) k = 0.0;
-            key[i] = k;
-        } else {
-            key[i] = INFINITY;
+            key[r] = k;
         }
-        idx[i] = i;
     }
-    __syncthreads();
-    for (int k = 2; k <= P; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < P; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const bool up = (i & k) == 0;
-                    const bool gt = key[i] > key[l] || (key[i] == key[l] && idx[i] > idx[l]);
-                    if (gt == up) {
-                        const double tk = key[i]; key[i] = key[l]; key[l] = tk;
-                        const int ti = idx[i]; idx[i] = idx[l]; idx[l] = ti;
-                    }
-                }
+    for (int k = 2; k <= P; k <<= 1) {
+        int j = k >> 1;
+        if (j >= 32) {
+            __syncthreads();   // the previous read-back is complete before the buffer is rewritten
+#pragma unroll
+            for (int r = 0; r < kQoMaxR; ++r) {
+                const int i = tid + 1024 * r;
+                if (r < R && i < P) { skey[i] = key[r]; sidx[i] = idx[r]; }
             }
             __syncthreads();
+            for (; j >= 32; j >>= 1) {
+                for (int i = tid; i < P; i += blockDim.x) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const bool up = (i & k) == 0;
+                        const bool gt = skey[i] > skey[l] || (skey[i] == skey[l] && sidx[i] > sidx[l]);
+                        if (gt == up) {
+                            const double tk = skey[i]; skey[i] = skey[l]; skey[l] = tk;
+                            const int ti = sidx[i]; sidx[i] = sidx[l]; sidx[l] = ti;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int r = 0; r < kQoMaxR; ++r) {
+                const int i = tid + 1024 * r;
+                if (r < R && i < P) { key[r] = skey[i]; idx[r] = sidx[i]; }
+            }
         }
-    for (int i = threadIdx.x; i < nq; i += blockDim.x) perm[(size_t)w * nq + i] = idx[i];
+        for (; j > 0; j >>= 1) {
+#pragma unroll
+            for (int r = 0; r < kQoMaxR; ++r) {
+                if (r < R) {   // uniform over the block: every lane of a warp shuffles together
+                    const int i = tid + 1024 * r;
+                    const double pk = __shfl_xor_sync(0xffffffffu, key[r], j);
+                    const int pi = __shfl_xor_sync(0xffffffffu, idx[r], j);
+                    const bool want_min = ((i & k) == 0) == ((i & j) == 0);
+                    const bool less = key[r] < pk || (key[r] == pk && idx[r] < pi);
+                    if (want_min != less) { key[r] = pk; idx[r] = pi; }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kQoMaxR; ++r) {
+        const int i = tid + 1024 * r;
+        if (r < R && i < nq) perm[(size_t)w * nq + i] = idx[r];
+    }
 }
 
 // identity order (boxes with more than 4096 q)
@@ -2492,7 +2534,7 @@ int run_iter(ldga_ctx* ctx, const BseArgs& a) {
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
     if (ctx->qperm_gen != ctx->chi0_gen) {
         if (a.nq <= 4096) {
-            int P = 1;
+            int P = 32;
             while (P < a.nq) P <<= 1;
             const size_t smq = (size_t)P * (sizeof(double) + sizeof(int));
             LDGA_CUDA(ctx, set_smem(ctx, k_bse_qorder, smq));
