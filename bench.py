@@ -335,21 +335,24 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
         if cfg.startswith("iter"):
             # MIXED preconditioned solve: the FP64 residual passes set the bound.  Executed work from
             # the kernel's own counters (ldga_bse_sweeps): every warp evaluates the residual of its q
-            # in lockstep, 8 N^2 + 8 N FP64 flops per q and pass; the FP32 corrections 8 N^2 each.
+            # in lockstep, 8 N^2 + 8 N FP64 flops per q and pass (6 N^2 + 8 N on the FP64 tensor
+            # path, whose complex product takes three real products); the FP32 corrections 8 N^2 each.
             peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
-            qpw = {"iter": 8, "iter8": 4, "iter8x2": 8}.get(cfg.split(":")[0], 8)
+            qpw = {"iter": 8, "iter8": 4, "iter8x2": 8, "iter8x2tc": 8, "iter8x2dm": 8}.get(cfg.split(":")[0], 8)
             passes, warps = sweeps if sweeps else (0, 1)
-            f64 = passes * qpw * (8.0 * nnu**2 + 8.0 * nnu) / max(cnt, 1)
+            prod = 6.0 if "dm" in cfg else 8.0
+            f64 = passes * qpw * (prod * nnu**2 + 8.0 * nnu) / max(cnt, 1)
             f32 = (passes - warps) * qpw * 8.0 * nnu**2 / max(cnt, 1)
             exe = f64 / t / 1e12
-            kname = ("k_bse_iter (FP32 group inverse; FP64 residual on the FP64 tensor path, mma.sync m8n8k4; "
-                     "FP32 product on tensor cores, mma.sync TF32)" if "dm" in cfg else
+            kname = ("k_bse_iter (FP32 group inverse; FP64 residual on the FP64 tensor path, mma.sync m8n8k4, "
+                     "three real products per complex tile; FP32 product on tensor cores, mma.sync TF32)"
+                     if "dm" in cfg else
                      "k_bse_iter (FP32 group inverse, FP64 residual passes, FP32 product on tensor cores: "
                      "mma.sync TF32)" if "tc" in cfg else "k_bse_iter (FP32 group inverse, FP64 residual passes)")
             return {"kernel": kname, "bound": "fp64",
                     "achieved": exe, "peak": peak, "unit": "TFLOP/s", "frac": exe / peak,
-                    "work": "executed FP64 flops of the residual passes (8 N^2 + 8 N per q and pass, warps in "
-                            "lockstep), counted by the kernel",
+                    "work": (f"executed FP64 flops of the residual passes ({prod:.0f} N^2 + 8 N per q and pass, "
+                             "warps in lockstep), counted by the kernel"),
                     "passes_per_warp": passes / max(warps, 1),
                     "fp32_tflops": f32 / t / 1e12,
                     "reference_formulation_tflops": ach,

@@ -1495,15 +1495,22 @@ __device__ __forceinline__ void dm_apply(const double2 (&x)[QPL][RPL], double2 (
     double dr[MT][2], di[MT][2];
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt) {
+        // three real tile products per complex tile (Karatsuba): t1 = Ar xr, t2 = Ai xi,
+        // t3 = (Ar + Ai)(xr + xi); Re = t1 - t2, Im = t3 - t1 - t2.  The operand sums are one FP64
+        // add per fragment register on the otherwise idle FP64 pipe.
         dr[mt][0] = dr[mt][1] = di[mt][0] = di[mt][1] = 0.0;
+        double t2[2] = {0.0, 0.0};
 #pragma unroll
         for (int kt = 0; kt < KT; ++kt) {
             const double ar = gr[(mt * KT + kt) * 32 + lane], ai = gi[(mt * KT + kt) * 32 + lane];
             mma_f64(dr[mt], ar, bre[kt]);
-            mma_f64(dr[mt], -ai, bim[kt]);
-            mma_f64(di[mt], ai, bre[kt]);
-            mma_f64(di[mt], ar, bim[kt]);
+            mma_f64(t2, ai, bim[kt]);
+            mma_f64(di[mt], ar + ai, bre[kt] + bim[kt]);
         }
+        di[mt][0] -= dr[mt][0] + t2[0];
+        di[mt][1] -= dr[mt][1] + t2[1];
+        dr[mt][0] -= t2[0];
+        dr[mt][1] -= t2[1];
     }
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
@@ -1525,8 +1532,8 @@ __device__ __forceinline__ void dm_apply(const double2 (&x)[QPL][RPL], double2 (
     }
 }
 
-// perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order.  One CTA per w,
-// bitonic sort of the next power of two >= nq (<= 4096) in shared memory; non-finite keys sort as 0.
+// perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order, one CTA per w
+// (nq <= 4096); non-finite keys sort as 0.
 // Bitonic sort of P = max(2^ceil(log2 nq), 32) keys (padding +inf) under the total order (key,
 // index).  Thread t holds positions t + 1024 r (r < P / 1024) in registers.  A compare-exchange
 // whose partner is fewer than 32 positions away stays inside the warp and runs on shuffles; only
@@ -2583,7 +2590,7 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2"}, {&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3"},
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3"}, {&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2"},
                                {&run_iter<40, 8, 3, 2, true, true>, "iter8x2tc:3"}, {&run_iter<40, 8, 2, 2, true, true>, "iter8x2tc:2"},
                                {&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
                                {&run_iter<40, 8, 2>, "iter8:2"}, {&run_iter<40, 4, 3>, "iter"},
