@@ -18,6 +18,10 @@ int pairs_per_cta(int total) {
     const size_t per = (size_t)(S::BUF_A + S::BUF_B) * sizeof(double2);
     int np = (int)(kSmemBudget / per);
     if (np > 16) np = 16;
+    // batch vectors into a CTA only when there are more vectors than SMs: a short list (the EoM
+    // inverse's numax vectors) runs one vector per CTA on as many SMs
+    const int spread = (total + 147) / 148;
+    if (np > spread) np = spread;
     if (np < 1) np = 1;
     if (np > total) np = total;
     return np;
@@ -43,11 +47,10 @@ template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_gloc_transform(
     const TMat<M> T, int nf, int fft_lo, double beta, double mu, const double* __restrict__ eps,
     const double2* __restrict__ sigma_loc, int n_sigma, double2* __restrict__ gloc, int from_sigma,
-    double2* __restrict__ ghat) {
+    double2* __restrict__ ghat, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)(gridDim.y);   // pairs per CTA passed through gridDim.y
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, nf - p0);
     double2* bufA = smem;
@@ -83,11 +86,10 @@ __global__ void __launch_bounds__(kThreads) k_gloc_transform(
 template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_bubble(
     const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double scale,
-    const double2* __restrict__ ghat, const int2* __restrict__ pairs, int total, double2* __restrict__ chi0) {
+    const double2* __restrict__ ghat, const int2* __restrict__ pairs, int total, double2* __restrict__ chi0, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, total - p0);
     double2* bufA = smem;
@@ -223,11 +225,10 @@ template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_eom_inverse(
     const TMat<M> T, int numax, int nchunk, double scale, double beta, double U, double hartree,
     const double* __restrict__ tail_sum, int tc, double chiloc_m_sum, const double2* __restrict__ partial,
-    double2* __restrict__ out, int out_ld, int add_hartree) {
+    double2* __restrict__ out, int out_ld, int add_hartree, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, numax - p0);
     double2* bufA = smem;
@@ -267,11 +268,10 @@ __global__ void __launch_bounds__(kThreads) k_eom_inverse(
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_vjp_sbar(const TMat<M> T, int numax, const double* __restrict__ kmult,
-                                                       const double2* __restrict__ sbar, double2* __restrict__ shat) {
+                                                       const double2* __restrict__ sbar, double2* __restrict__ shat, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, numax - p0);
     double2* bufA = smem;
@@ -296,11 +296,10 @@ __global__ void __launch_bounds__(kThreads) k_eom_vjp(
     const TMat<M> T, const EomVjpArgs a, const double* __restrict__ kmult, const double2* __restrict__ ghat,
     const double2* __restrict__ shat, const double* __restrict__ chi_m, const double2* __restrict__ gam_m,
     const double* __restrict__ chi_d, const double2* __restrict__ gam_d, double2* __restrict__ gm_bar,
-    double2* __restrict__ gd_bar, double2* __restrict__ l0_bar, double* __restrict__ cm, double* __restrict__ cd) {
+    double2* __restrict__ gd_bar, double2* __restrict__ l0_bar, double* __restrict__ cm, double* __restrict__ cd, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int total = a.numax * a.nw;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, total - p0);
@@ -403,11 +402,10 @@ template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_bubble_vjp(
     const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double sb,
     const double* __restrict__ kmult, const double2* __restrict__ ghat, const double2* __restrict__ chi0_bar,
-    double2* __restrict__ rows) {
+    double2* __restrict__ rows, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int total = nnu * nw;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, total - p0);
@@ -434,11 +432,10 @@ template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_eom_gvjp(
     const TMat<M> T, const EomArgs a, double c, const double* __restrict__ kmult, const double2* __restrict__ shat,
     const double* __restrict__ chi_m, const double2* __restrict__ gam_m, const double* __restrict__ chi_d,
-    const double2* __restrict__ gam_d, const double2* __restrict__ lambda0, double2* __restrict__ rows) {
+    const double2* __restrict__ gam_d, const double2* __restrict__ lambda0, double2* __restrict__ rows, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int total = a.numax * a.nw;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, total - p0);
@@ -479,11 +476,10 @@ __global__ void __launch_bounds__(kThreads) k_eom_gvjp(
 template <int DIM, int M>
 __global__ void __launch_bounds__(kThreads) k_vjp_transform(const TMat<M> T, int nf, int mul_kmult,
                                                             const double* __restrict__ kmult,
-                                                            const double2* __restrict__ in, double2* __restrict__ out) {
+                                                            const double2* __restrict__ in, double2* __restrict__ out, int np_max) {
     using S = TransformSmem<DIM, M>;
     constexpr int NQ = S::NQ;
     extern __shared__ double2 smem[];
-    const int np_max = (int)gridDim.y;
     const int p0 = blockIdx.x * np_max;
     const int np = min(np_max, nf - p0);
     double2* bufA = smem;
@@ -552,11 +548,11 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_gloc_transform<DIM, M>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-    dim3 grid((ctx->Nf + np - 1) / np, np);
+    dim3 grid((ctx->Nf + np - 1) / np);
     StageTimer st_(ctx, LDGA_STAGE_GLOC);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, ctx->fft_lo, ctx->mp.beta, ctx->mp.mu,
                                                ctx->d_eps, ctx->d_sigma_loc, ctx->n_sigma_loc, ctx->d_gloc,
-                                               from_sigma ? 1 : 0, ctx->d_ghat);
+                                               from_sigma ? 1 : 0, ctx->d_ghat, np);
     LDGA_LAUNCHED(ctx, "k_gloc_transform");
     return LDGA_OK;
 }
@@ -568,12 +564,12 @@ int run_bubble(ldga_ctx* ctx) {
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_bubble<DIM, M>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-    dim3 grid((total + np - 1) / np, np);
+    dim3 grid((total + np - 1) / np);
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
     StageTimer st_(ctx, LDGA_STAGE_BUBBLE);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
                                                ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_bub_pairs, total,
-                                               ctx->d_chi0);
+                                               ctx->d_chi0, np);
     LDGA_LAUNCHED(ctx, "k_bubble");
     return LDGA_OK;
 }
@@ -621,13 +617,13 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
     const size_t sm = smem_bytes<DIM, M>(np);
     auto kern = k_eom_inverse<DIM, M>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-    dim3 grid((numax + np - 1) / np, np);
+    dim3 grid((numax + np - 1) / np);
     const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);
     const double hartree = ctx->mp.n * ctx->mp.U / 2.0;
     StageTimer st_(ctx, LDGA_STAGE_EOM_INVERSE);
     kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
                                                hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,
-                                               add_hartree);
+                                               add_hartree, np);
     LDGA_LAUNCHED(ctx, "k_eom_inverse");
     return LDGA_OK;
 }
@@ -642,11 +638,11 @@ int run_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, in
         const size_t sm = smem_bytes<DIM, M>(np);
         auto kern = k_bubble_vjp<DIM, M>;
         LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-        dim3 grid((nbub + np - 1) / np, np);
+        dim3 grid((nbub + np - 1) / np);
         const double sb = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
         kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
                                                    ctx->sp.shift, ctx->fft_lo, sb, ctx->d_kmult, ctx->d_ghat, chi0_bar,
-                                                   rows);
+                                                   rows, np);
         LDGA_LAUNCHED(ctx, "k_bubble_vjp");
     }
     if (sbar) {
@@ -655,8 +651,8 @@ int run_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, in
             const size_t sm = smem_bytes<DIM, M>(np);
             auto kern = k_vjp_transform<DIM, M>;
             LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-            dim3 grid((numax + np - 1) / np, np);
-            kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, 0, ctx->d_kmult, sbar, shat);
+            dim3 grid((numax + np - 1) / np);
+            kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, 0, ctx->d_kmult, sbar, shat, np);
             LDGA_LAUNCHED(ctx, "k_vjp_transform");
         }
         const int total = numax * ctx->Nw;
@@ -669,11 +665,11 @@ int run_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, in
         a.fft_lo = ctx->fft_lo; a.numax = numax; a.w_per_chunk = 1;
         a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = -1;
         a.lam_m_dev = nullptr; a.lam_d_dev = nullptr;
-        dim3 grid((total + np - 1) / np, np);
+        dim3 grid((total + np - 1) / np);
         const double c = 1.0 / (ctx->mp.beta * (double)ctx->Nk * (double)ctx->Nk);
         kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, c, ctx->d_kmult, shat, ctx->d_chi[0], ctx->d_gam[0],
                                                    ctx->d_chi[1], ctx->d_gam[1], ctx->d_lambda0,
-                                                   rows + (size_t)2 * nbub * ctx->Nq);
+                                                   rows + (size_t)2 * nbub * ctx->Nq, np);
         LDGA_LAUNCHED(ctx, "k_eom_gvjp");
     }
     k_ghat_gather<<<2 * 148, 256, 0, ctx->stream>>>(ctx->Nf, ctx->Nq, start, idx, rows, gbar_hat);
@@ -683,8 +679,8 @@ int run_gloc_vjp(ldga_ctx* ctx, const double2* chi0_bar, const double2* sbar, in
         const size_t sm = smem_bytes<DIM, M>(np);
         auto kern = k_vjp_transform<DIM, M>;
         LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-        dim3 grid((ctx->Nf + np - 1) / np, np);
-        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, 1, ctx->d_kmult, gbar_hat, gbar);
+        dim3 grid((ctx->Nf + np - 1) / np);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, 1, ctx->d_kmult, gbar_hat, gbar, np);
         LDGA_LAUNCHED(ctx, "k_vjp_transform");
     }
     return LDGA_OK;
@@ -699,8 +695,8 @@ int run_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, co
         const size_t sm = smem_bytes<DIM, M>(np);
         auto kern = k_vjp_sbar<DIM, M>;
         LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
-        dim3 grid((numax + np - 1) / np, np);
-        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, ctx->d_kmult, sbar, shat);
+        dim3 grid((numax + np - 1) / np);
+        kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, ctx->d_kmult, sbar, shat, np);
         LDGA_LAUNCHED(ctx, "k_vjp_sbar");
     }
     {
@@ -713,10 +709,10 @@ int run_eom_vjp(ldga_ctx* ctx, int numax, double lam_m, double lam_d, int tc, co
         a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
         a.fft_lo = ctx->fft_lo; a.numax = numax; a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d;
         a.scale = 1.0 / (ctx->mp.beta * (double)ctx->Nk * (double)ctx->Nk);
-        dim3 grid((total + np - 1) / np, np);
+        dim3 grid((total + np - 1) / np);
         kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_kmult, ctx->d_ghat, shat, ctx->d_chi[0],
                                                    ctx->d_gam[0], ctx->d_chi[1], ctx->d_gam[1], gm_bar, gd_bar, l0_bar,
-                                                   cm, cd);
+                                                   cm, cd, np);
         LDGA_LAUNCHED(ctx, "k_eom_vjp");
     }
     if (tc) {
