@@ -43,9 +43,9 @@ CFG_NAMES = {
 METRIC = "(q,w)-points/s"
 PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
 REF_BUDGET_S = 120.0
-# DRAM bytes per BSE matrix (Nnu = 40, FP64) from one ncu capture (profiles/k_bse_lu_n40_fp64_3d16.md)
+# DRAM bytes per BSE matrix (Nnu = 40) from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch): the FP64 LU on 3D 16^3 (6765 matrices) and the MIXED preconditioned solve on 3D 32^3 (39 729)
 BSE_DRAM_BYTES_PER_MATRIX = 5423872 / 6765
-# the same for the MIXED preconditioned solve (profiles/k_bse_iter_n40_mixed_3d32.md: 3D 32^3, 39 729 matrices)
 BSE_ITER_DRAM_BYTES_PER_MATRIX = (26807808 + 100608) / 39729
 BSE_TILE = 8   # rows per diagonal block of the LU kernels at Nnu = 40
 
@@ -71,7 +71,10 @@ def parse():
                     help="load BSE configuration choices (ldga_tune_save format) instead of autotuning")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip timing the same chain in FP64 mode (mixed runs report mixed / FP64)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle chain (the CPU baseline and the accuracy check against it)")
+    ap.add_argument("--no-stage-events", action="store_true",
+                    help="time the chain without the per-stage CUDA events inside its graph (no stage times)")
     ap.add_argument("--ns", type=int, default=None, help="smaller k-grid (points per axis) for profiling captures")
     ap.add_argument("--out", default=None, help="also write the JSON line to this file")
     ap.add_argument("--workload", default="chain", choices=["chain", "batch", "adjoint"],
@@ -165,19 +168,111 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------------
 # CPU baseline: the oracle restatement of the reference algorithm on the host cores
 # ----------------------------------------------------------------------------------------------
-def cpu_chain_seconds(inp) -> float:
+def oracle_chain(inp):
+    """The oracle's whole lambda_m chain on the workload: (outputs, seconds)."""
     from oracle import ldga_ref as R
     R.set_workers(os.cpu_count() or 1)
     t0 = time.perf_counter()
-    R.run_chain(inp, lambda_type="m")
-    return time.perf_counter() - t0
+    ref = R.run_chain(inp, lambda_type="m")
+    return ref, time.perf_counter() - t0
 
 
-def cpu_baseline(inp, points: int) -> dict:
-    t = cpu_chain_seconds(inp)
+def cpu_chain_seconds(inp) -> float:
+    return oracle_chain(inp)[1]
+
+
+def cpu_baseline(t: float, points: int) -> dict:
     return {"value": points / t, "unit": METRIC, "cores": os.cpu_count() or 1, "kind": "port",
             "sample": f"one full chain of the workload ({t:.1f} s): NumPy/SciPy FP64 restatement of the "
                       "reference algorithm (oracle/ldga_ref.py), scipy.fft workers and OpenBLAS threads = all cores"}
+
+
+# ----------------------------------------------------------------------------------------------
+# accuracy of the timed step against the FP64 oracle
+# ----------------------------------------------------------------------------------------------
+# Elementwise relative errors divide by max(|ref|, ERR_FLOOR * max|ref|): an entry that cancels to
+# ~1e-6 of the array's largest one carries FP64 rounding of the large terms (~1e-16 of them), so
+# 1e-10 elementwise is the bar FP64 arithmetic itself can meet down to that floor.
+ERR_FLOOR = 1e-6
+
+
+def rel_err(a, b) -> dict:
+    a, b = np.asarray(a), np.asarray(b)
+    d = np.abs(a - b)
+    m = float(np.max(np.abs(b))) if b.size else 0.0
+    m = m if m > 0 else 1e-300
+    e = d / np.maximum(np.abs(b), ERR_FLOOR * m)
+    i = int(np.argmax(e))
+    return {"elementwise": float(e.flat[i]), "normwise": float(d.max() / m),
+            "worst": [int(x) for x in np.unravel_index(i, b.shape)]}
+
+
+def accuracy(chain, ref, lam_dev: float) -> dict:
+    """Errors of the handle's last chain step against the oracle chain on the same input.
+
+    chi0, chi_m, chi_d, gamma_m, gamma_d and lambda0 are compared directly.  lambda_m of this
+    workload is not a parity quantity (the reference's newton_right runs into the poles of f, see
+    `lambda_m`), so Sigma_ladder, G_ladder, mu and the energies are recomputed on the device at the
+    ORACLE's lambda_m (EoM, mu fit, calc_E) and compared with the oracle's values there."""
+    from oracle import ldga_ref as R
+    from ladderdga_b200 import _lib
+    ctx, h = chain.ctx, chain.h
+    nq, nnu, nw, numax = ctx.Nq, ctx.Nnu, ctx.Nw, chain.numax
+
+    def get(what, ch=0, real=False):
+        out = np.empty((nq, nw), order="F") if real else _lib.cplx_out((nq, nnu, nw))
+        ctx.call("ldga_get", what, ch, _lib.ptr(out))
+        return out
+
+    res = ref["result"]
+    errs = {"floor": f"elementwise denominators max(|oracle|, {ERR_FLOOR:g} max|oracle|)",
+            "chi0": rel_err(get(_lib.GET_CHI0), ref["chi0"]),
+            "chi_m": rel_err(get(_lib.GET_CHI, _lib.CH_M, True), ref["chi_m"].data),
+            "chi_d": rel_err(get(_lib.GET_CHI, _lib.CH_D, True), ref["chi_d"].data),
+            "gamma_m": rel_err(get(_lib.GET_GAMMA, _lib.CH_M), ref["gamma_m"]),
+            "gamma_d": rel_err(get(_lib.GET_GAMMA, _lib.CH_D), ref["gamma_d"]),
+            "lambda0": rel_err(get(_lib.GET_LAMBDA0), ref["lambda0"])}
+    # the lambda-dependent outputs at the oracle's lambda_m
+    lam = float(res.lam_m)
+    S = _lib.cplx_out((nq, numax))
+    ctx.call("ldga_eom", lam, 0.0, numax, 1, h.χloc_m_sum, _lib.ptr(S))
+    G = _lib.cplx_out((nq, ctx.Nf))
+    mu, ek, ep, n = (C.c_double() for _ in range(4))
+    ctx.call("ldga_g_ladder", None, 0, 1, h.mP.μ, C.byref(mu), _lib.ptr(G), C.byref(ek), C.byref(ep), C.byref(n))
+    errs["at_oracle_lambda_m"] = {
+        "lambda_m": lam,
+        "Sigma_ladder": rel_err(S, res.Sigma_ladder),
+        "G_ladder": rel_err(G, res.G_ladder),
+        "mu_abs": abs(mu.value - res.mu),
+        "E_kin_rel": abs(ek.value - res.EKin) / max(1.0, abs(res.EKin)),
+        "E_pot1_rel": abs(ep.value - res.EPot_p1) / max(1.0, abs(res.EPot_p1))}
+    # lambda_m itself: both values, and how well each solves the oracle's f(l) = sum_kw chi_l - rhs
+    rh, cm = ref["h"], ref["chi_m"]
+    rhs = 2 * rh.imp_density - R.sum_kw(rh.kG, ref["chi_d"])
+
+    def f(l):
+        return R.sum_kw(rh.kG, cm, transform=lambda x: R.chi_lambda(x, l)) - rhs
+
+    def scale(l):
+        return max(1.0, R.sum_kw(rh.kG, cm, transform=lambda x: np.abs(R.chi_lambda(x, l))))
+
+    neg = cm.data[cm.data < 0]
+    errs["lambda_m"] = {
+        "device": lam_dev, "oracle": lam, "abs_diff": abs(lam_dev - lam),
+        "device_root_residual": abs(f(lam_dev)) / scale(lam_dev), "oracle_root_residual": abs(f(lam)) / scale(lam),
+        "f_at_0": f(0.0), "df_c1_at_0": R.sum_kw(rh.kG, cm, transform=lambda x: R.dchi_lambda(x, 0.0)),
+        "first_pole": float(1.0 / np.max(-neg)) if neg.size else None,
+        "note": "newton_right's df carries the chi tail constants (df_c1 > 0 at 0 while f(0) < 0), so the "
+                "iteration walks right into the poles of f at lambda >= first_pole, where each iterate depends "
+                "on the rounding of the sums: every root it can land on solves f = 0, but which one is not a "
+                "parity quantity"}
+    worst = max(v["elementwise"] for k, v in errs.items() if isinstance(v, dict) and "elementwise" in v)
+    fixed = errs["at_oracle_lambda_m"]
+    worst_fixed = max(fixed["Sigma_ladder"]["elementwise"], fixed["G_ladder"]["elementwise"], fixed["mu_abs"],
+                      fixed["E_kin_rel"], fixed["E_pot1_rel"])
+    errs["max_elementwise"] = max(worst, worst_fixed)
+    errs["within_1e-10"] = bool(errs["max_elementwise"] <= 1e-10)
+    return errs
 
 
 def run_reference(args):
@@ -315,6 +410,36 @@ def stage_times(chain):
     return {STAGES[i]: (ms[i], cnt[i]) for i in range(10)}
 
 
+def measure_fp64_peak(device: int, n: int = 8192, reps: int = 5) -> float:
+    """FP64 throughput of a cuBLAS DGEMM (n^3, the FP64 tensor path) on this GPU in TFLOP/s: the
+    measured denominator of the FP64-bound kernels' roofline (the driver's peaks have no FP64 entry)."""
+    import torch
+    dev = torch.device("cuda", device)
+    g = torch.Generator(device=dev).manual_seed(0)
+    a = torch.rand(n, n, dtype=torch.float64, device=dev, generator=g)
+    b = torch.rand(n, n, dtype=torch.float64, device=dev, generator=g)
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(a, b, out=c)
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 * reps / t / 1e12
+
+
+def fp64_peak(peaks: dict, sm_mhz: float):
+    if peaks.get("fp64_tflops"):
+        return peaks["fp64_tflops"], peaks.get("fp64_source", "measured FP64 throughput")
+    return (148 * 64 * 2 * sm_mhz * 1e6 / 1e12,
+            f"nominal 64 FP64 FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (no FP64 figure measured)")
+
+
 def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
     """Dominant stage of the step and its roofline (algorithmic work per launch / CUDA-event time)."""
     name = max(stages, key=lambda k: stages[k][0])
@@ -337,7 +462,7 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
             # the kernel's own counters (ldga_bse_sweeps): every warp evaluates the residual of its q
             # in lockstep, 8 N^2 + 8 N FP64 flops per q and pass (6 N^2 + 8 N on the FP64 tensor
             # path, whose complex product takes three real products); the FP32 corrections 8 N^2 each.
-            peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+            peak, peak_src = fp64_peak(peaks, sm_mhz)
             qpw = {"iter": 8, "iter8": 4, "iter8x2": 8, "iter8x2tc": 8, "iter8x2dm": 8}.get(cfg.split(":")[0], 8)
             passes, warps = sweeps if sweeps else (0, 1)
             prod = 6.0 if "dm" in cfg else 8.0
@@ -359,12 +484,15 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
                     "traffic": BSE_ITER_DRAM_BYTES_PER_MATRIX * nq * nw if nnu == 40 else None,
                     "traffic_source": ("ncu dram__bytes_read+write of one launch on 3D 32^3 (39 729 matrices)"
                                        if nnu == 40 else "no capture at this Nnu"),
-                    "peak_source": f"nominal 64 FP64 FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (no FP64 figure "
-                                   "is measured)"}
+                    "peak_source": peak_src}
         # bound: FP32 (mixed) / FP64 CUDA-core pipes, nominal B200 rates at the measured max clock
         fp = "fp32" if chain.ctx.precision == 2 else "fp64"
         lanes = 128 if fp == "fp32" else 64
         peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
+        peak_src = (f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (the CUDA-core pipe, "
+                    "not HBM or tensor cores, bounds this kernel)")
+        if fp == "fp64":
+            peak, peak_src = fp64_peak(peaks, sm_mhz)
         kname = "k_bse_lu32 (FP32 LU + FP64 refinement)" if fp == "fp32" else "k_bse_lu (FP64 LU)"
         return {"kernel": kname, "bound": fp, "achieved": ach, "peak": peak,
                 "unit": "TFLOP/s", "frac": ach / peak,
@@ -376,9 +504,7 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
                 "traffic_source": ("ncu dram__bytes_read+write of one FP64 launch on 3D 16^3 (6765 matrices, "
                                    "802 B each), scaled by the matrix count" if nnu == 40 else
                                    "no capture at this Nnu"),
-                "peak_source": f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz "
-                               "(no FP64 figure is measured; the CUDA-core pipe, not HBM or tensor cores, "
-                               "bounds this kernel)"}
+                "peak_source": peak_src}
     # HBM-bound stages: algorithmic bytes per launch
     byts = {
         "bubble": (nq * (nnu + 1) * 16 * 2 + nq * nnu * nw * 16),
@@ -387,7 +513,8 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
     }.get(name, nq * nnu * nw * 16)
     ach = byts / t / 1e9
     return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": None, "peak_source": "measured hbm_gbs"}
+            "traffic": None,
+            "peak_source": peaks.get("source", "measured hbm_gbs (MEASURED_PEAKS.json)")}
 
 
 def run_ours(args):
@@ -406,7 +533,12 @@ def run_ours(args):
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
-        peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+        peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback (no MEASURED_PEAKS.json)"}
+    try:
+        peaks["fp64_tflops"] = measure_fp64_peak(local)
+        peaks["fp64_source"] = "cuBLAS DGEMM 8192^3 (FP64 tensor path) measured in this run"
+    except Exception as e:  # reported, not fatal: the roofline then states the nominal figure
+        peaks["fp64_error"] = str(e)
 
     def timed(src, outputs):
         times = []
@@ -421,7 +553,7 @@ def run_ours(args):
         return times
 
     # the stage events are recorded inside the graph, so profiling is on for capture and timing
-    chain.ctx.call("ldga_profile", 1)
+    chain.ctx.call("ldga_profile", 0 if args.no_stage_events else 1)
     for _ in range(max(args.warmup, 3)):
         scal = chain.step(chain.dev, False)
     torch.cuda.synchronize()
@@ -447,6 +579,12 @@ def run_ours(args):
     clk = clocks.stop()
     chain.ctx.call("ldga_profile", 0)
     newton = newton_period(chain)
+    # the oracle's chain on the same input: the CPU baseline's timing and the reference values of
+    # the accuracy check (rank 0 at N = 1 only)
+    oref, t_cpu, errors, errors64 = None, None, None, None
+    if world == 1 and not args.no_cpu_baseline:
+        oref, t_cpu = oracle_chain(inp)
+        errors = accuracy(chain, oref, scal[0])
     ms = float(np.mean(t_dev))
     ms_e2e = float(np.mean(t_e2e))
     if world > 1:
@@ -460,32 +598,38 @@ def run_ours(args):
     fp64_cmp = None
     if args.prec == "mixed" and world == 1 and not args.no_fp64_compare:
         # the same chain with the FP64 LU, same timing: the mixed / FP64 ratio of the headline metric
-        ref = Chain(inp, PREC_NAMES["fp64"], local)
-        ref_cfg = tune(ref)
-        ref.ctx.call("ldga_profile", 1)
+        c64 = Chain(inp, PREC_NAMES["fp64"], local)
+        cfg64 = tune(c64)
+        c64.ctx.call("ldga_profile", 0 if args.no_stage_events else 1)
         for _ in range(max(args.warmup, 3)):
-            ref.step(ref.dev, False)
+            scal64 = c64.step(c64.dev, False)
         torch.cuda.synchronize()
-        stage_times(ref)
+        stage_times(c64)
         tr = []
         for _ in range(args.steps):
             flush.fill_(1.0)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(ref.stream)
-            ref.step(ref.dev, False)
-            b.record(ref.stream)
+            a.record(c64.stream)
+            c64.step(c64.dev, False)
+            b.record(c64.stream)
             b.synchronize()
             tr.append(a.elapsed_time(b))
-        rst = stage_times(ref)
-        ref.ctx.call("ldga_profile", 0)
+        rst = stage_times(c64)
+        c64.ctx.call("ldga_profile", 0)
+        if oref is not None:
+            errors64 = accuracy(c64, oref, scal64[0])
         ms64 = float(np.mean(tr))
         bse64 = rst["bse"][0] / args.steps
-        bse_mx = stages["bse"][0] / args.steps
-        fp64_cmp = {"ms_per_step": ms64, "value": chain.points / (ms64 / 1e3), "bse_config": ref_cfg,
+        bse_mx = stages["bse"][0] / args.steps or float("nan")
+        fp64_cmp = {"ms_per_step": ms64, "value": chain.points / (ms64 / 1e3), "bse_config": cfg64,
                     "bse_ms_per_step": bse64, "mixed_over_fp64": ms64 / ms,
-                    "bse_mixed_over_fp64": bse64 / bse_mx}
+                    "bse_mixed_over_fp64": bse64 / bse_mx,
+                    "stages_ms_per_step": {k: v[0] / args.steps for k, v in rst.items() if v[1]}}
+        if errors64 is not None:
+            fp64_cmp["errors_max_elementwise"] = errors64["max_elementwise"]
     if rank == 0:
-        rl = roofline(stages, chain, peaks, (sp.value, sw.value))
+        rl = (roofline(stages, chain, peaks, (sp.value, sw.value)) if any(v[1] for v in stages.values())
+              else {"note": "no stage events (--no-stage-events)"})
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.prec != "mixed" else "f64+f32",
@@ -502,10 +646,12 @@ def run_ours(args):
                 "result": {"lambda_m": scal[0], "mu": scal[1], "E_kin": scal[2], "E_pot1": scal[3],
                            "newton_iterations": scal[6], "newton_rerun": newton},
                 "clocks": clk}
+        if errors is not None:
+            line["errors"] = errors
         if fp64_cmp is not None:
             line["fp64_compare"] = fp64_cmp
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(inp, chain.points)
+        if t_cpu is not None:
+            line["cpu_baseline"] = cpu_baseline(t_cpu, chain.points)
         print(json.dumps(line), flush=True)
         if args.out:
             open(args.out, "w").write(json.dumps(line) + "\n")

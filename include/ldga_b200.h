@@ -258,7 +258,9 @@ int ldga_set_lambda0(ldga_ctx* ctx, const double* lambda0);
  * Scratch: a built-in device array of 32768 (nu', w) columns (512 KiB, held by every GPU that loads
  * the library until exit); nnu*nw above that is rejected with LDGA_ERR_ARG.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress), so make that first call before
- * any stream capture.  Calls share the array: calls that overlap on one GPU race. */
+ * any stream capture.  The address is kept for the life of the process: after cudaDeviceReset on a
+ * device, do not call this entry point on that device again.  Pointers into another GPU's memory
+ * are rejected with LDGA_ERR_ARG.  Calls share the array: calls that overlap on one GPU race. */
 int ldga_lambda0_noalloc(const double* chi0, const double* F, int32_t nq, int32_t nnu, int32_t nw,
                          double beta, double* lambda0_out, void* stream);
 

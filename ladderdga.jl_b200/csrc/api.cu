@@ -595,10 +595,14 @@ int ldga_autotune_bse(ldga_ctx* ctx, int32_t channel, int32_t reps, int32_t* var
     // leave the channel's outputs as a regular ldga_bse would (fallback for flagged matrices included)
     LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
     TRY(launch_bse(ctx, channel, ctx->d_count + 1));
+    int32_t cnt[2] = {0, 0};
+    TRY(copy(ctx, cnt, ctx->d_count, 2 * sizeof(int32_t)));
     TRY(sync(ctx));
     ctx->have_chi[channel] = ctx->have_gam[channel] = true;
     if (variant) *variant = best;
     if (ms) *ms = best_ms;
+    if (cnt[1] > 0)
+        return ctx_fail(ctx, LDGA_ERR_NUMERIC, std::to_string(cnt[1]) + " BSE matrices are singular or non-finite");
     return LDGA_OK;
 }
 

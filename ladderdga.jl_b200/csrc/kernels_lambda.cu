@@ -792,10 +792,13 @@ double2* noalloc_colF(int device, cudaError_t* err) {
     return addr[device];
 }
 
-bool is_device_ptr(const void* p) {
+// Device (or managed) memory that belongs to `device`: a pointer into another GPU's memory would be
+// read as peer memory by the kernels, so it is refused like host memory.
+bool is_device_ptr(const void* p, int device) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 }  // namespace
 
@@ -808,11 +811,12 @@ extern "C" int ldga_lambda0_noalloc(const double* chi0, const double* F, int32_t
                         "ldga_lambda0_noalloc: Nnu*Nw = " + std::to_string((long)nnu * nw) +
                             " exceeds the built-in scratch of " + std::to_string(LDGA_NOALLOC_MAX_COLS) +
                             " (nu', w) columns");
-    if (!is_device_ptr(chi0) || !is_device_ptr(F) || !is_device_ptr(lambda0_out))
-        return ctx_fail(nullptr, LDGA_ERR_ARG, "ldga_lambda0_noalloc: chi0, F and lambda0_out must be device memory");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (!is_device_ptr(chi0, dev) || !is_device_ptr(F, dev) || !is_device_ptr(lambda0_out, dev))
+        return ctx_fail(nullptr, LDGA_ERR_ARG,
+                        "ldga_lambda0_noalloc: chi0, F and lambda0_out must be device memory of the current device");
     double2* colF = noalloc_colF(dev, &e);
     if (!colF) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -1,0 +1,214 @@
+"""GPU parity at the benchmarked sizes, through the C ABI, against the FP64 oracle.
+
+* Configuration 3 (3D sc 32^3, 969 irreducible q, beta = 20, U = 1.5, Nnu = 40, Nw = 41): the headline
+  workload in MIXED mode, run as the benchmark runs it -- autotuned BSE, the whole lambda_m chain in
+  one ldga_chain_m call, captured in a CUDA graph and replayed -- and every compiled configuration of
+  the preconditioned BSE at this size.
+* Configuration 2 (2D 64^2, 561 irreducible q, beta = 30, U = 2, Nnu = 60, Nw = 61): lambda_dm in FP64
+  and in MIXED mode.
+
+Tolerances: elementwise relative 1e-10 (denominator max(|oracle|, 1e-6 max|oracle|)) for chi0, chi_r,
+gamma_r, lambda0, Sigma_ladder and G_ladder; absolute 1e-10 for mu; relative 1e-10 for the energies.
+lambda_m of configuration 3 is not a parity quantity: newton_right (LambdaCorrection/helpers.jl:133-153)
+with the derivative df_c1 of conditions_new.jl:150-153, which carries the chi tail constants, walks
+away from f's root left of 0 into the poles of f (the synthetic chi_m < 0 at large |w|), where its
+iterates depend on the rounding of the sums.  There the device's lambda_m is checked to be a root of
+the oracle's f, and the lambda-dependent outputs are compared at the oracle's lambda_m.
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+import pytest
+
+import ladderdga_b200 as L
+from ladderdga_b200 import _lib
+from ladderdga_b200 import synthetic as S
+from oracle import ldga_ref as R
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-10
+FLOOR = 1e-6
+
+
+def rel(a, b):
+    """Elementwise relative difference max |a - b| / max(|b|, FLOOR max|b|)."""
+    a, b = np.asarray(a), np.asarray(b)
+    m = max(float(np.max(np.abs(b))), 1e-300)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), FLOOR * m)))
+
+
+def device_arrays(ctx):
+    nq, nnu, nw = ctx.Nq, ctx.Nnu, ctx.Nw
+
+    def get(what, ch=0, real=False):
+        out = np.empty((nq, nw), order="F") if real else _lib.cplx_out((nq, nnu, nw))
+        ctx.call("ldga_get", what, ch, _lib.ptr(out))
+        return out
+
+    return {"chi0": get(_lib.GET_CHI0), "chi_m": get(_lib.GET_CHI, _lib.CH_M, True),
+            "chi_d": get(_lib.GET_CHI, _lib.CH_D, True), "gamma_m": get(_lib.GET_GAMMA, _lib.CH_M),
+            "gamma_d": get(_lib.GET_GAMMA, _lib.CH_D), "lambda0": get(_lib.GET_LAMBDA0)}
+
+
+def check_arrays(dev, ref, what):
+    for k in ("chi0", "lambda0", "gamma_m", "gamma_d"):
+        assert rel(dev[k], ref[k]) < RTOL, (what, k, rel(dev[k], ref[k]))
+    for k in ("chi_m", "chi_d"):
+        assert rel(dev[k], ref[k].data) < RTOL, (what, k, rel(dev[k], ref[k].data))
+
+
+class ChainM:
+    """ldga_chain_m from pinned host buffers, as the benchmark's end-to-end leg calls it: the buffers
+    are allocated once, so the second call with use_graph captures the chain and later ones replay it."""
+
+    def __init__(self, h):
+        import torch
+        self.h, self.ctx = h, h.ctx
+
+        def pinned(a):
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+            return torch.from_numpy(v.copy()).pin_memory()
+
+        self.src = [pinned(x) for x in (h.Σ_loc, h.Γ_m, h.Γ_d, h.χDMFT_m, h.gImp)]
+        self.numax = h.sP.n_iν
+        self.S_out = torch.zeros(self.ctx.Nq * self.numax * 2, dtype=torch.float64).pin_memory()
+        self.sc = (C.c_double * 8)()
+
+    def __call__(self, use_graph):
+        h, p = self.h, [C.c_void_p(t.data_ptr()) for t in self.src]
+        self.ctx.call("ldga_chain_m", p[0], len(h.Σ_loc), p[1], p[2], p[3], p[4], len(h.gImp), h.imp_density,
+                      h.χloc_m_sum, use_graph, C.c_void_p(self.S_out.data_ptr()), None, None, self.sc)
+        S_ = self.S_out.numpy().view(np.complex128).reshape((self.ctx.Nq, self.numax), order="F").copy()
+        return list(self.sc), S_
+
+
+def at_lambda(h, lam_m, lam_d=0.0, numax=None):
+    """EoM, μ fit, G_ladder and energies on the device at the given λ (the chain's last stages)."""
+    ctx = h.ctx
+    numax = h.sP.n_iν if numax is None else numax
+    Sg = _lib.cplx_out((ctx.Nq, numax))
+    ctx.call("ldga_eom", lam_m, lam_d, numax, 1, h.χloc_m_sum, _lib.ptr(Sg))
+    G = _lib.cplx_out((ctx.Nq, ctx.Nf))
+    mu, ek, ep, n = (C.c_double() for _ in range(4))
+    ctx.call("ldga_g_ladder", None, 0, 1, h.mP.μ, C.byref(mu), _lib.ptr(G), C.byref(ek), C.byref(ep), C.byref(n))
+    return Sg, G, mu.value, ek.value, ep.value
+
+
+@pytest.fixture(scope="module")
+def cfg3(require_gpu):
+    R.set_workers(os.cpu_count() or 1)
+    inp = S.config_input(3)
+    return inp, R.run_chain(inp, lambda_type="m")
+
+
+def test_config3_mixed_chain_graph(cfg3):
+    """The benchmarked call: autotuned MIXED BSE, ldga_chain_m eager then captured and replayed."""
+    inp, ref = cfg3
+    h = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+    lib = h.ctx.lib
+    try:
+        h.ctx.call("ldga_bubble", None)
+        for t in ("m", "d"):
+            L.autotune_bse(h, t, reps=2)
+        name = lib.ldga_bse_config_name(h.ctx.Nnu, L.PREC_MIXED, -1).decode()
+        assert name.startswith("iter"), name            # the preconditioned solve is what runs here
+        res = ref["result"]
+        rh, cm = ref["h"], ref["chi_m"]
+        rhs = 2 * rh.imp_density - R.sum_kw(rh.kG, ref["chi_d"])
+        run = ChainM(h)
+        for use_graph in (0, 1, 1, 1):                  # eager, capture, replay
+            sc, S_chain = run(use_graph)
+            dev = device_arrays(h.ctx)
+            check_arrays(dev, ref, (name, use_graph))
+            # λm: a root of the oracle's f (which root newton_right reaches is not a parity quantity)
+            lam = sc[0]
+            f = R.sum_kw(rh.kG, cm, transform=lambda x: R.chi_lambda(x, lam)) - rhs
+            scale = R.sum_kw(rh.kG, cm, transform=lambda x: np.abs(R.chi_lambda(x, lam)))
+            assert abs(f) <= 1e-9 * max(1.0, scale), (lam, f)
+            # the chain's Σ_ladder is the EoM at its own λ
+            Sg, _, mu, _, ep = at_lambda(h, lam)
+            assert rel(S_chain, Sg) < 1e-12 and abs(mu - sc[1]) < 1e-12
+        # everything λ-dependent at the oracle's λm
+        Sg, G, mu, ek, ep = at_lambda(h, res.lam_m)
+        assert rel(Sg, res.Sigma_ladder) < RTOL
+        assert rel(G, res.G_ladder) < RTOL
+        assert abs(mu - res.mu) < 1e-10
+        assert abs(ek - res.EKin) <= RTOL * max(1.0, abs(res.EKin))
+        assert abs(ep - res.EPot_p1) <= RTOL * max(1.0, abs(res.EPot_p1))
+    finally:
+        L.tune_reset()
+
+
+def test_config3_every_mixed_bse_configuration(cfg3):
+    """Every compiled MIXED configuration at Nnu = 40 (the autotuner's candidates) on the headline
+    input: χ_r and γ_r against the oracle, no matrix left to the pivoted fallback."""
+    import tempfile
+    inp, ref = cfg3
+    h = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+    lib = h.ctx.lib
+    nnu = h.ctx.Nnu
+    names = []
+    while lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)):
+        names.append(lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)).decode())
+    chi0 = L.calc_bubble(h)
+    assert rel(chi0.data, ref["chi0"]) < RTOL
+    try:
+        for nm in names:
+            fd, path = tempfile.mkstemp()
+            os.write(fd, f"bse {nnu} {L.PREC_MIXED} {nm}\n".encode())
+            os.close(fd)
+            L.tune_reset()
+            L.tune_load(path)
+            os.unlink(path)
+            for r in ("m", "d"):
+                x, g = L.calc_χγ(r, h, chi0)
+                assert rel(x.data, ref[f"chi_{r}"].data) < RTOL, (nm, r, rel(x.data, ref[f"chi_{r}"].data))
+                assert rel(g.data, ref[f"gamma_{r}"]) < RTOL, (nm, r, rel(g.data, ref[f"gamma_{r}"]))
+                if nm.startswith("iter"):
+                    assert x.n_fallback == 0, (nm, r, x.n_fallback)
+    finally:
+        L.tune_reset()
+
+
+@pytest.fixture(scope="module")
+def cfg2(require_gpu):
+    R.set_workers(os.cpu_count() or 1)
+    inp = S.config_input(2)
+    return inp, R.run_chain(inp, lambda_type=None)
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_MIXED])
+def test_config2_lambda_dm(cfg2, prec):
+    """Configuration 2 as specified: both channels and λdm, in FP64 and in MIXED mode.  The arrays
+    before λ against the oracle; the device's (λm, λd) is a root of the ORACLE's λdm residual
+    (conditions_new.jl:250-276) to the Newton's atol 1e-8, and Σ_ladder, G_ladder, μ and the energies
+    at that root equal the oracle's there."""
+    inp, ref = cfg2
+    h = L.setup_synthetic(inp, precision=prec)
+    chi0 = L.calc_bubble(h)
+    xm, gm = L.calc_χγ("m", h, chi0)
+    xd, gd = L.calc_χγ("d", h, chi0)
+    l0 = L.calc_λ0(chi0, h)
+    dev = device_arrays(h.ctx)
+    check_arrays(dev, ref, prec)
+    res = L.λdm_correction(xm, gm, xd, gd, l0, h)
+    assert res.sc_converged, (res.λm, res.λd)
+    # reference properties (test/full_run.jl:151-165): PP and E_pot consistency at the root
+    assert abs(res.PP_p2 - 0.25) < 1e-8
+    assert abs(res.EPot_p1 - res.EPot_p2) < 1e-8
+    numax = res.Σ_ladder.shape[1]
+    hr = ref["h"]
+    state = {"mu": hr.mP.mu}
+    n, mu, ek, ep1, ep2, lhs_c1, Sr, Gr = R.lambda_dm_residual(np.array([res.λm, res.λd]), ref["chi_m"],
+                                                               ref["gamma_m"], ref["chi_d"], ref["gamma_d"],
+                                                               ref["lambda0"], hr, numax, state)
+    rhs_c1 = hr.mP.n / 2 * (1 - hr.mP.n / 2)
+    assert math.hypot(lhs_c1 - rhs_c1, ep1 - ep2) < 1e-8, (lhs_c1 - rhs_c1, ep1 - ep2)
+    assert rel(res.Σ_ladder, Sr) < RTOL
+    assert rel(res.G_ladder, Gr) < RTOL
+    assert abs(res.μ - mu) < 1e-10
+    for a, b in ((res.EKin, ek), (res.EPot_p1, ep1), (res.EPot_p2, ep2), (res.PP_p2, lhs_c1), (res.n, n)):
+        assert abs(a - b) <= RTOL * max(1.0, abs(b)), (a, b)
