@@ -69,6 +69,9 @@ def parse():
                          "to FP64 backward error 1e-14; fp64: the FP64 LU)")
     ap.add_argument("--tune-file", default=None,
                     help="load BSE configuration choices (ldga_tune_save format) instead of autotuning")
+    ap.add_argument("--bse-config", default=None,
+                    help="use this BSE configuration (a name ldga_bse_config_name reports, e.g. iter8x2dm:3) for the "
+                         "workload's box size and precision instead of autotuning")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip timing the same chain in FP64 mode (mixed runs report mixed / FP64)")
     ap.add_argument("--no-cpu-baseline", action="store_true",
@@ -368,6 +371,7 @@ class Chain:
 
 
 TUNE_FILE = None
+BSE_CONFIG = None
 
 
 def tune(chain) -> str:
@@ -377,7 +381,18 @@ def tune(chain) -> str:
     ctx = chain.ctx
     ctx.call("ldga_bubble", None)
     import ladderdga_b200 as L
-    if TUNE_FILE:
+    if BSE_CONFIG and ctx.precision == BSE_CONFIG[0]:
+        import tempfile
+        with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+            f.write(f"bse {ctx.Nnu} {ctx.precision} {BSE_CONFIG[1]}\n")
+        try:
+            L.tune_load(f.name)
+        finally:
+            os.unlink(f.name)
+        got = chain.lib.ldga_bse_config_name(ctx.Nnu, ctx.precision, -1)
+        if not got or got.decode() != BSE_CONFIG[1]:
+            raise SystemExit(f"--bse-config {BSE_CONFIG[1]}: not a configuration of Nnu={ctx.Nnu}, mode {ctx.precision}")
+    elif TUNE_FILE:
         L.tune_load(TUNE_FILE)
     else:
         for t in ("m", "d"):
@@ -848,9 +863,10 @@ def run_batch(args):
 
 
 def main():
-    global TUNE_FILE
+    global TUNE_FILE, BSE_CONFIG
     args = parse()
     TUNE_FILE = args.tune_file
+    BSE_CONFIG = (PREC_NAMES[args.prec], args.bse_config) if args.bse_config else None
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":

