@@ -37,12 +37,13 @@ WORKLOAD_NAME = "3D sc Nk=32^3 (969 irreducible q), beta=20, U=1.5, Nnu=40, Nw=4
 # the other single-point configurations, selectable with --cfg (the chain is the lambda_m chain for all)
 CFG_NAMES = {
     1: "2D sq Nk=16^2 (45 irreducible q), beta=10, U=1, Nnu=20, Nw=21, lambda_m",
-    2: "2D sq Nk=64^2 (561 irreducible q), beta=30, U=2, Nnu=60, Nw=61, lambda_m chain",
+    2: "2D sq Nk=64^2 (561 irreducible q), beta=30, U=2, Nnu=60, Nw=61, lambda_dm",
     3: WORKLOAD_NAME,
 }
 METRIC = "(q,w)-points/s"
 PREC_NAMES = {"fp64inv": 0, "fp64": 1, "mixed": 2}
 REF_BUDGET_S = 120.0
+REF_DM_STEPS = 10
 # DRAM bytes per BSE matrix (Nnu = 40) from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch): the FP64 LU on 3D 16^3 (6765 matrices) and the MIXED preconditioned solve on 3D 32^3 (39 729)
 BSE_DRAM_BYTES_PER_MATRIX = 5423872 / 6765
@@ -87,6 +88,8 @@ def parse():
     ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
     ap.add_argument("--cfg", type=int, default=3, choices=[1, 2, 3],
                     help="single-point configuration of the chain workload (3: the headline 3D 32^3 point)")
+    ap.add_argument("--lambda", dest="lam", default=None, choices=["m", "dm"],
+                    help="lambda correction of the chain workload (default: dm for --cfg 2, m otherwise)")
     ap.add_argument("--input", default=None,
                     help="a readConfig TOML file: run the chain workload on that DMFT impurity input "
                          "(e.g. tests/golden/b1u2_plain.toml) instead of a synthetic configuration")
@@ -107,7 +110,14 @@ def workload_input(args, rank: int = 0):
         return inp, name, f"DMFT impurity file {os.path.basename(env.inputVars)} (read by readConfig)"
     from ladderdga_b200 import synthetic as S
     over = {"ns": args.ns} if args.ns else {}
-    return S.config_input(args.cfg, point=rank, **over), CFG_NAMES[args.cfg], "synthetic"
+    name = CFG_NAMES[args.cfg]
+    if lam_type(args) != ("dm" if args.cfg == 2 else "m"):
+        name = name.rsplit(", ", 1)[0] + f", lambda_{lam_type(args)}"
+    return S.config_input(args.cfg, point=rank, **over), name, "synthetic"
+
+
+def lam_type(args) -> str:
+    return args.lam or ("dm" if args.cfg == 2 and not args.input else "m")
 
 
 def dist_env():
@@ -171,17 +181,27 @@ class ClockSampler:
 # ----------------------------------------------------------------------------------------------
 # CPU baseline: the oracle restatement of the reference algorithm on the host cores
 # ----------------------------------------------------------------------------------------------
-def oracle_chain(inp):
-    """The oracle's whole lambda_m chain on the workload: (outputs, seconds)."""
+def oracle_chain(inp, lambda_type="m"):
+    """The oracle's chain on the workload (with the lambda_m correction, or none): (outputs, seconds)."""
     from oracle import ldga_ref as R
     R.set_workers(os.cpu_count() or 1)
     t0 = time.perf_counter()
-    ref = R.run_chain(inp, lambda_type="m")
+    ref = R.run_chain(inp, lambda_type=lambda_type)
     return ref, time.perf_counter() - t0
 
 
-def cpu_chain_seconds(inp) -> float:
-    return oracle_chain(inp)[1]
+def cpu_chain_seconds(inp, lt: str = "m") -> float:
+    if lt == "m":
+        return oracle_chain(inp, "m")[1]
+    # lambda_dm: the oracle's chain up to lambda_0 and its own lambda_dm Newton, capped at REF_DM_STEPS
+    # iterations (at ~0.4 s a residual and 3 residuals an iteration the full 500-step budget of the
+    # reference's newton_right would take minutes per step): a lower bound of the step's time
+    from oracle import ldga_ref as R
+    ref, t = oracle_chain(inp, None)
+    t0 = time.perf_counter()
+    R.lambda_dm_correction(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"], ref["h"],
+                           nsteps=REF_DM_STEPS)
+    return t + time.perf_counter() - t0
 
 
 def cpu_baseline(t: float, points: int) -> dict:
@@ -210,17 +230,108 @@ def rel_err(a, b) -> dict:
             "worst": [int(x) for x in np.unravel_index(i, b.shape)]}
 
 
+def chi_err(dev_chi, ref, r: str, beta: float, U: float) -> dict:
+    """chi_r(q, w) = Re sum_nu y_nu / beta^2 sums terms of both signs; where they cancel, no FP64
+    evaluation is more accurate than the terms' magnitude allows.  'componentwise' divides each error by
+    that magnitude, sum_nu |y_nu| / beta^2 with y = gamma chi0 (1 + s U chi) from the oracle (the
+    reference's conditioning of the sum); 'elementwise' divides by |chi| with the usual floor."""
+    s = 1.0 if r == "m" else -1.0
+    chi_r = ref[f"chi_{r}"].data
+    y = ref[f"gamma_{r}"] * ref["chi0"] * (1.0 + s * U * chi_r)[:, None, :]
+    scale = np.abs(y).sum(axis=1) / beta ** 2
+    d = np.abs(np.asarray(dev_chi) - chi_r)
+    e = d / np.maximum(scale, 1e-300)
+    i = int(np.argmax(e))
+    out = rel_err(dev_chi, chi_r)
+    out["componentwise"] = float(e.flat[i])
+    out["componentwise_worst"] = [int(x) for x in np.unravel_index(i, chi_r.shape)]
+    return out
+
+
+def array_errors(chain, ref) -> dict:
+    """chi0, gamma_m, gamma_d and lambda0 elementwise, chi_m and chi_d componentwise (chi_err), from the
+    handle's device copies."""
+    from ladderdga_b200 import _lib
+    ctx, h = chain.ctx, chain.h
+    nq, nnu, nw = ctx.Nq, ctx.Nnu, ctx.Nw
+
+    def get(what, ch=0, real=False):
+        out = np.empty((nq, nw), order="F") if real else _lib.cplx_out((nq, nnu, nw))
+        ctx.call("ldga_get", what, ch, _lib.ptr(out))
+        return out
+
+    beta, U = h.mP.β, h.mP.U
+    return {"floor": f"elementwise denominators max(|oracle|, {ERR_FLOOR:g} max|oracle|)",
+            "chi0": rel_err(get(_lib.GET_CHI0), ref["chi0"]),
+            "chi_m": chi_err(get(_lib.GET_CHI, _lib.CH_M, True), ref, "m", beta, U),
+            "chi_d": chi_err(get(_lib.GET_CHI, _lib.CH_D, True), ref, "d", beta, U),
+            "gamma_m": rel_err(get(_lib.GET_GAMMA, _lib.CH_M), ref["gamma_m"]),
+            "gamma_d": rel_err(get(_lib.GET_GAMMA, _lib.CH_D), ref["gamma_d"]),
+            "lambda0": rel_err(get(_lib.GET_LAMBDA0), ref["lambda0"])}
+
+
+def accuracy_dm(chain, ref, scal) -> dict:
+    """Errors of the handle's last lambda_dm chain against the oracle on the same input.  The oracle's
+    own lambda_dm Newton takes minutes on this box (one residual = an FFT EoM, a mu fit and the energies,
+    ~0.4 s), so the device's root (lambda_m, lambda_d) is put into the ORACLE's residual (conditions_new.jl
+    residual_vals): |F| measures how well it solves the reference's equations, Sigma_ladder is compared
+    at that root, and the mu fit, G_ladder and energies are compared from the oracle's Sigma_ladder
+    ('isolated').  ref: the oracle chain without lambda correction; returns (errors, seconds of one
+    oracle residual)."""
+    from oracle import ldga_ref as R
+    from ladderdga_b200 import _lib
+    ctx, h = chain.ctx, chain.h
+    errs = array_errors(chain, ref)
+    lm, ld = scal[0], scal[8]
+    numax = chain.dm_numax
+    S_dev = _lib.cplx_out((ctx.Nq, numax))
+    ctx.call("ldga_get", _lib.GET_SIGMA, 0, _lib.ptr(S_dev))
+    hr = ref["h"]
+    t0 = time.perf_counter()
+    n, mu, ek, ep1, ep2, lhs_c1, Sr, Gr = R.lambda_dm_residual(np.array([lm, ld]), ref["chi_m"], ref["gamma_m"],
+                                                               ref["chi_d"], ref["gamma_d"], ref["lambda0"], hr,
+                                                               numax, {"mu": hr.mP.mu})
+    t_res = time.perf_counter() - t0
+    rhs_c1 = hr.mP.n / 2 * (1 - hr.mP.n / 2)
+    ctx.call("ldga_set_sigma", _lib.ptr(_lib.as_fc(Sr)), numax)
+    G = _lib.cplx_out((ctx.Nq, ctx.Nf))
+    mu_d, ek_d, ep_d, n_d = (C.c_double() for _ in range(4))
+    ctx.call("ldga_g_ladder", None, 0, 1, h.mP.μ, C.byref(mu_d), _lib.ptr(G), C.byref(ek_d), C.byref(ep_d),
+             C.byref(n_d))
+    iso = {"G_ladder": rel_err(G, Gr), "mu_abs": abs(mu_d.value - mu),
+           "E_kin_rel": abs(ek_d.value - ek) / max(1.0, abs(ek)), "E_pot1_rel": abs(ep_d.value - ep1) / max(1.0, abs(ep1))}
+    errs["at_device_root"] = {
+        "lambda_m": lm, "lambda_d": ld, "converged": bool(scal[6]),
+        "oracle_residual": [lhs_c1 - rhs_c1, ep1 - ep2],
+        "Sigma_ladder": rel_err(S_dev, Sr), "mu_abs": abs(scal[1] - mu), "isolated": iso}
+    checked = [errs[k]["elementwise"] for k in ("chi0", "gamma_m", "gamma_d", "lambda0")]
+    checked += [errs[k]["componentwise"] for k in ("chi_m", "chi_d")]
+    checked += [errs["at_device_root"]["Sigma_ladder"]["elementwise"], errs["at_device_root"]["mu_abs"],
+                iso["G_ladder"]["elementwise"], iso["mu_abs"], iso["E_kin_rel"], iso["E_pot1_rel"]]
+    errs["max_checked"] = float(max(checked))
+    errs["root_residual_ok"] = bool(math.hypot(lhs_c1 - rhs_c1, ep1 - ep2) <= 1e-8)
+    errs["checked"] = ("chi0, gamma, lambda0 elementwise; chi componentwise; Sigma_ladder and mu at the device's "
+                       "root; G_ladder, mu, energies isolated from the oracle's Sigma_ladder there; the root itself "
+                       "to the Newton's atol 1e-8 in the oracle's residual")
+    errs["within_1e-10"] = bool(errs["max_checked"] <= 1e-10 and errs["root_residual_ok"])
+    return errs, t_res
+
+
 def accuracy(chain, ref, lam_dev: float) -> dict:
     """Errors of the handle's last chain step against the oracle chain on the same input.
 
-    chi0, chi_m, chi_d, gamma_m, gamma_d and lambda0 are compared directly.  lambda_m of this
-    workload is not a parity quantity (the reference's newton_right runs into the poles of f, see
-    `lambda_m`), so Sigma_ladder, G_ladder, mu and the energies are recomputed on the device at the
-    ORACLE's lambda_m (EoM, mu fit, calc_E) and compared with the oracle's values there."""
+    chi0, gamma_m, gamma_d and lambda0 elementwise; chi_m, chi_d componentwise (chi_err).  lambda_m of
+    this workload is not a parity quantity (the reference's newton_right runs into the poles of f, see
+    `lambda_m`), so the lambda-dependent stages are checked at the ORACLE's lambda_m: 'isolated' gives
+    each stage the oracle's inputs (EoM from the oracle's chi, gamma, lambda0; mu fit, G_ladder and the
+    energies from the oracle's Sigma_ladder) and measures that stage alone; 'propagated' runs them on
+    the device's own upstream results, whose differences the near-pole chi_lambda = chi/(1 + lambda chi)
+    amplifies by `amplification` = max |1/(1 + lambda chi)|.  (This overwrites the handle's arrays.)"""
     from oracle import ldga_ref as R
     from ladderdga_b200 import _lib
     ctx, h = chain.ctx, chain.h
     nq, nnu, nw, numax = ctx.Nq, ctx.Nnu, ctx.Nw, chain.numax
+    beta, U = h.mP.β, h.mP.U
 
     def get(what, ch=0, real=False):
         out = np.empty((nq, nw), order="F") if real else _lib.cplx_out((nq, nnu, nw))
@@ -228,53 +339,69 @@ def accuracy(chain, ref, lam_dev: float) -> dict:
         return out
 
     res = ref["result"]
-    errs = {"floor": f"elementwise denominators max(|oracle|, {ERR_FLOOR:g} max|oracle|)",
-            "chi0": rel_err(get(_lib.GET_CHI0), ref["chi0"]),
-            "chi_m": rel_err(get(_lib.GET_CHI, _lib.CH_M, True), ref["chi_m"].data),
-            "chi_d": rel_err(get(_lib.GET_CHI, _lib.CH_D, True), ref["chi_d"].data),
-            "gamma_m": rel_err(get(_lib.GET_GAMMA, _lib.CH_M), ref["gamma_m"]),
-            "gamma_d": rel_err(get(_lib.GET_GAMMA, _lib.CH_D), ref["gamma_d"]),
-            "lambda0": rel_err(get(_lib.GET_LAMBDA0), ref["lambda0"])}
-    # the lambda-dependent outputs at the oracle's lambda_m
+    errs = array_errors(chain, ref)
     lam = float(res.lam_m)
-    S = _lib.cplx_out((nq, numax))
-    ctx.call("ldga_eom", lam, 0.0, numax, 1, h.χloc_m_sum, _lib.ptr(S))
-    G = _lib.cplx_out((nq, ctx.Nf))
-    mu, ek, ep, n = (C.c_double() for _ in range(4))
-    ctx.call("ldga_g_ladder", None, 0, 1, h.mP.μ, C.byref(mu), _lib.ptr(G), C.byref(ek), C.byref(ep), C.byref(n))
-    errs["at_oracle_lambda_m"] = {
-        "lambda_m": lam,
-        "Sigma_ladder": rel_err(S, res.Sigma_ladder),
-        "G_ladder": rel_err(G, res.G_ladder),
-        "mu_abs": abs(mu.value - res.mu),
-        "E_kin_rel": abs(ek.value - res.EKin) / max(1.0, abs(res.EKin)),
-        "E_pot1_rel": abs(ep.value - res.EPot_p1) / max(1.0, abs(res.EPot_p1))}
+
+    def downstream():
+        S = _lib.cplx_out((nq, numax))
+        ctx.call("ldga_eom", lam, 0.0, numax, 1, h.χloc_m_sum, _lib.ptr(S))
+        return S
+
+    def g_ladder():
+        G = _lib.cplx_out((nq, ctx.Nf))
+        mu, ek, ep, n = (C.c_double() for _ in range(4))
+        ctx.call("ldga_g_ladder", None, 0, 1, h.mP.μ, C.byref(mu), _lib.ptr(G), C.byref(ek), C.byref(ep),
+                 C.byref(n))
+        return G, mu.value, ek.value, ep.value
+
+    def stage_errs(S, G, mu, ek, ep):
+        return {"Sigma_ladder": rel_err(S, res.Sigma_ladder), "G_ladder": rel_err(G, res.G_ladder),
+                "mu_abs": abs(mu - res.mu), "E_kin_rel": abs(ek - res.EKin) / max(1.0, abs(res.EKin)),
+                "E_pot1_rel": abs(ep - res.EPot_p1) / max(1.0, abs(res.EPot_p1))}
+
+    # propagated: the device's own chi, gamma, lambda0 at the oracle's lambda_m
+    S = downstream()
+    prop = stage_errs(S, *g_ladder())
+    cm = ref["chi_m"].data
+    prop["amplification"] = float(np.max(np.abs(1.0 / (1.0 + lam * cm))))
+    # isolated: each stage from the oracle's inputs
+    ctx.call("ldga_set_chi", _lib.CH_M, _lib.ptr(np.asfortranarray(ref["chi_m"].data)))
+    ctx.call("ldga_set_chi", _lib.CH_D, _lib.ptr(np.asfortranarray(ref["chi_d"].data)))
+    ctx.call("ldga_set_gamma", _lib.CH_M, _lib.ptr(_lib.as_fc(ref["gamma_m"])))
+    ctx.call("ldga_set_gamma", _lib.CH_D, _lib.ptr(_lib.as_fc(ref["gamma_d"])))
+    ctx.call("ldga_set_lambda0", _lib.ptr(_lib.as_fc(ref["lambda0"])))
+    S_iso = downstream()
+    ctx.call("ldga_set_sigma", _lib.ptr(_lib.as_fc(res.Sigma_ladder)), numax)
+    iso = stage_errs(S_iso, *g_ladder())
+    errs["at_oracle_lambda_m"] = {"lambda_m": lam, "isolated": iso, "propagated": prop}
     # lambda_m itself: both values, and how well each solves the oracle's f(l) = sum_kw chi_l - rhs
-    rh, cm = ref["h"], ref["chi_m"]
+    rh, cmT = ref["h"], ref["chi_m"]
     rhs = 2 * rh.imp_density - R.sum_kw(rh.kG, ref["chi_d"])
 
     def f(l):
-        return R.sum_kw(rh.kG, cm, transform=lambda x: R.chi_lambda(x, l)) - rhs
+        return R.sum_kw(rh.kG, cmT, transform=lambda x: R.chi_lambda(x, l)) - rhs
 
     def scale(l):
-        return max(1.0, R.sum_kw(rh.kG, cm, transform=lambda x: np.abs(R.chi_lambda(x, l))))
+        return max(1.0, R.sum_kw(rh.kG, cmT, transform=lambda x: np.abs(R.chi_lambda(x, l))))
 
-    neg = cm.data[cm.data < 0]
+    neg = cm[cm < 0]
     errs["lambda_m"] = {
         "device": lam_dev, "oracle": lam, "abs_diff": abs(lam_dev - lam),
         "device_root_residual": abs(f(lam_dev)) / scale(lam_dev), "oracle_root_residual": abs(f(lam)) / scale(lam),
-        "f_at_0": f(0.0), "df_c1_at_0": R.sum_kw(rh.kG, cm, transform=lambda x: R.dchi_lambda(x, 0.0)),
+        "f_at_0": f(0.0), "df_c1_at_0": R.sum_kw(rh.kG, cmT, transform=lambda x: R.dchi_lambda(x, 0.0)),
         "first_pole": float(1.0 / np.max(-neg)) if neg.size else None,
         "note": "newton_right's df carries the chi tail constants (df_c1 > 0 at 0 while f(0) < 0), so the "
                 "iteration walks right into the poles of f at lambda >= first_pole, where each iterate depends "
                 "on the rounding of the sums: every root it can land on solves f = 0, but which one is not a "
                 "parity quantity"}
-    worst = max(v["elementwise"] for k, v in errs.items() if isinstance(v, dict) and "elementwise" in v)
-    fixed = errs["at_oracle_lambda_m"]
-    worst_fixed = max(fixed["Sigma_ladder"]["elementwise"], fixed["G_ladder"]["elementwise"], fixed["mu_abs"],
-                      fixed["E_kin_rel"], fixed["E_pot1_rel"])
-    errs["max_elementwise"] = max(worst, worst_fixed)
-    errs["within_1e-10"] = bool(errs["max_elementwise"] <= 1e-10)
+    checked = [errs[k]["elementwise"] for k in ("chi0", "gamma_m", "gamma_d", "lambda0")]
+    checked += [errs[k]["componentwise"] for k in ("chi_m", "chi_d")]
+    checked += [iso["Sigma_ladder"]["elementwise"], iso["G_ladder"]["elementwise"], iso["mu_abs"],
+                iso["E_kin_rel"], iso["E_pot1_rel"]]
+    errs["max_checked"] = float(max(checked))
+    errs["checked"] = ("chi0, gamma, lambda0 elementwise; chi componentwise; Sigma_ladder, G_ladder, mu, "
+                       "energies isolated at the oracle's lambda_m")
+    errs["within_1e-10"] = bool(errs["max_checked"] <= 1e-10)
     return errs
 
 
@@ -288,14 +415,16 @@ def run_reference(args):
     # one step is a whole chain (about 10 s on 8 cores): the warm-up is capped at one chain and the
     # timed steps stop once REF_BUDGET_S seconds are spent, so the arm ends within a few minutes
     for _ in range(min(args.warmup, 1)):
-        cpu_chain_seconds(inp)
+        cpu_chain_seconds(inp, lam_type(args))
     ts = []
     t_start = time.perf_counter()
     while len(ts) < args.steps and (not ts or time.perf_counter() - t_start < REF_BUDGET_S):
-        ts.append(cpu_chain_seconds(inp))
+        ts.append(cpu_chain_seconds(inp, lam_type(args)))
     ms = 1000.0 * float(np.mean(ts))
     value = points / (ms / 1000.0)
-    sample = (f"{len(ts)} full chain(s) of the workload after {min(args.warmup, 1)} warm-up chain(s) "
+    what = ("full chain(s)" if lam_type(args) == "m" else
+            f"chain(s) with the lambda_dm Newton capped at {REF_DM_STEPS} iterations (a lower bound of the step)")
+    sample = (f"{len(ts)} {what} of the workload after {min(args.warmup, 1)} warm-up chain(s) "
               f"(steps capped by a {REF_BUDGET_S:.0f} s budget); NumPy/SciPy FP64 restatement of the reference "
               "algorithm (oracle/ldga_ref.py), scipy.fft workers and OpenBLAS threads = all cores")
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": len(ts),
@@ -318,11 +447,12 @@ def run_reference(args):
 class Chain:
     """The device chain for one parameter point, driven through the C ABI."""
 
-    def __init__(self, inp, prec: int, device: int, stream=None):
+    def __init__(self, inp, prec: int, device: int, stream=None, lam_type: str = "m"):
         import torch
         import ladderdga_b200 as L
         self.L, self.torch = L, torch
         self.inp = inp
+        self.lam_type = lam_type
         self.h = L.setup_synthetic(inp, precision=prec, device=device)
         self.ctx = self.h.ctx
         self.lib = self.ctx.lib
@@ -348,7 +478,10 @@ class Chain:
         self.out_chi_m = torch.empty(nq * nw, dtype=torch.float64).pin_memory()
         self.out_chi_d = torch.empty(nq * nw, dtype=torch.float64).pin_memory()
         self.d2h_bytes = (self.out_sigma.numel() + self.out_chi_m.numel() + self.out_chi_d.numel()) * 8 + 5 * 8
+        if lam_type == "dm":   # Sigma_ladder (at most n_iv frequencies) and 7 scalars come back
+            self.d2h_bytes = self.out_sigma.numel() * 8 + 7 * 8
         self.points = nq * nw
+        self.dm_evals = 0
 
     def io(self, src: dict, outputs: bool, sc):
         """This point's ldga_chain_io (ldga_batch_chain_m)."""
@@ -359,8 +492,36 @@ class Chain:
                             p(self.out_sigma) if outputs else None, p(self.out_chi_m) if outputs else None,
                             p(self.out_chi_d) if outputs else None, C.addressof(sc))
 
+    def step_dm(self, src: dict, outputs: bool):
+        """One parameter point through the lambda_dm chain of the C ABI: ldga_gloc -> ldga_bubble ->
+        ldga_bse (m, d) -> ldga_F_from_chi -> ldga_lambda0 -> ldga_lambda_dm (the reference's 2-D
+        newton_right on the host, every residual an EoM + mu fit + energies on the device).
+        Scalars as ldga_chain_m's, [6] = converged, [8] = lambda_d."""
+        from ladderdga_b200 import _lib
+        p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        ctx = self.ctx
+        ctx.call("ldga_gloc", p(src["sigma_loc"]), self.n_sigma, None)
+        ctx.call("ldga_bubble", None)
+        ctx.call("ldga_bse", _lib.CH_M, p(src["gamma_m"]), None, None, None)
+        ctx.call("ldga_bse", _lib.CH_D, p(src["gamma_d"]), None, None, None)
+        ctx.call("ldga_F_from_chi", p(src["chi_loc_m"]), p(src["gimp"]), self.n_gimp, None)
+        ctx.call("ldga_lambda0", None, None)
+        lm, ld, conv, nu = C.c_double(), C.c_double(), C.c_int32(), C.c_int32()
+        out7 = (C.c_double * 7)()
+        st = self.lib.ldga_lambda_dm(ctx.h, self.h.χloc_m_sum, -1, 1e-4, 1e-8, 500, C.byref(lm), C.byref(ld),
+                                     C.byref(conv), out7, C.byref(nu), p(self.out_sigma) if outputs else None, None)
+        if st != _lib.LDGA_ERR_NOCONV:
+            ctx.check(st)
+        ev = C.c_int32()
+        ctx.call("ldga_lambda_dm_evals", C.byref(ev))
+        self.dm_evals, self.dm_numax = ev.value, nu.value
+        n, mu, ek, ep1, ep2, pp1, pp2 = list(out7)
+        return [lm.value, mu, ek, ep1, ep2, pp2, float(conv.value), n, ld.value]
+
     def step(self, src: dict, outputs: bool, graph: bool = True):
         """One parameter point through ldga_chain_m (captured once in a CUDA graph, then replayed)."""
+        if self.lam_type == "dm":
+            return self.step_dm(src, outputs)
         p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
         sc = (C.c_double * 8)()
         self.ctx.call("ldga_chain_m", p(src["sigma_loc"]), self.n_sigma, p(src["gamma_m"]), p(src["gamma_d"]),
@@ -415,6 +576,23 @@ def newton_period(chain):
                 "executed": per[0] + (its.value - per[0]) % per[1] if per[1] else its.value}
     except Exception as e:  # reported, not fatal: the bench line stands without it
         return {"error": str(e)}
+
+
+STAGE_BSE_MASK = 1 << 2   # LDGA_STAGE_BSE
+
+
+def stage_breakdown(chain, steps: int) -> dict:
+    """Per-stage device time of the chain (ms per step) from `steps` untimed replays with every
+    stage's events in the graph; profiling is off afterwards."""
+    chain.ctx.call("ldga_profile", 1)
+    for _ in range(2):                      # the first call re-captures the graph with the events
+        chain.step(chain.dev, False)
+    stage_times(chain)
+    for _ in range(steps):
+        chain.step(chain.dev, False)
+    st = stage_times(chain)
+    chain.ctx.call("ldga_profile", 0)
+    return {k: v[0] / steps for k, v in st.items() if v[1]}
 
 
 def stage_times(chain):
@@ -541,7 +719,8 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     inp, wname, data = workload_input(args, rank)
-    chain = Chain(inp, PREC_NAMES[args.prec], local)
+    lt = lam_type(args)
+    chain = Chain(inp, PREC_NAMES[args.prec], local, lam_type=lt)
     bse_config = tune(chain)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     peaks = {}
@@ -567,8 +746,10 @@ def run_ours(args):
             times.append(a.elapsed_time(b))
         return times
 
-    # the stage events are recorded inside the graph, so profiling is on for capture and timing
-    chain.ctx.call("ldga_profile", 0 if args.no_stage_events else 1)
+    # Inside the timed region only the BSE launches (the dominant kernel, whose duration the roofline
+    # needs) are bracketed by CUDA events: every event is a node of the chain's graph and delays it.
+    # The per-stage breakdown comes from a separate, untimed pass with every stage's events.
+    chain.ctx.call("ldga_profile_stages", 0 if args.no_stage_events else STAGE_BSE_MASK)
     for _ in range(max(args.warmup, 3)):
         scal = chain.step(chain.dev, False)
     torch.cuda.synchronize()
@@ -592,14 +773,24 @@ def run_ours(args):
     t_e2e = timed(chain.pin, True)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    chain.ctx.call("ldga_profile", 0)
-    newton = newton_period(chain)
+    breakdown = stage_breakdown(chain, min(args.steps, 10))
+    newton = newton_period(chain) if lt == "m" else {"lambda_dm_residual_evaluations": chain.dm_evals}
     # the oracle's chain on the same input: the CPU baseline's timing and the reference values of
     # the accuracy check (rank 0 at N = 1 only)
     oref, t_cpu, errors, errors64 = None, None, None, None
     if world == 1 and not args.no_cpu_baseline:
-        oref, t_cpu = oracle_chain(inp)
-        errors = accuracy(chain, oref, scal[0])
+        if lt == "m":
+            oref, t_cpu = oracle_chain(inp, "m")
+            errors = accuracy(chain, oref, scal[0])
+        else:
+            # the oracle's chain up to lambda_0, then one residual of its lambda_dm at the device's root;
+            # the CPU time of a whole step counts that residual as many times as the device's Newton
+            # evaluated its own
+            oref, t_cpu = oracle_chain(inp, None)
+            scal = chain.step(chain.dev, False)
+            errors, t_res = accuracy_dm(chain, oref, scal)
+            t_cpu_sample = (t_cpu, t_res, chain.dm_evals)
+            t_cpu = t_cpu + chain.dm_evals * t_res
     ms = float(np.mean(t_dev))
     ms_e2e = float(np.mean(t_e2e))
     if world > 1:
@@ -613,9 +804,9 @@ def run_ours(args):
     fp64_cmp = None
     if args.prec == "mixed" and world == 1 and not args.no_fp64_compare:
         # the same chain with the FP64 LU, same timing: the mixed / FP64 ratio of the headline metric
-        c64 = Chain(inp, PREC_NAMES["fp64"], local)
+        c64 = Chain(inp, PREC_NAMES["fp64"], local, lam_type=lt)
         cfg64 = tune(c64)
-        c64.ctx.call("ldga_profile", 0 if args.no_stage_events else 1)
+        c64.ctx.call("ldga_profile_stages", 0 if args.no_stage_events else STAGE_BSE_MASK)
         for _ in range(max(args.warmup, 3)):
             scal64 = c64.step(c64.dev, False)
         torch.cuda.synchronize()
@@ -631,17 +822,18 @@ def run_ours(args):
             tr.append(a.elapsed_time(b))
         rst = stage_times(c64)
         c64.ctx.call("ldga_profile", 0)
+        brk64 = stage_breakdown(c64, min(args.steps, 10))
         if oref is not None:
-            errors64 = accuracy(c64, oref, scal64[0])
+            errors64 = accuracy(c64, oref, scal64[0]) if lt == "m" else accuracy_dm(c64, oref, scal64)[0]
         ms64 = float(np.mean(tr))
         bse64 = rst["bse"][0] / args.steps
         bse_mx = stages["bse"][0] / args.steps or float("nan")
         fp64_cmp = {"ms_per_step": ms64, "value": chain.points / (ms64 / 1e3), "bse_config": cfg64,
                     "bse_ms_per_step": bse64, "mixed_over_fp64": ms64 / ms,
                     "bse_mixed_over_fp64": bse64 / bse_mx,
-                    "stages_ms_per_step": {k: v[0] / args.steps for k, v in rst.items() if v[1]}}
+                    "stages_ms_per_step": brk64}
         if errors64 is not None:
-            fp64_cmp["errors_max_elementwise"] = errors64["max_elementwise"]
+            fp64_cmp["errors"] = errors64
     if rank == 0:
         rl = (roofline(stages, chain, peaks, (sp.value, sw.value)) if any(v[1] for v in stages.values())
               else {"note": "no stage events (--no-stage-events)"})
@@ -656,9 +848,13 @@ def run_ours(args):
                         "d2h_bytes_per_step": chain.d2h_bytes, "ms_per_step": ms_e2e,
                         "path": "C ABI (ldga_*) from pinned host buffers"},
                 "roofline": rl,
-                "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items() if v[1]},
+                "stages_ms_per_step": breakdown,
+                "stages_note": "untimed pass with CUDA events around every stage (the events delay the graph; "
+                               "the timed region brackets only the BSE launches)",
                 "gpu_launches": launches,
                 "result": {"lambda_m": scal[0], "mu": scal[1], "E_kin": scal[2], "E_pot1": scal[3],
+                           **({"lambda_d": scal[8], "converged": bool(scal[6]), "E_pot2": scal[4], "PP_p2": scal[5]}
+                              if lt == "dm" else {}),
                            "newton_iterations": scal[6], "newton_rerun": newton},
                 "clocks": clk}
         if errors is not None:
@@ -667,6 +863,13 @@ def run_ours(args):
             line["fp64_compare"] = fp64_cmp
         if t_cpu is not None:
             line["cpu_baseline"] = cpu_baseline(t_cpu, chain.points)
+            if lt == "dm":
+                tc, tr, nr = t_cpu_sample
+                line["cpu_baseline"]["sample"] = (
+                    f"the oracle's chain up to lambda_0 ({tc:.1f} s) and one residual of its lambda_dm Newton "
+                    f"({tr:.2f} s), counted {nr} times (the residual evaluations of the device's Newton on this "
+                    "input): NumPy/SciPy FP64 restatement of the reference algorithm (oracle/ldga_ref.py), "
+                    "scipy.fft workers and OpenBLAS threads = all cores")
         print(json.dumps(line), flush=True)
         if args.out:
             open(args.out, "w").write(json.dumps(line) + "\n")

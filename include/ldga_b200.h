@@ -104,6 +104,9 @@ int ldga_set_stream(ldga_ctx* ctx, void* stream);
 #define LDGA_STAGE_EOM_INVERSE 8
 #define LDGA_STAGE_GLADDER 9
 int ldga_profile(ldga_ctx* ctx, int32_t enable);
+/* Profile only the stages whose bits are set in mask (bit LDGA_STAGE_*; 0 turns profiling off).  Every
+ * stage's events are nodes of the chain's CUDA graph and delay it: timing one stage needs only its own. */
+int ldga_profile_stages(ldga_ctx* ctx, uint32_t mask);
 int ldga_stage_times(ldga_ctx* ctx, double* ms, int32_t* counts);
 /* Number of kernels this handle has launched since it was created. */
 int ldga_launch_count(const ldga_ctx* ctx, int64_t* n);

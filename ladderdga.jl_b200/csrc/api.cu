@@ -29,7 +29,7 @@ int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what) {
 // While a graph is captured the two event records become graph nodes; their (stage, slot) pairs are
 // kept with the graph and read after every replay (ldga_chain_m).
 StageTimer::StageTimer(ldga_ctx* ctx, int st) : c(ctx), stage(st), slot(-1) {
-    if (!c || !c->profiling) return;
+    if (!c || !c->profiling || !((c->prof_mask >> st) & 1u)) return;
     if (c->ev_free.empty()) {
         ldga_ctx::EvPair p;
         if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) return;
@@ -396,6 +396,14 @@ int ldga_set_stream(ldga_ctx* ctx, void* stream) {
 int ldga_profile(ldga_ctx* ctx, int32_t enable) {
     if (!ctx) return LDGA_ERR_ARG;
     ctx->profiling = enable != 0;
+    ctx->prof_mask = enable != 0 ? (1u << LDGA_N_STAGES) - 1u : 0u;
+    return LDGA_OK;
+}
+
+int ldga_profile_stages(ldga_ctx* ctx, uint32_t mask) {
+    if (!ctx) return LDGA_ERR_ARG;
+    ctx->prof_mask = mask & ((1u << LDGA_N_STAGES) - 1u);
+    ctx->profiling = ctx->prof_mask != 0;
     return LDGA_OK;
 }
 
@@ -1153,7 +1161,7 @@ int chain_m_submit(ldga_ctx* ctx, const ChainArgs& a, bool use_graph, bool* repl
         key.insert(key.end(), {(uint64_t)n_sigma, (uint64_t)n_gimp, dbits(a.imp_density), dbits(a.chiloc_m_sum),
                                dbits(ctx->mp.U), dbits(ctx->mp.mu), dbits(ctx->mp.beta), dbits(ctx->mp.n),
                                dbits(ctx->mp.Ekin_DMFT), (uint64_t)ctx->prec, (uint64_t)(uintptr_t)ctx->stream,
-                               (uint64_t)ctx->profiling});
+                               (uint64_t)ctx->profiling, (uint64_t)ctx->prof_mask});
     }
     if (graphable && ctx->graph_exec && key == ctx->graph_key) {
         LDGA_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));

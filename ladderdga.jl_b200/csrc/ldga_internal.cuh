@@ -134,6 +134,7 @@ struct ldga_ctx {
 
     // stage timing (ldga_profile / ldga_stage_times)
     bool profiling = false;
+    uint32_t prof_mask = 0;       // stages whose events are recorded while profiling (bit = stage)
     struct EvPair { cudaEvent_t a = nullptr, b = nullptr; };
     std::vector<EvPair> ev_pool;
     std::vector<int> ev_free;
