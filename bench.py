@@ -679,14 +679,18 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
                                        if nnu == 40 else "no capture at this Nnu"),
                     "peak_source": peak_src}
         # bound: FP32 (mixed) / FP64 CUDA-core pipes, nominal B200 rates at the measured max clock
-        fp = "fp32" if chain.ctx.precision == 2 else "fp64"
+        # the FP32 eliminations (MIXED's lu32 / warp configurations) or the FP64 LU (FP64 mode, and
+        # MIXED where the autotuner found it fastest)
+        fp = "fp32" if cfg.startswith(("lu32", "warp")) else "fp64"
         lanes = 128 if fp == "fp32" else 64
         peak = 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
         peak_src = (f"nominal {lanes} {fp.upper()} FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (the CUDA-core pipe, "
                     "not HBM or tensor cores, bounds this kernel)")
         if fp == "fp64":
             peak, peak_src = fp64_peak(peaks, sm_mhz)
-        kname = "k_bse_lu32 (FP32 LU + FP64 refinement)" if fp == "fp32" else "k_bse_lu (FP64 LU)"
+        kname = ("k_bse_warp32 (FP32 LU per warp + FP64 refinement)" if cfg.startswith("warp") else
+                 "k_bse_lu32 (FP32 LU + FP64 refinement)" if fp == "fp32" else "k_bse_lu (FP64 LU)")
+        kname += f" [{cfg}]"
         return {"kernel": kname, "bound": fp, "achieved": ach, "peak": peak,
                 "unit": "TFLOP/s", "frac": ach / peak,
                 "work": "8 N^3 + 8 N^2 flops per matrix (the reference's LU + inverse formulation)",

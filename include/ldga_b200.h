@@ -388,19 +388,30 @@ int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam
                    double atol, int32_t nsteps, double* lam_m, double* lam_d, int32_t* converged,
                    double* out7, int32_t* numax_out, double* sigma_out, double* G_out);
 
-/* run_sc / run_sc! (conditions_new.jl:342-556) with update_χ_tail = false: the self-consistent ladder
- * loop.  Each iteration: EoM at (lam_m, lam_d) on the current G transform -> linear mixing of
- * Sigma_ladder with the previous one (from the second iteration) -> G_from_Σladder! (μ fit when
- * fit_mu) -> calc_E -> the transform of G_ladder feeds the next EoM; it stops when E_pot,1 and
- * E_pot,2 change by less than conv_abs, or after maxit iterations.
- * redo_dm != 0 (types :dm, :pre_dm): from the second iteration λ is found again by λdm_correction on
- * the current G, starting from the previous root; otherwise (types :fix, :m, :pre_m) λ stays fixed --
- * the reference's `type == [:pre_m, :m]` test is never true, so :m keeps its first λ as well.
+/* run_sc / run_sc! (conditions_new.jl:342-556): the self-consistent ladder loop.  Each iteration:
+ * EoM at (lam_m, lam_d) on the current G transform -> linear mixing of Sigma_ladder with the previous
+ * one (from the second iteration) -> G_from_Σladder! (μ fit when fit_mu) -> calc_E -> the transform of
+ * G_ladder feeds the next EoM; it stops when E_pot,1 and E_pot,2 change by less than conv_abs, or after
+ * maxit iterations.  flags:
+ *   LDGA_SC_REDO_DM (types :dm, :pre_dm): from the second iteration λ is found again by
+ *     λdm_correction on the current G, starting from the previous root; otherwise (types :fix, :m,
+ *     :pre_m) λ stays fixed -- the reference's `type == [:pre_m, :m]` test is never true, so :m keeps
+ *     its first λ as well;
+ *   LDGA_SC_UPDATE_CHI_TAIL (update_χ_tail = true, :519-545): after the loop both channels' c2 tail
+ *     is set to E_kin (update_tail!, which shifts chi by Re(Δc2/(i w)^2)), the sum rules are evaluated
+ *     again and, unless they hold to conv_abs or 20 updates were made, the loop restarts at it = 1;
+ *     the handle's chi and tail coefficient (ldga_model.Ekin_DMFT) are restored on return;
+ *   LDGA_SC_LAMBDA_TYPE (types :m, :dm, :pre_m, :pre_dm): a restarted loop takes its first λ from
+ *     χ.λ, which is 0 after the first pass (run_sc! resets χ in its first iteration).
+ * A flags value of 0 or 1 keeps the meaning of the former redo_dm argument.
  * numax <= 0: min(n_iv, floor(3 Nw / 8)).  The handle's G and its transform are restored on return
  * (the reference iterates on a deepcopy of gLoc_rfft).
  * out[12] = {λm, λd, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n, μ, sc_converged, iterations, νmax};
  * sigma_out [Nq, νmax] and G_out [Nq, Nf] (the last Sigma_ladder / G_ladder) may be NULL. */
-int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t redo_dm, double mu, double chiloc_m_sum,
+#define LDGA_SC_REDO_DM 1
+#define LDGA_SC_UPDATE_CHI_TAIL 2
+#define LDGA_SC_LAMBDA_TYPE 4
+int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t flags, double mu, double chiloc_m_sum,
                 int32_t numax, int32_t maxit, double mixing, double conv_abs, int32_t fit_mu, double lam_min_delta,
                 double* out, double* sigma_out, double* G_out);
 

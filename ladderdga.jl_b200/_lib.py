@@ -17,6 +17,7 @@ LDGA_OK, LDGA_ERR_ARG, LDGA_ERR_CUDA, LDGA_ERR_STATE = 0, 1, 2, 3
 LDGA_ERR_NUMERIC, LDGA_ERR_NOCONV, LDGA_ERR_TYPE = 4, 5, 6
 PREC_FP64_INV, PREC_FP64, PREC_MIXED = 0, 1, 2
 CH_M, CH_D = 0, 1
+SC_REDO_DM, SC_UPDATE_CHI_TAIL, SC_LAMBDA_TYPE = 1, 2, 4     # ldga_run_sc flags
 
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [

@@ -26,7 +26,8 @@ from typing import Callable
 import numpy as np
 
 from . import _lib
-from ._lib import CH_D, CH_M, PREC_FP64, PREC_FP64_INV, PREC_MIXED, Context, LdgaError, as_fc, ptr
+from ._lib import (CH_D, CH_M, PREC_FP64, PREC_FP64_INV, PREC_MIXED, SC_LAMBDA_TYPE, SC_REDO_DM,
+                   SC_UPDATE_CHI_TAIL, Context, LdgaError, as_fc, ptr)
 
 _CH = {"m": CH_M, "d": CH_D, ":m": CH_M, ":d": CH_D}
 
@@ -1209,7 +1210,47 @@ def λdm_vjp(h: lDΓAHelper, χm: χT, γm: γT, χd: χT, γd: γT, λ0, res: "
     Gmb, c0m = calc_χγ_vjp("m", h, xmb, gmb)
     Gdb, c0d = calc_χγ_vjp("d", h, xdb, gdb)
     slb, gb = gloc_vjp(h, c0m + c0d, l0b, SL + w[1] * SE, λm=lm, λd=ld, νmax=nu)
-    return {"Γ_m": Gmb, "Γ_d": Gdb, "Σ_loc": slb, "χ0": c0m + c0d, "λ0": l0b, "w": w, "J": J, "∂L/∂λ": dL}
+    # the EoM's tail term -U (sum_kω χm^λ - χloc_m_sum)/(iν_n) (ladderDGATools_singleCore.jl:133):
+    # ∂Σ(q, n)/∂χloc_m_sum = U/(iν_n), through L directly and through E_pot,1 of the λ condition
+    ivn = 1j * (2 * np.arange(nu) + 1) * math.pi / β
+    sbar_tot = SL + w[1] * SE
+    s_bar = float(np.real(np.sum(np.conj(sbar_tot) * (U / ivn)[None, :])))
+    out = {"Γ_m": Gmb, "Γ_d": Gdb, "Σ_loc": slb, "χ0": c0m + c0d, "λ0": l0b, "χloc_m_sum": s_bar,
+           "w": w, "J": J, "∂L/∂λ": dL}
+    out.update(local_vertex_vjp(h, Gmb, Gdb, l0b, s_bar))
+    return out
+
+
+def local_vertex_vjp(h: lDΓAHelper, Γ̄m, Γ̄d, λ̄0, χ̄loc_m_sum: float = 0.0) -> dict:
+    """The gradient continued from the lattice inputs to the local susceptibilities χ_loc,r = χDMFT_r
+    (setup_LDGA, runHelpers.jl:132-187): Γ_r = χ_loc,r⁻¹ - diag(1/χ₀,loc) per ω (the identity the local
+    Bethe-Salpeter step of the reference's setup reproduces), F_m = F_from_χ(χ_loc,m)
+    (BSETools.jl:40-53) through λ₀ = χ₀ Σ_ν F / β² (BSETools.jl:129-141), and χloc_m_sum = the tail-
+    corrected sum_ω of the local χ_m, whose ω-terms are Re Σ_νν' χ_loc,m / β².  G_imp is held fixed.
+        χ̄_loc,r = -χ_loc,r⁻ᴴ Γ̄_r χ_loc,r⁻ᴴ  (+ for m: conj(∂F/∂χ) F̄ + χ̄loc_m_sum / β³),
+        F̄[ν, ν', ω] = Σ_q conj(χ₀[q, ν', ω]) λ̄₀[q, ν', ω] / β².
+    For the synthetic inputs χ_loc,d = χ₀,loc + C and χ_loc,m = χ₀,loc - C, so C̄ = χ̄_loc,d - χ̄_loc,m.
+    Gradients use ā = ∂L/∂Re a + i ∂L/∂Im a."""
+    sP, β = h.sP, h.mP.β
+    Xm, Xd = as_fc(h.χDMFT_m), as_fc(h.χDMFT_d)
+    nnu, _, nw = Xm.shape
+    c0 = np.asarray(_fetch(h.ctx, "chi0"))
+    Fbar_col = np.einsum("qvw,qvw->vw", np.conj(c0), as_fc(λ̄0)) / β**2          # [ν', ω]
+    out_m = np.empty_like(Xm)
+    out_d = np.empty_like(Xd)
+    for wi in range(nw):
+        Ym, Yd = np.linalg.inv(Xm[:, :, wi]), np.linalg.inv(Xd[:, :, wi])
+        out_m[:, :, wi] = -Ym.conj().T @ as_fc(Γ̄m)[:, :, wi] @ Ym.conj().T
+        out_d[:, :, wi] = -Yd.conj().T @ as_fc(Γ̄d)[:, :, wi] @ Yd.conj().T
+        # F_m = -(χ + δ β g1 g2)/(g1 g2 g3 g4): ∂F/∂χ = -1/(g1 g2 g3 g4); F̄[ν, ν', ω] = Fbar_col[ν', ω]
+        g = np.empty((nnu, 2), dtype=np.complex128)
+        for vi in range(nnu):
+            wn, vn = OneToIndex_to_Freq(wi + 1, vi + 1, sP)
+            g[vi] = (h.gimp_at(vn), h.gimp_at(vn + wn))
+        den = (g[:, 0] * g[:, 1])[:, None] * (g[:, 0] * g[:, 1])[None, :]
+        out_m[:, :, wi] += np.conj(-1.0 / den) * Fbar_col[None, :, wi]
+    out_m += χ̄loc_m_sum / β**3
+    return {"χ_loc_m": out_m, "χ_loc_d": out_d, "C": out_d - out_m}
 
 
 def calc_Σ_parts(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, tc: bool = True, λm: float = 0.0,
@@ -1345,14 +1386,74 @@ def λm_correction_full(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHel
                     μnew, h.mP.n)
 
 
+def _λdm_sc_correction(χm, γm, χd, γd, λ0, h, νmax, λ_min_δ, λ_val_only, validate_threshold, atol, nsteps,
+                       sc_max_it, sc_mixing, sc_conv, update_χ_tail):
+    """``λdm_correction`` with sc_max_it > 0 (conditions_new.jl:272-283): every residual is the
+    self-consistent loop run_sc! at fixed (λm, λd) on the device (ldga_run_sc from the handle's G and
+    μ = mP.μ, at most sc_max_it iterations); the 2-D newton_right on the host."""
+    t = "dm_tsc" if update_χ_tail else "dm_sc"
+    nan = float("nan")
+    if update_χ_tail:
+        # residual_vals_sc λ-corrects χ before run_sc!, whose tail update then sums it with an external
+        # λ: the reference raises there for every λ != 0 (the FD Jacobian's first step), its
+        # newton_right call catches the error and the root is NaN (conditions_new.jl:292-300)
+        print("Error: χ already λ-corrected, but external λ provided!")
+        print("WARNING: No λ root was found!")
+        if λ_val_only:
+            return nan, nan, False
+        return λ_result(nan, nan, t, True, False)
+    _prepare_eom(h, χm, γm, χd, γd, λ0)
+    χm._device_λ()
+    χd._device_λ()
+    ctx = h.ctx
+    rhs_c1 = h.mP.n / 2 * (1 - h.mP.n / 2)
+    out = np.zeros(12)
+    nu_auto = min(h.sP.n_iν, math.floor(3 * len(usable_ωindices(h.sP, χm, χd)) / 8))
+    nu = nu_auto if νmax < 1 else min(nu_auto, νmax)
+    S = _lib.cplx_out((ctx.Nq, max(nu, 1)))
+    G = _lib.cplx_out((ctx.Nq, ctx.Nf))
+
+    def vals(lam, keep=False):
+        ctx.call("ldga_run_sc", float(lam[0]), float(lam[1]), 0, float(h.mP.μ), h.χloc_m_sum, int(νmax),
+                 int(sc_max_it), float(sc_mixing), float(sc_conv), 1, float(λ_min_δ), ptr(out),
+                 ptr(S) if keep else None, ptr(G) if keep else None)
+        return out.copy()
+
+    def residual(lam):
+        o = vals(lam)
+        return np.array([o[3] - rhs_c1, o[4] - o[5]])
+
+    lmin = np.array([get_λ_min(χm), get_λ_min(χd)])
+    xmin = lmin + λ_min_δ * np.abs(lmin)
+    try:
+        root = _newton_right_nd(residual, np.zeros(2), xmin, nsteps=nsteps, atol=atol)
+    except RuntimeError as e:
+        print(f"Error: {e}")
+        root = np.array([nan, nan])
+    if not np.all(np.isfinite(root)):
+        print("WARNING: No λ root was found!")
+        if λ_val_only:
+            return float(root[0]), float(root[1]), False
+        return λ_result(float(root[0]), float(root[1]), t, True, False)
+    o = vals(root, keep=True)
+    lhs_c1, ep1, ep2, ek, n, μ = o[3], o[4], o[5], o[6], o[7], o[8]
+    conv = abs(rhs_c1 - lhs_c1) <= validate_threshold and abs(ep1 - ep2) <= validate_threshold
+    if λ_val_only:
+        return float(root[0]), float(root[1]), conv
+    return λ_result(float(root[0]), float(root[1]), t, True, conv, ek, ep1, ep2, rhs_c1, lhs_c1, [], G, S[:, :nu],
+                    μ, n)
+
+
 def λdm_correction(χm: χT, γm: γT, χd: χT, γd: γT, λ0, h: lDΓAHelper, νmax: int = -1, λ_min_δ: float = 1e-4,
                    λ_val_only: bool = False, validate_threshold: float = 1e-8, atol: float = 1e-8,
-                   nsteps: int = 500, sc_max_it: int = 0, verbose: bool = False, par: bool = False, tc: bool = True):
+                   nsteps: int = 500, sc_max_it: int = 0, sc_mixing: float = 0.2, sc_conv: float = 1e-8,
+                   update_χ_tail: bool = False, verbose: bool = False, par: bool = False, tc: bool = True):
     """``λdm_correction`` plain branch (conditions_new.jl:207-324); the whole root search runs in the library."""
-    if sc_max_it > 0:
-        raise NotImplementedError("self-consistent λdm (run_sc!) is not built")
     if χm.λ != 0 or χd.λ != 0:
         raise RuntimeError("λ parameter already set. Aborting λdm calculation")
+    if sc_max_it > 0:
+        return _λdm_sc_correction(χm, γm, χd, γd, λ0, h, νmax, λ_min_δ, λ_val_only, validate_threshold, atol, nsteps,
+                                  sc_max_it, sc_mixing, sc_conv, update_χ_tail)
     _prepare_eom(h, χm, γm, χd, γd, λ0)
     χm._device_λ()
     χd._device_λ()
@@ -1413,8 +1514,10 @@ def run_sc(χm: χT, γm: γT, χd: χT, γd: γT, λ0, μ: float, h: lDΓAHelpe
     t = str(type).lstrip(":")
     if not fit_μ:
         warnings.warn("Not fitting μ can lead to unphysical results!")
-    if update_χ_tail:
-        raise NotImplementedError("run_sc: update_χ_tail = true (the χ tail update loop) is not built")
+    if update_χ_tail and t == "fix" and (λm != 0 or λd != 0):
+        # run_sc! sums the λ-corrected χ with the external λ = 0 of :fix after a tail update
+        # (conditions_new.jl:527-528, DataTypes.jl:216)
+        raise RuntimeError("χ already λ-corrected, but external λ provided!")
     if not tc:
         raise NotImplementedError("run_sc: the EoM of the loop uses the tail correction (tc = true)")
     if t not in ("fix", "m", "dm", "pre_m", "pre_dm"):
@@ -1441,7 +1544,9 @@ def run_sc(χm: χT, γm: γT, χd: χT, γd: γT, λ0, μ: float, h: lDΓAHelpe
     out = np.zeros(12)
     S = _lib.cplx_out((ctx.Nq, max(nu, 1)))
     G = _lib.cplx_out((ctx.Nq, ctx.Nf))
-    ctx.call("ldga_run_sc", float(λm), float(λd), int(t in ("dm", "pre_dm")), float(μ), h.χloc_m_sum, int(νmax),
+    flags = ((SC_REDO_DM if t in ("dm", "pre_dm") else 0) | (SC_UPDATE_CHI_TAIL if update_χ_tail else 0)
+             | (SC_LAMBDA_TYPE if t in ("m", "dm", "pre_m", "pre_dm") else 0))
+    ctx.call("ldga_run_sc", float(λm), float(λd), flags, float(μ), h.χloc_m_sum, int(νmax),
              int(maxit), float(mixing), float(conv_abs), int(bool(fit_μ)), float(λ_min_δ), ptr(out), ptr(S), ptr(G))
     lm, ld, rhs_c1, lhs_c1, ep1, ep2, ek, n, μr, scc = out[:10]
     if t == "fix":

@@ -1437,18 +1437,39 @@ __global__ void k_sigma_mix(double2* sigma, const double2* old, size_t n, double
 // Device buffers of one run_sc call, freed on every exit path.
 struct ScBuffers {
     double2 *sigma_old = nullptr, *ghat_save = nullptr, *gloc_save = nullptr;
+    double* chi_save = nullptr;   // update_χ_tail: both channels' chi, restored on return
     ~ScBuffers() {
         if (sigma_old) cudaFree(sigma_old);
         if (ghat_save) cudaFree(ghat_save);
         if (gloc_save) cudaFree(gloc_save);
+        if (chi_save) cudaFree(chi_save);
+    }
+};
+
+// The χ tail update of run_sc! changes the handle's chi data and the c2 tail coefficient (ModelParameters'
+// E_kin_DMFT, which the sums use); both are put back when the loop returns, also on errors.
+struct TailRestore {
+    ldga_ctx* ctx = nullptr;
+    double* chi_save = nullptr;
+    double ekin = 0.0;
+    ~TailRestore() {
+        if (!ctx) return;
+        const size_t n = (size_t)ctx->Nq * ctx->Nw;
+        cudaMemcpyAsync(ctx->d_chi[0], chi_save, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+        cudaMemcpyAsync(ctx->d_chi[1], chi_save + n, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->mp.Ekin_DMFT = ekin;
     }
 };
 }  // namespace
 
-int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t redo_dm, double mu, double chiloc_m_sum,
+int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t flags, double mu, double chiloc_m_sum,
                 int32_t numax, int32_t maxit, double mixing, double conv_abs, int32_t fit_mu, double lam_min_delta,
                 double* out, double* sigma_out, double* G_out) {
     if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    const bool redo_dm = (flags & LDGA_SC_REDO_DM) != 0;
+    const bool update_tail = (flags & LDGA_SC_UPDATE_CHI_TAIL) != 0;
+    const bool lam_types = (flags & LDGA_SC_LAMBDA_TYPE) != 0;
     TRY(eom_inputs_ready(ctx));
     NEED(ctx, ctx->d_sigma_loc != nullptr, "run_sc: Sigma_loc missing (call ldga_gloc)");
     NEED(ctx, ctx->have_ghat, "run_sc: G missing (call ldga_gloc or ldga_set_gloc)");
@@ -1481,11 +1502,22 @@ int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t redo_dm, doub
         *ep2 = (U / 2.0) * (r[1] - r[0]) + U * (nn / 2.0 * nn / 2.0);
         return LDGA_OK;
     };
+    TailRestore restore;
+    if (update_tail) {
+        const size_t nqw = (size_t)ctx->Nq * ctx->Nw;
+        TRY(dev_alloc(ctx, &b.chi_save, 2 * nqw));
+        TRY(copy(ctx, b.chi_save, ctx->d_chi[0], nqw * sizeof(double)));
+        TRY(copy(ctx, b.chi_save + nqw, ctx->d_chi[1], nqw * sizeof(double)));
+        restore.ctx = ctx;
+        restore.chi_save = b.chi_save;
+        restore.ekin = ctx->mp.Ekin_DMFT;
+    }
     double lhs_c1 = 0.0, E_pot_2 = 0.0, E_pot_1 = INFINITY, E_kin = INFINITY, n_fill = NAN;
     TRY(sums(&lhs_c1, &E_pot_2));
     bool converged = false;
-    int it = 1, iters = 0;
+    int it = 1, iters = 0, tail_it = 1;
     double r[4] = {mu, NAN, NAN, NAN};
+    for (;;) {   // χ tail updates (one pass without update_χ_tail)
     while (true) {
         if (it > 1 && redo_dm) {
             // λdm_correction on the current G transform, from the previous root (conditions_new.jl:431-436)
@@ -1535,6 +1567,25 @@ int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t redo_dm, doub
         }
         if (it >= maxit) break;
         it += 1;
+    }
+    if (!update_tail) break;
+    // conditions_new.jl:519-545: c2 = E_kin on both channels (update_tail!), the sum rules again, and
+    // a restarted loop (it = 1) unless they hold or 20 updates were made
+    if (!std::isfinite(E_kin)) {
+        E_pot_1 = NAN;
+    } else {
+        const double dc2 = E_kin - ctx->mp.Ekin_DMFT;
+        if (dc2 != 0.0) {
+            TRY(launch_chi_tail_shift(ctx, LDGA_CH_M, dc2));
+            TRY(launch_chi_tail_shift(ctx, LDGA_CH_D, dc2));
+            ctx->mp.Ekin_DMFT = E_kin;
+        }
+    }
+    TRY(sums(&lhs_c1, &E_pot_2));
+    if (tail_it >= 20 || (std::fabs(E_pot_1 - E_pot_2) < conv_abs && std::fabs(lhs_c1 - rhs_c1) < conv_abs)) break;
+    it = 1;
+    if (lam_types) { lm = 0.0; ld = 0.0; }   // run_sc! takes the first λ of a loop from χ.λ, 0 after a pass
+    tail_it += 1;
     }
     if (sigma_out) TRY(copy(ctx, sigma_out, ctx->d_sigma, nsig * sizeof(double2)));
     if (G_out) TRY(copy(ctx, G_out, ctx->d_gladder, ngf * sizeof(double2)));

@@ -707,6 +707,25 @@ int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_ou
     return LDGA_OK;
 }
 
+// update_tail! (DataTypes.jl:315-345) of the c2/(i w)^2 tail: chi[:, w] += Re((c2_new - c2_old)/(i w_m)^2)
+// = -(c2_new - c2_old)/w_m^2 for every w_m = 2 pi m / beta != 0.
+__global__ void k_chi_tail_shift(int nq, int nw, int n_iw, double beta, double dc2, double* __restrict__ chi) {
+    const size_t total = (size_t)nq * nw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(e / nq) - n_iw;
+        if (m == 0) continue;
+        const double wm = 2.0 * M_PI * (double)m / beta;
+        chi[e] -= dc2 / (wm * wm);
+    }
+}
+
+int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2) {
+    k_chi_tail_shift<<<2 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nw, ctx->sp.n_iw, ctx->mp.beta, dc2,
+                                                      ctx->d_chi[channel]);
+    LDGA_LAUNCHED(ctx, "k_chi_tail_shift");
+    return LDGA_OK;
+}
+
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
     const int w0 = (ctx->Nw + 1) / 2 - 1;   // ω0_index = ceil(Nw/2), 1-based
     StageTimer st_(ctx, LDGA_STAGE_SUMS);

@@ -233,6 +233,7 @@ int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const doubl
                double2* out, int out_ld, int add_hartree);
 int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev = nullptr);
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
+int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2);
 // newton_right's defaults (LambdaCorrection/helpers.jl:133): nsteps 100, atol 1e-13
 int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out /*[5]*/,
                     int nsteps = 100, double atol = 1e-13);

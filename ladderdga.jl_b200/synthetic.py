@@ -118,8 +118,12 @@ def _freq(w_i: int, v_i: int, n_iw: int, n_iv: int, shift: bool):
 
 
 def make_input(dim: int, ns: int, beta: float, U: float, n_iv: int, n_iw: int, seed: int,
-               t: float = 1.0, shift: bool = False) -> SyntheticInput:
-    """Build the seeded local inputs for one parameter point."""
+               t: float = 1.0, shift: bool = False, C_add=None) -> SyntheticInput:
+    """Build the seeded local inputs for one parameter point.
+
+    C_add ([Nnu, Nnu, Nw] complex, optional) is added to the symmetrised vertex noise C before the
+    local susceptibilities and vertices are formed (a perturbation for gradient checks with respect to
+    C); the C used is returned in ``tags["C"]``."""
     mu = U / 2.0
     nden = 1.0
     L = 2 * (n_iv + n_iw)
@@ -151,6 +155,8 @@ def make_input(dim: int, ns: int, beta: float, U: float, n_iv: int, n_iw: int, s
     dv = np.abs(vn_tab[:, None, :] - vn_tab[None, :, :]).astype(np.float64)
     C = g * (U / beta**2) / (1.0 + dv)
     C = 0.5 * (C + np.conj(np.transpose(C, (1, 0, 2))))
+    if C_add is not None:
+        C = C + np.asarray(C_add, dtype=np.complex128).reshape(C.shape, order="F")
 
     chi_m = np.zeros((nnu, nnu, nw), dtype=np.complex128, order="F")
     chi_d = np.zeros((nnu, nnu, nw), dtype=np.complex128, order="F")
@@ -181,7 +187,7 @@ def make_input(dim: int, ns: int, beta: float, U: float, n_iv: int, n_iw: int, s
     return SyntheticInput(dim=dim, ns=ns, t=t, beta=beta, U=U, mu=mu, n=nden, n_iw=n_iw,
                           n_iv=n_iv, shift=shift, Ekin_DMFT=Ekin, Epot_DMFT=0.0, sVk=sVk,
                           sigma_loc=sigma_loc, gimp=gimp, chi_loc_m=chi_m, chi_loc_d=chi_d,
-                          gamma_m=gam_m, gamma_d=gam_d, seed=seed)
+                          gamma_m=gam_m, gamma_d=gam_d, seed=seed, tags={"C": C})
 
 
 # The five benchmark configurations (lattice, temperature, coupling, frequency box).

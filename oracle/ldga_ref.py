@@ -1136,12 +1136,93 @@ def lambda_dm_correction(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, h:
                         None, None, float("nan"), float("nan"))
 
 
+def _sc_loop(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, mu: float, h: Helper, lm: float, ld: float,
+             lam_types: bool, redo_dm: bool, numax: int, maxit: int, mixing: float, conv_abs: float, fit_mu: bool,
+             update_chi_tail: bool):
+    """The loop of ``run_sc!`` (conditions_new.jl:409-556) on deep copies of chi and G: EoM at (lm, ld)
+    -> mixing -> G_from_Σladder! (μ fit) -> calc_E -> G_rfft! (the next EoM's G transform), until both
+    potential energies change by less than conv_abs or maxit iterations; :dm types (redo_dm) re-solve
+    λdm from the second iteration.  With update_chi_tail the finished loop is followed by the χ tail
+    update (update_tail! with c2 = E_kin on both channels) and restarted (it = 1) until the sum rules
+    hold to conv_abs or 20 tail updates (conditions_new.jl:519-545).  lam_types: run_sc! takes the λ of
+    its first iteration from χ.λ (types :m, :dm, :pre_m, :pre_dm), which is 0 after the first pass, so
+    a restarted loop begins at λ = 0 there; for :fix the given λ stays.
+    Returns (λm, λd, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n, μ, converged, it, Σ, G)."""
+    import dataclasses
+    mP, kG, sP = h.mP, h.kG, h.sP
+    off = -sP.fft_range[0]
+    grhat = h.grhat
+    xm, xd = chi_m.copy(), chi_d.copy()
+    wgrid = xm.wn_grid()
+    S = np.zeros((kG.Nq, numax), dtype=np.complex128)
+    G = None
+    rhs_c1 = mP.n / 2 * (1 - mP.n / 2)
+
+    def sums(lm_, ld_):
+        cm, cd = xm.copy(), xd.copy()
+        chi_lambda_inplace(cm, lm_)
+        chi_lambda_inplace(cd, ld_)
+        a, b = sum_kw(kG, cm), sum_kw(kG, cd)
+        return (b + a) / 2, (mP.U / 2) * (b - a) + mP.U * (mP.n / 2 * mP.n / 2)
+
+    lhs_c1, E_pot_2 = sums(lm, ld)
+    E_pot_1, E_kin, n = np.inf, np.inf, float("nan")
+    converged = False
+    it = 1
+    tail_it = 1
+    while True:
+        while True:
+            if it > 1 and redo_dm:
+                hc = dataclasses.replace(h, grhat=grhat)
+                r = lambda_dm_correction(xm, gamma_m, xd, gamma_d, lambda0, hc, numax=numax, lam_min_delta=1e-4,
+                                         lam_init=(lm, ld), mu0=mu)
+                lm, ld, mu = r.lam_m, r.lam_d, r.mu
+                if not (np.isfinite(lm) and np.isfinite(ld)):
+                    break
+            S_work = S.copy()
+            cm, cd = xm.copy(), xd.copy()
+            chi_lambda_inplace(cm, lm)
+            chi_lambda_inplace(cd, ld)
+            S = calc_Sigma_inner(cm, gamma_m, cd, gamma_d, h.chiloc_m_sum, lambda0, grhat, kG, mP, sP, numax, True)
+            if mixing != 0 and it > 1:
+                S = (1 - mixing) * S + mixing * S_work
+            mu, G = G_from_Sigma_ladder(S, h.sigma_loc, kG, mP, sP.fft_range, fix_n=fit_mu, mu=mu)
+            if np.isnan(mu):
+                break
+            E_pot_1_old, E_pot_2_old = E_pot_1, E_pot_2
+            E_kin, E_pot_1 = calc_E(G[:, off:off + numax], S, mu, kG, mP)
+            n = filling_pos(kG.kintegrate(G[:, off:off + numax], 0), mP.U, mu, mP.beta)
+            _, grhat = G_fft(kG, G)
+            lhs_c1, E_pot_2 = sums(lm, ld)
+            if abs(E_pot_1 - E_pot_1_old) < conv_abs and abs(E_pot_2 - E_pot_2_old) < conv_abs:
+                converged = True
+                break
+            if it >= maxit:
+                break
+            it += 1
+        if not update_chi_tail:
+            break
+        if not np.isfinite(E_kin):
+            E_pot_1 = float("nan")
+        else:
+            update_tail(xm, [0, 0, E_kin], wgrid)
+            update_tail(xd, [0, 0, E_kin], wgrid)
+        lhs_c1, E_pot_2 = sums(lm, ld)
+        if tail_it >= 20 or (abs(E_pot_1 - E_pot_2) < conv_abs and abs(lhs_c1 - rhs_c1) < conv_abs):
+            break
+        it = 1
+        if lam_types:
+            lm, ld = 0.0, 0.0
+        tail_it += 1
+    return lm, ld, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n, mu, converged, it, S, G
+
+
 def run_sc(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, mu: float, h: Helper, type: str = "fix",
            lam_m: float = 0.0, lam_d: float = 0.0, numax: int = -1, maxit: int = 100, mixing: float = 0.2,
-           conv_abs: float = 1e-8, fit_mu: bool = True, lam_min_delta: float = 1e-4) -> LambdaResult:
-    """``run_sc`` (conditions_new.jl:342-407) and its loop ``run_sc!`` (:409-556), update_χ_tail = false,
-    tc = true.  Returns the reference's λ_result (its positional order: converged <- sc_converged)."""
-    import dataclasses
+           conv_abs: float = 1e-8, fit_mu: bool = True, lam_min_delta: float = 1e-4,
+           update_chi_tail: bool = False) -> LambdaResult:
+    """``run_sc`` (conditions_new.jl:342-407) with its loop ``run_sc!`` (:409-556), tc = true.  Returns
+    the reference's λ_result (its positional order: converged <- sc_converged)."""
     mP, kG, sP = h.mP, h.kG, h.sP
     wind, nu_auto = gen_nu_w_indices(chi_m, chi_d, mP, sP)
     numax = nu_auto if numax < 1 else min(nu_auto, numax)
@@ -1158,54 +1239,12 @@ def run_sc(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, mu: float, h: He
     nan = float("nan")
     if not (valid and np.isfinite(lam_m) and np.isfinite(lam_d)):
         return LambdaResult(nan, nan, type, False, False, nan, nan, nan, nan, nan, None, None, nan, nan)
-    redo_dm = type in ("dm", "pre_dm")
-    off = -sP.fft_range[0]
-    grhat = h.grhat
-    S = np.zeros((kG.Nq, numax), dtype=np.complex128)
-    G = None
-    rhs_c1 = mP.n / 2 * (1 - mP.n / 2)
-
-    def sums(lm, ld):
-        cm, cd = chi_m.copy(), chi_d.copy()
-        chi_lambda_inplace(cm, lm)
-        chi_lambda_inplace(cd, ld)
-        xm, xd = sum_kw(kG, cm), sum_kw(kG, cd)
-        return (xd + xm) / 2, (mP.U / 2) * (xd - xm) + mP.U * (mP.n / 2 * mP.n / 2)
-
-    lm, ld = lam_m, lam_d
-    lhs_c1, E_pot_2 = sums(lm, ld)
-    E_pot_1, E_kin, n = np.inf, np.inf, nan
-    converged = False
-    it = 1
-    while True:
-        if it > 1 and redo_dm:
-            hc = dataclasses.replace(h, grhat=grhat)
-            r = lambda_dm_correction(chi_m, gamma_m, chi_d, gamma_d, lambda0, hc, numax=numax,
-                                     lam_min_delta=1e-4, lam_init=(lm, ld), mu0=mu)
-            lm, ld, mu = r.lam_m, r.lam_d, r.mu
-            if not (np.isfinite(lm) and np.isfinite(ld)):
-                break
-        S_work = S.copy()
-        cm, cd = chi_m.copy(), chi_d.copy()
-        chi_lambda_inplace(cm, lm)
-        chi_lambda_inplace(cd, ld)
-        S = calc_Sigma_inner(cm, gamma_m, cd, gamma_d, h.chiloc_m_sum, lambda0, grhat, kG, mP, sP, numax, True)
-        if mixing != 0 and it > 1:
-            S = (1 - mixing) * S + mixing * S_work
-        mu, G = G_from_Sigma_ladder(S, h.sigma_loc, kG, mP, sP.fft_range, fix_n=fit_mu, mu=mu)
-        if np.isnan(mu):
-            break
-        E_pot_1_old, E_pot_2_old = E_pot_1, E_pot_2
-        E_kin, E_pot_1 = calc_E(G[:, off:off + numax], S, mu, kG, mP)
-        n = filling_pos(kG.kintegrate(G[:, off:off + numax], 0), mP.U, mu, mP.beta)
-        _, grhat = G_fft(kG, G)
-        lhs_c1, E_pot_2 = sums(lm, ld)
-        if abs(E_pot_1 - E_pot_1_old) < conv_abs and abs(E_pot_2 - E_pot_2_old) < conv_abs:
-            converged = True
-            break
-        if it >= maxit:
-            break
-        it += 1
+    if update_chi_tail and type == "fix" and (lam_m != 0 or lam_d != 0):
+        # run_sc! sums the λ-corrected χ with the external λ = 0 of :fix after the tail update
+        raise RuntimeError("χ already λ-corrected, but external λ provided!")
+    lm, ld, rhs_c1, lhs_c1, E_pot_1, E_pot_2, E_kin, n, mu, converged, it, S, G = _sc_loop(
+        chi_m, gamma_m, chi_d, gamma_d, lambda0, mu, h, lam_m, lam_d, type in ("m", "dm", "pre_m", "pre_dm"),
+        type in ("dm", "pre_dm"), numax, maxit, mixing, conv_abs, fit_mu, update_chi_tail)
     if type == "fix":
         lm, ld = 0.0, 0.0      # run_sc! returns its loop-local λ, never set for :fix
     conv = (converged and np.isfinite(lhs_c1) and np.isfinite(E_pot_2) and abs(rhs_c1 - lhs_c1) <= conv_abs
@@ -1214,6 +1253,45 @@ def run_sc(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, mu: float, h: He
                        rhs_c1, float(lhs_c1), G, S, float(mu), float(n))
     res.iterations = it
     return res
+
+
+def lambda_dm_sc_correction(chi_m: ChiT, gamma_m, chi_d: ChiT, gamma_d, lambda0, h: Helper, sc_max_it: int,
+                            sc_mixing: float = 0.2, sc_conv: float = 1e-8, numax: int = -1,
+                            lam_min_delta: float = 1e-4, validate_threshold: float = 1e-8, atol: float = 1e-8,
+                            nsteps: int = 500) -> LambdaResult:
+    """``λdm_correction`` with sc_max_it > 0 (conditions_new.jl:272-283, 290-324): every residual is the
+    self-consistent loop ``run_sc!`` at fixed (λm, λd), from the handle's G and μ = mP.μ, with at most
+    sc_max_it iterations; the root of [PP_2 - n/2(1 - n/2), E_pot,1 - E_pot,2] by the 2-D newton_right."""
+    if chi_m.lam != 0 or chi_d.lam != 0:
+        raise RuntimeError("λ parameter already set. Aborting λdm calculation")
+    mP = h.mP
+    wind, nu_auto = gen_nu_w_indices(chi_m, chi_d, mP, h.sP)
+    numax = nu_auto if numax < 1 else min(nu_auto, numax)
+    rhs_c1 = mP.n / 2 * (1 - mP.n / 2)
+
+    def vals(lam):
+        return _sc_loop(chi_m, gamma_m, chi_d, gamma_d, lambda0, mP.mu, h, float(lam[0]), float(lam[1]), False,
+                        False, numax, sc_max_it, sc_mixing, sc_conv, True, False)
+
+    def residual_f(lam):
+        r = vals(lam)
+        return np.array([r[3] - rhs_c1, r[4] - r[5]])
+
+    lmt = get_lambda_min(chi_m.data)
+    ldt = get_lambda_min(chi_d.data)
+    xmin = np.array([lmt + lam_min_delta * abs(lmt), ldt + lam_min_delta * abs(ldt)])
+    try:
+        root = newton_right_nd(residual_f, np.array([0.0, 0.0]), xmin, nsteps=nsteps, atol=atol)
+    except RuntimeError:
+        root = np.array([np.nan, np.nan])
+    nan = float("nan")
+    if not np.all(np.isfinite(root)):
+        return LambdaResult(float(root[0]), float(root[1]), "dm_sc", True, False, nan, nan, nan, nan, nan, None,
+                            None, nan, nan)
+    lm, ld, rhs_c1, lhs_c1, ep1, ep2, ek, n, mu, sc_conv_, it, S, G = vals(root)
+    conv = abs(rhs_c1 - lhs_c1) <= validate_threshold and abs(ep1 - ep2) <= validate_threshold
+    return LambdaResult(float(root[0]), float(root[1]), "dm_sc", True, conv, ek, ep1, ep2, rhs_c1, lhs_c1, G, S,
+                        mu, n)
 
 
 # =============================================================================================

@@ -469,6 +469,63 @@ def test_run_sc(sc_type, require_gpu):
     assert rel(s1, s0) < RTOL
 
 
+@pytest.mark.parametrize("sc_type,lam", [("fix", None), ("m", (0.3, 0.0)), ("pre_m", None), ("pre_dm", None)])
+def test_run_sc_update_chi_tail(sc_type, lam, require_gpu):
+    """run_sc with update_χ_tail = true (conditions_new.jl:519-556): after each converged loop the χ tails
+    take c2 = E_kin (update_tail!, DataTypes.jl:315-345) and the loop restarts until the sum rules hold or
+    20 updates; against the oracle's loop.  The handle's χ and tail coefficient are unchanged afterwards."""
+    inp = S.make_input(dim=3, ns=8, beta=5.0, U=1.2, n_iv=4, n_iw=4, seed=77)
+    ref = R.run_chain(inp, lambda_type=None)
+    r = ref["h"]
+    g = gpu_chain(inp)
+    h = g["h"]
+    kw = dict(maxit=25, mixing=0.2, conv_abs=1e-8)
+    lk = dict(λm=lam[0], λd=lam[1]) if lam else {}
+    chi_before = np.array(g["chi_m"].data)
+    res = L.run_sc(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], h.mP.μ, h, type=sc_type,
+                   update_χ_tail=True, **lk, **kw)
+    o = R.run_sc(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"], r.mP.mu, r, type=sc_type,
+                 lam_m=lam[0] if lam else 0.0, lam_d=lam[1] if lam else 0.0, update_chi_tail=True, **kw)
+    assert res.converged == o.converged and res.sc_converged == o.sc_converged
+    tol = 1e-8 if sc_type != "pre_dm" else 1e-5
+    assert abs(res.λm - o.lam_m) < tol and abs(res.λd - o.lam_d) < tol
+    if math.isfinite(o.mu):
+        assert abs(res.μ - o.mu) < tol
+        assert rel(res.Σ_ladder, o.Sigma_ladder) < tol
+        for a, b in ((res.EPot_p1, o.EPot_p1), (res.EPot_p2, o.EPot_p2), (res.PP_p2, o.PP_p2), (res.EKin, o.EKin)):
+            assert abs(a - b) <= tol * max(1.0, abs(b)), (a, b)
+    # the tail update worked on the loop's own copy: χ and the sums of the handle are as before
+    x = np.empty_like(chi_before, order="F")
+    h.ctx.call("ldga_get", L._lib.GET_CHI, L.CH_M, L._lib.ptr(x))
+    assert np.array_equal(x, chi_before)
+    assert abs(L.sum_kω(h.kG, g["chi_m"]) - R.sum_kw(r.kG, ref["chi_m"])) < 1e-10
+    if sc_type == "fix":
+        with pytest.raises(RuntimeError, match="λ-corrected"):
+            L.run_sc(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], h.mP.μ, h, type="fix",
+                     λm=0.2, update_χ_tail=True, **kw)
+
+
+def test_lambda_dm_sc(require_gpu):
+    """λdm_correction with sc_max_it > 0 (conditions_new.jl:272-283): every residual of the 2-D Newton is
+    the self-consistent loop at fixed λ; against the oracle's restatement."""
+    inp = S.make_input(dim=3, ns=8, beta=5.0, U=1.2, n_iv=4, n_iw=4, seed=77)
+    ref = R.run_chain(inp, lambda_type=None)
+    g = gpu_chain(inp)
+    res = L.λdm_correction(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], g["h"], sc_max_it=10)
+    o = R.lambda_dm_sc_correction(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"], ref["h"],
+                                  sc_max_it=10)
+    assert res.type == "dm_sc" and res.sc_converged == o.sc_converged
+    # the Newton stops at |F| < 1e-8 on both sides: λ is determined to ~1e-8
+    assert abs(res.λm - o.lam_m) < 1e-7 and abs(res.λd - o.lam_d) < 1e-7
+    if o.sc_converged:
+        assert abs(res.PP_p2 - 0.25) < 1e-8 and abs(res.EPot_p1 - res.EPot_p2) < 1e-8
+        assert rel(res.Σ_ladder, o.Sigma_ladder) < 1e-6
+    # update_χ_tail = true there: the reference's residual raises for every λ != 0 and returns NaN
+    nan_res = L.λdm_correction(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], g["h"],
+                               sc_max_it=10, update_χ_tail=True)
+    assert math.isnan(nan_res.λm) and not nan_res.sc_converged
+
+
 def _cgauss(rng, shape):
     return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
 
@@ -736,3 +793,46 @@ def test_lambda_dm_vjp(require_gpu):
         an = float(np.sum(np.real(np.conj(grad[key]) * d)))
         assert abs(fd - an) <= 1e-5 * np.sum(np.abs(grad[key]) * np.abs(d)), (key, fd, an)
     forward(Gm0, sig0)
+
+
+def test_lambda_dm_vjp_local_vertex(require_gpu):
+    """Configuration 4's loss L = Σ_k,ν |Σ_ladder|² + E_pot,1 after the λdm correction, differentiated with
+    respect to the synthetic vertex noise C (χ_loc,d = χ₀,loc + C, χ_loc,m = χ₀,loc - C): through Γ_r
+    = χ_loc,r⁻¹ - diag(1/χ₀,loc), F_m (λ₀) and χloc_m_sum, with the implicit dependence of (λm, λd).
+    Against central differences of the GPU chain re-solved at every point (λdm to a residual of 1e-12)
+    and of the oracle's FP64 chain (the reference path's directional gradient)."""
+    base = dict(dim=3, ns=8, beta=5.0, U=1.2, n_iv=4, n_iw=4, seed=77)
+    rng = np.random.default_rng(16)
+
+    def forward(dC=None):
+        inp = S.make_input(**base, C_add=dC)
+        h = L.setup_synthetic(inp)
+        chi0 = L.calc_bubble(h)
+        xm, gm = L.calc_χγ("m", h, chi0)
+        xd, gd = L.calc_χγ("d", h, chi0)
+        l0 = L.calc_λ0(chi0, h)
+        res = L.λdm_correction(xm, gm, xd, gd, l0, h, atol=1e-12, nsteps=500)
+        loss = float(np.sum(h.ctx.kmult[:, None] * np.abs(res.Σ_ladder) ** 2) + res.EPot_p1)
+        return loss, (h, xm, gm, xd, gd, l0, res, inp)
+
+    def oracle_loss(dC):
+        inp = S.make_input(**base, C_add=dC)
+        ref = R.run_chain(inp, lambda_type=None)
+        r = R.lambda_dm_correction(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"],
+                                   ref["h"], atol=1e-12)
+        return float(np.sum(ref["h"].kG.kMult[:, None] * np.abs(r.Sigma_ladder) ** 2) + r.EPot_p1)
+
+    L0, (h, xm, gm, xd, gd, l0, res, inp) = forward()
+    assert res.sc_converged
+    grad = L.λdm_vjp(h, xm, gm, xd, gd, l0, res, Σ̄=2.0 * h.ctx.kmult[:, None] * res.Σ_ladder, Ē=1.0)
+    C0 = inp.tags["C"]
+    for k in range(3):
+        d = _cgauss(rng, C0.shape)
+        eps = 1e-6 * np.max(np.abs(C0)) / np.max(np.abs(d))
+        fd = (forward(eps * d)[0] - forward(-eps * d)[0]) / (2 * eps)
+        an = float(np.sum(np.real(np.conj(grad["C"]) * d)))
+        assert abs(fd - an) <= 1e-5 * np.sum(np.abs(grad["C"]) * np.abs(d)), (k, fd, an)
+        if k == 0:
+            eps_o = 1e-5 * np.max(np.abs(C0)) / np.max(np.abs(d))
+            fd_o = (oracle_loss(eps_o * d) - oracle_loss(-eps_o * d)) / (2 * eps_o)
+            assert abs(fd_o - an) <= 1e-5 * np.sum(np.abs(grad["C"]) * np.abs(d)), (fd_o, an)
