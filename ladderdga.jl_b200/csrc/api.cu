@@ -1,6 +1,7 @@
 // C ABI of libldga_b200 (declarations and reference citations in include/ldga_b200.h).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -353,6 +354,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     if (device < 0 || device >= ndev) return ctx_fail(nullptr, LDGA_ERR_ARG, "device index out of range");
     ldga_ctx* c = new (std::nothrow) ldga_ctx();
     if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
+    if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "cuda") != 0;
     DeviceGuard g(device);
     c->device = device;
     c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;

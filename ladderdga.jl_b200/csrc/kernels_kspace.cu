@@ -11,12 +11,14 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr size_t kSmemBudget = 200 * 1024;
+// the tensor-path transform kernels run two CTAs per SM: half the shared memory each
+constexpr size_t kSmemBudgetTC = 110 * 1024;
 
 template <int DIM, int M>
-int pairs_per_cta(int total) {
+int pairs_per_cta(int total, size_t budget = kSmemBudget) {
     using S = TransformSmem<DIM, M>;
     const size_t per = (size_t)(S::BUF_A + S::BUF_B) * sizeof(double2);
-    int np = (int)(kSmemBudget / per);
+    int np = (int)(budget / per);
     if (np > 16) np = 16;
     // batch vectors into a CTA only when there are more vectors than SMs: a short list (the EoM
     // inverse's numax vectors) runs one vector per CTA on as many SMs
@@ -43,8 +45,8 @@ TMat<M> make_T(const ldga_ctx* ctx) {
 // ---------------------------------------------------------------------------------------------
 // a1: G(k, nu) for nu in fft_range and Ghat = S(G)
 // ---------------------------------------------------------------------------------------------
-template <int DIM, int M>
-__global__ void __launch_bounds__(kThreads) k_gloc_transform(
+template <int DIM, int M, bool TC>
+__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_gloc_transform(
     const TMat<M> T, int nf, int fft_lo, double beta, double mu, const double* __restrict__ eps,
     const double2* __restrict__ sigma_loc, int n_sigma, double2* __restrict__ gloc, int from_sigma,
     double2* __restrict__ ghat, int np_max) {
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(kThreads) k_gloc_transform(
         bufA[p * NQ + q] = g;
     }
     __syncthreads();
-    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+    sym_transform_any<DIM, M, TC>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
         ghat[(size_t)(p0 + p) * NQ + q] = v;
     });
 }
@@ -83,8 +85,8 @@ __global__ void __launch_bounds__(kThreads) k_gloc_transform(
 // and a pair whose partner lies in the box is computed once: `pairs` lists the representatives
 // (pair index vi + Nnu wi, partner's index or -1), built on the host with the handle.
 // ---------------------------------------------------------------------------------------------
-template <int DIM, int M>
-__global__ void __launch_bounds__(kThreads) k_bubble(
+template <int DIM, int M, bool TC>
+__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_bubble(
     const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double scale,
     const double2* __restrict__ ghat, const int2* __restrict__ pairs, int total, double2* __restrict__ chi0, int np_max) {
     using S = TransformSmem<DIM, M>;
@@ -105,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) k_bubble(
         bufA[p * NQ + q] = cmul(a, b);
     }
     __syncthreads();
-    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+    sym_transform_any<DIM, M, TC>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
         const int2 pp = pairs[p0 + p];
         const double2 c = cscale(v, scale);
         chi0[(size_t)pp.x * NQ + q] = c;
@@ -165,8 +167,8 @@ __device__ __forceinline__ double2 eom_value(const EomArgs& a, double2 gm, doubl
     }
 }
 
-template <int DIM, int M>
-__global__ void __launch_bounds__(kThreads) k_eom_forward(
+template <int DIM, int M, bool TC>
+__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_eom_forward(
     const TMat<M> T, const EomArgs a, const double2* __restrict__ ghat, const double* __restrict__ chi_m,
     const double2* __restrict__ gam_m, const double* __restrict__ chi_d, const double2* __restrict__ gam_d,
     const double2* __restrict__ lambda0, double2* __restrict__ partial) {
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) k_eom_forward(
         bufA[p * NQ + q] = K;
     }
     __syncthreads();
-    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+    sym_transform_any<DIM, M, TC>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
         const int wi = w0 + p;
         const int wn = wi - a.n_iw;
         double2 r = make_double2(0.0, 0.0);
@@ -221,8 +223,8 @@ __global__ void __launch_bounds__(kThreads) k_eom_forward(
     }
 }
 
-template <int DIM, int M>
-__global__ void __launch_bounds__(kThreads) k_eom_inverse(
+template <int DIM, int M, bool TC>
+__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_eom_inverse(
     const TMat<M> T, int numax, int nchunk, double scale, double beta, double U, double hartree,
     const double* __restrict__ tail_sum, int tc, double chiloc_m_sum, const double2* __restrict__ partial,
     double2* __restrict__ out, int out_ld, int add_hartree, int np_max) {
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) k_eom_inverse(
     __syncthreads();
     // tail: (tc ? -U (sum_kω χm - χloc_m_sum) : 0) / (i ν_n), ν_n = (2n+1)π/β
     const double tnum = tc ? -U * (tail_sum[0] - chiloc_m_sum) : 0.0;
-    sym_transform<DIM, M>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
+    sym_transform_any<DIM, M, TC>(np, bufA, bufB, T, [&](int p, int q, double2 v) {
         const int nu = p0 + p;
         const double w = (2.0 * nu + 1.0) * M_PI / beta;
         // tnum / (i w) = -i tnum / w
@@ -544,9 +546,10 @@ __global__ void __launch_bounds__(256) k_sigma_loc_grad(int nq, int nf, int fft_
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M>
 int run_gloc(ldga_ctx* ctx, bool from_sigma) {
-    const int np = pairs_per_cta<DIM, M>(ctx->Nf);
+    const bool tc = ctx->transform_tc;
+    const int np = pairs_per_cta<DIM, M>(ctx->Nf, tc ? kSmemBudgetTC : kSmemBudget);
     const size_t sm = smem_bytes<DIM, M>(np);
-    auto kern = k_gloc_transform<DIM, M>;
+    auto kern = tc ? k_gloc_transform<DIM, M, true> : k_gloc_transform<DIM, M, false>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((ctx->Nf + np - 1) / np);
     StageTimer st_(ctx, LDGA_STAGE_GLOC);
@@ -560,9 +563,10 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
 template <int DIM, int M>
 int run_bubble(ldga_ctx* ctx) {
     const int total = ctx->n_bub_pairs;
-    const int np = pairs_per_cta<DIM, M>(total);
+    const bool tc = ctx->transform_tc;
+    const int np = pairs_per_cta<DIM, M>(total, tc ? kSmemBudgetTC : kSmemBudget);
     const size_t sm = smem_bytes<DIM, M>(np);
-    auto kern = k_bubble<DIM, M>;
+    auto kern = tc ? k_bubble<DIM, M, true> : k_bubble<DIM, M, false>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((total + np - 1) / np);
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
@@ -579,7 +583,8 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
             int part, int& nchunk_out) {
     using S = TransformSmem<DIM, M>;
     const size_t per = (size_t)(S::BUF_A + S::BUF_B + S::NQ) * sizeof(double2);
-    int wpc = (int)(kSmemBudget / per);
+    const bool tc = ctx->transform_tc;
+    int wpc = (int)((tc ? kSmemBudgetTC : kSmemBudget) / per);
     if (wpc > 16) wpc = 16;
     if (wpc < 1) wpc = 1;
     // spread the w axis over enough CTAs to fill the machine
@@ -599,7 +604,7 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
     a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = part;
     a.lam_m_dev = lm_dev; a.lam_d_dev = ld_dev;
     const size_t sm = (size_t)wpc * per;
-    auto kern = k_eom_forward<DIM, M>;
+    auto kern = tc ? k_eom_forward<DIM, M, true> : k_eom_forward<DIM, M, false>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid(nchunk, numax);
     StageTimer st_(ctx, LDGA_STAGE_EOM_FORWARD);
@@ -613,9 +618,10 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
 template <int DIM, int M>
 int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, int tc, double chiloc_m_sum,
                     double2* out, int out_ld, int add_hartree) {
-    const int np = pairs_per_cta<DIM, M>(numax);
+    const bool ttc = ctx->transform_tc;
+    const int np = pairs_per_cta<DIM, M>(numax, ttc ? kSmemBudgetTC : kSmemBudget);
     const size_t sm = smem_bytes<DIM, M>(np);
-    auto kern = k_eom_inverse<DIM, M>;
+    auto kern = ttc ? k_eom_inverse<DIM, M, true> : k_eom_inverse<DIM, M, false>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((numax + np - 1) / np);
     const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);

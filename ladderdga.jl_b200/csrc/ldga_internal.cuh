@@ -132,6 +132,10 @@ struct ldga_ctx {
     int64_t graph_launches = 0;                  // kernels per replay of the captured graph
     double* h_stage = nullptr;     // pinned host staging for the chain's scalars (64 doubles + 4 ints)
 
+    // k-space transforms of the G setup, bubble and EoM on the FP64 tensor path (mma.sync m8n8k4);
+    // false: the CUDA-core form (environment LDGA_TRANSFORM=cuda at ldga_create, for comparisons)
+    bool transform_tc = true;
+
     // stage timing (ldga_profile / ldga_stage_times)
     bool profiling = false;
     uint32_t prof_mask = 0;       // stages whose events are recorded while profiling (bit = stage)

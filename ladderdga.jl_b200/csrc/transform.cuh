@@ -128,6 +128,151 @@ __device__ void sym_transform(int np, double2* bufA, double2* bufB, const TMat<M
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// The same transform on the FP64 tensor path.  Every stage is T times a set of columns, T fixed: with
+// mma.sync.m8n8k4 (FP64 operands, FP64 accumulation) T is the A operand, kept in registers as
+// fragments of its 8 x 4 tiles (rows and k padded with zeros to multiples of 8 and 4), and the
+// columns -- real and imaginary parts of 4 complex columns per 8-column tile -- are the B operand,
+// gathered from shared memory (lane l holds B[k = l % 4][n = l / 4], n = 2 j + part of complex column
+// j).  The accumulator gives lane l the complex output of row l / 4, column l % 4 (C[g][2t], C[g][2t+1]
+// are its real and imaginary parts).  Warps take 8-column tiles in turn; a tile computes only the
+// row tiles its columns need (stage y: qy <= qx, stage z: qz <= qy).  One tensor instruction replaces
+// 256 FP64 FMAs, and no thread holds a column in registers (the CUDA-core form keeps M complex values
+// per thread), so the kernels need far fewer registers.
+template <int M>
+struct TFrag {
+    static constexpr int RT = (M + 7) / 8, KT = (M + 3) / 4;
+    double a[RT][KT];
+};
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+template <int M>
+__device__ __forceinline__ void load_tfrag(const TMat<M>& T, TFrag<M>& F, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int rt = 0; rt < TFrag<M>::RT; ++rt)
+#pragma unroll
+        for (int kt = 0; kt < TFrag<M>::KT; ++kt) {
+            const int r = rt * 8 + g, k = kt * 4 + t;
+            F.a[rt][kt] = (r < M && k < M) ? T.t[r * M + k] : 0.0;
+        }
+}
+
+// One stage over `ncol` complex columns.  colB(j, k) returns column j's k-th input (k < M, j < ncol);
+// rows(j) the largest output row column j needs (< M); out(j, r, v) receives row r of column j for every
+// r <= rows(j).
+template <int M, class ColB, class Rows, class Out>
+__device__ __forceinline__ void tc_stage(const TFrag<M>& F, int ncol, ColB&& colB, Rows&& rows, Out&& out) {
+    constexpr int RT = TFrag<M>::RT, KT = TFrag<M>::KT;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int ntile = (ncol + 3) / 4;
+    for (int ct = warp; ct < ntile; ct += nwarp) {
+        const int jb = ct * 4 + (g >> 1), part = g & 1;
+        double b[KT];
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) {
+            const int k = kt * 4 + t;
+            double v = 0.0;
+            if (jb < ncol && k < M) {
+                const double2 z = colB(jb, k);
+                v = part ? z.y : z.x;
+            }
+            b[kt] = v;
+        }
+        int rmax = -1;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (ct * 4 + c < ncol) rmax = max(rmax, rows(ct * 4 + c));
+        const int jo = ct * 4 + t;
+#pragma unroll
+        for (int rt = 0; rt < RT; ++rt) {
+            if (rt * 8 > rmax) break;   // uniform over the warp
+            double acc[2] = {0.0, 0.0};
+#pragma unroll
+            for (int kt = 0; kt < KT; ++kt) dmma(acc, F.a[rt][kt], b[kt]);
+            const int r = rt * 8 + g;
+            if (jo < ncol && r <= rows(jo)) out(jo, r, make_double2(acc[0], acc[1]));
+        }
+    }
+}
+
+// sym_transform's interface and buffers on the tensor path.
+template <int DIM, int M, class Consumer>
+__device__ void sym_transform_tc(int np, double2* bufA, double2* bufB, const TMat<M>& T, Consumer&& consume) {
+    using S = TransformSmem<DIM, M>;
+    constexpr int P2 = S::P2;
+    constexpr int NQ = S::NQ;
+    TFrag<M> F;
+    load_tfrag<M>(T, F, threadIdx.x & 31);
+    if constexpr (DIM == 2) {
+        // stage x: W1[qx][b] = sum_a T[qx][a] f(a, b); column j = (p, b)
+        tc_stage<M>(F, np * M,
+            [&](int j, int k) { const int p = j / M, b = j - p * M; return bufA[p * NQ + sidx2(k, b)]; },
+            [&](int) { return M - 1; },
+            [&](int j, int r, double2 v) { const int p = j / M, b = j - p * M; bufB[p * (M * M) + r * M + b] = v; });
+        __syncthreads();
+        // stage y: out(qx, qy) = sum_b T[qy][b] W1[qx][b], qy <= qx; column j = (p, qx)
+        tc_stage<M>(F, np * M,
+            [&](int j, int k) { const int p = j / M, qx = j - p * M; return bufB[p * (M * M) + qx * M + k]; },
+            [&](int j) { return j % M; },
+            [&](int j, int r, double2 v) { const int p = j / M, qx = j - p * M; consume(p, widx2(qx, r), v); });
+        __syncthreads();
+    } else {
+        // stage x: W1[qx][(b, c)] = sum_a T[qx][a] f(a, b, c), b >= c; column j = (p, pair)
+        tc_stage<M>(F, np * P2,
+            [&](int j, int k) {
+                const int p = j / P2, pr = j - p * P2;
+                int b, c;
+                decode_pair(pr, b, c);
+                return bufA[p * NQ + sidx3(k, b, c)];
+            },
+            [&](int) { return M - 1; },
+            [&](int j, int r, double2 v) { const int p = j / P2, pr = j - p * P2; bufB[p * (M * P2) + r * P2 + pr] = v; });
+        __syncthreads();
+        // stage y: W2[(qx, qy)][c] = sum_b T[qy][b] W1[qx][(b, c)], qy <= qx; column j = (p, qx, c)
+        tc_stage<M>(F, np * M * M,
+            [&](int j, int k) {
+                const int p = j / (M * M), rr = j - p * (M * M), qx = rr / M, c = rr - qx * M;
+                return bufB[p * (M * P2) + qx * P2 + sidx2(k, c)];
+            },
+            [&](int j) { return (j % (M * M)) / M; },
+            [&](int j, int r, double2 v) {
+                const int p = j / (M * M), rr = j - p * (M * M), qx = rr / M, c = rr - qx * M;
+                bufA[p * S::BUF_A + widx2(qx, r) * M + c] = v;
+            });
+        __syncthreads();
+        // stage z: out(qx, qy, qz) = sum_c T[qz][c] W2[(qx, qy)][c], qz <= qy; column j = (p, pair)
+        tc_stage<M>(F, np * P2,
+            [&](int j, int k) { const int p = j / P2, pq = j - p * P2; return bufA[p * S::BUF_A + pq * M + k]; },
+            [&](int j) {
+                int qx, qy;
+                decode_pair(j % P2, qx, qy);
+                return qy;
+            },
+            [&](int j, int r, double2 v) {
+                const int p = j / P2, pq = j - p * P2;
+                int qx, qy;
+                decode_pair(pq, qx, qy);
+                consume(p, widx3(qx, qy, r), v);
+            });
+        __syncthreads();
+    }
+}
+
+// the CUDA-core or the tensor-path form, chosen at compile time
+template <int DIM, int M, bool TC, class Consumer>
+__device__ __forceinline__ void sym_transform_any(int np, double2* bufA, double2* bufB, const TMat<M>& T,
+                                                  Consumer&& consume) {
+    if constexpr (TC) sym_transform_tc<DIM, M>(np, bufA, bufB, T, consume);
+    else sym_transform<DIM, M>(np, bufA, bufB, T, consume);
+}
+
 }  // namespace ldga
 
 // Instantiation list: (DIM, M) pairs the library is built for.  M = N/2 + 1.
