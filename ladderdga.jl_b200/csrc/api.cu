@@ -354,7 +354,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     if (device < 0 || device >= ndev) return ctx_fail(nullptr, LDGA_ERR_ARG, "device index out of range");
     ldga_ctx* c = new (std::nothrow) ldga_ctx();
     if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
-    if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "cuda") != 0;
+    if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "tc") == 0;
     DeviceGuard g(device);
     c->device = device;
     c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;
@@ -1299,9 +1299,11 @@ bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
     ldga_ctx* ctx = s.ctx;
     s.evals++;
     if (lm > 1e5 || ld > 1e5) { F[0] = F[1] = NAN; return true; }
-    int st = eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum);
+    int st = eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum);   // d_red[8] = sum_kω(χm^λm), the EoM tail's
     if (!st) st = launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, ctx->d_red + 24);
-    if (!st) st = launch_sum_kw(ctx, LDGA_CH_M, lm, 0, ctx->d_red + 32);
+    if (!st && cudaMemcpyAsync(ctx->d_red + 32, ctx->d_red + 8, sizeof(double), cudaMemcpyDeviceToDevice,
+                               ctx->stream) != cudaSuccess)
+        st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaMemcpyAsync");
     if (!st) st = launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33);
     double r[10];
     if (!st) st = copy(ctx, r, ctx->d_red + 24, 10 * sizeof(double));
@@ -1334,10 +1336,12 @@ bool dm_newton(DmState& s, const double start[2], const double xmin[2], double a
     const int max_reset = 5;
     const double reset_backoff = 1.0;
     while (true) {
-        double fi[2], f0[2], f1[2], J[2][2];
+        double fi[2], f1[2], J[2][2];
         if (!dm_residual(s, xi[0], xi[1], fi)) return false;
-        // forward-difference Jacobian; FiniteDiff evaluates f(x) again
-        if (!dm_residual(s, xi[0], xi[1], f0)) return false;
+        // forward-difference Jacobian.  FiniteDiff evaluates f(x) once more; the residual is a
+        // deterministic function of x (its μ fit converges to |Δn| < 1e-14 from any warm start), so
+        // the value just computed is used
+        const double* f0 = fi;
         for (int j = 0; j < 2; ++j) {
             double x1[2] = {xi[0], xi[1]};
             const double e = fd_step(xi[j]);

@@ -132,9 +132,9 @@ struct ldga_ctx {
     int64_t graph_launches = 0;                  // kernels per replay of the captured graph
     double* h_stage = nullptr;     // pinned host staging for the chain's scalars (64 doubles + 4 ints)
 
-    // k-space transforms of the G setup, bubble and EoM on the FP64 tensor path (mma.sync m8n8k4);
-    // false: the CUDA-core form (environment LDGA_TRANSFORM=cuda at ldga_create, for comparisons)
-    bool transform_tc = true;
+    // k-space transforms of the G setup, bubble and EoM on the FP64 tensor path (mma.sync m8n8k4,
+    // environment LDGA_TRANSFORM=tc at ldga_create); the CUDA-core form is the default
+    bool transform_tc = false;
 
     // stage timing (ldga_profile / ldga_stage_times)
     bool profiling = false;

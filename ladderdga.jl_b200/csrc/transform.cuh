@@ -47,6 +47,46 @@ __device__ __forceinline__ double2 trow(const TMat<M>& T, int row, const double2
     return make_double2(re, im);
 }
 
+// Output rows of a stage are split into RS chunks so that each stage has enough independent work
+// items for the CTA (a stage has only M, P2 or M^2 columns per vector).  A chunk is a compile-time
+// row range, so every T coefficient stays an immediate constant-bank operand of its FMA; the items of
+// one chunk are padded to whole warps, so every warp applies one chunk.
+template <int DIM, int M>
+struct RowSplit {
+    static constexpr int RS = M >= 17 ? (DIM == 2 ? 4 : 2) : (M >= 9 ? 2 : 1);
+    static constexpr int CH = (M + RS - 1) / RS;
+};
+
+// rows r = C CH .. C CH + CH - 1 (r < M, r <= lim) of T v, each handed to f(r, value)
+template <int M, int CH, int C, class F>
+__device__ __forceinline__ void rows_chunk(const TMat<M>& T, const double2 (&v)[M], int lim, F&& f) {
+#pragma unroll
+    for (int qq = 0; qq < CH; ++qq) {
+        const int r = C * CH + qq;
+        if (r < M && r <= lim) f(r, trow<M>(T, r, v));
+    }
+}
+
+template <int DIM, int M, class F>
+__device__ __forceinline__ void rows_of(int chunk, const TMat<M>& T, const double2 (&v)[M], int lim, F&& f) {
+    using R = RowSplit<DIM, M>;
+    if (chunk == 0) rows_chunk<M, R::CH, 0>(T, v, lim, f);
+    if constexpr (R::RS > 1) { if (chunk == 1) rows_chunk<M, R::CH, 1>(T, v, lim, f); }
+    if constexpr (R::RS > 2) { if (chunk == 2) rows_chunk<M, R::CH, 2>(T, v, lim, f); }
+    if constexpr (R::RS > 3) { if (chunk == 3) rows_chunk<M, R::CH, 3>(T, v, lim, f); }
+}
+
+// for it in [0, RS * IPC): chunk = it / IPC, local item = it % IPC (< n), IPC = n rounded up to 32
+template <int DIM, int M, class Body>
+__device__ __forceinline__ void for_items(int n, Body&& body) {
+    using R = RowSplit<DIM, M>;
+    const int ipc = (n + 31) & ~31;
+    for (int it = threadIdx.x; it < R::RS * ipc; it += blockDim.x) {
+        const int chunk = it / ipc, loc = it - chunk * ipc;
+        if (loc < n) body(chunk, loc);
+    }
+}
+
 // Apply S to `np` vectors: in[p*NQ + q] (wedge-indexed).  `consume(p, q_wedge, value)` receives
 // every output exactly once.  bufA holds the inputs and is overwritten (3D stage 2); bufB is scratch.
 // All threads of the CTA must call this; it synchronises internally and on exit.
@@ -55,35 +95,31 @@ __device__ void sym_transform(int np, double2* bufA, double2* bufB, const TMat<M
     using S = TransformSmem<DIM, M>;
     constexpr int P2 = S::P2;
     constexpr int NQ = S::NQ;
-    const int tid = threadIdx.x, nth = blockDim.x;
     if constexpr (DIM == 2) {
         // stage x: W1[qx][b] = sum_a T[qx][a] f(a, b)
-        for (int it = tid; it < np * M; it += nth) {
+        for_items<DIM, M>(np * M, [&](int chunk, int it) {
             const int p = it / M, b = it - p * M;
             double2 v[M];
 #pragma unroll
             for (int a = 0; a < M; ++a) v[a] = bufA[p * NQ + sidx2(a, b)];
             double2* w = bufB + p * (M * M);
-#pragma unroll
-            for (int qx = 0; qx < M; ++qx) w[qx * M + b] = trow<M>(T, qx, v);
-        }
+            rows_of<DIM, M>(chunk, T, v, M - 1, [&](int qx, double2 y) { w[qx * M + b] = y; });
+        });
         __syncthreads();
         // stage y: out(qx, qy) = sum_b T[qy][b] W1[qx][b], qy <= qx
-        for (int it = tid; it < np * M; it += nth) {
+        for_items<DIM, M>(np * M, [&](int chunk, int it) {
             const int p = it / M, qx = it - p * M;
+            if (chunk * RowSplit<DIM, M>::CH > qx) return;
             double2 v[M];
             const double2* w = bufB + p * (M * M) + qx * M;
 #pragma unroll
             for (int b = 0; b < M; ++b) v[b] = w[b];
-#pragma unroll
-            for (int qy = 0; qy < M; ++qy) {
-                if (qy <= qx) consume(p, widx2(qx, qy), trow<M>(T, qy, v));
-            }
-        }
+            rows_of<DIM, M>(chunk, T, v, qx, [&](int qy, double2 y) { consume(p, widx2(qx, qy), y); });
+        });
         __syncthreads();
     } else {
         // stage x: W1[qx][(b,c)] = sum_a T[qx][a] f(a, b, c) for b >= c
-        for (int it = tid; it < np * P2; it += nth) {
+        for_items<DIM, M>(np * P2, [&](int chunk, int it) {
             const int p = it / P2, j = it - p * P2;
             int b, c;
             decode_pair(j, b, c);
@@ -91,39 +127,34 @@ __device__ void sym_transform(int np, double2* bufA, double2* bufB, const TMat<M
 #pragma unroll
             for (int a = 0; a < M; ++a) v[a] = bufA[p * NQ + sidx3(a, b, c)];
             double2* w = bufB + p * (M * P2);
-#pragma unroll
-            for (int qx = 0; qx < M; ++qx) w[qx * P2 + j] = trow<M>(T, qx, v);
-        }
+            rows_of<DIM, M>(chunk, T, v, M - 1, [&](int qx, double2 y) { w[qx * P2 + j] = y; });
+        });
         __syncthreads();
         // stage y: W2[(qx,qy)][c] = sum_b T[qy][b] W1[qx][(b,c)], qy <= qx  (W1 symmetric in b,c)
-        for (int it = tid; it < np * M * M; it += nth) {
+        for_items<DIM, M>(np * M * M, [&](int chunk, int it) {
             const int p = it / (M * M), r = it - p * (M * M);
             const int qx = r / M, c = r - qx * M;
+            if (chunk * RowSplit<DIM, M>::CH > qx) return;
             double2 v[M];
             const double2* w = bufB + p * (M * P2) + qx * P2;
 #pragma unroll
             for (int b = 0; b < M; ++b) v[b] = w[sidx2(b, c)];
             double2* o = bufA + p * S::BUF_A;
-#pragma unroll
-            for (int qy = 0; qy < M; ++qy) {
-                if (qy <= qx) o[widx2(qx, qy) * M + c] = trow<M>(T, qy, v);
-            }
-        }
+            rows_of<DIM, M>(chunk, T, v, qx, [&](int qy, double2 y) { o[widx2(qx, qy) * M + c] = y; });
+        });
         __syncthreads();
         // stage z: out(qx,qy,qz) = sum_c T[qz][c] W2[(qx,qy)][c], qz <= qy
-        for (int it = tid; it < np * P2; it += nth) {
+        for_items<DIM, M>(np * P2, [&](int chunk, int it) {
             const int p = it / P2, pq = it - p * P2;
             int qx, qy;
             decode_pair(pq, qx, qy);
+            if (chunk * RowSplit<DIM, M>::CH > qy) return;
             double2 v[M];
             const double2* w = bufA + p * S::BUF_A + pq * M;
 #pragma unroll
             for (int c = 0; c < M; ++c) v[c] = w[c];
-#pragma unroll
-            for (int qz = 0; qz < M; ++qz) {
-                if (qz <= qy) consume(p, widx3(qx, qy, qz), trow<M>(T, qz, v));
-            }
-        }
+            rows_of<DIM, M>(chunk, T, v, qy, [&](int qz, double2 y) { consume(p, widx3(qx, qy, qz), y); });
+        });
         __syncthreads();
     }
 }
@@ -190,14 +221,20 @@ __device__ __forceinline__ void tc_stage(const TFrag<M>& F, int ncol, ColB&& col
         for (int c = 0; c < 4; ++c)
             if (ct * 4 + c < ncol) rmax = max(rmax, rows(ct * 4 + c));
         const int jo = ct * 4 + t;
+        // the row tiles' accumulations are independent chains: interleaved over k so that consecutive
+        // tensor instructions do not wait for each other (the row-tile guard is uniform over the warp)
+        double acc[RT][2];
+#pragma unroll
+        for (int rt = 0; rt < RT; ++rt) acc[rt][0] = acc[rt][1] = 0.0;
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt)
+#pragma unroll
+            for (int rt = 0; rt < RT; ++rt)
+                if (rt * 8 <= rmax) dmma(acc[rt], F.a[rt][kt], b[kt]);
 #pragma unroll
         for (int rt = 0; rt < RT; ++rt) {
-            if (rt * 8 > rmax) break;   // uniform over the warp
-            double acc[2] = {0.0, 0.0};
-#pragma unroll
-            for (int kt = 0; kt < KT; ++kt) dmma(acc, F.a[rt][kt], b[kt]);
             const int r = rt * 8 + g;
-            if (jo < ncol && r <= rows(jo)) out(jo, r, make_double2(acc[0], acc[1]));
+            if (rt * 8 <= rmax && jo < ncol && r <= rows(jo)) out(jo, r, make_double2(acc[rt][0], acc[rt][1]));
         }
     }
 }
