@@ -633,7 +633,7 @@ def fp64_peak(peaks: dict, sm_mhz: float):
             f"nominal 64 FP64 FMA/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (no FP64 figure measured)")
 
 
-def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
+def roofline(stages: dict, chain, peaks: dict, sweeps=None, steps: int = 1) -> dict:
     """Dominant stage of the step and its roofline (algorithmic work per launch / CUDA-event time)."""
     name = max(stages, key=lambda k: stages[k][0])
     tot, cnt = stages[name]
@@ -642,11 +642,13 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
     hbm = peaks.get("hbm_gbs", 6650.0)
     if name == "bse":
         # algorithmic work per (q, w) matrix: the reference's complex LU + inverse (zgetrf + zgetri,
-        # 8 N^3 real flops) plus the sums (8 N^2); one launch = one channel, N_q N_w matrices.
-        flops = nq * nw * (8.0 * nnu**3 + 8.0 * nnu**2)
+        # 8 N^3 real flops) plus the sums (8 N^2); a step solves both channels, N_q N_w matrices each,
+        # in one launch (the preconditioned solve) or two
+        chans = 2.0 * steps / max(cnt, 1)
+        flops = chans * nq * nw * (8.0 * nnu**3 + 8.0 * nnu**2)
         ach = flops / t / 1e12
         # what the kernel executes: elimination of [B | 1] alone (BSE_EXEC_CMACS complex multiply-adds)
-        exe = nq * nw * 8.0 * BSE_EXEC_CMACS(nnu) / t / 1e12
+        exe = chans * nq * nw * 8.0 * BSE_EXEC_CMACS(nnu) / t / 1e12
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
         cfg = chain.lib.ldga_bse_config_name(nnu, chain.ctx.precision, -1)
         cfg = cfg.decode() if cfg else ""
@@ -674,7 +676,8 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
                     "passes_per_warp": passes / max(warps, 1),
                     "fp32_tflops": f32 / t / 1e12,
                     "reference_formulation_tflops": ach,
-                    "traffic": BSE_ITER_DRAM_BYTES_PER_MATRIX * nq * nw if nnu == 40 else None,
+                    "channels_per_launch": chans,
+                    "traffic": BSE_ITER_DRAM_BYTES_PER_MATRIX * chans * nq * nw if nnu == 40 else None,
                     "traffic_source": ("ncu dram__bytes_read+write of one launch on 3D 32^3 (39 729 matrices)"
                                        if nnu == 40 else "no capture at this Nnu"),
                     "peak_source": peak_src}
@@ -697,7 +700,8 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None) -> dict:
                 "executed": {"tflops": exe, "frac": exe / peak,
                              "work": "flops of the LU solve of [B | 1], its back substitution and the "
                                      "backward-error check (one pass; refinement sweeps not counted)"},
-                "traffic": BSE_DRAM_BYTES_PER_MATRIX * nq * nw if nnu == 40 else None,
+                "channels_per_launch": chans,
+                "traffic": BSE_DRAM_BYTES_PER_MATRIX * chans * nq * nw if nnu == 40 else None,
                 "traffic_source": ("ncu dram__bytes_read+write of one FP64 launch on 3D 16^3 (6765 matrices, "
                                    "802 B each), scaled by the matrix count" if nnu == 40 else
                                    "no capture at this Nnu"),
@@ -842,7 +846,7 @@ def run_ours(args):
         if errors64 is not None:
             fp64_cmp["errors"] = errors64
     if rank == 0:
-        rl = (roofline(stages, chain, peaks, (sp.value, sw.value)) if any(v[1] for v in stages.values())
+        rl = (roofline(stages, chain, peaks, (sp.value, sw.value), args.steps) if any(v[1] for v in stages.values())
               else {"note": "no stage events (--no-stage-events)"})
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

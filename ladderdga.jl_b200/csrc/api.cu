@@ -191,7 +191,7 @@ int alloc_all(ldga_ctx* c) {
 void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
-                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_list, c->d_count,
+                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_count,
                     c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1099,8 +1099,7 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     TRY(launch_gloc_transform(ctx, true));                       // a1
     TRY(launch_bubble(ctx));                                     // a2
     LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
-    TRY(launch_bse(ctx, LDGA_CH_M, ctx->d_count + 1));           // a7
-    TRY(launch_bse(ctx, LDGA_CH_D, ctx->d_count + 1));
+    TRY(launch_bse_pair(ctx, ctx->d_count + 1));                  // a7, both channels
     TRY(launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp));   // a5
     TRY(launch_lambda0(ctx));                                    // a6
     // λm_correction_full (conditions_new.jl:174-190): rhs = 2 imp_density - sum_kω(chi_d)

@@ -1633,7 +1633,12 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
 }
 
 template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM>
-__global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a, const int32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a_m, const BseArgs a_d,
+                                                                       const int32_t* __restrict__ perm) {
+    // blockIdx.z selects the channel: one launch may cover both (they share chi0 and the q order),
+    // so the second channel's CTAs fill the SMs the first one's tail leaves idle
+    BseArgs a = a_m;
+    if (blockIdx.z) { a.s = a_d.s; a.Gamma = a_d.Gamma; a.chi = a_d.chi; a.gam = a_d.gam; a.flags = a_d.flags; }
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
     static_assert(!DM || (GSM && TC), "the FP64 tensor product is built with the tensor-core FP32 product");
     constexpr int LD = S::LD;
@@ -2534,8 +2539,9 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
+using BseRunPair = int (*)(ldga_ctx*, const BseArgs&, const BseArgs&);
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
-int run_iter(ldga_ctx* ctx, const BseArgs& a) {
+int run_iter(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d = nullptr) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
     auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM>;
@@ -2556,15 +2562,21 @@ int run_iter(ldga_ctx* ctx, const BseArgs& a) {
         }
         ctx->qperm_gen = ctx->chi0_gen;
     }
-    dim3 grid((a.nq + kIterQ - 1) / kIterQ, a.nw);
-    kern<<<grid, kIterQ * LPQ / QPL, S::bytes, ctx->stream>>>(a, ctx->d_qperm);
+    dim3 grid((a.nq + kIterQ - 1) / kIterQ, a.nw, a_d ? 2 : 1);
+    kern<<<grid, kIterQ * LPQ / QPL, S::bytes, ctx->stream>>>(a, a_d ? *a_d : a, ctx->d_qperm);
     LDGA_LAUNCHED(ctx, "k_bse_iter");
     return LDGA_OK;
+}
+
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
+int run_iter_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) {
+    return run_iter<N, LPQ, MINB, QPL, GSM, TC, DM>(ctx, a_m, &a_d);
 }
 
 struct BseVariant {
     BseRun run;
     const char* name;
+    BseRunPair run_pair = nullptr;   // both channels in one launch (the preconditioned solve)
 };
 
 #define LDGA_SMALL_BOX(N)                                                                              \
@@ -2593,7 +2605,8 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3"}, {&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2"},
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3", &run_iter_pair<40, 8, 3, 2, true, true, true>},
+                               {&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2", &run_iter_pair<40, 8, 2, 2, true, true, true>},
                                {&run_iter<40, 8, 3, 2, true, true>, "iter8x2tc:3"}, {&run_iter<40, 8, 2, 2, true, true>, "iter8x2tc:2"},
                                {&run_iter<40, 8, 2, 2>, "iter8x2:2"}, {&run_iter<40, 8, 3, 2>, "iter8x2:3"},
                                {&run_iter<40, 8, 2>, "iter8:2"}, {&run_iter<40, 4, 3>, "iter"},
@@ -2733,6 +2746,43 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     // matrices that stayed non-finite after the pivoted solve, accumulated into *d_fail
     k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, d_fail);
     LDGA_LAUNCHED(ctx, "k_count_flags");
+    return LDGA_OK;
+}
+
+// Both channels of the chain: one launch of the tuned configuration when it has a two-channel form
+// (channel d flags into d_flags2), then each channel's pivoted re-solve of flagged matrices as in
+// launch_bse; otherwise launch_bse for m, then d.
+int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail) {
+    const BseVariant* v = nullptr;
+    const int nv = variants_of(ctx->Nnu, ctx->prec, &v);
+    int i = nv > 0 ? tuned_index(ctx->Nnu, ctx->prec) : 0;
+    if (i >= nv) i = 0;
+    if (nv == 0 || !v[i].run_pair) {
+        TRY(launch_bse(ctx, LDGA_CH_M, d_fail));
+        return launch_bse(ctx, LDGA_CH_D, d_fail);
+    }
+    const int n = ctx->Nq * ctx->Nw;
+    if (!ctx->d_flags2) LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_flags2), (size_t)n * sizeof(int32_t)));
+    BseArgs am = bse_args(ctx, LDGA_CH_M), ad = bse_args(ctx, LDGA_CH_D);
+    ad.flags = ctx->d_flags2;
+    TRY(v[i].run_pair(ctx, am, ad));
+    const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;
+    if (in_hbm && !ctx->d_pivot_scratch) return ctx_fail(ctx, LDGA_ERR_ARG, "pivoted BSE scratch missing");
+    const size_t smp = in_hbm ? 64 * sizeof(double) + 16 : bse_pivot_smem(ctx->Nnu);
+    double2* gscr = in_hbm ? ctx->d_pivot_scratch : nullptr;
+    LDGA_CUDA(ctx, set_smem(ctx, k_bse_lu_pivot, smp));
+    for (const BseArgs* a : {&am, &ad}) {
+        LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, sizeof(int32_t), ctx->stream));
+        k_compact_flags<<<148, 256, 0, ctx->stream>>>(a->flags, n, ctx->d_list, ctx->d_count);
+        LDGA_LAUNCHED(ctx, "k_compact_flags");
+        {
+            StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
+            k_bse_lu_pivot<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(*a, ctx->d_list, 0, ctx->d_count, gscr);
+            LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
+        }
+        k_count_flags<<<148, 256, 0, ctx->stream>>>(a->flags, n, d_fail);
+        LDGA_LAUNCHED(ctx, "k_count_flags");
+    }
     return LDGA_OK;
 }
 

@@ -103,6 +103,7 @@ struct ldga_ctx {
     size_t partial_elems = 0;
     double* d_red = nullptr;       // reduction scratch
     int32_t* d_flags = nullptr;    // BSE fallback flags [Nq*Nw]
+    int32_t* d_flags2 = nullptr;   // the d channel's flags when both channels run in one launch
     int32_t* d_list = nullptr;     // compacted fallback list
     int32_t* d_count = nullptr;
     double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
@@ -206,6 +207,7 @@ int launch_bubble(ldga_ctx* ctx);
 // BSE for one channel; enqueues the fallback for flagged matrices on the device (no host sync).
 // d_fail (device int32) receives the number of matrices that stayed unsolved.
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail);
+int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail);
 // Adjoint of one BSE channel: chi0_bar (written, or added to when accumulate), y and z buffers
 // [Nq, Nnu, Nw], Gamma_bar [Nnu, Nnu, Nw]; the number of adjoint solves above the backward-error
 // threshold is added to d_fail.
