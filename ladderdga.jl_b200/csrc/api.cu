@@ -355,6 +355,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     ldga_ctx* c = new (std::nothrow) ldga_ctx();
     if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
     if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "tc") == 0;
+    if (const char* nw = std::getenv("LDGA_NEWTON")) c->newton_async = std::strcmp(nw, "barrier") != 0;
     DeviceGuard g(device);
     c->device = device;
     c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;

@@ -2541,7 +2541,7 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
 using BseRunPair = int (*)(ldga_ctx*, const BseArgs&, const BseArgs&);
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
-int run_iter(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d = nullptr) {
+int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
     auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM>;
@@ -2569,8 +2569,13 @@ int run_iter(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d = nullptr) {
 }
 
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
+int run_iter(ldga_ctx* ctx, const BseArgs& a) {
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM>(ctx, a, nullptr);
+}
+
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false>
 int run_iter_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) {
-    return run_iter<N, LPQ, MINB, QPL, GSM, TC, DM>(ctx, a_m, &a_d);
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM>(ctx, a_m, &a_d);
 }
 
 struct BseVariant {
@@ -2758,14 +2763,15 @@ int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail) {
     int i = nv > 0 ? tuned_index(ctx->Nnu, ctx->prec) : 0;
     if (i >= nv) i = 0;
     if (nv == 0 || !v[i].run_pair) {
-        TRY(launch_bse(ctx, LDGA_CH_M, d_fail));
-        return launch_bse(ctx, LDGA_CH_D, d_fail);
+        const int st = launch_bse(ctx, LDGA_CH_M, d_fail);
+        return st != LDGA_OK ? st : launch_bse(ctx, LDGA_CH_D, d_fail);
     }
     const int n = ctx->Nq * ctx->Nw;
     if (!ctx->d_flags2) LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_flags2), (size_t)n * sizeof(int32_t)));
     BseArgs am = bse_args(ctx, LDGA_CH_M), ad = bse_args(ctx, LDGA_CH_D);
     ad.flags = ctx->d_flags2;
-    TRY(v[i].run_pair(ctx, am, ad));
+    const int st = v[i].run_pair(ctx, am, ad);
+    if (st != LDGA_OK) return st;
     const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;
     if (in_hbm && !ctx->d_pivot_scratch) return ctx_fail(ctx, LDGA_ERR_ARG, "pivoted BSE scratch missing");
     const size_t smp = in_hbm ? 64 * sizeof(double) + 16 : bse_pivot_smem(ctx->Nnu);

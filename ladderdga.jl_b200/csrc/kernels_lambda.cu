@@ -136,6 +136,84 @@ __device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW>& s
     parity ^= 1;
 }
 
+// The same all-reduce without a cluster barrier.  Lanes 0..kCluster-1 of every warp write the warp's
+// NV values into CTA l's slot with st.async, which completes its bytes on that CTA's mbarrier of the
+// slot; each CTA arms its own mbarrier for the bytes of all kCluster * NW sources (one arrive with
+// expect_tx by thread 0) and its threads wait for that phase -- no release fence over the cluster and
+// no barrier that every CTA must reach.  Slot s of a CTA is rewritten (iteration i + 2) only after
+// every source received this CTA's iteration i + 1 values, which each warp sends after it has read
+// slot s (its shuffles of iteration i); the mbarrier of slot s advances one phase per use, so the
+// waiters of iteration i see phase parity (i / 2) & 1.  Waits are bounded: after kAsyncSpins
+// non-blocking polls (mbarrier.test_wait, well under a second) the call returns false and the caller
+// stops its loop and reports NaN.
+constexpr long long kAsyncSpins = 1ll << 22;
+
+template <int NV, int NW>
+struct ClAsync {
+    alignas(16) double part[2][kCluster * NW][NV];
+    alignas(8) unsigned long long bar[2];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <int NV, int NW>
+__device__ __forceinline__ void async_allsum_init(ClAsync<NV, NW>& s) {
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s.bar[0])), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s.bar[1])), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cg::this_cluster().sync();   // every CTA's barriers exist before any remote write
+}
+
+template <int NV, int NW>
+__device__ __forceinline__ bool async_allsum(double (&v)[NV], ClAsync<NV, NW>& s, int iter) {
+    static_assert(NV == 2, "the exchange moves one 16-byte value pair per source");
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int slot = iter & 1;
+    const uint32_t phase = (uint32_t)((iter >> 1) & 1);
+    const uint32_t src = cg::this_cluster().block_rank() * NW + w;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        double x = v[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[j] = x;
+    }
+    const uint32_t bar = smem_addr(&s.bar[slot]);
+    if (threadIdx.x == 0) {
+        constexpr uint32_t bytes = kCluster * NW * NV * sizeof(double);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    }
+    if (l < kCluster) {
+        uint32_t raddr, rbar;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(raddr) : "r"(smem_addr(&s.part[slot][src][0])), "r"(l));
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rbar) : "r"(bar), "r"(l));
+        asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];"
+                     ::"r"(raddr), "d"(v[0]), "d"(v[1]), "r"(rbar) : "memory");
+    }
+    uint32_t done = 0;
+    for (long long k = 0; k < kAsyncSpins && !done; ++k)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+    const bool ok = __all_sync(0xffffffffu, done != 0);
+    constexpr int P = kCluster * NW;
+    double x[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) x[j] = 0.0;
+#pragma unroll
+    for (int i = l; i < P; i += 32) {
+        const double2 p = *reinterpret_cast<const double2*>(s.part[slot][i]);
+        x[0] += p.x;
+        x[1] += p.y;
+    }
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        for (int o = 16; o > 0; o >>= 1) x[j] += __shfl_xor_sync(0xffffffffu, x[j], o);
+        v[j] = x[j];
+    }
+    return ok;
+}
+
 __device__ __forceinline__ int cl_tid() { return cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int cl_nth() { return kCluster * blockDim.x; }
 
@@ -278,12 +356,15 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 // the trajectory has period p = i - checkpoint and whole periods up to nsteps are skipped; the last
 // < p iterations then run as usual.  xi and i come out bit for bit as from the full loop.
 // out[3], out[4]: the iteration at which the repeat was recognised and p (0, 0: nothing skipped).
-template <int K>
+template <int K, bool ASYNC>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kNewtonThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
            const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out) {
     __shared__ ClAll<2, kNewtonThreads / 32> ca;
-    int parity = 0;
+    __shared__ ClAsync<2, kNewtonThreads / 32> cs;
+    int parity = 0, iter = 0;
+    bool exchange_ok = true;
+    if constexpr (ASYNC) async_allsum_init(cs);
     const double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
     const double xmin = xmin_dev[0];
     const double delta = 1e-4;
@@ -364,7 +445,11 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
                 v[1] = fma(km, -t * t, v[1]);
             }
         }
-        cluster_allsum<2>(v, ca, parity);
+        if constexpr (ASYNC) {
+            if (!async_allsum(v, cs, iter++)) { exchange_ok = false; xi = NAN; break; }
+        } else {
+            cluster_allsum<2>(v, ca, parity);
+        }
         const double fi = (v[0] * a.inv_nk - tail + cst) * inv_beta - rhs;
         const double dfi = (v[1] * a.inv_nk - tail + cst) * inv_beta;
         const double dfii = 1.0 / dfi;
@@ -387,7 +472,7 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
         }
     }
     if (tid == 0) {
-        out[0] = xi;
+        out[0] = exchange_ok ? xi : NAN;   // an exchange that timed out leaves no valid λ
         out[1] = (double)i;
         out[3] = (double)skip_at;
         out[4] = (double)skip_p;
@@ -743,9 +828,16 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
     const SumArgs sa = sum_args(ctx);
     const int per = (sa.nq * sa.nw + kCluster * kNewtonThreads - 1) / (kCluster * kNewtonThreads);
-    auto kern = per <= 2 ? k_lambda_m<2> : per <= 4 ? k_lambda_m<4> : per <= 6 ? k_lambda_m<6>
-              : per <= 8 ? k_lambda_m<8> : per <= 12 ? k_lambda_m<12> : per <= 16 ? k_lambda_m<16>
-              : per <= 20 ? k_lambda_m<20> : per <= 24 ? k_lambda_m<24> : k_lambda_m<0>;
+    const bool as = ctx->newton_async;
+    auto kern = per <= 2 ? (as ? k_lambda_m<2, true> : k_lambda_m<2, false>)
+              : per <= 4 ? (as ? k_lambda_m<4, true> : k_lambda_m<4, false>)
+              : per <= 6 ? (as ? k_lambda_m<6, true> : k_lambda_m<6, false>)
+              : per <= 8 ? (as ? k_lambda_m<8, true> : k_lambda_m<8, false>)
+              : per <= 12 ? (as ? k_lambda_m<12, true> : k_lambda_m<12, false>)
+              : per <= 16 ? (as ? k_lambda_m<16, true> : k_lambda_m<16, false>)
+              : per <= 20 ? (as ? k_lambda_m<20, true> : k_lambda_m<20, false>)
+              : per <= 24 ? (as ? k_lambda_m<24, true> : k_lambda_m<24, false>)
+              : (as ? k_lambda_m<0, true> : k_lambda_m<0, false>);
     kern<<<kCluster, kNewtonThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
                                                    d_out + 2, nsteps, atol, d_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");

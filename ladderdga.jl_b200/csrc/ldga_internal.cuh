@@ -136,6 +136,9 @@ struct ldga_ctx {
     // k-space transforms of the G setup, bubble and EoM on the FP64 tensor path (mma.sync m8n8k4,
     // environment LDGA_TRANSFORM=tc at ldga_create); the CUDA-core form is the default
     bool transform_tc = false;
+    // the λm Newton's cluster all-reduce by st.async + mbarrier instead of a cluster barrier per
+    // iteration (environment LDGA_NEWTON=barrier at ldga_create selects the barrier form)
+    bool newton_async = true;
 
     // stage timing (ldga_profile / ldga_stage_times)
     bool profiling = false;
