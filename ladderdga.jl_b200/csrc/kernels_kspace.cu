@@ -10,6 +10,11 @@ using namespace ldga;
 namespace {
 
 constexpr int kThreads = 256;
+// the CUDA-core transform kernels of the G setup, bubble and EoM: 16 warps per CTA where a thread's
+// column (M complex values in registers) fits 128 registers, so one CTA per SM still has warps to hide
+// the shared-memory and FMA latencies; 8 warps above
+template <int M, bool TC>
+constexpr int kThr = (!TC && M <= 17) ? 512 : kThreads;
 constexpr size_t kSmemBudget = 200 * 1024;
 // the tensor-path transform kernels run two CTAs per SM: half the shared memory each
 constexpr size_t kSmemBudgetTC = 110 * 1024;
@@ -46,7 +51,7 @@ TMat<M> make_T(const ldga_ctx* ctx) {
 // a1: G(k, nu) for nu in fft_range and Ghat = S(G)
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M, bool TC>
-__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_gloc_transform(
+__global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_gloc_transform(
     const TMat<M> T, int nf, int fft_lo, double beta, double mu, const double* __restrict__ eps,
     const double2* __restrict__ sigma_loc, int n_sigma, double2* __restrict__ gloc, int from_sigma,
     double2* __restrict__ ghat, int np_max) {
@@ -86,7 +91,7 @@ __global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_gloc_transform(
 // (pair index vi + Nnu wi, partner's index or -1), built on the host with the handle.
 // ---------------------------------------------------------------------------------------------
 template <int DIM, int M, bool TC>
-__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_bubble(
+__global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_bubble(
     const TMat<M> T, int nnu, int nw, int n_iv, int n_iw, int shift, int fft_lo, double scale,
     const double2* __restrict__ ghat, const int2* __restrict__ pairs, int total, double2* __restrict__ chi0, int np_max) {
     using S = TransformSmem<DIM, M>;
@@ -168,7 +173,7 @@ __device__ __forceinline__ double2 eom_value(const EomArgs& a, double2 gm, doubl
 }
 
 template <int DIM, int M, bool TC>
-__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_eom_forward(
+__global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_eom_forward(
     const TMat<M> T, const EomArgs a, const double2* __restrict__ ghat, const double* __restrict__ chi_m,
     const double2* __restrict__ gam_m, const double* __restrict__ chi_d, const double2* __restrict__ gam_d,
     const double2* __restrict__ lambda0, double2* __restrict__ partial) {
@@ -224,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_eom_forward(
 }
 
 template <int DIM, int M, bool TC>
-__global__ void __launch_bounds__(kThreads, TC ? 2 : 1) k_eom_inverse(
+__global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_eom_inverse(
     const TMat<M> T, int numax, int nchunk, double scale, double beta, double U, double hartree,
     const double* __restrict__ tail_sum, int tc, double chiloc_m_sum, const double2* __restrict__ partial,
     double2* __restrict__ out, int out_ld, int add_hartree, int np_max) {
@@ -553,7 +558,7 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid((ctx->Nf + np - 1) / np);
     StageTimer st_(ctx, LDGA_STAGE_GLOC);
-    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, ctx->fft_lo, ctx->mp.beta, ctx->mp.mu,
+    kern<<<grid, tc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nf, ctx->fft_lo, ctx->mp.beta, ctx->mp.mu,
                                                ctx->d_eps, ctx->d_sigma_loc, ctx->n_sigma_loc, ctx->d_gloc,
                                                from_sigma ? 1 : 0, ctx->d_ghat, np);
     LDGA_LAUNCHED(ctx, "k_gloc_transform");
@@ -571,7 +576,7 @@ int run_bubble(ldga_ctx* ctx) {
     dim3 grid((total + np - 1) / np);
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
     StageTimer st_(ctx, LDGA_STAGE_BUBBLE);
-    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
+    kern<<<grid, tc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
                                                ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_bub_pairs, total,
                                                ctx->d_chi0, np);
     LDGA_LAUNCHED(ctx, "k_bubble");
@@ -608,7 +613,7 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
     LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
     dim3 grid(nchunk, numax);
     StageTimer st_(ctx, LDGA_STAGE_EOM_FORWARD);
-    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_ghat, ctx->d_chi[0], ctx->d_gam[0],
+    kern<<<grid, tc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), a, ctx->d_ghat, ctx->d_chi[0], ctx->d_gam[0],
                                                ctx->d_chi[1], ctx->d_gam[1], ctx->d_lambda0, ctx->d_partial);
     LDGA_LAUNCHED(ctx, "k_eom_forward");
     nchunk_out = nchunk;
@@ -627,7 +632,7 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
     const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);
     const double hartree = ctx->mp.n * ctx->mp.U / 2.0;
     StageTimer st_(ctx, LDGA_STAGE_EOM_INVERSE);
-    kern<<<grid, kThreads, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
+    kern<<<grid, ttc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
                                                hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,
                                                add_hartree, np);
     LDGA_LAUNCHED(ctx, "k_eom_inverse");
