@@ -383,6 +383,11 @@ int ldga_destroy(ldga_ctx* ctx) {
     if (ctx->d_gimp) cudaFree(ctx->d_gimp);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     for (auto& p : ctx->ev_pool) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    if (ctx->io_stream) {
+        cudaStreamDestroy(ctx->io_stream);
+        for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_gamma, ctx->ev_loc, ctx->ev_chi, ctx->ev_join})
+            if (e) cudaEventDestroy(e);
+    }
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return LDGA_OK;
@@ -1088,33 +1093,53 @@ struct ChainArgs {
     double *sigma_out, *chi_m_out, *chi_d_out;
 };
 
-// Enqueue the whole chain on ctx->stream; nothing here waits for the device.
+// Enqueue the whole chain on ctx->stream; nothing here waits for the device.  The inputs the first
+// stages do not need (Γ_m, Γ_d, χ_loc,m, G_imp) are copied on io_stream while the G transform and the
+// bubble run, and χ_m, χ_d are copied out there while the λ and EoM stages run; the main stream waits
+// for each copy through an event before its first use and for all of them at the end (under capture
+// the events become graph edges).
 int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     const size_t nG = (size_t)ctx->Nnu * ctx->Nnu * ctx->Nw * sizeof(double2);
+    const size_t nX = (size_t)ctx->Nq * ctx->Nw * sizeof(double);
     const int numax = ctx->Nnu / 2;
+    cudaStream_t io = ctx->io_stream;
+    auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+        LDGA_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, io));
+        return LDGA_OK;
+    };
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(io, ctx->ev_fork, 0));
+    TRY(cp(ctx->d_Gamma[0], a.gamma_m, nG));
+    TRY(cp(ctx->d_Gamma[1], a.gamma_d, nG));
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_gamma, io));
+    TRY(cp(ctx->d_chiloc, a.chi_loc_m, nG));
+    TRY(cp(ctx->d_gimp, a.gimp, (size_t)a.n_gimp * sizeof(double2)));
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_loc, io));
     TRY(copy(ctx, ctx->d_sigma_loc, a.sigma_loc, (size_t)a.n_sigma * sizeof(double2)));
-    TRY(copy(ctx, ctx->d_Gamma[0], a.gamma_m, nG));
-    TRY(copy(ctx, ctx->d_Gamma[1], a.gamma_d, nG));
-    TRY(copy(ctx, ctx->d_chiloc, a.chi_loc_m, nG));
-    TRY(copy(ctx, ctx->d_gimp, a.gimp, (size_t)a.n_gimp * sizeof(double2)));
     TRY(launch_gloc_transform(ctx, true));                       // a1
     TRY(launch_bubble(ctx));                                     // a2
     LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_gamma, 0));
     TRY(launch_bse_pair(ctx, ctx->d_count + 1));                  // a7, both channels
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_chi, ctx->stream));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(io, ctx->ev_chi, 0));
+    if (a.chi_m_out) TRY(cp(a.chi_m_out, ctx->d_chi[0], nX));
+    if (a.chi_d_out) TRY(cp(a.chi_d_out, ctx->d_chi[1], nX));
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_join, io));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_loc, 0));
     TRY(launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp));   // a5
     TRY(launch_lambda0(ctx));                                    // a6
-    // λm_correction_full (conditions_new.jl:174-190): rhs = 2 imp_density - sum_kω(chi_d)
-    TRY(launch_sum_kw(ctx, LDGA_CH_D, 0.0, 0, ctx->d_red + 56));
-    TRY(launch_lambda_m(ctx, 2.0 * a.imp_density, ctx->d_red + 56, ctx->d_red + 16));
-    TRY(launch_sum_kw(ctx, LDGA_CH_M, 0.0, 0, ctx->d_red + 8, ctx->d_red + 16));   // sum_kω(chi_m, λ = λm)
+    // λm_correction_full (conditions_new.jl:174-190): rhs = 2 imp_density - sum_kω(chi_d), the Newton, and
+    // sum_kω(chi_m, λ = λm) for the EoM's tail, all in the Newton kernel (d_red[56], d_red[16], d_red[8])
+    TRY(launch_lambda_m(ctx, 2.0 * a.imp_density, nullptr, ctx->d_red + 16, 100, 1e-13, ctx->d_red + 56,
+                        ctx->d_red + 8));
     TRY(launch_eom(ctx, numax, 0.0, 0.0, ctx->d_red + 16, nullptr, -1, ctx->d_red + 8, 1, a.chiloc_m_sum,
                    ctx->d_sigma, ctx->Nq, 1));                   // a10 at λm
     TRY(launch_g_ladder(ctx, numax, 1, ctx->mp.mu, ctx->d_red + 24));   // a15: μ fit, energies
     if (a.sigma_out) TRY(copy(ctx, a.sigma_out, ctx->d_sigma, (size_t)ctx->Nq * numax * sizeof(double2)));
-    if (a.chi_m_out) TRY(copy(ctx, a.chi_m_out, ctx->d_chi[0], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
-    if (a.chi_d_out) TRY(copy(ctx, a.chi_d_out, ctx->d_chi[1], (size_t)ctx->Nq * ctx->Nw * sizeof(double)));
     TRY(copy(ctx, ctx->h_stage, ctx->d_red, 64 * sizeof(double)));
     TRY(copy(ctx, ctx->h_stage + 64, ctx->d_count, 4 * sizeof(int32_t)));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
     return LDGA_OK;
 }
 
@@ -1153,6 +1178,11 @@ int chain_m_submit(ldga_ctx* ctx, const ChainArgs& a, bool use_graph, bool* repl
         ctx->n_gimp_alloc = n_gimp;
     }
     if (!ctx->h_stage) LDGA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), 64 * sizeof(double) + 16));
+    if (!ctx->io_stream) {
+        LDGA_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&ctx->ev_fork, &ctx->ev_gamma, &ctx->ev_loc, &ctx->ev_chi, &ctx->ev_join})
+            LDGA_CUDA(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     const void* ptrs[] = {a.sigma_loc, a.gamma_m, a.gamma_d, a.chi_loc_m, a.gimp, a.sigma_out, a.chi_m_out, a.chi_d_out};
     bool graphable = use_graph;
     for (const void* p : ptrs)

@@ -9,6 +9,7 @@
 // bitwise identical.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -241,16 +242,23 @@ __global__ void k_F_from_chi(int nnu, int nw, int n_iv, int n_iw, int shift, dou
     }
 }
 
-// colF[nu', w] = sum_nu F[nu, nu', w] in order nu = 0..Nnu-1
+// colF[nu', w] = sum_nu F[nu, nu', w]: one warp per column (nu', w), coalesced loads, then a fixed-order
+// shuffle reduction (bitwise reproducible).  A thread per column summed its 40 values one dependent
+// load after another.
 __global__ void k_colsum_F(int nnu, int nw, const double2* __restrict__ F, double2* __restrict__ colF) {
-    const int total = nnu * nw;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-        const int vp = e % nnu, w = e / nnu;
+    const int lane = threadIdx.x & 31;
+    const int ncol = nnu * nw, nwarp_all = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncol; c += nwarp_all) {
+        const double2* col = F + (size_t)c * nnu;
         double2 acc = make_double2(0.0, 0.0);
-        const double2* col = F + ((size_t)w * nnu + vp) * nnu;
-        for (int v = 0; v < nnu; ++v) acc = cadd(acc, col[v]);
-        colF[e] = acc;
+        for (int v = lane; v < nnu; v += 32) acc = cadd(acc, col[v]);
+        for (int o = 16; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        if (lane == 0) colF[c] = acc;
     }
+}
 }
 
 __global__ void k_lambda0(int nq, int nnu, int nw, double inv_beta2, const double2* __restrict__ chi0,
@@ -359,13 +367,18 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 template <int K, bool ASYNC>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kNewtonThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
-           const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out) {
+           const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out,
+           const double* __restrict__ chi_d, double* sum_d_out, double* sum_m_out) {
     __shared__ ClAll<2, kNewtonThreads / 32> ca;
     __shared__ ClAsync<2, kNewtonThreads / 32> cs;
     int parity = 0, iter = 0;
     bool exchange_ok = true;
     if constexpr (ASYNC) async_allsum_init(cs);
-    const double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
+    auto allsum = [&](double (&v)[2]) -> bool {
+        if constexpr (ASYNC) return async_allsum(v, cs, iter++);
+        cluster_allsum<2>(v, ca, parity);
+        return true;
+    };
     const double xmin = xmin_dev[0];
     const double delta = 1e-4;
     const int total = a.nq * a.nw;
@@ -380,6 +393,17 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
         const int e = tid + j * nth;
         xv[j] = e < total ? chi[e] : 0.0;
         kv[j] = e < total ? kmult[e % a.nq] : 0.0;
+    }
+    // the chain's rhs = rhs_const - sum_kω(chi_d) formed here (chi_d given) instead of by a k_sum_kw
+    // launch before the Newton; the same elements and weights as the chi_m sums below
+    double rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0.0);
+    if (chi_d) {
+        double v[2] = {0.0, 0.0};
+        for (int e = tid; e < total; e += nth) v[0] = fma(kmult[e % a.nq], chi_d[e], v[0]);
+        if (!allsum(v)) exchange_ok = false;
+        const double sd = (v[0] * a.inv_nk - tail + cst) * inv_beta;
+        rhs = rhs_const - sd;
+        if (tid == 0 && sum_d_out) sum_d_out[0] = sd;
     }
     double x0 = 0.0, xi = x0;
     int i = 1;
@@ -445,11 +469,7 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
                 v[1] = fma(km, -t * t, v[1]);
             }
         }
-        if constexpr (ASYNC) {
-            if (!async_allsum(v, cs, iter++)) { exchange_ok = false; xi = NAN; break; }
-        } else {
-            cluster_allsum<2>(v, ca, parity);
-        }
+        if (!exchange_ok || !allsum(v)) { exchange_ok = false; xi = NAN; break; }
         const double fi = (v[0] * a.inv_nk - tail + cst) * inv_beta - rhs;
         const double dfi = (v[1] * a.inv_nk - tail + cst) * inv_beta;
         const double dfii = 1.0 / dfi;
@@ -470,6 +490,16 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
             ck_xi = bxi;
             ck_i = i;
         }
+    }
+    // the chain's sum_kω(chi_m) at the final λ (the EoM's tail term), instead of a k_sum_kw launch after
+    if (sum_m_out) {
+        double v[2] = {0.0, 0.0};
+        for (int e = tid; e < total; e += nth) {
+            const double x = chi[e];
+            v[0] = fma(kmult[e % a.nq], xi != 0.0 ? x / (xi * x + 1.0) : x, v[0]);
+        }
+        if (exchange_ok && !allsum(v)) exchange_ok = false;
+        if (tid == 0) sum_m_out[0] = exchange_ok ? (v[0] * a.inv_nk - tail + cst) * inv_beta : NAN;
     }
     if (tid == 0) {
         out[0] = exchange_ok ? xi : NAN;   // an exchange that timed out leaves no valid λ
@@ -764,7 +794,7 @@ int launch_epot_vjp(ldga_ctx* ctx, int numax, double mu, const double2* sigma, d
 
 int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar) {
     double2* colF = reinterpret_cast<double2*>(ctx->d_red + 64);
-    k_colsum_F<<<64, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
+    k_colsum_F<<<std::min(4 * 148, (ctx->Nnu * ctx->Nw + 7) / 8), 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
     LDGA_LAUNCHED(ctx, "k_colsum_F");
     k_lambda0_vjp<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, ctx->Nw, 1.0 / (ctx->mp.beta * ctx->mp.beta),
                                                     colF, l0_bar, chi0_bar);
@@ -775,7 +805,7 @@ int launch_lambda0_vjp(ldga_ctx* ctx, const double2* l0_bar, double2* chi0_bar) 
 int launch_lambda0(ldga_ctx* ctx) {
     double2* colF = reinterpret_cast<double2*>(ctx->d_red + 64);
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA0);
-    k_colsum_F<<<64, 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
+    k_colsum_F<<<std::min(4 * 148, (ctx->Nnu * ctx->Nw + 7) / 8), 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
     LDGA_LAUNCHED(ctx, "k_colsum_F");
     k_lambda0<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, ctx->Nw, 1.0 / (ctx->mp.beta * ctx->mp.beta),
                                                 ctx->d_chi0, colF, ctx->d_lambda0);
@@ -822,7 +852,7 @@ int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
 // lambda_m Newton: rhs = rhs_const - *rhs_sub_dev (if given); d_out[0] = lambda, d_out[1] = iterations;
 // d_out[2] receives lambda_min; d_out[3..4] the periodic-trajectory skip (iteration, period).
 int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out, int nsteps,
-                    double atol) {
+                    double atol, double* sum_d_out, double* sum_m_out) {
     int st = launch_lambda_min(ctx, LDGA_CH_M, d_out + 2);
     if (st) return st;
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
@@ -839,7 +869,8 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
               : per <= 24 ? (as ? k_lambda_m<24, true> : k_lambda_m<24, false>)
               : (as ? k_lambda_m<0, true> : k_lambda_m<0, false>);
     kern<<<kCluster, kNewtonThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
-                                                   d_out + 2, nsteps, atol, d_out);
+                                                   d_out + 2, nsteps, atol, d_out,
+                                                   sum_d_out ? ctx->d_chi[LDGA_CH_D] : nullptr, sum_d_out, sum_m_out);
     LDGA_LAUNCHED(ctx, "k_lambda_m");
     return LDGA_OK;
 }
@@ -931,7 +962,7 @@ extern "C" int ldga_lambda0_noalloc(const double* chi0, const double* F, int32_t
     double2* colF = noalloc_colF(dev, &e);
     if (!colF) return ctx_fail(nullptr, LDGA_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_colsum_F<<<64, 256, 0, s>>>(nnu, nw, reinterpret_cast<const double2*>(F), colF);
+    k_colsum_F<<<std::min(4 * 148, (nnu * nw + 7) / 8), 256, 0, s>>>(nnu, nw, reinterpret_cast<const double2*>(F), colF);
     k_lambda0<<<4 * 148, 256, 0, s>>>(nq, nnu, nw, 1.0 / (beta * beta), reinterpret_cast<const double2*>(chi0), colF,
                                       reinterpret_cast<double2*>(lambda0_out));
     e = cudaGetLastError();

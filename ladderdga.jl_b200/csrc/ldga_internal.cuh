@@ -120,6 +120,10 @@ struct ldga_ctx {
     int n_bub_pairs = 0;
 
     cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
+    // ldga_chain_m's copies that overlap its kernels: the vertices and local inputs go in on io_stream
+    // while G and the bubble run, chi_m/chi_d come out there while the λ and EoM stages run
+    cudaStream_t io_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_gamma = nullptr, ev_loc = nullptr, ev_chi = nullptr, ev_join = nullptr;
     bool capturing = false;              // a CUDA graph of the chain is being captured
 
     // fused chain (ldga_chain_m): persistent input buffers and the captured graph
@@ -243,9 +247,12 @@ int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const doubl
 int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev = nullptr);
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
 int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2);
-// newton_right's defaults (LambdaCorrection/helpers.jl:133): nsteps 100, atol 1e-13
+// newton_right's defaults (LambdaCorrection/helpers.jl:133): nsteps 100, atol 1e-13.  sum_d_out given:
+// rhs = rhs_const - sum_kω(chi_d) is formed in the kernel and the sum stored there (rhs_sub_dev unused);
+// sum_m_out given: sum_kω(chi_m) at the final λ is stored there.
 int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out /*[5]*/,
-                    int nsteps = 100, double atol = 1e-13);
+                    int nsteps = 100, double atol = 1e-13, double* sum_d_out = nullptr,
+                    double* sum_m_out = nullptr);
 int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[4]*/);
 int launch_g_ladder_full(ldga_ctx* ctx, int numax, const double* mu_dev);
 int launch_calc_E(ldga_ctx* ctx, const double2* G, int ldg, const double2* sigma, int numax, double mu,
