@@ -259,7 +259,6 @@ __global__ void k_colsum_F(int nnu, int nw, const double2* __restrict__ F, doubl
         if (lane == 0) colF[c] = acc;
     }
 }
-}
 
 __global__ void k_lambda0(int nq, int nnu, int nw, double inv_beta2, const double2* __restrict__ chi0,
                           const double2* __restrict__ colF, double2* __restrict__ l0) {
