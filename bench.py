@@ -658,13 +658,18 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None, steps: int = 1) -> d
             # in lockstep, 8 N^2 + 8 N FP64 flops per q and pass (6 N^2 + 8 N on the FP64 tensor
             # path, whose complex product takes three real products); the FP32 corrections 8 N^2 each.
             peak, peak_src = fp64_peak(peaks, sm_mhz)
-            qpw = {"iter": 8, "iter8": 4, "iter8x2": 8, "iter8x2tc": 8, "iter8x2dm": 8}.get(cfg.split(":")[0], 8)
+            qpw = {"iter": 8, "iter8": 4, "iter8x2": 8, "iter8x2tc": 8, "iter8x2dm": 8,
+                   "iter8x2dm2": 8}.get(cfg.split(":")[0], 8)
+            nprod = 2.0 if "dm2" in cfg else 1.0   # the second-order correction: two TF32 products a pass
             passes, warps = sweeps if sweeps else (0, 1)
             prod = 6.0 if "dm" in cfg else 8.0
             f64 = passes * qpw * (prod * nnu**2 + 8.0 * nnu) / max(cnt, 1)
-            f32 = (passes - warps) * qpw * 8.0 * nnu**2 / max(cnt, 1)
+            f32 = nprod * (passes - warps) * qpw * 8.0 * nnu**2 / max(cnt, 1)
             exe = f64 / t / 1e12
             kname = ("k_bse_iter (FP32 group inverse; FP64 residual on the FP64 tensor path, mma.sync m8n8k4, "
+                     "three real products per complex tile; second-order correction C r - C (dD C r), two TF32 "
+                     "tensor-core products a pass)" if "dm2" in cfg else
+                     "k_bse_iter (FP32 group inverse; FP64 residual on the FP64 tensor path, mma.sync m8n8k4, "
                      "three real products per complex tile; FP32 product on tensor cores, mma.sync TF32)"
                      if "dm" in cfg else
                      "k_bse_iter (FP32 group inverse, FP64 residual passes, FP32 product on tensor cores: "
@@ -676,6 +681,7 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None, steps: int = 1) -> d
                     "passes_per_warp": passes / max(warps, 1),
                     "fp32_tflops": f32 / t / 1e12,
                     "reference_formulation_tflops": ach,
+                    "reference_formulation_frac_of_bf16": ach / peaks.get("bf16_tflops", 1590.0),
                     "channels_per_launch": chans,
                     "traffic": BSE_ITER_DRAM_BYTES_PER_MATRIX * chans * nq * nw if nnu == 40 else None,
                     "traffic_source": ("ncu dram__bytes_read+write of one launch on 3D 32^3 (39 729 matrices)"
