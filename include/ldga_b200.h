@@ -224,6 +224,16 @@ const char* ldga_bse_config_name(int32_t nnu, int32_t precision, int32_t index);
 int ldga_bse_sweeps(ldga_ctx* ctx, int64_t* passes, int64_t* warps);
 /* Forget every recorded choice: all box sizes use their default configuration again. */
 int ldga_tune_reset(void);
+/* Device self-test of the tensor-core group inverse that the MIXED BSE's preconditioner uses (no
+ * reference counterpart; it stands in for LapackWrapper.jl's inverse inside the preconditioner):
+ * Newton-Schulz iterations X <- X (2I - b X) on tcgen05 tensor cores (TF32 operands, FP32
+ * accumulation in tensor memory), one CTA on the current device.  b, x0, x_out: n x n complex,
+ * row-major interleaved FP32 host arrays (n = 40).  its >= 0: x_out = the iterate after `its`
+ * iterations from x0, err_out[0] = max_i sum_j |I - b X|_ij of the iterate before the last update;
+ * its < 0: x_out = the single product b x0 (TF32 factors), err_out[0] = 0.  Returns LDGA_ERR_ARG
+ * for other n, LDGA_ERR_NUMERIC when a tensor-core completion wait ran out. */
+int ldga_selftest_group_inverse(int32_t n, const float* b, const float* x0, int32_t its, float* x_out,
+                                float* err_out);
 
 /* Copy a device-resident array of the handle to `out` (host or device) without recomputing it.
  * No reference counterpart: the reference's arrays live in Julia memory; here they stay in HBM

@@ -39,6 +39,7 @@
 #include <mutex>
 
 #include "ldga_internal.cuh"
+#include "ns_inverse.cuh"
 
 #ifndef LDGA_LU_LOOKAHEAD
 #define LDGA_LU_LOOKAHEAD true
@@ -1351,6 +1352,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 // that the LPQ distinct rows of a warp fetch in one wavefront (row stride N + 1).  Warps iterate
 // independently (no CTA barrier in the loop) until all q of the warp have converged.
 constexpr int kIterQ = 32;      // q per CTA: one preconditioner
+constexpr int kNsMaxIts = 6;    // Newton-Schulz iterations at most (tensor-core group inverse)
+constexpr float kNsTol = 1e-2f; // stop once (max row sum of |I - B_bar X|)^2 <= kNsTol
 constexpr int kIterMax = 40;    // sweeps before a q is handed to the pivoted solve
 constexpr double kIterTol = 1e-14;
 
@@ -1360,7 +1363,12 @@ constexpr double kIterTol = 1e-14;
 // residuals into B-fragment order and the products back to the lanes that own the rows.
 // DM: the FP64 residual product runs on the FP64 tensor path (mma.sync m8n8k4 .f64): Gamma^T is kept
 // as the A fragments of its real and imaginary parts (N/8 x N/4 tiles of 8 x 4) instead of row-major.
-template <int N, bool GSM = true, bool TC = false, int NWARP = 4, bool DM = false>
+// NS: the group inverse is formed by Newton-Schulz iterations on tcgen05 tensor cores
+// (ns_inverse.cuh) instead of the Gauss-Jordan elimination, which stays as the fallback when the
+// iteration does not converge.  Its operand buffers occupy [0, NsSmem::bytes) during the set-up,
+// where the Gamma^T fragments and the C fragments / exchange buffers go afterwards, so D moves
+// behind them; the mbarrier, the TMEM address and a reduction scratch follow the pivot buffers.
+template <int N, bool GSM = true, bool TC = false, int NWARP = 4, bool DM = false, bool NS = false>
 struct IterSmem {
     static constexpr int LD = N + 1;
     static constexpr int MT = (N + 15) / 16, KT = N / 8, XS = 2 * N + 4;   // TC tiles, exchange stride
@@ -1371,10 +1379,14 @@ struct IterSmem {
                                          : (size_t)N * LD * sizeof(float2);
     // Gt [N][LD] double2 (GSM: Gamma staged in shared memory; otherwise read through L1/L2); DM: the
     // A fragments [2][N/8][N/4][32] doubles
-    static constexpr size_t off_D = DM ? (size_t)N * N * sizeof(double2) : GSM ? (size_t)N * LD * sizeof(double2) : 0;
-    static constexpr size_t off_C = off_D + (size_t)kIterQ * N * sizeof(double2);  // D [32][N] double2
+    static constexpr size_t g_bytes = DM ? (size_t)N * N * sizeof(double2) : GSM ? (size_t)N * LD * sizeof(double2) : 0;
+    static constexpr size_t d_bytes = (size_t)kIterQ * N * sizeof(double2);      // D [32][N] double2
+    static constexpr size_t ns_bytes = NS ? ns::NsSmem<(N % 8 == 0 ? N : 8)>::bytes : 0;
+    static constexpr size_t c_end = g_bytes + ((c_bytes + 15) & ~size_t(15));
+    static constexpr size_t off_D = NS ? (c_end > ns_bytes ? c_end : ns_bytes) : g_bytes;
+    static constexpr size_t off_C = NS ? g_bytes : off_D + d_bytes;
     static constexpr size_t off_X = off_C + (TC ? (size_t)2 * MT * KT * 32 * 4 * sizeof(float) : 0);  // TC exchange
-    static constexpr size_t off_rowabs = off_C + ((c_bytes + 15) & ~size_t(15));
+    static constexpr size_t off_rowabs = NS ? off_D + d_bytes : off_C + ((c_bytes + 15) & ~size_t(15));
     static constexpr size_t off_dbar = off_rowabs + (((size_t)N * sizeof(double) + 15) & ~size_t(15));
     // Gauss-Jordan pivot buffers [2][columns k, k+1: 2 N float2][rows k, k+1 interleaved: RW float4],
     // RW = the row width the owning threads cover (N rounded up to their segments)
@@ -1382,7 +1394,10 @@ struct IterSmem {
     static constexpr int RW = (N + TPR - 1) / TPR * TPR;
     static constexpr size_t pc_half = 2 * (size_t)N * sizeof(float2) + (size_t)RW * sizeof(float4);
     static constexpr size_t off_pc = off_dbar + (size_t)N * sizeof(double2);
-    static constexpr size_t bytes = off_pc + 2 * pc_half;
+    // NS: mbarrier (8 bytes), TMEM address (4, padded to 8), reduction scratch [NWARP] floats
+    static constexpr size_t off_bar = off_pc + 2 * pc_half, off_slot = off_bar + 8, off_red = off_bar + 16;
+    static constexpr size_t bytes = NS ? off_red + ((NWARP * sizeof(float) + 15) & ~size_t(15)) : off_pc + 2 * pc_half;
+    static_assert(!NS || off_bar % 8 == 0, "mbarrier alignment");
 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -1632,15 +1647,17 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
     return acc;
 }
 
-template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2>
+template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2, bool NS>
 __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a_m, const BseArgs a_d,
                                                                        const int32_t* __restrict__ perm) {
     // blockIdx.z selects the channel: one launch may cover both (they share chi0 and the q order),
     // so the second channel's CTAs fill the SMs the first one's tail leaves idle
     BseArgs a = a_m;
     if (blockIdx.z) { a.s = a_d.s; a.Gamma = a_d.Gamma; a.chi = a_d.chi; a.gam = a_d.gam; a.flags = a_d.flags; }
-    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM, NS>;
     static_assert(!DM || (GSM && TC), "the FP64 tensor product is built with the tensor-core FP32 product");
+    static_assert(!NS || (DM && N % 8 == 0 && kIterQ * LPQ / QPL == 128),
+                  "the tensor-core group inverse is built for the DM configuration, 128 threads");
     constexpr int LD = S::LD;
     constexpr int LDG = GSM ? LD : N;   // row stride of Gamma^T where it is read
     constexpr int RPL = (N + LPQ - 1) / LPQ;
@@ -1677,7 +1694,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             return Gt[i * LDG + j];
         }
     };
-    if constexpr (GSM) {
+    auto stage_gamma = [&]() {
+      if constexpr (GSM) {
         constexpr int NG = (N * N + NT - 1) / NT;
         double2 gv[NG];
 #pragma unroll
@@ -1699,6 +1717,20 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 }
             }
         }
+      }
+    };
+    // NS: the tensor-core group inverse's mbarrier and TMEM (128 columns; 3 CTAs per SM take 384 of
+    // the 512), set up while D loads; Gamma^T is staged after the inverse, whose buffers it reuses
+    uint64_t* ns_bar = reinterpret_cast<uint64_t*>(it_raw + S::off_bar);
+    uint32_t* ns_slot = reinterpret_cast<uint32_t*>(it_raw + S::off_slot);
+    if constexpr (NS) {
+        if (tid == 0) {
+            tc05::mbar_init(ns_bar, 1);
+            tc05::mbar_fence_init();
+        }
+        if (tid < 32) tc05::tmem_alloc(ns_slot, ns::NsSmem<N>::tmem_cols);
+    } else {
+        stage_gamma();
     }
     {
         constexpr int ND = (kIterQ * N + NT - 1) / NT;
@@ -1747,14 +1779,18 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     // |row|_1 of Gamma^T (one thread per row) and the group's mean diagonal (one thread per nu, in
     // another warp), each a sequential sum in a fixed order: no shuffle chains on the set-up path
     static_assert(NT >= 64 + N, "row sums in threads 0..N-1, diagonal means in threads 64..63+N");
-    if (tid < N) {
-        double sacc = 0.0;
-        for (int j = 0; j < N; ++j) {
-            const double2 v = gelt(tid, j);
-            sacc += fabs(v.x) + fabs(v.y);
+    auto row_sums = [&]() {
+        if (tid < N) {
+            double sacc = 0.0;
+            for (int j = 0; j < N; ++j) {
+                const double2 v = gelt(tid, j);
+                sacc += fabs(v.x) + fabs(v.y);
+            }
+            rowabs[tid] = sacc;
         }
-        rowabs[tid] = sacc;
-    } else if (tid >= 64 && tid < 64 + N) {
+    };
+    if constexpr (!NS) row_sums();
+    if (tid >= 64 && tid < 64 + N) {
         const int i = tid - 64;
         double2 m = dmk(0.0, 0.0);
         for (int q = 0; q < nvalid; ++q) m = cadd(m, Dq[q * N + i]);
@@ -1770,7 +1806,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     // the same update writes -(a_i,k:k+1 P^-1) into columns k, k+1 (the Gauss-Jordan column entries)
     // with no per-element branch; the pivot rows become P^-1 u (and P^-1 in the pivot columns, which
     // is the +I term's product minus the identity).  Mathematically two single-pivot steps.
-    {
+    // elt(i, j): element B_ij without the diagonal term.
+    auto gauss_jordan = [&](auto&& elt) {
         static_assert(N % 2 == 0, "pivot pairs");
         constexpr int TPR = NT / N > 0 ? NT / N : 1;
         constexpr int CPT = (N + TPR - 1) / TPR;
@@ -1782,7 +1819,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             const int jj = j0 + c;
             ce[c] = make_float2(0.f, 0.f);
             if (own && jj < N) {
-                double2 v = gelt(gi, jj);
+                double2 v = elt(gi, jj);
                 if (gi == jj) v = cadd(v, dbar[gi]);
                 ce[c] = make_float2((float)v.x, (float)v.y);
             }
@@ -1877,6 +1914,92 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                     if (j0 + c < N) C[gi * LD + j0 + c] = ce[c];
             }
         }
+    };
+    if constexpr (!NS) {
+        gauss_jordan(gelt);
+    } else {
+        // ---- C = B_bar^-1 by Newton-Schulz iterations on the tensor cores (ns_inverse.cuh) from the
+        // Jacobi seed X_0 = diag(1 / B_bar_ii): B_bar's rows come from Gamma(w) in global memory (L2)
+        // and D_bar.  Where the seed is too far (the iteration diverges) the Gauss-Jordan elimination
+        // above forms C instead; either way C only sets the sweep count, which the FP64 residual checks.
+        using NSm = ns::NsSmem<N>;
+        constexpr int FR = S::MT * S::KT * 32 * 4;
+        unsigned char* nsb = it_raw;
+        float* ns_red = reinterpret_cast<float*>(it_raw + S::off_red);
+        if (tid < N) {
+            const double2* grow = Gw + (size_t)tid * N;
+            float2 dinv = make_float2(0.f, 0.f);
+#pragma unroll 1
+            for (int k = 0; k < N; k += 4) {
+                float re[4], im[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    double2 v = grow[k + u];
+                    if (k + u == tid) {
+                        v = cadd(v, dbar[tid]);
+                        dinv = vinv(make_float2((float)v.x, (float)v.y));
+                    }
+                    re[u] = (float)v.x;
+                    im[u] = (float)v.y;
+                }
+                ns::store_a4<N>(nsb + NSm::off_br, tid, k, re[0], re[1], re[2], re[3]);
+                ns::store_a4<N>(nsb + NSm::off_bi, tid, k, im[0], im[1], im[2], im[3]);
+            }
+#pragma unroll 1
+            for (int k = 0; k < N; k += 4) {
+                float xr4[4], xi4[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    xr4[u] = k + u == tid ? dinv.x : 0.f;
+                    xi4[u] = k + u == tid ? dinv.y : 0.f;
+                    ns::store_b<N>(nsb + NSm::off_tr, tid, k + u, xr4[u]);
+                    ns::store_b<N>(nsb + NSm::off_ti, tid, k + u, xi4[u]);
+                }
+                ns::store_a4<N>(nsb + NSm::off_xr, tid, k, xr4[0], xr4[1], xr4[2], xr4[3]);
+                ns::store_a4<N>(nsb + NSm::off_xi, tid, k, xi4[0], xi4[1], xi4[2], xi4[3]);
+            }
+        }
+        tc05::fence_before();
+        __syncthreads();                           // the TMEM address is visible
+        tc05::fence_after();
+        ns::NsState st{*ns_slot, 0u, true};
+        auto emit_cf = [&](int t, int c, const float (&re)[16], const float (&im)[16]) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int jj = c + j;
+                if (jj < N) {
+                    const int mt = t >> 4, m16 = t & 15, kt = jj >> 3, k8 = jj & 7;
+                    const int idx = ((mt * S::KT + kt) * 32 + (m16 & 7) * 4 + (k8 & 3)) * 4 + (m16 >> 3) + 2 * (k8 >> 2);
+                    Cf[idx] = to_tf32(re[j]);
+                    Cf[FR + idx] = to_tf32(im[j]);
+                }
+            }
+        };
+        const bool ok = ns::newton_schulz<N>(nsb, ns_bar, ns_red, st, kNsMaxIts, kNsTol, emit_cf, nullptr);
+        ns::drain(st, ns_bar);
+        tc05::fence_before();
+        __syncthreads();
+        if (tid < 32) {
+            tc05::fence_after();
+            tc05::tmem_free(st.tmem, NSm::tmem_cols);
+        }
+        if (ok) {
+            // zero rows N .. 16 MT - 1 of the fragments (the inverse's buffers overlapped them)
+            if (tid >= N && tid < 16 * S::MT) {
+                for (int jj = 0; jj < N; ++jj) {
+                    const int mt = tid >> 4, m16 = tid & 15, kt = jj >> 3, k8 = jj & 7;
+                    const int idx = ((mt * S::KT + kt) * 32 + (m16 & 7) * 4 + (k8 & 3)) * 4 + (m16 >> 3) + 2 * (k8 >> 2);
+                    Cf[idx] = 0u;
+                    Cf[FR + idx] = 0u;
+                }
+            }
+        } else {
+            gauss_jordan([&](int i, int j) { return Gw[(size_t)i * N + j]; });
+        }
+        __syncthreads();
+        stage_gamma();
+        __syncthreads();
+        row_sums();
     }
     __syncthreads();
 
@@ -2566,11 +2689,12 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 // autotuner (ldga_autotune_bse) times all entries on the handle's own data and records the fastest.
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
 using BseRunPair = int (*)(ldga_ctx*, const BseArgs&, const BseArgs&);
-template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false>
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
+          bool NS = false>
 int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
-    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM>;
-    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2>;
+    using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM, NS>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2, NS>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
@@ -2594,14 +2718,16 @@ int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
     return LDGA_OK;
 }
 
-template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false>
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
+          bool NS = false>
 int run_iter(ldga_ctx* ctx, const BseArgs& a) {
-    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2>(ctx, a, nullptr);
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS>(ctx, a, nullptr);
 }
 
-template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false>
+template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
+          bool NS = false>
 int run_iter_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) {
-    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2>(ctx, a_m, &a_d);
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS>(ctx, a_m, &a_d);
 }
 
 struct BseVariant {
@@ -2636,7 +2762,10 @@ LDGA_ITER_BOX(30, 4, 3)
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
-const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true, true, true>, "iter8x2dm2:3", &run_iter_pair<40, 8, 3, 2, true, true, true, true>},
+// the default: the group inverse by Newton-Schulz on tcgen05 tensor cores (Gauss-Jordan as its fallback)
+const BseVariant mixed_40[] = {{&run_iter<40, 8, 3, 2, true, true, true, true, true>, "iter8x2dm2ns:3",
+                                &run_iter_pair<40, 8, 3, 2, true, true, true, true, true>},
+                               {&run_iter<40, 8, 3, 2, true, true, true, true>, "iter8x2dm2:3", &run_iter_pair<40, 8, 3, 2, true, true, true, true>},
                                {&run_iter<40, 8, 2, 2, true, true, true, true>, "iter8x2dm2:2", &run_iter_pair<40, 8, 2, 2, true, true, true, true>},
                                {&run_iter<40, 8, 3, 2, true, true, true>, "iter8x2dm:3", &run_iter_pair<40, 8, 3, 2, true, true, true>},
                                {&run_iter<40, 8, 2, 2, true, true, true>, "iter8x2dm:2", &run_iter_pair<40, 8, 2, 2, true, true, true>},
@@ -2857,4 +2986,129 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
     k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, ctx->Nq * ctx->Nw, d_fail);
     LDGA_LAUNCHED(ctx, "k_count_flags");
     return LDGA_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Self-test of the tcgen05 Newton-Schulz group inverse (ns_inverse.cuh), one CTA of 128 threads on
+// an N x N complex matrix b (row-major float2) and seed x0.  its >= 0: its iterations from x0, x_out
+// = the iterate, err_out[0] = max_i sum_j |I - b X|_ij of the iterate before the last update (0 when
+// its = 0); its < 0: x_out = the single product b x0 (both factors rounded to TF32).
+namespace {
+
+template <int N>
+struct NsTestSmem {
+    using S = ns::NsSmem<N>;
+    // 4 KB beyond the operand buffers: every byte the descriptors can address stays inside the
+    // allocation whichever of the two strides the hardware applies to rows
+    static constexpr uint32_t off_bar = S::bytes + 4096, off_slot = off_bar + 8, off_red = off_bar + 16;
+    static constexpr uint32_t bytes = off_red + 64;
+};
+
+template <int N>
+__global__ void __launch_bounds__(128) k_ns_selftest(const float2* __restrict__ b, const float2* __restrict__ x0,
+                                                      int its, float2* __restrict__ xout, float* __restrict__ err,
+                                                      int32_t* __restrict__ status) {
+    using S = ns::NsSmem<N>;
+    using T = NsTestSmem<N>;
+    extern __shared__ __align__(128) unsigned char ns_raw[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ns_raw + T::off_bar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(ns_raw + T::off_slot);
+    float* red = reinterpret_cast<float*>(ns_raw + T::off_red);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) {
+        tc05::mbar_init(bar, 1);
+        tc05::mbar_fence_init();
+    }
+    if (warp == 0) tc05::tmem_alloc(slot, S::tmem_cols);
+    if (tid < N) {
+        for (int k = 0; k < N; k += 4) {
+            float v[4][4];
+            for (int u = 0; u < 4; ++u) {
+                const float2 bb = b[tid * N + k + u], xx = x0[tid * N + k + u];
+                v[0][u] = bb.x; v[1][u] = bb.y; v[2][u] = xx.x; v[3][u] = xx.y;
+            }
+            ns::store_a4<N>(ns_raw + S::off_br, tid, k, v[0][0], v[0][1], v[0][2], v[0][3]);
+            ns::store_a4<N>(ns_raw + S::off_bi, tid, k, v[1][0], v[1][1], v[1][2], v[1][3]);
+            ns::store_a4<N>(ns_raw + S::off_xr, tid, k, v[2][0], v[2][1], v[2][2], v[2][3]);
+            ns::store_a4<N>(ns_raw + S::off_xi, tid, k, v[3][0], v[3][1], v[3][2], v[3][3]);
+            for (int u = 0; u < 4; ++u) {
+                ns::store_b<N>(ns_raw + S::off_tr, tid, k + u, v[2][u]);
+                ns::store_b<N>(ns_raw + S::off_ti, tid, k + u, v[3][u]);
+            }
+        }
+        if (its == 0)
+            for (int j = 0; j < N; ++j) xout[tid * N + j] = x0[tid * N + j];
+    }
+    tc05::fence_before();
+    __syncthreads();
+    tc05::fence_after();
+    ns::NsState st{*slot, 0u, true};
+    float e = 0.f;
+    auto emit = [&](int t, int c, const float (&re)[16], const float (&im)[16]) {
+        for (int j = 0; j < 16; ++j)
+            if (c + j < N) xout[t * N + c + j] = make_float2(re[j], im[j]);
+    };
+    if (its > 0) {
+        ns::newton_schulz<N>(ns_raw, bar, red, st, its, 0.f, emit, &e);
+    } else if (its < 0) {
+        const uint32_t base = tc05::smem_addr(ns_raw);
+        ns::product<N>(st, bar, base + S::off_br, base + S::off_bi, base + S::off_tr, base + S::off_ti);
+        if (warp < (N + 31) / 32) {
+            for (int c = 0; c < N; c += 16) {
+                float re[16], im[16];
+                ns::load_chunk(st.tmem + ((uint32_t)(32 * warp) << 16), c, re, im);
+                if (tid < N) emit(tid, c, re, im);
+            }
+        }
+    }
+    ns::drain(st, bar);
+    tc05::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc05::fence_after();
+        tc05::tmem_free(st.tmem, S::tmem_cols);
+    }
+    if (tid == 0) {
+        err[0] = e;
+        status[0] = st.ok ? 0 : 1;
+    }
+}
+
+}  // namespace
+
+extern "C" int ldga_selftest_group_inverse(int32_t n, const float* b, const float* x0, int32_t its, float* x_out,
+                                           float* err_out) {
+    if (n != 40 || !b || !x0 || !x_out || !err_out || its > 16) return LDGA_ERR_ARG;
+    using T = NsTestSmem<40>;
+    const size_t mb = (size_t)n * n * 2 * sizeof(float);
+    float2 *db = nullptr, *dx = nullptr, *dout = nullptr;
+    float* derr = nullptr;
+    int32_t* dst = nullptr;
+    int rc = LDGA_OK;
+    int32_t status = 0;
+    float err = 0.f;
+    if (cudaMalloc(&db, mb) != cudaSuccess || cudaMalloc(&dx, mb) != cudaSuccess || cudaMalloc(&dout, mb) != cudaSuccess ||
+        cudaMalloc(&derr, sizeof(float)) != cudaSuccess || cudaMalloc(&dst, sizeof(int32_t)) != cudaSuccess) {
+        rc = LDGA_ERR_CUDA;
+    }
+    if (rc == LDGA_OK && (cudaMemcpy(db, b, mb, cudaMemcpyHostToDevice) != cudaSuccess ||
+                          cudaMemcpy(dx, x0, mb, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = LDGA_ERR_CUDA;
+    if (rc == LDGA_OK) {
+        auto kern = k_ns_selftest<40>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::bytes) != cudaSuccess) {
+            rc = LDGA_ERR_CUDA;
+        } else {
+            kern<<<1, 128, T::bytes>>>(db, dx, its, dout, derr, dst);
+            if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = LDGA_ERR_CUDA;
+        }
+    }
+    if (rc == LDGA_OK && (cudaMemcpy(x_out, dout, mb, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                          cudaMemcpy(&err, derr, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                          cudaMemcpy(&status, dst, sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess))
+        rc = LDGA_ERR_CUDA;
+    cudaFree(db); cudaFree(dx); cudaFree(dout); cudaFree(derr); cudaFree(dst);
+    if (rc != LDGA_OK) return rc;
+    err_out[0] = err;
+    return status == 0 ? LDGA_OK : LDGA_ERR_NUMERIC;
 }
