@@ -86,6 +86,10 @@ def parse():
                          "adjoint: the chain's vector-Jacobian product (ldga_chain_vjp) against its forward "
                          "(ldga_chain_m) on 2D 48^2, Nnu=40, Nw=41")
     ap.add_argument("--points", type=int, default=64, help="points of the batch workload")
+    ap.add_argument("--shard", default="points", choices=["points", "omega"],
+                    help="points: every rank runs its own parameter point (weak scaling, the default); omega: "
+                         "the ranks split one point's bosonic frequencies (strong scaling; the chain runs stage "
+                         "by stage with one all-reduce of chi and one of Sigma_ladder)")
     ap.add_argument("--cfg", type=int, default=3, choices=[1, 2, 3],
                     help="single-point configuration of the chain workload (3: the headline 3D 32^3 point)")
     ap.add_argument("--lambda", dest="lam", default=None, choices=["m", "dm"],
@@ -724,6 +728,81 @@ def roofline(stages: dict, chain, peaks: dict, sweeps=None, steps: int = 1) -> d
             "peak_source": peaks.get("source", "measured hbm_gbs (MEASURED_PEAKS.json)")}
 
 
+def run_omega_sharded(args):
+    """One parameter point's λm chain with its ω range split over the ranks (parallel.py): every
+    step is bubble -> BSE (m, d) -> λ₀ on this rank's block, one all-reduce of χ_m and χ_d, the λm
+    Newton, this block's Σ_ladder part, one all-reduce of Σ_ladder, the μ fit and the energies.
+    Strong scaling: value = the point's (q, ω) units / the slowest rank's step time (CUDA events on
+    the handle's stream around each step; the step's library calls return after their work)."""
+    import torch
+    import ladderdga_b200 as L
+    from ladderdga_b200 import parallel as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    group = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    inp, wname, data = workload_input(args, 0)          # every rank: the same point
+    if lam_type(args) != "m":
+        raise SystemExit("--shard omega runs the lambda_m chain")
+    h = L.setup_synthetic(inp, precision=PREC_NAMES[args.prec], device=local)
+    stream = torch.cuda.current_stream(local)
+    h.ctx.call("ldga_set_stream", C.c_void_p(stream.cuda_stream))
+    stages = P.HandleStages(h)
+    points = h.ctx.Nq * h.ctx.Nw
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    n0 = C.c_int64()
+    res = None
+    for _ in range(max(args.warmup, 3)):
+        res = P.λm_chain_omega_sharded(stages, group)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    h.ctx.call("ldga_launch_count", C.byref(n0))
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        res = P.λm_chain_omega_sharded(stages, group)
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    n1 = C.c_int64()
+    h.ctx.call("ldga_launch_count", C.byref(n1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = float(np.mean(times))
+    if world > 1:
+        from ladderdga_b200.parallel import max_over_ranks
+        ms = max_over_ranks(ms, device=torch.device("cuda", local))
+    if rank == 0:
+        line = {"metric": METRIC, "value": points / (ms / 1e3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64+f32" if args.prec == "mixed" else "f64", "data": data,
+                "impl": "ours", "precision_mode": args.prec,
+                "config": {"workload": wname, "global_batch": 1, "seq_len": None, "parallelism": f"omega{world}",
+                           "l2": "flushed (256 MiB write) before each step", "points_per_step": points,
+                           "omega_block": list(res["block"])},
+                "gpu_launches": int(n1.value - n0.value),
+                "result": {"lambda_m": res["lambda_m"], "mu": res["mu"], "E_kin": res["E_kin"],
+                           "E_pot1": res["E_pot1"], "newton_iterations": res["newton_iterations"]},
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(line) + "\n")
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -1093,6 +1172,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.shard == "omega":
+        return run_omega_sharded(args)
     return run_ours(args)
 
 

@@ -113,6 +113,18 @@ int ldga_launch_count(const ldga_ctx* ctx, int64_t* n);
 
 /* Replace the model parameters (e.g. a new mu); mutable ModelParameters, Config.jl:39. */
 int ldga_set_model(ldga_ctx* ctx, const ldga_model* mp);
+/* ω shard of one parameter point over several handles (one per GPU): the reference's partition of
+ * the bosonic frequencies over workers (gen_ω_part / par_partition, parallelization_helpers.jl:22-53;
+ * calc_bubble_par / calc_χγ_par / calc_Σ_par, ladderDGATools.jl:46-245).  After the call,
+ * ldga_bubble, ldga_bse, ldga_lambda0 and ldga_eom cover the indices [w_lo, w_hi) of 0..Nw-1 only
+ * (arrays keep the whole layout; entries outside the shard are not written).  ldga_eom then returns
+ * this shard's part of Sigma_ladder; the 1/(i nu) tail and the Hartree term are added only where
+ * constants != 0, so the shards' parts sum to the whole Sigma_ladder (given the whole chi_m).
+ * The sums, lambda_min and the lambda_m Newton read the whole chi arrays (set them with
+ * ldga_set_chi after gathering the shards).  ldga_chain_m, ldga_batch_chain_m, ldga_lambda_dm,
+ * ldga_run_sc, ldga_eom_parts and the adjoints return LDGA_ERR_STATE on a sharded handle.
+ * ldga_set_omega_shard(ctx, 0, Nw, 1) restores the whole range. */
+int ldga_set_omega_shard(ldga_ctx* ctx, int32_t w_lo, int32_t w_hi, int32_t constants);
 int ldga_set_precision(ldga_ctx* ctx, int32_t precision);
 
 /* k-grid of the handle: kG.kMult, kG.ϵkGrid and the wedge coordinates (Dispersions.jl; used at

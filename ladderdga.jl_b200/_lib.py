@@ -30,7 +30,7 @@ EXPORTS = [
     "ldga_get", "ldga_chain_m", "ldga_lambda0_noalloc", "ldga_batch_chain_m", "ldga_run_sc", "ldga_bse_vjp",
     "ldga_eom_vjp", "ldga_autotune_bse", "ldga_tune_save", "ldga_tune_load",
     "ldga_tune_reset", "ldga_bse_config_name", "ldga_gloc_vjp", "ldga_epot_vjp", "ldga_chain_vjp",
-    "ldga_bse_sweeps", "ldga_profile_stages", "ldga_selftest_group_inverse",
+    "ldga_bse_sweeps", "ldga_profile_stages", "ldga_selftest_group_inverse", "ldga_set_omega_shard",
 ]
 GET_CHI0, GET_CHI, GET_GAMMA, GET_LAMBDA0, GET_SIGMA, GET_GLOC = 0, 1, 2, 3, 4, 5
 STAGES = ["gloc", "bubble", "bse", "bse_fallback", "lambda0", "sums", "lambda_newton", "eom_forward",
@@ -117,6 +117,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ldga_profile": (C.c_int, [P, I32]),
         "ldga_profile_stages": (C.c_int, [P, C.c_uint32]),
         "ldga_selftest_group_inverse": (C.c_int, [I32, P, P, I32, P, P]),
+        "ldga_set_omega_shard": (C.c_int, [P, I32, I32, I32]),
         "ldga_stage_times": (C.c_int, [P, PD, PI32]),
         "ldga_launch_count": (C.c_int, [P, C.POINTER(C.c_int64)]),
         "ldga_get": (C.c_int, [P, I32, I32, P]),

@@ -27,6 +27,14 @@ int ctx_cuda(ldga_ctx* ctx, cudaError_t e, const char* what) {
     return ctx_fail(ctx, LDGA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+int require_unsharded(ldga_ctx* ctx, const char* what) {
+    if (ctx && sharded(ctx))
+        return ctx_fail(ctx, LDGA_ERR_STATE, std::string(what) + " needs every bosonic frequency: the handle covers "
+                                                 "the ω shard [" + std::to_string(ctx->w_lo) + ", " +
+                                                 std::to_string(ctx->w_hi) + "); reset it with ldga_set_omega_shard");
+    return LDGA_OK;
+}
+
 // While a graph is captured the two event records become graph nodes; their (stage, slot) pairs are
 // kept with the graph and read after every replay (ldga_chain_m).
 StageTimer::StageTimer(ldga_ctx* ctx, int st) : c(ctx), stage(st), slot(-1) {
@@ -179,6 +187,13 @@ int alloc_all(ldga_ctx* c) {
                 pairs.push_back(make_int2(pi, pj));
             }
         c->n_bub_pairs = (int)pairs.size();
+        // the list is ω-major (a pair and its partner share ω): first pair of each ω for shards
+        c->bub_pair_w_start.assign(nw + 1, c->n_bub_pairs);
+        for (int p = c->n_bub_pairs - 1; p >= 0; --p) c->bub_pair_w_start[pairs[p].x / (int)nnu] = p;
+        for (int w = (int)nw - 1; w >= 0; --w)
+            c->bub_pair_w_start[w] = std::min(c->bub_pair_w_start[w], c->bub_pair_w_start[w + 1]);
+        c->w_lo = 0;
+        c->w_hi = (int)nw;
         TRY(dev_alloc(c, &c->d_bub_pairs, pairs.size()));
         TRY(copy(c, c->d_bub_pairs, pairs.data(), pairs.size() * sizeof(int2)));
         TRY(sync(c));   // the host vector goes out of scope
@@ -448,6 +463,26 @@ int ldga_set_model(ldga_ctx* ctx, const ldga_model* mp) {
     return LDGA_OK;
 }
 
+int ldga_set_omega_shard(ldga_ctx* ctx, int32_t w_lo, int32_t w_hi, int32_t constants) {
+    if (!ctx) return LDGA_ERR_ARG;
+    if (w_lo < 0 || w_hi > ctx->Nw || w_lo >= w_hi)
+        return ctx_fail(ctx, LDGA_ERR_ARG, "ω shard [" + std::to_string(w_lo) + ", " + std::to_string(w_hi) +
+                                               ") outside [0, " + std::to_string(ctx->Nw) + ") or empty");
+    DeviceGuard g(ctx->device);
+    if (w_lo != ctx->w_lo || w_hi != ctx->w_hi) {
+        ctx->w_lo = w_lo;
+        ctx->w_hi = w_hi;
+        ctx->qperm_gen = ~0ull;   // the q order is per ω: recompute it for the new shard
+        // flags outside the shard must read "solved": the fallback scans the shard's range only, but
+        // a later whole-range call scans all of them
+        LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, (size_t)ctx->Nq * ctx->Nw * sizeof(int32_t), ctx->stream));
+        if (ctx->d_flags2)
+            LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_flags2, 0, (size_t)ctx->Nq * ctx->Nw * sizeof(int32_t), ctx->stream));
+    }
+    ctx->shard_constants = constants != 0;
+    return LDGA_OK;
+}
+
 int ldga_set_precision(ldga_ctx* ctx, int32_t precision) {
     if (!ctx) return LDGA_ERR_ARG;
     if (precision < LDGA_PREC_FP64_INV || precision > LDGA_PREC_MIXED)
@@ -532,6 +567,7 @@ int ldga_bse(ldga_ctx* ctx, int32_t channel, const double* gamma_r_in, double* c
 int ldga_bse_vjp(ldga_ctx* ctx, int32_t channel, const double* chi_bar, const double* gam_bar, double* Gamma_bar,
                  double* chi0_bar, int32_t* n_flagged) {
     if (!ctx) return LDGA_ERR_ARG;
+    TRY(require_unsharded(ctx, "ldga_bse_vjp"));
     if (channel != LDGA_CH_M && channel != LDGA_CH_D) return ctx_fail(ctx, LDGA_ERR_TYPE, "Unkown type");
     NEED(ctx, ctx->have_chi0 && ctx->have_Gamma[channel] && ctx->have_chi[channel] && ctx->have_gam[channel],
          "calc_χγ adjoint: run ldga_bse for this channel first");
@@ -840,6 +876,7 @@ int ldga_eom(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t t
 int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32_t tc, const double* sigma_bar,
                  double* chi_m_bar, double* gam_m_bar, double* chi_d_bar, double* gam_d_bar, double* lambda0_bar) {
     if (!ctx || !sigma_bar) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_eom_vjp"));
     TRY(eom_inputs_ready(ctx));
     if (!std::isfinite(lam_m) || !std::isfinite(lam_d)) return ctx_fail(ctx, LDGA_ERR_ARG, "λ must be finite");
     if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
@@ -872,6 +909,7 @@ int ldga_eom_vjp(ldga_ctx* ctx, double lam_m, double lam_d, int32_t numax, int32
 int ldga_gloc_vjp(ldga_ctx* ctx, const double* chi0_bar, const double* lambda0_bar, const double* sigma_bar,
                   double lam_m, double lam_d, int32_t numax, int32_t n_sigma, double* sigma_loc_bar, double* gloc_bar) {
     if (!ctx) return LDGA_ERR_ARG;
+    TRY(require_unsharded(ctx, "ldga_gloc_vjp"));
     NEED(ctx, ctx->have_ghat, "G adjoint: call ldga_gloc first");
     if (lambda0_bar) NEED(ctx, ctx->have_F, "G adjoint: F_m missing (call ldga_F_from_chi)");
     if (sigma_bar) {
@@ -913,6 +951,7 @@ int ldga_chain_vjp(ldga_ctx* ctx, const double* sigma_bar, double lam_m, double 
                    double* Gamma_m_bar, double* Gamma_d_bar, int32_t n_sigma, double* sigma_loc_bar,
                    double* chi0_bar, int32_t* n_flagged) {
     if (!ctx || !sigma_bar) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_chain_vjp"));
     TRY(eom_inputs_ready(ctx));
     NEED(ctx, ctx->have_chi0 && ctx->have_Gamma[0] && ctx->have_Gamma[1],
          "chain adjoint: run the bubble and both BSE channels first");
@@ -971,6 +1010,7 @@ int ldga_chain_vjp(ldga_ctx* ctx, const double* sigma_bar, double lam_m, double 
 
 int ldga_eom_parts(ldga_ctx* ctx, double lam_m, double lam_d, int32_t tc, double chiloc_m_sum, double* parts_out) {
     if (!ctx || !parts_out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_eom_parts"));
     TRY(eom_inputs_ready(ctx));
     DeviceGuard g(ctx->device);
     const int numax = ctx->sp.n_iv;
@@ -1269,6 +1309,7 @@ int ldga_chain_m(ldga_ctx* ctx, const double* sigma_loc, int32_t n_sigma, const 
                  double imp_density, double chiloc_m_sum, int32_t use_graph, double* sigma_out,
                  double* chi_m_out, double* chi_d_out, double* scalars_out) {
     if (!ctx) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_chain_m"));
     DeviceGuard g(ctx->device);
     ChainArgs a{sigma_loc, gamma_m, gamma_d, chi_loc_m, gimp, n_sigma, n_gimp, imp_density, chiloc_m_sum,
                 sigma_out, chi_m_out, chi_d_out};
@@ -1282,6 +1323,8 @@ int ldga_batch_chain_m(int32_t n, ldga_ctx* const* ctxs, const ldga_chain_io* io
     if (n < 0 || (n > 0 && (!ctxs || !io))) return ctx_fail(nullptr, LDGA_ERR_ARG, "null argument");
     std::vector<int> st(n, LDGA_OK);
     std::vector<char> rep(n, 0);
+    for (int i = 0; i < n; ++i)
+        if (ctxs[i] && sharded(ctxs[i])) return require_unsharded(ctxs[i], "ldga_batch_chain_m");
     for (int i = 0; i < n; ++i) {        // every point's chain is in flight before the first wait
         ldga_ctx* c = ctxs[i];
         if (!c) { st[i] = LDGA_ERR_ARG; continue; }
@@ -1413,6 +1456,7 @@ int ldga_lambda_dm(ldga_ctx* ctx, double chiloc_m_sum, int32_t numax, double lam
                    int32_t nsteps, double* lam_m, double* lam_d, int32_t* converged, double* out7,
                    int32_t* numax_out, double* sigma_out, double* G_out) {
     if (!ctx || !lam_m || !lam_d) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_lambda_dm"));
     TRY(eom_inputs_ready(ctx));
     NEED(ctx, ctx->d_sigma_loc != nullptr, "λdm_correction: Sigma_loc missing (call ldga_gloc)");
     DeviceGuard g(ctx->device);
@@ -1503,6 +1547,7 @@ int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t flags, double
                 int32_t numax, int32_t maxit, double mixing, double conv_abs, int32_t fit_mu, double lam_min_delta,
                 double* out, double* sigma_out, double* G_out) {
     if (!ctx || !out) return ctx_fail(ctx, LDGA_ERR_ARG, "null argument");
+    TRY(require_unsharded(ctx, "ldga_run_sc"));
     const bool redo_dm = (flags & LDGA_SC_REDO_DM) != 0;
     const bool update_tail = (flags & LDGA_SC_UPDATE_CHI_TAIL) != 0;
     const bool lam_types = (flags & LDGA_SC_LAMBDA_TYPE) != 0;

@@ -2814,16 +2814,19 @@ int tuned_index(int nnu, int prec) {
     return it == g_tune.end() ? 0 : it->second;
 }
 
+// The kernels see the ω shard as a whole problem of shard_nw frequencies: every array has ω as its
+// slowest index, so the shard is the same arrays advanced to w_lo.
 BseArgs bse_args(ldga_ctx* ctx, int channel) {
     BseArgs a;
-    a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.qchunk = 1;
+    const size_t w0 = (size_t)ctx->w_lo, nq = (size_t)ctx->Nq, nnu = (size_t)ctx->Nnu;
+    a.nq = ctx->Nq; a.nnu = ctx->Nnu; a.nw = shard_nw(ctx); a.qchunk = 1;
     a.beta = ctx->mp.beta; a.U = ctx->mp.U;
     a.s = channel == LDGA_CH_D ? -1 : 1;
-    a.Gamma = ctx->d_Gamma[channel];
-    a.chi0 = ctx->d_chi0;
-    a.chi = ctx->d_chi[channel];
-    a.gam = ctx->d_gam[channel];
-    a.flags = ctx->d_flags;
+    a.Gamma = ctx->d_Gamma[channel] + w0 * nnu * nnu;
+    a.chi0 = ctx->d_chi0 + w0 * nq * nnu;
+    a.chi = ctx->d_chi[channel] + w0 * nq;
+    a.gam = ctx->d_gam[channel] + w0 * nq * nnu;
+    a.flags = ctx->d_flags + w0 * nq;
     a.stats = ctx->d_iter_stats;
     return a;
 }
@@ -2871,7 +2874,7 @@ int bse_run_variant(ldga_ctx* ctx, int channel, int i) {
 
 int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
     const BseArgs a = bse_args(ctx, channel);
-    const int n = ctx->Nq * ctx->Nw;
+    const int n = ctx->Nq * shard_nw(ctx);
     int st = LDGA_OK;
     bool generic = false;
     {
@@ -2899,14 +2902,14 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
         // flagged matrices: compacted on the device, re-solved by a grid-stride pivoted kernel that reads
         // the count from device memory (zero work when nothing was flagged)
         LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, sizeof(int32_t), ctx->stream));
-        k_compact_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, ctx->d_list, ctx->d_count);
+        k_compact_flags<<<148, 256, 0, ctx->stream>>>(a.flags, n, ctx->d_list, ctx->d_count);
         LDGA_LAUNCHED(ctx, "k_compact_flags");
         StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
         k_bse_lu_pivot<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(a, ctx->d_list, 0, ctx->d_count, gscr);
         LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
     }
     // matrices that stayed non-finite after the pivoted solve, accumulated into *d_fail
-    k_count_flags<<<148, 256, 0, ctx->stream>>>(ctx->d_flags, n, d_fail);
+    k_count_flags<<<148, 256, 0, ctx->stream>>>(a.flags, n, d_fail);
     LDGA_LAUNCHED(ctx, "k_count_flags");
     return LDGA_OK;
 }
@@ -2923,10 +2926,14 @@ int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail) {
         const int st = launch_bse(ctx, LDGA_CH_M, d_fail);
         return st != LDGA_OK ? st : launch_bse(ctx, LDGA_CH_D, d_fail);
     }
-    const int n = ctx->Nq * ctx->Nw;
-    if (!ctx->d_flags2) LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_flags2), (size_t)n * sizeof(int32_t)));
+    const int n = ctx->Nq * shard_nw(ctx);
+    const size_t nall = (size_t)ctx->Nq * ctx->Nw;
+    if (!ctx->d_flags2) {
+        LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_flags2), nall * sizeof(int32_t)));
+        LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_flags2, 0, nall * sizeof(int32_t), ctx->stream));
+    }
     BseArgs am = bse_args(ctx, LDGA_CH_M), ad = bse_args(ctx, LDGA_CH_D);
-    ad.flags = ctx->d_flags2;
+    ad.flags = ctx->d_flags2 + (size_t)ctx->w_lo * ctx->Nq;
     const int st = v[i].run_pair(ctx, am, ad);
     if (st != LDGA_OK) return st;
     const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;

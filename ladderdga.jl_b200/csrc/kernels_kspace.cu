@@ -127,6 +127,7 @@ __global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_bubble(
 // ---------------------------------------------------------------------------------------------
 struct EomArgs {
     int nnu, nw, n_iv, n_iw, shift, fft_lo, numax, w_per_chunk;
+    int w_begin = 0, w_end = 0;   // the ω range the forward kernel sums ([0, nw) without a shard)
     double U, lam_m, lam_d;
     const double* lam_m_dev;   // device scalars added to lam_m / lam_d (may be null)
     const double* lam_d_dev;
@@ -182,8 +183,8 @@ __global__ void __launch_bounds__((kThr<M, TC>), TC ? 2 : 1) k_eom_forward(
     extern __shared__ double2 smem[];
     const int np_max = a.w_per_chunk;
     const int chunk = blockIdx.x, nu_n = blockIdx.y;
-    const int w0 = chunk * np_max;
-    const int np = min(np_max, a.nw - w0);
+    const int w0 = a.w_begin + chunk * np_max;
+    const int np = min(np_max, a.w_end - w0);
     double2* bufA = smem;
     double2* bufB = smem + np_max * S::BUF_A;
     double2* outb = smem + np_max * (S::BUF_A + S::BUF_B);     // [np_max][NQ] products
@@ -567,7 +568,10 @@ int run_gloc(ldga_ctx* ctx, bool from_sigma) {
 
 template <int DIM, int M>
 int run_bubble(ldga_ctx* ctx) {
-    const int total = ctx->n_bub_pairs;
+    // an ω shard takes the pairs of its frequencies: a contiguous range of the ω-major list
+    const int first = ctx->bub_pair_w_start[ctx->w_lo];
+    const int total = ctx->bub_pair_w_start[ctx->w_hi] - first;
+    if (total <= 0) return LDGA_OK;
     const bool tc = ctx->transform_tc;
     const int np = pairs_per_cta<DIM, M>(total, tc ? kSmemBudgetTC : kSmemBudget);
     const size_t sm = smem_bytes<DIM, M>(np);
@@ -577,8 +581,8 @@ int run_bubble(ldga_ctx* ctx) {
     const double scale = -ctx->mp.beta / ((double)ctx->Nk * (double)ctx->Nk);
     StageTimer st_(ctx, LDGA_STAGE_BUBBLE);
     kern<<<grid, tc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), ctx->Nnu, ctx->Nw, ctx->sp.n_iv, ctx->sp.n_iw,
-                                               ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_bub_pairs, total,
-                                               ctx->d_chi0, np);
+                                               ctx->sp.shift, ctx->fft_lo, scale, ctx->d_ghat, ctx->d_bub_pairs + first,
+                                               total, ctx->d_chi0, np);
     LDGA_LAUNCHED(ctx, "k_bubble");
     return LDGA_OK;
 }
@@ -592,10 +596,11 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
     int wpc = (int)((tc ? kSmemBudgetTC : kSmemBudget) / per);
     if (wpc > 16) wpc = 16;
     if (wpc < 1) wpc = 1;
-    // spread the w axis over enough CTAs to fill the machine
+    // spread the w axis (the shard's range) over enough CTAs to fill the machine
+    const int nws = shard_nw(ctx);
     const int target_ctas = 2 * 148;
-    while (wpc > 1 && (long)numax * ((ctx->Nw + wpc - 1) / wpc) < target_ctas) --wpc;
-    const int nchunk = (ctx->Nw + wpc - 1) / wpc;
+    while (wpc > 1 && (long)numax * ((nws + wpc - 1) / wpc) < target_ctas) --wpc;
+    const int nchunk = (nws + wpc - 1) / wpc;
     const size_t need = (size_t)nchunk * numax * ctx->Nq;
     if (need > ctx->partial_elems) {
         if (ctx->d_partial) cudaFree(ctx->d_partial);
@@ -606,6 +611,7 @@ int run_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const double* 
     EomArgs a;
     a.nnu = ctx->Nnu; a.nw = ctx->Nw; a.n_iv = ctx->sp.n_iv; a.n_iw = ctx->sp.n_iw; a.shift = ctx->sp.shift;
     a.fft_lo = ctx->fft_lo; a.numax = numax; a.w_per_chunk = wpc;
+    a.w_begin = ctx->w_lo; a.w_end = ctx->w_hi;
     a.U = ctx->mp.U; a.lam_m = lam_m; a.lam_d = lam_d; a.part = part;
     a.lam_m_dev = lm_dev; a.lam_d_dev = ld_dev;
     const size_t sm = (size_t)wpc * per;
@@ -631,6 +637,10 @@ int run_eom_inverse(ldga_ctx* ctx, int numax, int nchunk, const double* d_tail, 
     dim3 grid((numax + np - 1) / np);
     const double scale = 1.0 / ((double)ctx->Nk * (double)ctx->Nk);
     const double hartree = ctx->mp.n * ctx->mp.U / 2.0;
+    if (!ctx->shard_constants) {   // another rank of the ω shards adds the tail and Hartree terms
+        tc = 0;
+        add_hartree = 0;
+    }
     StageTimer st_(ctx, LDGA_STAGE_EOM_INVERSE);
     kern<<<grid, ttc ? kThr<M, true> : kThr<M, false>, sm, ctx->stream>>>(make_T<M>(ctx), numax, nchunk, scale, ctx->mp.beta, ctx->mp.U,
                                                hartree, d_tail, tc, chiloc_m_sum, ctx->d_partial, out, out_ld,

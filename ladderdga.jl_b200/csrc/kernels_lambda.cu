@@ -806,8 +806,11 @@ int launch_lambda0(ldga_ctx* ctx) {
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA0);
     k_colsum_F<<<std::min(4 * 148, (ctx->Nnu * ctx->Nw + 7) / 8), 256, 0, ctx->stream>>>(ctx->Nnu, ctx->Nw, ctx->d_F, colF);
     LDGA_LAUNCHED(ctx, "k_colsum_F");
-    k_lambda0<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, ctx->Nw, 1.0 / (ctx->mp.beta * ctx->mp.beta),
-                                                ctx->d_chi0, colF, ctx->d_lambda0);
+    // an ω shard: the same arrays advanced to w_lo (ω is their slowest index)
+    const size_t w0 = (size_t)ctx->w_lo, nqv = (size_t)ctx->Nq * ctx->Nnu;
+    k_lambda0<<<4 * 148, 256, 0, ctx->stream>>>(ctx->Nq, ctx->Nnu, shard_nw(ctx), 1.0 / (ctx->mp.beta * ctx->mp.beta),
+                                                ctx->d_chi0 + w0 * nqv, colF + w0 * ctx->Nnu,
+                                                ctx->d_lambda0 + w0 * nqv);
     LDGA_LAUNCHED(ctx, "k_lambda0");
     return LDGA_OK;
 }

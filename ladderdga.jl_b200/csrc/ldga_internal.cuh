@@ -118,6 +118,12 @@ struct ldga_ctx {
     char* d_arena = nullptr;
     size_t arena_cap = 0, arena_used = 0, arena_want = 0;
     int n_bub_pairs = 0;
+    // ω shard (ldga_set_omega_shard): the bubble, BSE, lambda_0 and EoM stages cover the bosonic
+    // indices [w_lo, w_hi) only; the EoM's 1/iν tail and Hartree terms are added where
+    // shard_constants is set (one rank), so the ranks' Σ_ladder add up to the whole one
+    int w_lo = 0, w_hi = 0;
+    bool shard_constants = true;
+    std::vector<int> bub_pair_w_start;    // [Nw + 1] first bubble pair of each ω (pairs are ω-major)
 
     cudaStream_t own_stream = nullptr;   // created by the handle; `stream` may be a caller's stream
     // ldga_chain_m's copies that overlap its kernels: the vertices and local inputs go in on io_stream
@@ -184,6 +190,13 @@ inline cudaError_t set_smem(ldga_ctx* c, F* f, size_t sm) {
     if (c->capturing) return cudaSuccess;
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
 }
+
+// ω shard helpers: the number of bosonic indices the stages cover, and whether a shard is set
+inline int shard_nw(const ldga_ctx* c) { return c->w_hi - c->w_lo; }
+inline bool sharded(const ldga_ctx* c) { return c->w_lo != 0 || c->w_hi != c->Nw; }
+// entry points whose stages need every ω (the λdm and self-consistent loops, the fused chain, the
+// adjoints) refuse a sharded handle
+int require_unsharded(ldga_ctx* ctx, const char* what);
 
 bool bse_has_fast_path(int nnu);
 // BSE kernel configurations (autotuning): count and name per (Nν, precision), the chosen index,

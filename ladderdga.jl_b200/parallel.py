@@ -17,6 +17,8 @@ the BSE work of each point (N_q · N_ω · Nν³ per channel), which dominates t
 from __future__ import annotations
 
 import heapq
+
+import numpy as np
 from typing import Any, Callable, Sequence
 
 
@@ -165,3 +167,118 @@ def run_points(weights: Sequence[float], run_one: Callable[[int], Any], group=No
     if missing:
         raise RuntimeError(f"points without a result: {sorted(missing)}")
     return {i: merged[i] for i in range(len(weights))}
+
+
+# ------------------------------------------------------------------------------------------------
+# One parameter point sharded by bosonic frequency (the reference's worker split: gen_ω_part,
+# parallelization_helpers.jl:49-53, used by calc_bubble_par / calc_χγ_par / calc_Σ_par,
+# ladderDGATools.jl:46-245).  Every rank computes the bubble, both BSE channels and λ₀ on its ω
+# block (par_partition of 0..Nω-1), the ranks assemble the whole χ_m and χ_d (one all-reduce each,
+# every rank contributing its block and zeros elsewhere: exact), run the λm Newton on the whole χ
+# (every rank the same kernel on the same data: the same λm), form their ω block's part of
+# Σ_ladder, and sum those parts with one all-reduce; the tail and Hartree terms come from rank 0
+# only.  The μ fit and the energies then run on every rank on the same Σ_ladder.  The exchanged
+# data are N_q N_ω doubles per channel and N_q νmax complex values: 0.3 MB each on the 3D 32³ point.
+# ------------------------------------------------------------------------------------------------
+class HandleStages:
+    """The sharded chain's stages on a library handle (``core.lDΓAHelper``), through the C ABI.
+    Exchange buffers are torch tensors on ``device`` (a CUDA device for NCCL, the CPU for gloo);
+    the library reads and writes them directly (host or device pointers)."""
+
+    def __init__(self, h):
+        self.h = h
+        self.ctx = h.ctx
+        self.Nq, self.Nnu, self.Nw = self.ctx.Nq, self.ctx.Nnu, self.ctx.Nw
+
+    @staticmethod
+    def _ptr(t):
+        import ctypes as C
+        return C.c_void_p(t.data_ptr())
+
+    def set_shard(self, w_lo: int, w_hi: int, constants: bool) -> None:
+        self.ctx.call("ldga_set_omega_shard", int(w_lo), int(w_hi), int(bool(constants)))
+
+    def bubble(self) -> None:
+        self.ctx.call("ldga_bubble", None)
+
+    def bse(self, ch: int) -> None:
+        import ctypes as C
+        from ._lib import as_fc, ptr
+        nfb = C.c_int32(0)
+        Γ = self.h.Γ_m if ch == 0 else self.h.Γ_d
+        self.ctx.call("ldga_bse", ch, ptr(as_fc(Γ)), None, None, C.byref(nfb))
+
+    def lambda0(self) -> None:
+        from ._lib import ptr
+        h = self.h
+        self.ctx.call("ldga_F_from_chi", ptr(h.χDMFT_m), ptr(h.gImp), len(h.gImp), None)
+        self.ctx.call("ldga_lambda0", None, None)
+
+    def get_chi(self, ch: int, buf) -> None:
+        from . import _lib
+        self.ctx.call("ldga_get", _lib.GET_CHI, ch, self._ptr(buf))
+
+    def set_chi(self, ch: int, buf) -> None:
+        self.ctx.call("ldga_set_chi", ch, self._ptr(buf))
+
+    def lambda_m(self) -> tuple[float, int]:
+        import ctypes as C
+        s = C.c_double()
+        self.ctx.call("ldga_sum_kw", 1, 0.0, 0, C.byref(s))
+        rhs = 2.0 * self.h.imp_density - s.value
+        lam, its = C.c_double(), C.c_int32()
+        self.ctx.call("ldga_lambda_m", rhs, C.byref(lam), C.byref(its))
+        return lam.value, its.value
+
+    def eom(self, lam_m: float, numax: int, out) -> None:
+        self.ctx.call("ldga_eom", float(lam_m), 0.0, int(numax), 1, self.h.χloc_m_sum, self._ptr(out))
+
+    def finish(self, lam_m: float, numax: int, sigma) -> dict:
+        from .core import G_from_Σladder, calc_E
+        h = self.h
+        S = sigma.cpu().numpy().view(np.complex128)[..., 0].T.copy()          # [Nq, numax]
+        mu, G = G_from_Σladder(S, h.Σ_loc, h.kG, h.mP, h.sP, fix_n=True, h=h)
+        off = -h.sP.fft_range[0]
+        ek, ep = calc_E(G[:, off:off + numax], S, mu, h.kG, h.mP, h=h)
+        return {"lambda_m": lam_m, "mu": mu, "E_kin": ek, "E_pot1": ep, "Sigma_ladder": S}
+
+
+def λm_chain_omega_sharded(stages, group=None, numax: int | None = None) -> dict:
+    """The λm chain (run_minimal.jl: bubble -> χ, γ of m and d -> λ₀ -> λm_correction_full,
+    conditions_new.jl:174-190) of one parameter point with its bosonic frequencies split over the
+    ranks of ``group`` (all stages of ``stages`` on this rank's block).  Without a process group
+    the whole range runs here.  Returns λm, the Newton iterations, μ, the energies and Σ_ladder
+    (the same on every rank) and this rank's block."""
+    import torch
+    dist = _dist()
+    rank, world = (dist.get_rank(group), dist.get_world_size(group)) if dist else (0, 1)
+    backend = dist.get_backend(group) if dist else "gloo"
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    nq, nnu, nw = stages.Nq, stages.Nnu, stages.Nw
+    block = par_partition(nw, world)[rank]
+    numax = nnu // 2 if numax is None else int(numax)
+    stages.set_shard(block.start, block.stop, rank == 0)
+    try:
+        stages.bubble()
+        stages.bse(0)
+        stages.bse(1)
+        stages.lambda0()
+        for ch in (0, 1):
+            buf = torch.zeros((nw, nq), dtype=torch.float64, device=dev)     # column-major [q, ω]
+            stages.get_chi(ch, buf)
+            buf[: block.start] = 0.0                                           # other ranks' blocks
+            buf[block.stop:] = 0.0
+            if dist:
+                dist.all_reduce(buf, group=group)
+            stages.set_chi(ch, buf)
+        lam, its = stages.lambda_m()
+        sigma = torch.zeros((numax, nq, 2), dtype=torch.float64, device=dev)  # column-major [q, ν] complex
+        stages.eom(lam, numax, sigma)
+        if dist:
+            dist.all_reduce(sigma, group=group)
+        res = stages.finish(lam, numax, sigma)
+    finally:
+        stages.set_shard(0, nw, True)
+    res["newton_iterations"] = its
+    res["block"] = (block.start, block.stop)
+    return res
