@@ -2782,6 +2782,8 @@ const BseVariant mixed_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu32<60,
                                {&run_lu32<60, 16, 1, 2>, "lu32x16:2"}, {&run_iter<60, 8, 1>, "iter"}};
 const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64_INV>, "gj16x1"}};
 // Nν = 120: Gamma(w) (230 KB) exceeds shared memory and is read through L1/L2; FP64_INV solves by LU
+// (32 x 32 threads per matrix -- a 4 x 4 register tile instead of 16 x 16 threads' spilling 8 x 8 --
+// measured 1.76x slower: 120 steps of a 1024-thread barrier over little work per thread)
 const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};
 // (no preconditioned configuration at Nν = 120: on the test matrices its condition numbers reach 1e4,
 // where the iteration's backward error of 1e-14 no longer guarantees the 1e-10 forward accuracy)
@@ -2798,7 +2800,7 @@ int variants_of(int nnu, int prec, const BseVariant** out) {
         LDGA_BOX(40) LDGA_BOX(60)
         case 120:
             if (prec == LDGA_PREC_MIXED) { *out = mixed_120; return (int)(sizeof(mixed_120) / sizeof(BseVariant)); }
-            *out = fp64_120; return 1;
+            *out = fp64_120; return (int)(sizeof(fp64_120) / sizeof(BseVariant));
         default: *out = nullptr; return 0;
     }
 #undef LDGA_BOX

@@ -405,6 +405,38 @@ def test_bse_large_box(n_iv, prec, require_gpu):
     assert rel(np.asarray(g["lambda0"]), ref["lambda0"]) < RTOL
 
 
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_MIXED])
+def test_bse_large_box_every_configuration(prec, require_gpu):
+    """Every compiled configuration at Nν = 120 (FP64 and FP32 eliminations) against the oracle, no
+    matrix left to the pivoted fallback."""
+    import os
+    import tempfile
+    inp = S.make_input(dim=2, ns=4, beta=40.0, U=1.0, n_iv=60, n_iw=2, seed=150)
+    ref = R.run_chain(inp, lambda_type=None)
+    h = L.setup_synthetic(inp, precision=prec)
+    lib = h.ctx.lib
+    names = []
+    while lib.ldga_bse_config_name(120, prec, len(names)):
+        names.append(lib.ldga_bse_config_name(120, prec, len(names)).decode())
+    assert "lu16g:1" in names
+    chi0 = L.calc_bubble(h)
+    try:
+        for nm in names:
+            fd, path = tempfile.mkstemp()
+            os.write(fd, f"bse 120 {prec} {nm}\n".encode())
+            os.close(fd)
+            L.tune_reset()
+            L.tune_load(path)
+            os.unlink(path)
+            for r in ("m", "d"):
+                x, g = L.calc_χγ(r, h, chi0)
+                assert x.n_fallback == 0, (nm, r)
+                assert chi_rel(x.data, ref, r) < RTOL, (nm, r)
+                assert rel(g.data, ref[f"gamma_{r}"]) < RTOL, (nm, r)
+    finally:
+        L.tune_reset()
+
+
 def test_batch_chain_uneven_points(require_gpu):
     """ldga_batch_chain_m over points of different Nν (4, 16, 30) and U: each point equals the
     single-point λm chain and, within the parity tolerance, the oracle."""
