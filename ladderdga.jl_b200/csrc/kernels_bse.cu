@@ -1926,37 +1926,36 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         constexpr int FR = S::MT * S::KT * 32 * 4;
         unsigned char* nsb = it_raw;
         float* ns_red = reinterpret_cast<float*>(it_raw + S::off_red);
-        if (tid < N) {
-            const double2* grow = Gw + (size_t)tid * N;
-            float2 dinv = make_float2(0.f, 0.f);
-#pragma unroll 1
-            for (int k = 0; k < N; k += 4) {
-                float re[4], im[4];
+        // every thread takes elements e = tid + NT m of B_bar (row-major), all loads in flight at
+        // once: B_bar_ij into the A buffers, X_0 = diag(1 / B_bar_ii) into the A buffers (row i)
+        // and the B buffers (column i; element (j, i))
+        {
+            constexpr int NE = (N * N + NT - 1) / NT;
+            double2 gv[NE];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    double2 v = grow[k + u];
-                    if (k + u == tid) {
-                        v = cadd(v, dbar[tid]);
-                        dinv = vinv(make_float2((float)v.x, (float)v.y));
-                    }
-                    re[u] = (float)v.x;
-                    im[u] = (float)v.y;
-                }
-                ns::store_a4<N>(nsb + NSm::off_br, tid, k, re[0], re[1], re[2], re[3]);
-                ns::store_a4<N>(nsb + NSm::off_bi, tid, k, im[0], im[1], im[2], im[3]);
+            for (int m = 0; m < NE; ++m) {
+                const int e = tid + NT * m;
+                gv[m] = e < N * N ? Gw[e] : dmk(0.0, 0.0);
             }
-#pragma unroll 1
-            for (int k = 0; k < N; k += 4) {
-                float xr4[4], xi4[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    xr4[u] = k + u == tid ? dinv.x : 0.f;
-                    xi4[u] = k + u == tid ? dinv.y : 0.f;
-                    ns::store_b<N>(nsb + NSm::off_tr, tid, k + u, xr4[u]);
-                    ns::store_b<N>(nsb + NSm::off_ti, tid, k + u, xi4[u]);
+            for (int m = 0; m < NE; ++m) {
+                const int e = tid + NT * m;
+                if (e < N * N) {
+                    const int i = e / N, j = e - (e / N) * N;
+                    double2 v = gv[m];
+                    float2 xv = make_float2(0.f, 0.f);
+                    if (i == j) {
+                        v = cadd(v, dbar[i]);
+                        xv = vinv(make_float2((float)v.x, (float)v.y));
+                    }
+                    const uint32_t oa = tc05::kmajor_offset(N, i, j), ob = tc05::kmajor_offset(N, j, i);
+                    *reinterpret_cast<float*>(nsb + NSm::off_br + oa) = tc05::to_tf32f((float)v.x);
+                    *reinterpret_cast<float*>(nsb + NSm::off_bi + oa) = tc05::to_tf32f((float)v.y);
+                    *reinterpret_cast<float*>(nsb + NSm::off_xr + oa) = tc05::to_tf32f(xv.x);
+                    *reinterpret_cast<float*>(nsb + NSm::off_xi + oa) = tc05::to_tf32f(xv.y);
+                    *reinterpret_cast<float*>(nsb + NSm::off_tr + ob) = tc05::to_tf32f(xv.x);
+                    *reinterpret_cast<float*>(nsb + NSm::off_ti + ob) = tc05::to_tf32f(xv.y);
                 }
-                ns::store_a4<N>(nsb + NSm::off_xr, tid, k, xr4[0], xr4[1], xr4[2], xr4[3]);
-                ns::store_a4<N>(nsb + NSm::off_xi, tid, k, xi4[0], xi4[1], xi4[2], xi4[3]);
             }
         }
         tc05::fence_before();
