@@ -1647,7 +1647,10 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
     return acc;
 }
 
-template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2, bool NS>
+// NL: the box size Nν of the data; the tiles use N >= NL (a multiple of 8 for the tensor paths).
+// Rows and columns NL .. N-1 are an identity block with a zero right-hand side: Gamma^T is padded
+// with zeros, 1/chi0 with ones, so x and r stay zero there and the first NL rows solve B y = 1.
+template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2, bool NS, int NL>
 __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a_m, const BseArgs a_d,
                                                                        const int32_t* __restrict__ perm) {
     // blockIdx.z selects the channel: one launch may cover both (they share chi0 and the q order),
@@ -1658,6 +1661,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     static_assert(!DM || (GSM && TC), "the FP64 tensor product is built with the tensor-core FP32 product");
     static_assert(!NS || (DM && N % 8 == 0 && kIterQ * LPQ / QPL == 128),
                   "the tensor-core group inverse is built for the DM configuration, 128 threads");
+    static_assert(NL <= N && NL % 2 == 0, "padded box");
     constexpr int LD = S::LD;
     constexpr int LDG = GSM ? LD : N;   // row stride of Gamma^T where it is read
     constexpr int RPL = (N + LPQ - 1) / LPQ;
@@ -1681,8 +1685,12 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 
     // ---- B rows: B_ij = Gamma[w][i N + j] + delta_ij D_i;  D = 1/chi0 of the CTA's q
     // fixed trip counts, fully unrolled: every global load of a thread is in flight at once
-    const double2* Gw = a.Gamma + (size_t)w * N * N;
+    const double2* Gw = a.Gamma + (size_t)w * NL * NL;
     const double2* Gt = GSM ? Gs : Gw;
+    // element (i, j) of Gamma(w) as stored, zero in the padding
+    auto gglob = [&](int i, int j) -> double2 {
+        return (i < NL && j < NL) ? Gw[(size_t)i * NL + j] : dmk(0.0, 0.0);
+    };
     double* Gfr = reinterpret_cast<double*>(it_raw);            // DM: A fragments of Re B, then Im B
     double* Gfi = Gfr + N * N;
     // element B_ij without the diagonal term, from wherever Gamma^T is kept
@@ -1701,7 +1709,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int m = 0; m < NG; ++m) {
             const int e = tid + NT * m;
-            if (e < N * N) gv[m] = Gw[e];
+            if (e < N * N) gv[m] = NL == N ? Gw[e] : gglob(e / N, e - (e / N) * N);
         }
 #pragma unroll
         for (int m = 0; m < NG; ++m) {
@@ -1744,7 +1752,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int m = 0; m < ND; ++m) {
             const int e = tid + NT * m, v = e - (e / N) * N;
-            cv[m] = qg[m] >= 0 ? a.chi0[(size_t)qg[m] + (size_t)a.nq * (v + (size_t)N * w)] : dmk(0.0, 0.0);
+            // padding rows: chi0 = 1, so D = 1 there
+            cv[m] = qg[m] >= 0 ? (v < NL ? a.chi0[(size_t)qg[m] + (size_t)a.nq * (v + (size_t)NL * w)] : dmk(1.0, 0.0))
+                               : dmk(0.0, 0.0);
         }
         // 1/chi0 = conj(chi0) / |chi0|^2 by batch inversion (Montgomery's trick): prefix products of
         // the ND squared moduli, one division, two products per reciprocal, instead of ND scaled
@@ -1935,7 +1945,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
             for (int m = 0; m < NE; ++m) {
                 const int e = tid + NT * m;
-                gv[m] = e < N * N ? Gw[e] : dmk(0.0, 0.0);
+                gv[m] = e < N * N ? (NL == N ? Gw[e] : gglob(e / N, e - (e / N) * N)) : dmk(0.0, 0.0);
             }
 #pragma unroll
             for (int m = 0; m < NE; ++m) {
@@ -1993,7 +2003,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 }
             }
         } else {
-            gauss_jordan([&](int i, int j) { return Gw[(size_t)i * N + j]; });
+            gauss_jordan(gglob);
         }
         __syncthreads();
         stage_gamma();
@@ -2019,9 +2029,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             if constexpr (!TC) {
                 float2 s2 = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int j = 0; j < N; j += 2) {
+                for (int j = 0; j < NL; j += 2) {          // C 1 over the box's columns
                     sacc = fadd(sacc, C[i * LD + j]);
-                    if (j + 1 < N) s2 = fadd(s2, C[i * LD + j + 1]);
+                    if (j + 1 < NL) s2 = fadd(s2, C[i * LD + j + 1]);
                 }
                 sacc = fadd(sacc, s2);
             }
@@ -2068,7 +2078,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int c = 0; c < QPL; ++c)
 #pragma unroll
-            for (int r = 0; r < RPL; ++r) one[c][r] = make_float2(1.f, 0.f);
+            for (int r = 0; r < RPL; ++r) one[c][r] = make_float2(h * RPL + r < NL ? 1.f : 0.f, 0.f);
         tc_apply<N, RPL, QPL, LPQ>(one, d0, Ffr, Ffi, xbw, lane, h);
         if constexpr (P2) second_order(d0, one);
 #pragma unroll
@@ -2135,7 +2145,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 rr[c][r] = make_float2(0.f, 0.f);
                 if (N % LPQ == 0 || i < N) {
                     const double2 t = cadd(acc[c][r], cmul(Dq[(ql0 + c) * N + i], x[c][r]));
-                    const double rx = 1.0 - t.x, ry = -t.y;
+                    const double rx = (i < NL ? 1.0 : 0.0) - t.x, ry = -t.y;
                     res = fmax(res, fabs(rx) + fabs(ry));
                     xn = fmax(xn, fabs(x[c][r].x) + fabs(x[c][r].y));
                     rr[c][r] = make_float2((float)rx, (float)ry);
@@ -2205,7 +2215,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         double sx = 0.0;
 #pragma unroll
         for (int r = 0; r < RPL; ++r)
-            if (N % LPQ == 0 || h * RPL + r < N) sx += x[c][r].x;
+            if (h * RPL + r < NL) sx += x[c][r].x;
 #pragma unroll
         for (int o = 1; o < LPQ; o <<= 1) sx += __shfl_xor_sync(0xffffffffu, sx, o);
         const int ql = ql0 + c;
@@ -2221,8 +2231,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int r = 0; r < RPL; ++r) {
             const int i = h * RPL + r;
-            if (N % LPQ == 0 || i < N)
-                a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)N * w)] = cscale(cmul(x[c][r], Dq[ql * N + i]), rf);
+            if (i < NL)
+                a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)NL * w)] = cscale(cmul(x[c][r], Dq[ql * N + i]), rf);
         }
     }
 }
@@ -2689,11 +2699,11 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
 using BseRunPair = int (*)(ldga_ctx*, const BseArgs&, const BseArgs&);
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
-          bool NS = false>
+          bool NS = false, int NL = N>
 int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM, NS>;
-    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2, NS>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2, NS, NL>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
@@ -2703,7 +2713,7 @@ int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
             while (P < a.nq) P <<= 1;
             const size_t smq = (size_t)P * (sizeof(double) + sizeof(int));
             LDGA_CUDA(ctx, set_smem(ctx, k_bse_qorder, smq));
-            k_bse_qorder<<<a.nw, 1024, smq, ctx->stream>>>(a.nq, N, a.chi0, ctx->d_qperm);
+            k_bse_qorder<<<a.nw, 1024, smq, ctx->stream>>>(a.nq, NL, a.chi0, ctx->d_qperm);
             LDGA_LAUNCHED(ctx, "k_bse_qorder");
         } else {
             k_bse_qorder_id<<<148, 256, 0, ctx->stream>>>(a.nq, a.nw, ctx->d_qperm);
@@ -2718,15 +2728,15 @@ int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
 }
 
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
-          bool NS = false>
+          bool NS = false, int NL = N>
 int run_iter(ldga_ctx* ctx, const BseArgs& a) {
-    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS>(ctx, a, nullptr);
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS, NL>(ctx, a, nullptr);
 }
 
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
-          bool NS = false>
+          bool NS = false, int NL = N>
 int run_iter_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) {
-    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS>(ctx, a_m, &a_d);
+    return run_iter_impl<N, LPQ, MINB, QPL, GSM, TC, DM, P2, NS, NL>(ctx, a_m, &a_d);
 }
 
 struct BseVariant {
@@ -2777,7 +2787,11 @@ const BseVariant fp64_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu<60, 16
                               {&run_lu<60, 16, 1, 3>, "lu16:3"}};
 // MIXED may pick any configuration whose results meet the FP64 backward-error bound, the FP64 LU
 // included: at Nν = 60 and 120 that is the fastest one measured
-const BseVariant mixed_60[] = {{&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu32<60, 16, 1, 3>, "lu32x16:3"},
+// the preconditioned iteration on tiles padded to 64 (an identity block below the box), both products
+// on tensor cores and the group inverse on tcgen05, one 128-thread CTA per SM (151 KB of shared memory)
+const BseVariant mixed_60[] = {{&run_iter<64, 8, 1, 2, true, true, true, true, true, 60>, "iter8x2dm2ns64:1",
+                                &run_iter_pair<64, 8, 1, 2, true, true, true, true, true, 60>},
+                               {&run_lu<60, 16, 1, 2>, "lu16:2"}, {&run_lu32<60, 16, 1, 3>, "lu32x16:3"},
                                {&run_lu32<60, 16, 1, 2>, "lu32x16:2"}, {&run_iter<60, 8, 1>, "iter"}};
 const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64_INV>, "gj16x1"}};
 // Nν = 120: Gamma(w) (230 KB) exceeds shared memory and is read through L1/L2; FP64_INV solves by LU

@@ -217,6 +217,39 @@ def cfg2(require_gpu):
     return inp, R.run_chain(inp, lambda_type=None)
 
 
+def test_config2_every_mixed_bse_configuration(cfg2):
+    """Every compiled MIXED configuration at Nν = 60 on configuration 2's matrices -- the preconditioned
+    iteration on tiles padded to 64 (the default) and the LU forms: χ_r and γ_r against the oracle,
+    no matrix left to the pivoted fallback by the iteration."""
+    import tempfile
+    inp, ref = cfg2
+    h = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+    lib = h.ctx.lib
+    nnu = h.ctx.Nnu
+    names = []
+    while lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)):
+        names.append(lib.ldga_bse_config_name(nnu, L.PREC_MIXED, len(names)).decode())
+    assert names[0].startswith("iter") and "64" in names[0]
+    chi0 = L.calc_bubble(h)
+    assert rel(chi0.data, ref["chi0"]) < RTOL
+    try:
+        for nm in names:
+            fd, path = tempfile.mkstemp()
+            os.write(fd, f"bse {nnu} {L.PREC_MIXED} {nm}\n".encode())
+            os.close(fd)
+            L.tune_reset()
+            L.tune_load(path)
+            os.unlink(path)
+            for r in ("m", "d"):
+                x, g = L.calc_χγ(r, h, chi0)
+                assert chi_rel(x.data, ref, r) < RTOL, (nm, r, chi_rel(x.data, ref, r))
+                assert rel(g.data, ref[f"gamma_{r}"]) < RTOL, (nm, r, rel(g.data, ref[f"gamma_{r}"]))
+                if nm == names[0]:
+                    assert x.n_fallback == 0, (nm, r, x.n_fallback)
+    finally:
+        L.tune_reset()
+
+
 @pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_MIXED])
 def test_config2_lambda_dm(cfg2, prec):
     """Configuration 2 as specified: both channels and λdm, in FP64 and in MIXED mode.  The arrays
