@@ -2759,15 +2759,20 @@ LDGA_SMALL_BOX(12)
 #undef LDGA_SMALL_BOX
 // Nν = 16..30: the warp LU stays the MIXED default (its N^3 is small); the q-shared preconditioned
 // iteration is a configuration the autotuner may pick
-#define LDGA_ITER_BOX(N, LPQ, MINB)                                                                     \
+// ...and the tensor-core preconditioned iteration (both products on tensor cores, the group inverse
+// on tcgen05) on tiles of NP >= N rows, NP a multiple of 8, as a candidate: with few q per ω its
+// groups are wide, so the autotuner decides
+#define LDGA_ITER_BOX(N, LPQ, MINB, NP, MINB_TC, TCNAME)                                                \
     const BseVariant fp64_##N[] = {{&run_lu<N, 8, 1, 2>, "lu8:2"}, {&run_lu<N, 8, 1, 4>, "lu8:4"},     \
                                    {&run_lu<N, 8, 1, 8>, "lu8:8"}};                                     \
     const BseVariant mixed_##N[] = {{&run_warp32<N, 8, 4, 4, 1>, "warp:1"}, {&run_warp32<N, 8, 4, 4, 3>, "warp:3"}, \
-                                    {&run_iter<N, LPQ, MINB>, "iter"}};                                \
+                                    {&run_iter<N, LPQ, MINB>, "iter"},                                 \
+                                    {&run_iter<NP, 8, MINB_TC, 2, true, true, true, true, true, N>, TCNAME, \
+                                     &run_iter_pair<NP, 8, MINB_TC, 2, true, true, true, true, true, N>}}; \
     const BseVariant inv_##N[] = {{&run_tile<N, 8, 8, 2, 1, double, LDGA_PREC_FP64_INV>, "gj8x2"}};
-LDGA_ITER_BOX(16, 4, 4)
-LDGA_ITER_BOX(20, 4, 4)
-LDGA_ITER_BOX(30, 4, 3)
+LDGA_ITER_BOX(16, 4, 4, 16, 4, "iter8x2dm2ns16:4")
+LDGA_ITER_BOX(20, 4, 4, 24, 4, "iter8x2dm2ns24:4")
+LDGA_ITER_BOX(30, 4, 3, 32, 3, "iter8x2dm2ns32:3")
 #undef LDGA_ITER_BOX
 const BseVariant fp64_40[] = {{&run_lu<40, 8, 1, 6>, "lu8:6"}, {&run_lu<40, 8, 1, 4>, "lu8:4"},
                               {&run_lu<40, 8, 1, 5>, "lu8:5"}};
