@@ -206,7 +206,7 @@ int alloc_all(ldga_ctx* c) {
 void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
-                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_count,
+                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_list2, c->d_count,
                     c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -371,6 +371,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
     if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "tc") == 0;
     if (const char* nw = std::getenv("LDGA_NEWTON")) c->newton_async = std::strcmp(nw, "barrier") != 0;
+    if (const char* sw = std::getenv("LDGA_ITER_SWEEPS")) c->iter_sweeps = std::min(std::max(std::atoi(sw), 0), 1000);
     DeviceGuard g(device);
     c->device = device;
     c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;
@@ -1158,7 +1159,7 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     TRY(copy(ctx, ctx->d_sigma_loc, a.sigma_loc, (size_t)a.n_sigma * sizeof(double2)));
     TRY(launch_gloc_transform(ctx, true));                       // a1
     TRY(launch_bubble(ctx));                                     // a2
-    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 2 * sizeof(int32_t), ctx->stream));
+    LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 4 * sizeof(int32_t), ctx->stream));   // fails, lists
     LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_gamma, 0));
     TRY(launch_bse_pair(ctx, ctx->d_count + 1));                  // a7, both channels
     LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_chi, ctx->stream));

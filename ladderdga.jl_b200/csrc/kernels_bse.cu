@@ -106,6 +106,10 @@ struct BseArgs {
     double2* gam;           // [Nq, Nnu, Nw]
     int32_t* flags;         // [Nq, Nw]
     unsigned long long* stats = nullptr;   // [2] k_bse_iter: residual passes and warps (may be null)
+    // k_bse_iter: a flagged matrix is also appended (q + Nq w) to fail_list at atomicAdd(fail_count)
+    int32_t* fail_list = nullptr;
+    int32_t* fail_count = nullptr;
+    int max_sweeps = 40;    // k_bse_iter: residual sweeps before a q is flagged
 };
 
 __device__ __forceinline__ double2 dmk(double r, double i) { return make_double2(r, i); }
@@ -1343,7 +1347,8 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 // group then iterates (Richardson refinement with the approximate inverse C)
 //     r = 1 - B_q x   (FP64, one N^2 product),   x += C r   (FP32 product, FP64 update)
 // from x = C 1 until the FP64 backward error of x -- the measure of the LU kernels -- is at most
-// 1e-14, or kIterMax sweeps; a q still above 1e-14 is flagged for the pivoted FP64 solve.  The
+// 1e-14, or max_sweeps sweeps (40 unless the handle sets another); a q still above 1e-14 is flagged
+// for the pivoted FP64 solve.  The
 // sweep count is set by how far B_q is from B_bar (about 7 on the 3D 32^3 matrices), so the FP64
 // work per matrix is ~7 N^2 instead of the elimination's N^3 / 3 plus its latency-bound steps.
 // Layout: LPQ adjacent lanes per q; lane h of a q owns rows [h RPL, (h+1) RPL) of x, r and of the
@@ -1354,7 +1359,6 @@ __global__ void __launch_bounds__(32 * WPC, MINB) k_bse_warp32(const BseArgs a) 
 constexpr int kIterQ = 32;      // q per CTA: one preconditioner
 constexpr int kNsMaxIts = 6;    // Newton-Schulz iterations at most (tensor-core group inverse)
 constexpr float kNsTol = 1e-2f; // stop once (max row sum of |I - B_bar X|)^2 <= kNsTol
-constexpr int kIterMax = 40;    // sweeps before a q is handed to the pivoted solve
 constexpr double kIterTol = 1e-14;
 
 // TC: the FP32 product x += C r runs on tensor cores (mma.sync m16n8k8, TF32 operands, FP32
@@ -1656,7 +1660,10 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     // blockIdx.z selects the channel: one launch may cover both (they share chi0 and the q order),
     // so the second channel's CTAs fill the SMs the first one's tail leaves idle
     BseArgs a = a_m;
-    if (blockIdx.z) { a.s = a_d.s; a.Gamma = a_d.Gamma; a.chi = a_d.chi; a.gam = a_d.gam; a.flags = a_d.flags; }
+    if (blockIdx.z) {
+        a.s = a_d.s; a.Gamma = a_d.Gamma; a.chi = a_d.chi; a.gam = a_d.gam; a.flags = a_d.flags;
+        a.fail_list = a_d.fail_list; a.fail_count = a_d.fail_count;
+    }
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM, NS>;
     static_assert(!DM || (GSM && TC), "the FP64 tensor product is built with the tensor-core FP32 product");
     static_assert(!NS || (DM && N % 8 == 0 && kIterQ * LPQ / QPL == 128),
@@ -2161,7 +2168,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
             all = all && conv[c];
         }
         passes = it + 1;
-        if (__all_sync(0xffffffffu, all) || it >= kIterMax) break;
+        if (__all_sync(0xffffffffu, all) || it >= a.max_sweeps) break;
         // correction x += C r (FP32 product; every C element read serves the QPL q)
         float2 dx[QPL][RPL];
         if constexpr (TC) {
@@ -2226,6 +2233,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         if (h == 0) {
             a.chi[(size_t)q + (size_t)a.nq * w] = chi;
             a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+            if (!ok && a.fail_list) a.fail_list[atomicAdd(a.fail_count, 1)] = q + a.nq * w;
         }
         const double rf = 1.0 / (1.0 + a.s * a.U * chi);
 #pragma unroll
@@ -2527,6 +2535,82 @@ __device__ __forceinline__ double block_sum_det(double v, double* red) {
 // matrices and for box sizes without a tiled instantiation.  list == nullptr: all (q, w);
 // count_dev (may be null) holds the number of list entries (written earlier on the stream).
 // gscratch (may be null): LDGA_PIVOT_GRID matrices in HBM, used when [N][N+1] exceeds shared memory.
+// One flagged matrix lin = q + Nq w: the pivoted FP64 LU of [B | 1] in B (the CTA's [N][N+1] scratch);
+// writes chi, gamma and the flag (0 solved, 2 non-finite); returns true when chi is finite.  Every
+// thread of the CTA calls it.
+__device__ bool pivot_solve(const BseArgs& a, int lin, double2* B, double* red, int* piv_s) {
+    const int N = a.nnu;
+    const int ld = N + 1;
+    const int q = lin % a.nq, w = lin / a.nq;
+    const double2* Gw = a.Gamma + (size_t)w * N * N;
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        const int ii = e / N, j = e - ii * N;
+        double2 g = Gw[(size_t)ii * N + j];       // Gamma[j, ii] -> B[ii][j]
+        if (ii == j) g = cadd(g, cinv(a.chi0[(size_t)q + (size_t)a.nq * (ii + (size_t)N * w)]));
+        B[ii * ld + j] = g;
+    }
+    for (int ii = threadIdx.x; ii < N; ii += blockDim.x) B[ii * ld + N] = dmk(1.0, 0.0);
+    __syncthreads();
+    for (int k = 0; k < N; ++k) {
+        // pivot search (cabs1, as izamax) by warp 0
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = k;
+            for (int r = k + threadIdx.x; r < N; r += 32) {
+                const double v = fabs(B[r * ld + k].x) + fabs(B[r * ld + k].y);
+                if (v > best) { best = v; bi = r; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (threadIdx.x == 0) piv_s[0] = bi;
+        }
+        __syncthreads();
+        const int p = piv_s[0];
+        if (p != k) {
+            for (int j = threadIdx.x; j <= N; j += blockDim.x) {
+                const double2 t = B[k * ld + j];
+                B[k * ld + j] = B[p * ld + j];
+                B[p * ld + j] = t;
+            }
+        }
+        __syncthreads();
+        const double2 inv = cinv(B[k * ld + k]);
+        const int rows = N - k - 1, cols = N - k;   // columns k+1..N (incl. rhs)
+        for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
+            const int r = k + 1 + e / cols, j = k + 1 + e % cols;
+            const double2 m = cmul(B[r * ld + k], inv);
+            B[r * ld + j] = csub(B[r * ld + j], cmul(m, B[k * ld + j]));
+        }
+        __syncthreads();
+    }
+    // back substitution (serial in k, parallel dot products)
+    for (int k = N - 1; k >= 0; --k) {
+        double2 part = dmk(0.0, 0.0);
+        for (int j = k + 1 + threadIdx.x; j < N; j += blockDim.x) part = cadd(part, cmul(B[k * ld + j], B[j * ld + N]));
+        double re = block_sum_det(part.x, red);
+        double im = block_sum_det(part.y, red);
+        if (threadIdx.x == 0) B[k * ld + N] = cdiv(csub(B[k * ld + N], dmk(re, im)), B[k * ld + k]);
+        __syncthreads();
+    }
+    double ys = 0.0;
+    for (int ii = threadIdx.x; ii < N; ii += blockDim.x) ys += B[ii * ld + N].x;
+    const double chi = block_sum_det(ys, red) / (a.beta * a.beta);
+    if (threadIdx.x == 0) {
+        a.chi[(size_t)q + (size_t)a.nq * w] = chi;
+        a.flags[(size_t)q + (size_t)a.nq * w] = isfinite(chi) ? 0 : 2;
+    }
+    const double f = 1.0 + a.s * a.U * chi;
+    for (int ii = threadIdx.x; ii < N; ii += blockDim.x) {
+        const size_t ci = (size_t)q + (size_t)a.nq * (ii + (size_t)N * w);
+        a.gam[ci] = cdiv(B[ii * ld + N], cscale(a.chi0[ci], f));
+    }
+    __syncthreads();
+    return isfinite(chi);
+}
+
 __global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int32_t* list, int count,
                                                        const int32_t* count_dev, double2* gscratch) {
     extern __shared__ double2 sm[];
@@ -2535,77 +2619,28 @@ __global__ void __launch_bounds__(256) k_bse_lu_pivot(const BseArgs a, const int
     int* piv_s = reinterpret_cast<int*>(red + 64);                    // [4]
     double2* B = gscratch ? gscratch + (size_t)blockIdx.x * N * (N + 1)   // [N][N+1] row-major, rhs last
                           : reinterpret_cast<double2*>(piv_s + 4);
-    const int ld = N + 1;
     if (count_dev) count = count_dev[0];
-    for (int item = blockIdx.x; item < count; item += gridDim.x) {
-        const int lin = list ? list[item] : item;
-        const int q = lin % a.nq, w = lin / a.nq;
-        const double2* Gw = a.Gamma + (size_t)w * N * N;
-        for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-            const int ii = e / N, j = e - ii * N;
-            double2 g = Gw[(size_t)ii * N + j];       // Gamma[j, ii] -> B[ii][j]
-            if (ii == j) g = cadd(g, cinv(a.chi0[(size_t)q + (size_t)a.nq * (ii + (size_t)N * w)]));
-            B[ii * ld + j] = g;
-        }
-        for (int ii = threadIdx.x; ii < N; ii += blockDim.x) B[ii * ld + N] = dmk(1.0, 0.0);
-        __syncthreads();
-        for (int k = 0; k < N; ++k) {
-            // pivot search (cabs1, as izamax) by warp 0
-            if (threadIdx.x < 32) {
-                double best = -1.0;
-                int bi = k;
-                for (int r = k + threadIdx.x; r < N; r += 32) {
-                    const double v = fabs(B[r * ld + k].x) + fabs(B[r * ld + k].y);
-                    if (v > best) { best = v; bi = r; }
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    const double ob = __shfl_down_sync(0xffffffffu, best, o);
-                    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                    if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-                }
-                if (threadIdx.x == 0) piv_s[0] = bi;
-            }
-            __syncthreads();
-            const int p = piv_s[0];
-            if (p != k) {
-                for (int j = threadIdx.x; j <= N; j += blockDim.x) {
-                    const double2 t = B[k * ld + j];
-                    B[k * ld + j] = B[p * ld + j];
-                    B[p * ld + j] = t;
-                }
-            }
-            __syncthreads();
-            const double2 inv = cinv(B[k * ld + k]);
-            const int rows = N - k - 1, cols = N - k;   // columns k+1..N (incl. rhs)
-            for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
-                const int r = k + 1 + e / cols, j = k + 1 + e % cols;
-                const double2 m = cmul(B[r * ld + k], inv);
-                B[r * ld + j] = csub(B[r * ld + j], cmul(m, B[k * ld + j]));
-            }
-            __syncthreads();
-        }
-        // back substitution (serial in k, parallel dot products)
-        for (int k = N - 1; k >= 0; --k) {
-            double2 part = dmk(0.0, 0.0);
-            for (int j = k + 1 + threadIdx.x; j < N; j += blockDim.x) part = cadd(part, cmul(B[k * ld + j], B[j * ld + N]));
-            double re = block_sum_det(part.x, red);
-            double im = block_sum_det(part.y, red);
-            if (threadIdx.x == 0) B[k * ld + N] = cdiv(csub(B[k * ld + N], dmk(re, im)), B[k * ld + k]);
-            __syncthreads();
-        }
-        double ys = 0.0;
-        for (int ii = threadIdx.x; ii < N; ii += blockDim.x) ys += B[ii * ld + N].x;
-        const double chi = block_sum_det(ys, red) / (a.beta * a.beta);
-        if (threadIdx.x == 0) {
-            a.chi[(size_t)q + (size_t)a.nq * w] = chi;
-            a.flags[(size_t)q + (size_t)a.nq * w] = isfinite(chi) ? 0 : 2;
-        }
-        const double f = 1.0 + a.s * a.U * chi;
-        for (int ii = threadIdx.x; ii < N; ii += blockDim.x) {
-            const size_t ci = (size_t)q + (size_t)a.nq * (ii + (size_t)N * w);
-            a.gam[ci] = cdiv(B[ii * ld + N], cscale(a.chi0[ci], f));
-        }
-        __syncthreads();
+    for (int item = blockIdx.x; item < count; item += gridDim.x) pivot_solve(a, list ? list[item] : item, B, red, piv_s);
+}
+
+// Both channels' flagged matrices of a two-channel preconditioned solve in one launch: the lists the
+// solve appended (counts on the device), items of m first; a matrix whose result stays non-finite
+// adds one to *d_fail.
+__global__ void __launch_bounds__(256) k_bse_lu_pivot_pair(const BseArgs am, const BseArgs ad, double2* gscratch,
+                                                            int32_t* d_fail) {
+    extern __shared__ double2 sm[];
+    const int N = am.nnu;
+    double* red = reinterpret_cast<double*>(sm);
+    int* piv_s = reinterpret_cast<int*>(red + 64);
+    double2* B = gscratch ? gscratch + (size_t)blockIdx.x * N * (N + 1) : reinterpret_cast<double2*>(piv_s + 4);
+    // the lists hold at most one entry per (q, w) of the launch
+    const int cap = am.nq * am.nw;
+    const int cm = min(max(am.fail_count[0], 0), cap), cd = min(max(ad.fail_count[0], 0), cap);
+    for (int item = blockIdx.x; item < cm + cd; item += gridDim.x) {
+        const bool is_m = item < cm;
+        const bool ok = is_m ? pivot_solve(am, am.fail_list[item], B, red, piv_s)
+                             : pivot_solve(ad, ad.fail_list[item - cm], B, red, piv_s);
+        if (threadIdx.x == 0 && !ok) atomicAdd(d_fail, 1);
     }
 }
 
@@ -2848,6 +2883,7 @@ BseArgs bse_args(ldga_ctx* ctx, int channel) {
     a.gam = ctx->d_gam[channel] + w0 * nq * nnu;
     a.flags = ctx->d_flags + w0 * nq;
     a.stats = ctx->d_iter_stats;
+    a.max_sweeps = ctx->iter_sweeps;
     return a;
 }
 
@@ -2935,8 +2971,9 @@ int launch_bse(ldga_ctx* ctx, int channel, int32_t* d_fail) {
 }
 
 // Both channels of the chain: one launch of the tuned configuration when it has a two-channel form
-// (channel d flags into d_flags2), then each channel's pivoted re-solve of flagged matrices as in
-// launch_bse; otherwise launch_bse for m, then d.
+// (channel d flags into d_flags2); the matrices it leaves above its backward-error bound are appended
+// to one list per channel (counts in d_count[2], d_count[3], zeroed by the caller with d_fail) and
+// re-solved by one pivoted launch over both lists.  Otherwise launch_bse for m, then d.
 int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail) {
     const BseVariant* v = nullptr;
     const int nv = variants_of(ctx->Nnu, ctx->prec, &v);
@@ -2946,33 +2983,28 @@ int launch_bse_pair(ldga_ctx* ctx, int32_t* d_fail) {
         const int st = launch_bse(ctx, LDGA_CH_M, d_fail);
         return st != LDGA_OK ? st : launch_bse(ctx, LDGA_CH_D, d_fail);
     }
-    const int n = ctx->Nq * shard_nw(ctx);
     const size_t nall = (size_t)ctx->Nq * ctx->Nw;
     if (!ctx->d_flags2) {
         LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_flags2), nall * sizeof(int32_t)));
         LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_flags2, 0, nall * sizeof(int32_t), ctx->stream));
     }
+    if (!ctx->d_list2) LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_list2), nall * sizeof(int32_t)));
     BseArgs am = bse_args(ctx, LDGA_CH_M), ad = bse_args(ctx, LDGA_CH_D);
     ad.flags = ctx->d_flags2 + (size_t)ctx->w_lo * ctx->Nq;
+    am.fail_list = ctx->d_list;
+    am.fail_count = ctx->d_count + 2;
+    ad.fail_list = ctx->d_list2;
+    ad.fail_count = ctx->d_count + 3;
     const int st = v[i].run_pair(ctx, am, ad);
     if (st != LDGA_OK) return st;
     const bool in_hbm = bse_pivot_smem(ctx->Nnu) > LDGA_PIVOT_SMEM_MAX;
     if (in_hbm && !ctx->d_pivot_scratch) return ctx_fail(ctx, LDGA_ERR_ARG, "pivoted BSE scratch missing");
     const size_t smp = in_hbm ? 64 * sizeof(double) + 16 : bse_pivot_smem(ctx->Nnu);
     double2* gscr = in_hbm ? ctx->d_pivot_scratch : nullptr;
-    LDGA_CUDA(ctx, set_smem(ctx, k_bse_lu_pivot, smp));
-    for (const BseArgs* a : {&am, &ad}) {
-        LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, sizeof(int32_t), ctx->stream));
-        k_compact_flags<<<148, 256, 0, ctx->stream>>>(a->flags, n, ctx->d_list, ctx->d_count);
-        LDGA_LAUNCHED(ctx, "k_compact_flags");
-        {
-            StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
-            k_bse_lu_pivot<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(*a, ctx->d_list, 0, ctx->d_count, gscr);
-            LDGA_LAUNCHED(ctx, "k_bse_lu_pivot");
-        }
-        k_count_flags<<<148, 256, 0, ctx->stream>>>(a->flags, n, d_fail);
-        LDGA_LAUNCHED(ctx, "k_count_flags");
-    }
+    LDGA_CUDA(ctx, set_smem(ctx, k_bse_lu_pivot_pair, smp));
+    StageTimer st_(ctx, LDGA_STAGE_BSE_FALLBACK);
+    k_bse_lu_pivot_pair<<<LDGA_PIVOT_GRID, 256, smp, ctx->stream>>>(am, ad, gscr, d_fail);
+    LDGA_LAUNCHED(ctx, "k_bse_lu_pivot_pair");
     return LDGA_OK;
 }
 

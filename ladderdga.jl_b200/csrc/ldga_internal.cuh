@@ -104,7 +104,8 @@ struct ldga_ctx {
     double* d_red = nullptr;       // reduction scratch
     int32_t* d_flags = nullptr;    // BSE fallback flags [Nq*Nw]
     int32_t* d_flags2 = nullptr;   // the d channel's flags when both channels run in one launch
-    int32_t* d_list = nullptr;     // compacted fallback list
+    int32_t* d_list = nullptr;     // compacted fallback list (the m channel's list of a pair launch)
+    int32_t* d_list2 = nullptr;    // the d channel's list of a pair launch
     int32_t* d_count = nullptr;
     double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
     int2* d_bub_pairs = nullptr;          // bubble pairs computed directly (pair, conjugate partner or -1)
@@ -149,6 +150,9 @@ struct ldga_ctx {
     // the λm Newton's cluster all-reduce by st.async + mbarrier instead of a cluster barrier per
     // iteration (environment LDGA_NEWTON=barrier at ldga_create selects the barrier form)
     bool newton_async = true;
+    // residual sweeps of MIXED's preconditioned BSE iteration before a matrix is handed to the pivoted
+    // FP64 solve (environment LDGA_ITER_SWEEPS at ldga_create, 0..1000; 0 hands every matrix over)
+    int iter_sweeps = 40;
 
     // stage timing (ldga_profile / ldga_stage_times)
     bool profiling = false;

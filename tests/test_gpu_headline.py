@@ -179,6 +179,47 @@ def test_config3_mixed_chain_graph(cfg3):
         L.tune_reset()
 
 
+def test_config3_chain_pivoted_fallback_of_every_matrix(cfg3):
+    """The chain's two-channel BSE with every matrix handed to the pivoted FP64 solve: with the sweep
+    limit at 0 (LDGA_ITER_SWEEPS=0 when the handle is made) the preconditioned iteration stops after
+    its first residual, appends every matrix (q + Nq w) to its channel's list, and one pivoted launch
+    re-solves both lists.  χ and γ of both channels against the oracle at the parity tolerance (the
+    first residual alone is far from it), eager, captured and replayed; λm a root of the oracle's f."""
+    import tempfile
+    inp, ref = cfg3
+    fd, path = tempfile.mkstemp()
+    os.write(fd, f"bse 40 {L.PREC_MIXED} iter8x2dm2ns:3\n".encode())
+    os.close(fd)
+    os.environ["LDGA_ITER_SWEEPS"] = "0"
+    try:
+        L.tune_reset()
+        L.tune_load(path)
+        h = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+    finally:
+        del os.environ["LDGA_ITER_SWEEPS"]
+        os.unlink(path)
+    try:
+        rh, cm = ref["h"], ref["chi_m"]
+        rhs = 2 * rh.imp_density - R.sum_kw(rh.kG, ref["chi_d"])
+        run = ChainM(h)
+        h.ctx.call("ldga_bse_sweeps", None, None)      # clear the sweep counters
+        for use_graph in (0, 1, 1):
+            sc, S_chain = run(use_graph)
+            passes, warps = C.c_int64(), C.c_int64()
+            h.ctx.call("ldga_bse_sweeps", C.byref(passes), C.byref(warps))
+            assert warps.value > 0 and passes.value == warps.value, (passes.value, warps.value)   # one sweep
+            dev = device_arrays(h.ctx)
+            check_arrays(dev, ref, ("all pivoted", use_graph))
+            lam = sc[0]
+            f = R.sum_kw(rh.kG, cm, transform=lambda x: R.chi_lambda(x, lam)) - rhs
+            scale = R.sum_kw(rh.kG, cm, transform=lambda x: np.abs(R.chi_lambda(x, lam)))
+            assert abs(f) <= 1e-9 * max(1.0, scale), (lam, f)
+            Sg, _, mu, _, _ = at_lambda(h, lam)
+            assert rel(S_chain, Sg) < 1e-12 and abs(mu - sc[1]) < 1e-12
+    finally:
+        L.tune_reset()
+
+
 def test_config3_every_mixed_bse_configuration(cfg3):
     """Every compiled MIXED configuration at Nnu = 40 (the autotuner's candidates) on the headline
     input: χ_r and γ_r against the oracle, no matrix left to the pivoted fallback."""
