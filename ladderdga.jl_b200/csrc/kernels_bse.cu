@@ -2727,6 +2727,8 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
     return LDGA_OK;
 }
 
+#include "bse_jacobi.cuh"
+
 // ------------------------------------------------------------------------------------------------
 // Configurations per box size and precision mode (threads per matrix, matrices per CTA, resident
 // CTAs per SM the register allocation must allow).  Entry 0 of every list is the default; the
@@ -2838,9 +2840,11 @@ const BseVariant inv_60[] = {{&run_tile<60, 16, 16, 1, 1, double, LDGA_PREC_FP64
 // (32 x 32 threads per matrix -- a 4 x 4 register tile instead of 16 x 16 threads' spilling 8 x 8 --
 // measured 1.76x slower: 120 steps of a 1024-thread barrier over little work per thread)
 const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};
-// (no preconditioned configuration at Nν = 120: on the test matrices its condition numbers reach 1e4,
-// where the iteration's backward error of 1e-14 no longer guarantees the 1e-10 forward accuracy)
-const BseVariant mixed_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}, {&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
+// MIXED at Nν = 120: the Jacobi refinement (bse_jacobi.cuh), whose stop test bounds the forward error
+// too (the test matrices' condition numbers reach 1e4, where a backward error of 1e-14 alone would
+// not guarantee the 1e-10 forward accuracy), then the LU forms
+const BseVariant mixed_120[] = {{&run_jacobi<120>, "jac", &run_jacobi_pair<120>},
+                                {&run_lu<120, 16, 1, 1, false>, "lu16g:1"}, {&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
 
 int variants_of(int nnu, int prec, const BseVariant** out) {
 #define LDGA_BOX(N)                                                                                      \

@@ -437,6 +437,66 @@ def test_bse_large_box_every_configuration(prec, require_gpu):
         L.tune_reset()
 
 
+@pytest.mark.parametrize("sweeps", [None, 0])
+def test_bse_large_box_jacobi_pair(sweeps, require_gpu):
+    """MIXED's Jacobi refinement at Nν = 120 ("jac") inside ldga_chain_m, where both channels run
+    in one launch: χ_m and χ_d against the oracle and, bit for bit, against the step-by-step
+    single-channel launches. With the sweep limit at 0 (LDGA_ITER_SWEEPS=0) every matrix is handed
+    to the pivoted solve. Its 120 × 121 working matrices live in HBM; in the chain, one launch
+    re-solves both channels' lists."""
+    import ctypes as C
+    import os
+    import tempfile
+    import torch
+    inp = S.make_input(dim=2, ns=4, beta=40.0, U=1.0, n_iv=60, n_iw=2, seed=150)
+    ref = R.run_chain(inp, lambda_type=None)
+    fd, path = tempfile.mkstemp()
+    os.write(fd, f"bse 120 {L.PREC_MIXED} jac\n".encode())
+    os.close(fd)
+    if sweeps is not None:
+        os.environ["LDGA_ITER_SWEEPS"] = str(sweeps)
+    try:
+        L.tune_reset()
+        L.tune_load(path)
+        h = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+        h2 = L.setup_synthetic(inp, precision=L.PREC_MIXED)
+    finally:
+        os.environ.pop("LDGA_ITER_SWEEPS", None)
+        os.unlink(path)
+    try:
+        ctx = h.ctx
+        chi0 = L.calc_bubble(h)
+        step = {}
+        for r in ("m", "d"):
+            x, g = L.calc_χγ(r, h, chi0)
+            want = 0 if sweeps is None else ctx.Nq * ctx.Nw
+            assert x.n_fallback == want, (r, x.n_fallback, want)
+            assert chi_rel(x.data, ref, r) < RTOL, r
+            assert rel(g.data, ref[f"gamma_{r}"]) < RTOL, r
+            step[r] = np.array(x.data)
+
+        def pinned(a):
+            v = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(-1, order="F")).view(np.float64)
+            return torch.from_numpy(v.copy()).pin_memory()
+
+        c2 = h2.ctx
+        src = [pinned(a) for a in (h2.Σ_loc, h2.Γ_m, h2.Γ_d, h2.χDMFT_m, h2.gImp)]
+        numax = h2.sP.n_iν
+        S_out = torch.zeros(c2.Nq * numax * 2, dtype=torch.float64).pin_memory()
+        cm = torch.zeros(c2.Nq * c2.Nw, dtype=torch.float64).pin_memory()
+        cd = torch.zeros(c2.Nq * c2.Nw, dtype=torch.float64).pin_memory()
+        sc = (C.c_double * 8)()
+        p = [C.c_void_p(t.data_ptr()) for t in src]
+        c2.call("ldga_chain_m", p[0], len(h2.Σ_loc), p[1], p[2], p[3], p[4], len(h2.gImp), h2.imp_density,
+                h2.χloc_m_sum, 0, C.c_void_p(S_out.data_ptr()), C.c_void_p(cm.data_ptr()),
+                C.c_void_p(cd.data_ptr()), sc)
+        for t, r in ((cm, "m"), (cd, "d")):
+            got = t.numpy().reshape((c2.Nq, c2.Nw), order="F")
+            assert np.array_equal(got, step[r]), r                # the same kernel, one launch for both
+    finally:
+        L.tune_reset()
+
+
 def test_batch_chain_uneven_points(require_gpu):
     """ldga_batch_chain_m over points of different Nν (4, 16, 30) and U: each point equals the
     single-point λm chain and, within the parity tolerance, the oracle."""
