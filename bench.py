@@ -1066,77 +1066,90 @@ BATCH_NAME = ("uneven batch: {n} points of 2D sc Nk=32^2 (153 irreducible q), U 
 def run_batch(args):
     """The uneven (U, beta) scan: every point's chain in flight together (one stream per point)."""
     import torch
-    import ladderdga_b200 as L
     from ladderdga_b200 import _lib
     from ladderdga_b200 import synthetic as S
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     pts = S.batch_points(args.points, ns=args.ns or 32)
-    chains = []
-    for p in pts:
-        chains.append(Chain(S.make_input(**p), PREC_NAMES[args.prec], local, stream=torch.cuda.Stream(local)))
-    n = len(chains)
-    tuned = {}
-    for c in chains:                                   # one autotuning run per box size
-        if c.ctx.Nnu not in tuned:
-            tuned[c.ctx.Nnu] = tune(c)
-    main = torch.cuda.current_stream(local)
-    scs = [(C.c_double * 8)() for _ in chains]
-    handles = (C.c_void_p * n)(*[c.ctx.h.value for c in chains])
-    status = (C.c_int32 * n)()
-    ios = {}
-    for key, outputs in (("dev", False), ("pin", True)):
-        arr = (_lib.ChainIO * n)()
-        for i, c in enumerate(chains):
-            arr[i] = c.io(c.dev if key == "dev" else c.pin, outputs, scs[i])
-        ios[key] = arr
+    main_stream = torch.cuda.current_stream(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    lib = chains[0].lib
-    for c in chains:
-        c.ctx.call("ldga_profile", 1)
 
-    def timed(key):
+    def build(prec):
+        chains = [Chain(S.make_input(**p), prec, local, stream=torch.cuda.Stream(local)) for p in pts]
+        tuned = {}
+        for c in chains:                               # one autotuning run per box size
+            if c.ctx.Nnu not in tuned:
+                tuned[c.ctx.Nnu] = tune(c)
+        scs = [(C.c_double * 8)() for _ in chains]
+        ios = {}
+        for key, outputs in (("dev", False), ("pin", True)):
+            arr = (_lib.ChainIO * len(chains))()
+            for i, c in enumerate(chains):
+                arr[i] = c.io(c.dev if key == "dev" else c.pin, outputs, scs[i])
+            ios[key] = arr
+        return chains, tuned, scs, ios
+
+    def timed(chains, ios, key, steps, sel=None):
+        """Mean device time of `steps` ldga_batch_chain_m calls over the points `sel` (all: None)."""
+        idx = list(range(len(chains))) if sel is None else sel
+        sub = [chains[i] for i in idx]
+        handles = (C.c_void_p * len(sub))(*[c.ctx.h.value for c in sub])
+        arr = (_lib.ChainIO * len(sub))(*[ios[key][i] for i in idx])
+        status = (C.c_int32 * len(sub))()
+        lib = sub[0].lib
         times = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.fill_(1.0)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(main)
-            for c in chains:
+            a.record(main_stream)
+            for c in sub:
                 c.stream.wait_event(a)
-            st = lib.ldga_batch_chain_m(n, handles, ios[key], 1, status)
+            st = lib.ldga_batch_chain_m(len(sub), handles, arr, 1, status)
             if st != 0:
-                raise RuntimeError(f"ldga_batch_chain_m failed: {[lib.ldga_last_error(c.ctx.h).decode() for c in chains]}")
-            for c in chains:
+                raise RuntimeError(f"ldga_batch_chain_m failed: {[lib.ldga_last_error(c.ctx.h).decode() for c in sub]}")
+            for c in sub:
                 e = torch.cuda.Event()
                 e.record(c.stream)
-                main.wait_event(e)
-            b.record(main)
+                main_stream.wait_event(e)
+            b.record(main_stream)
             b.synchronize()
             times.append(a.elapsed_time(b))
-        return times
+        return float(np.mean(times))
 
-    for key in ("dev", "pin"):
+    def warm(chains, ios, key):
+        handles = (C.c_void_p * len(chains))(*[c.ctx.h.value for c in chains])
+        status = (C.c_int32 * len(chains))()
         for _ in range(max(args.warmup, 3)):
-            lib.ldga_batch_chain_m(n, handles, ios[key], 1, status)
-    torch.cuda.synchronize()
+            chains[0].lib.ldga_batch_chain_m(len(chains), handles, ios[key], 1, status)
+        torch.cuda.synchronize()
+
+    def launches(chains):
+        tot = 0
+        for c in chains:
+            v = C.c_int64()
+            c.ctx.call("ldga_launch_count", C.byref(v))
+            tot += v.value
+        return tot
+
+    chains, tuned, scs, ios = build(PREC_NAMES[args.prec])
+    n = len(chains)
+    for key in ("dev", "pin"):
+        warm(chains, ios, key)
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    cnt0 = []
-    for c in chains:
-        v = C.c_int64()
-        c.ctx.call("ldga_launch_count", C.byref(v))
-        cnt0.append(v.value)
-    t_dev = timed("dev")
-    cnt1 = []
-    for c in chains:
-        v = C.c_int64()
-        c.ctx.call("ldga_launch_count", C.byref(v))
-        cnt1.append(v.value)
-    t_e2e = timed("pin")
+    cnt0 = launches(chains)
+    ms = timed(chains, ios, "dev", args.steps)
+    cnt1 = launches(chains)
+    ms_e2e = timed(chains, ios, "pin", args.steps)
     clk = clocks.stop()
+    # each box size's points alone (untimed for the line's value): where the batch's time goes
+    few = max(3, args.steps // 4)
+    by_box = {}
+    for nnu in sorted(tuned):
+        sel = [i for i, c in enumerate(chains) if c.ctx.Nnu == nnu]
+        by_box[str(nnu)] = {"points": len(sel), "ms": timed(chains, ios, "dev", few, sel)}
     points = sum(c.points for c in chains)
-    ms, ms_e2e = float(np.mean(t_dev)), float(np.mean(t_e2e))
     from ladderdga_b200 import parallel as P
     ms, ms_e2e = P.max_over_ranks(ms), P.max_over_ranks(ms_e2e)
     nnu = sorted({c.ctx.Nnu for c in chains})
@@ -1152,8 +1165,20 @@ def run_batch(args):
                     "h2d_bytes_per_step": sum(c.h2d_bytes for c in chains),
                     "d2h_bytes_per_step": sum(c.d2h_bytes for c in chains), "ms_per_step": ms_e2e,
                     "path": "C ABI (ldga_batch_chain_m) from pinned host buffers"},
-            "gpu_launches": int(sum(cnt1) - sum(cnt0)),
+            "gpu_launches": int(cnt1 - cnt0),
+            "by_box_size": by_box,
+            "by_box_note": "each box size's points alone in one ldga_batch_chain_m call (device time)",
             "clocks": clk}
+    if args.prec == "mixed" and not args.no_fp64_compare:
+        # the same batch in FP64 mode (LU solves throughout), device-resident inputs
+        del chains, ios
+        torch.cuda.synchronize()
+        c64, tuned64, _, ios64 = build(PREC_NAMES["fp64"])
+        warm(c64, ios64, "dev")
+        ms64 = P.max_over_ranks(timed(c64, ios64, "dev", few))
+        line["fp64_compare"] = {"ms_per_step": ms64, "value": world * points / (ms64 / 1e3), "steps": few,
+                                "bse_config": {str(k): v for k, v in sorted(tuned64.items())},
+                                "mixed_over_fp64": ms64 / ms}
     if rank == 0:
         print(json.dumps(line), flush=True)
         if args.out:

@@ -1326,7 +1326,14 @@ int ldga_batch_chain_m(int32_t n, ldga_ctx* const* ctxs, const ldga_chain_io* io
     std::vector<char> rep(n, 0);
     for (int i = 0; i < n; ++i)
         if (ctxs[i] && sharded(ctxs[i])) return require_unsharded(ctxs[i], "ldga_batch_chain_m");
-    for (int i = 0; i < n; ++i) {        // every point's chain is in flight before the first wait
+    // every point's chain is in flight before the first wait.  The largest boxes go first: their input
+    // copies lead the copy engine's queue and their long BSE launches start while the small points'
+    // copies and chains fill in behind them (the order of submission changes no result)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    auto work = [&](int i) { return ctxs[i] ? (double)ctxs[i]->Nnu * ctxs[i]->Nnu * ctxs[i]->Nw : 0.0; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
+    for (int i : order) {
         ldga_ctx* c = ctxs[i];
         if (!c) { st[i] = LDGA_ERR_ARG; continue; }
         DeviceGuard g(c->device);

@@ -18,51 +18,66 @@
 // Γ(ω) from L2 once per sweep, in tiles of 8 columns (cp.async, double-buffered).  All 32 q use
 // every tile:
 //     R = Γᵀ X  (N × 32 complex),
-// as FP64 tensor-core products (mma.sync m8n8k4 .f64).  Each complex tile product takes three real
-// ones (Karatsuba):
-//     S1 = Re·Re,  S2 = Im·Im,  S3 = (Re + Im)·(Re + Im),
-//     Re = S1 - S2,  Im = S3 - S1 - S2.
-// 12 warps: warp (g, n) owns rows [g N/3, (g+1) N/3) (N/24 m-tiles of 8) of the 8 q of n-tile n.
-// Lane l of a warp owns rows 8 mt + l/4 and the q pair 8 n + 2 (l%4) + {0, 1} of every m-tile mt.
-// It forms r there and updates x in shared memory; reductions over rows run by shuffles within the
-// warp, then over the three row groups through shared memory.
+// as FP64 tensor-core products (mma.sync m8n8k4 .f64).  The default (K3, Karatsuba) takes three
+// real products per complex tile: S1 = Re·Re, S2 = Im·Im, S3 = (Re + Im)·(Re + Im), then
+// Re = S1 - S2 and Im = S3 - S1 - S2.  The form with four ("jac4": Re = Σ Re·Re + Im·(-Im),
+// Im = Σ Re·Im + Im·Re) needs no FP64 add before a product and one accumulator less.  It does a
+// third more tensor work, and measured 10 % slower on the β = 40 points; the autotuner times both.
+// A CTA of Q q (32 or 16) runs 3 Q/8 warps: warp (g, n) owns rows [g N/3, (g+1) N/3) (N/24
+// m-tiles of 8) of the 8 q of n-tile n.  Lane l of a warp owns rows 8 mt + l/4 and the q pair
+// 8 n + 2 (l%4) + {0, 1} of every m-tile mt.  It forms r there and updates x in shared memory;
+// reductions over rows run by shuffles within the warp, then over the three row groups through
+// shared memory.  Q = 32 runs one CTA per SM with NBUF = 4 tile buffers; Q = 16 runs two CTAs per
+// SM, so that one CTA's barriers and epilogue overlap the other's products; Γ then crosses L2
+// twice as often per q.
 //
-// Shared memory (JacSmem<N>): two Γ tiles [N][LDG] complex; x [N][LDX] complex; D = 1/χ₀ [N][LDX]
-// complex; the diagonal of Γ and its off-diagonal row sums [N]; reduction slots.  The strides make
-// the fragment loads conflict-free: a 16-byte load serves 8 lanes per wavefront, so a tile row
-// stride ≡ 4 (mod 8) complex and an x row stride ≡ 2 (mod 8).
-constexpr int kJacQ = 32;             // q per CTA
+// Shared memory (JacSmem): NBUF Γ tiles [N][8] complex; x and D = 1/χ₀, each [N][Q + 2] complex;
+// the diagonal of Γ and its off-diagonal row sums [N]; reduction slots.  The fragment loads are
+// conflict-free (a 16-byte load serves 8 lanes per wavefront):
+//   - a tile row stores its 8 columns XOR-swizzled by 4 on odd rows;
+//   - the x and D rows have a stride ≡ 2 (mod 8) complex.
 constexpr int kJacKC = 8;             // Γ columns per streamed tile
-constexpr int kJacWarps = 12;         // 3 row groups x 4 n-tiles of 8 q
-constexpr int kJacThreads = 32 * kJacWarps;
 constexpr double kSqrt2 = 1.4142135623730951;
 
-template <int N>
+template <int N, int Q, int NBUF>
 struct JacSmem {
     static_assert(N % 24 == 0, "three row groups of whole 8-row tiles");
+    static_assert(Q == 16 || Q == 32, "q per CTA");
+    static_assert(NBUF >= 2, "double buffering at least");
     static constexpr int MTW = N / 24;                  // m-tiles per warp
-    static constexpr int LDG = kJacKC + 4;              // ≡ 4 (mod 8)
-    static constexpr int LDX = kJacQ + 2;               // ≡ 2 (mod 8)
-    static constexpr size_t off_g = 0;                                          // [2][N][LDG] double2
-    static constexpr size_t off_x = off_g + 2 * (size_t)N * LDG * sizeof(double2);   // [N][LDX] double2
-    static constexpr size_t off_d = off_x + (size_t)N * LDX * sizeof(double2);       // [N][LDX] double2
-    static constexpr size_t off_diag = off_d + (size_t)N * LDX * sizeof(double2);    // [N] double2
-    static constexpr size_t off_row = off_diag + (size_t)N * sizeof(double2);        // [N] double
-    static constexpr size_t off_red = off_row + (size_t)N * sizeof(double);          // [5][3][kJacQ] double
-    static constexpr size_t off_conv = off_red + 15 * (size_t)kJacQ * sizeof(double); // [kJacQ] int
-    static constexpr size_t bytes = off_conv + kJacQ * sizeof(int);
+    static constexpr int NWN = Q / 8;                   // n-tiles
+    static constexpr int WARPS = 3 * NWN;
+    static constexpr int THREADS = 32 * WARPS;
+    static constexpr int LDX = Q + 2;                   // ≡ 2 (mod 8)
+    static constexpr size_t tile = (size_t)N * kJacKC;  // complex per tile
+    static constexpr size_t off_g = 0;                                                 // [NBUF][N][8] double2
+    static constexpr size_t off_x = off_g + NBUF * tile * sizeof(double2);             // [N][LDX] double2
+    static constexpr size_t off_d = off_x + (size_t)N * LDX * sizeof(double2);         // [N][LDX] double2
+    static constexpr size_t off_diag = off_d + (size_t)N * LDX * sizeof(double2);      // [N] double2
+    static constexpr size_t off_row = off_diag + (size_t)N * sizeof(double2);          // [N] double
+    static constexpr size_t off_red = off_row + (size_t)N * sizeof(double);            // [5][3][Q] double
+    static constexpr size_t off_conv = off_red + 15 * (size_t)Q * sizeof(double);      // [Q] int
+    static constexpr size_t bytes = off_conv + Q * sizeof(int);
 };
+
+// element (row i, column c < 8) of a tile
+__device__ __forceinline__ int jac_tile_idx(int i, int c) { return i * kJacKC + (c ^ ((i & 1) << 2)); }
 
 __device__ __forceinline__ void jac_cp16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
                  : "memory");
 }
 __device__ __forceinline__ void jac_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void jac_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void jac_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory"); }
 
-template <int N>
-__global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m, const BseArgs a_d) {
-    using S = JacSmem<N>;
+template <int N, int Q, int NBUF, bool K3>
+__global__ void __launch_bounds__(JacSmem<N, Q, NBUF>::THREADS, Q == 16 ? 2 : 1)
+k_bse_jacobi(const BseArgs a_m, const BseArgs a_d) {
+    using S = JacSmem<N, Q, NBUF>;
+    constexpr int kJacQ = Q;
+    constexpr int kJacThreads = S::THREADS;
+    constexpr int kJacWarps = S::WARPS;
     constexpr int NT = N / kJacKC;                     // Γ tiles per sweep
     BseArgs a = a_m;
     if (blockIdx.z) {
@@ -79,7 +94,7 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m
     int* conv = reinterpret_cast<int*>(jac_raw + S::off_conv);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wg = warp >> 2, wn = warp & 3;           // row group, n-tile
+    const int wg = warp / S::NWN, wn = warp % S::NWN;  // row group, n-tile
     const int w = blockIdx.y, q0 = blockIdx.x * kJacQ;
     const int nvalid = min(kJacQ, a.nq - q0);
     const double2* Gw = a.Gamma + (size_t)w * N * N;   // row i of B (without its diagonal term): Gw[i N + j]
@@ -111,12 +126,15 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m
         X[i * S::LDX + c] = c < nvalid ? cinv(cadd(gdiag[i], D[i * S::LDX + c])) : dmk(0.0, 0.0);
     }
 
-    // one tile of Γ: rows 0..N-1, columns [kJacKC t, kJacKC (t + 1)), as 16-byte copies
-    auto load_tile = [&](int t, int buf) {
-        double2* dst = G + (size_t)buf * N * S::LDG;
-        for (int e = tid; e < N * kJacKC; e += kJacThreads) {
-            const int i = e / kJacKC, c = e - i * kJacKC;
-            jac_cp16(dst + i * S::LDG + c, Gw + (size_t)i * N + kJacKC * t + c);
+    // one tile of Γ: rows 0..N-1, columns [kJacKC t, kJacKC (t + 1)), as 16-byte copies; every call
+    // commits one group (empty past the last tile), so group t is tile t in every sweep
+    auto load_tile = [&](int t) {
+        if (t < NT) {
+            double2* dst = G + (size_t)(t % NBUF) * S::tile;
+            for (int e = tid; e < N * kJacKC; e += kJacThreads) {
+                const int i = e / kJacKC, c = e - i * kJacKC;
+                jac_cp16(dst + jac_tile_idx(i, c), Gw + (size_t)i * N + kJacKC * t + c);
+            }
         }
         jac_commit();
     };
@@ -126,26 +144,46 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m
     int it = 0;
     for (;; ++it) {
         // ---- R = B x without the diagonal 1/χ₀ term, on the FP64 tensor path
-        double s1[S::MTW][2], s2[S::MTW][2], s3[S::MTW][2];
+        // K3: S1 = Σ Re·Re, S2 = Σ Im·Im, S3 = Σ (Re + Im)(Re + Im); otherwise S1 = Re, S2 = Im directly
+        double s1[S::MTW][2], s2[S::MTW][2], s3[K3 ? S::MTW : 1][2];
 #pragma unroll
-        for (int m = 0; m < S::MTW; ++m) s1[m][0] = s1[m][1] = s2[m][0] = s2[m][1] = s3[m][0] = s3[m][1] = 0.0;
-        load_tile(0, 0);
+        for (int m = 0; m < S::MTW; ++m) s1[m][0] = s1[m][1] = s2[m][0] = s2[m][1] = 0.0;
+#pragma unroll
+        for (int m = 0; m < (K3 ? S::MTW : 1); ++m) s3[m][0] = s3[m][1] = 0.0;
+#pragma unroll
+        for (int t = 0; t < NBUF - 1; ++t) load_tile(t);
         for (int t = 0; t < NT; ++t) {
-            jac_wait_all();
+            jac_wait<NBUF - 2>();                      // group t (tile t) complete
             __syncthreads();                           // tile t visible; tile t - 1's buffer free
-            if (t + 1 < NT) load_tile(t + 1, (t + 1) & 1);
-            const double2* Gt = G + (size_t)(t & 1) * N * S::LDG;
+            load_tile(t + NBUF - 1);                   // into tile t - 1's buffer
+            const double2* Gt = G + (size_t)(t % NBUF) * S::tile;
 #pragma unroll
             for (int kk = 0; kk < kJacKC; kk += 4) {
                 const double2 b = X[(kJacKC * t + kk + fc) * S::LDX + 8 * wn + fr];
-                const double bs = b.x + b.y;
+                double2 g[S::MTW];
 #pragma unroll
-                for (int m = 0; m < S::MTW; ++m) {
-                    const int row = 8 * (wg * S::MTW + m) + fr;
-                    const double2 g = Gt[row * S::LDG + kk + fc];
-                    mma_f64(s1[m], g.x, b.x);
-                    mma_f64(s2[m], g.y, b.y);
-                    mma_f64(s3[m], g.x + g.y, bs);
+                for (int m = 0; m < S::MTW; ++m) g[m] = Gt[jac_tile_idx(8 * (wg * S::MTW + m) + fr, kk + fc)];
+                if constexpr (K3) {
+                    const double bs = b.x + b.y;
+#pragma unroll
+                    for (int m = 0; m < S::MTW; ++m) {
+                        mma_f64(s1[m], g[m].x, b.x);
+                        mma_f64(s2[m], g[m].y, b.y);
+                        mma_f64(s3[m], g[m].x + g[m].y, bs);
+                    }
+                } else {
+                    // four real products, in two rounds so that no accumulator is used twice in a row
+                    const double bn = -b.y;
+#pragma unroll
+                    for (int m = 0; m < S::MTW; ++m) {
+                        mma_f64(s1[m], g[m].x, b.x);
+                        mma_f64(s2[m], g[m].x, b.y);
+                    }
+#pragma unroll
+                    for (int m = 0; m < S::MTW; ++m) {
+                        mma_f64(s1[m], g[m].y, bn);
+                        mma_f64(s2[m], g[m].y, b.x);
+                    }
                 }
             }
         }
@@ -163,7 +201,9 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m
                 const double2 x = X[i * S::LDX + q];
                 const double2 d = D[i * S::LDX + q];
                 const double2 bx = cmul(d, x);
-                const double2 r = dmk(1.0 - (s1[m][c] - s2[m][c]) - bx.x, -(s3[m][c] - s1[m][c] - s2[m][c]) - bx.y);
+                const double2 gx = K3 ? dmk(s1[m][c] - s2[m][c], s3[K3 ? m : 0][c] - s1[m][c] - s2[m][c])
+                                      : dmk(s1[m][c], s2[m][c]);
+                const double2 r = dmk(1.0 - gx.x - bx.x, -gx.y - bx.y);
                 const double2 bii = cadd(gdiag[i], d);
                 const double2 dx = cdiv(r, bii);
                 dv[m][c] = dx;
@@ -283,20 +323,22 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_bse_jacobi(const BseArgs a_m
     }
 }
 
-template <int N>
+template <int N, int Q, int NBUF, bool K3>
 int run_jacobi_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
-    using S = JacSmem<N>;
-    auto kern = k_bse_jacobi<N>;
+    using S = JacSmem<N, Q, NBUF>;
+    auto kern = k_bse_jacobi<N, Q, NBUF, K3>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
-    dim3 grid((a.nq + kJacQ - 1) / kJacQ, a.nw, a_d ? 2 : 1);
-    kern<<<grid, kJacThreads, S::bytes, ctx->stream>>>(a, a_d ? *a_d : a);
+    dim3 grid((a.nq + Q - 1) / Q, a.nw, a_d ? 2 : 1);
+    kern<<<grid, S::THREADS, S::bytes, ctx->stream>>>(a, a_d ? *a_d : a);
     LDGA_LAUNCHED(ctx, "k_bse_jacobi");
     return LDGA_OK;
 }
 
-template <int N>
-int run_jacobi(ldga_ctx* ctx, const BseArgs& a) { return run_jacobi_impl<N>(ctx, a, nullptr); }
+template <int N, int Q, int NBUF, bool K3>
+int run_jacobi(ldga_ctx* ctx, const BseArgs& a) { return run_jacobi_impl<N, Q, NBUF, K3>(ctx, a, nullptr); }
 
-template <int N>
-int run_jacobi_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) { return run_jacobi_impl<N>(ctx, a_m, &a_d); }
+template <int N, int Q, int NBUF, bool K3>
+int run_jacobi_pair(ldga_ctx* ctx, const BseArgs& a_m, const BseArgs& a_d) {
+    return run_jacobi_impl<N, Q, NBUF, K3>(ctx, a_m, &a_d);
+}

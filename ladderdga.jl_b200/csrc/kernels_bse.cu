@@ -2843,7 +2843,9 @@ const BseVariant fp64_120[] = {{&run_lu<120, 16, 1, 1, false>, "lu16g:1"}};
 // MIXED at Nν = 120: the Jacobi refinement (bse_jacobi.cuh), whose stop test bounds the forward error
 // too (the test matrices' condition numbers reach 1e4, where a backward error of 1e-14 alone would
 // not guarantee the 1e-10 forward accuracy), then the LU forms
-const BseVariant mixed_120[] = {{&run_jacobi<120>, "jac", &run_jacobi_pair<120>},
+const BseVariant mixed_120[] = {{&run_jacobi<120, 32, 4, true>, "jac", &run_jacobi_pair<120, 32, 4, true>},
+                                {&run_jacobi<120, 32, 4, false>, "jac4", &run_jacobi_pair<120, 32, 4, false>},
+                                {&run_jacobi<120, 16, 2, true>, "jac16:2", &run_jacobi_pair<120, 16, 2, true>},
                                 {&run_lu<120, 16, 1, 1, false>, "lu16g:1"}, {&run_lu32<120, 16, 1, 1, false>, "lu32x16g:1"}};
 
 int variants_of(int nnu, int prec, const BseVariant** out) {
