@@ -206,7 +206,7 @@ int alloc_all(ldga_ctx* c) {
 void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
-                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_list2, c->d_count,
+                    c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_list2, c->d_gamma_t, c->d_count,
                     c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);

@@ -110,6 +110,9 @@ struct BseArgs {
     int32_t* fail_list = nullptr;
     int32_t* fail_count = nullptr;
     int max_sweeps = 40;    // k_bse_iter: residual sweeps before a q is flagged
+    // k_bse_iter<..., ADJ = true>: right-hand sides [Nq, NL, Nw] instead of ones; the conjugate of the
+    // solution goes to gam (which may be rhs itself), chi is not written
+    const double2* rhs = nullptr;
 };
 
 __device__ __forceinline__ double2 dmk(double r, double i) { return make_double2(r, i); }
@@ -1654,7 +1657,7 @@ __device__ __forceinline__ float2 f2_fma(float2 c, float2 r, float2 acc) {
 // NL: the box size Nν of the data; the tiles use N >= NL (a multiple of 8 for the tensor paths).
 // Rows and columns NL .. N-1 are an identity block with a zero right-hand side: Gamma^T is padded
 // with zeros, 1/chi0 with ones, so x and r stay zero there and the first NL rows solve B y = 1.
-template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2, bool NS, int NL>
+template <int N, int LPQ, int QPL, int MINB, bool GSM, bool TC, bool DM, bool P2, bool NS, int NL, bool ADJ = false>
 __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const BseArgs a_m, const BseArgs a_d,
                                                                        const int32_t* __restrict__ perm) {
     // blockIdx.z selects the channel: one launch may cover both (they share chi0 and the q order),
@@ -1669,6 +1672,7 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     static_assert(!NS || (DM && N % 8 == 0 && kIterQ * LPQ / QPL == 128),
                   "the tensor-core group inverse is built for the DM configuration, 128 threads");
     static_assert(NL <= N && NL % 2 == 0, "padded box");
+    static_assert(!ADJ || TC, "general right-hand sides enter through the tensor-core product");
     constexpr int LD = S::LD;
     constexpr int LDG = GSM ? LD : N;   // row stride of Gamma^T where it is read
     constexpr int RPL = (N + LPQ - 1) / LPQ;
@@ -2019,11 +2023,15 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
     }
     __syncthreads();
 
-    // ---- per q: norm of B_q's rows, x = C 1
+    // ---- per q: norm of B_q's rows, x = C 1 (ADJ: x = C b, b and max |b| in registers)
     double rown[QPL];
     double2 x[QPL][RPL];
+    double2 bq[ADJ ? QPL : 1][ADJ ? RPL : 1];
+    double bn[ADJ ? QPL : 1];
 #pragma unroll
     for (int c = 0; c < QPL; ++c) rown[c] = 0.0;
+#pragma unroll
+    for (int c = 0; c < (ADJ ? QPL : 1); ++c) bn[c] = 0.0;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
         const int i = h * RPL + r;
@@ -2050,6 +2058,12 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 const double2 d = Dq[(ql0 + c) * N + i];
                 rown[c] = fmax(rown[c], rowg + fabs(g.x + d.x) + fabs(g.y + d.y));
                 x[c][r] = dmk((double)sacc.x, (double)sacc.y);
+            }
+            if constexpr (ADJ) {
+                double2& b = bq[ADJ ? c : 0][ADJ ? r : 0];
+                b = dmk(0.0, 0.0);
+                if (i < NL && ql0 + c < nvalid) b = a.rhs[(size_t)pw[ql0 + c] + (size_t)a.nq * (i + (size_t)NL * w)];
+                bn[ADJ ? c : 0] = fmax(bn[ADJ ? c : 0], fabs(b.x) + fabs(b.y));
             }
         }
     }
@@ -2085,7 +2099,9 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
         for (int c = 0; c < QPL; ++c)
 #pragma unroll
-            for (int r = 0; r < RPL; ++r) one[c][r] = make_float2(h * RPL + r < NL ? 1.f : 0.f, 0.f);
+            for (int r = 0; r < RPL; ++r)
+                one[c][r] = ADJ ? make_float2((float)bq[ADJ ? c : 0][ADJ ? r : 0].x, (float)bq[ADJ ? c : 0][ADJ ? r : 0].y)
+                                : make_float2(h * RPL + r < NL ? 1.f : 0.f, 0.f);
         tc_apply<N, RPL, QPL, LPQ>(one, d0, Ffr, Ffi, xbw, lane, h);
         if constexpr (P2) second_order(d0, one);
 #pragma unroll
@@ -2099,7 +2115,10 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
 #pragma unroll
     for (int c = 0; c < QPL; ++c) {
 #pragma unroll
-        for (int o = 1; o < LPQ; o <<= 1) rown[c] = fmax(rown[c], __shfl_xor_sync(0xffffffffu, rown[c], o));
+        for (int o = 1; o < LPQ; o <<= 1) {
+            rown[c] = fmax(rown[c], __shfl_xor_sync(0xffffffffu, rown[c], o));
+            if constexpr (ADJ) bn[ADJ ? c : 0] = fmax(bn[ADJ ? c : 0], __shfl_xor_sync(0xffffffffu, bn[ADJ ? c : 0], o));
+        }
         conv[c] = ql0 + c >= nvalid;
         berr[c] = 0.0;
     }
@@ -2152,7 +2171,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 rr[c][r] = make_float2(0.f, 0.f);
                 if (N % LPQ == 0 || i < N) {
                     const double2 t = cadd(acc[c][r], cmul(Dq[(ql0 + c) * N + i], x[c][r]));
-                    const double rx = (i < NL ? 1.0 : 0.0) - t.x, ry = -t.y;
+                    const double2 bv = ADJ ? bq[ADJ ? c : 0][ADJ ? r : 0] : dmk(i < NL ? 1.0 : 0.0, 0.0);
+                    const double rx = bv.x - t.x, ry = bv.y - t.y;
                     res = fmax(res, fabs(rx) + fabs(ry));
                     xn = fmax(xn, fabs(x[c][r].x) + fabs(x[c][r].y));
                     rr[c][r] = make_float2((float)rx, (float)ry);
@@ -2163,7 +2183,8 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
                 res = fmax(res, __shfl_xor_sync(0xffffffffu, res, o));
                 xn = fmax(xn, __shfl_xor_sync(0xffffffffu, xn, o));
             }
-            if (!conv[c]) berr[c] = res / (rown[c] * xn + 1.0);
+            // normwise backward error |b - B x| / (|B| |x| + |b|), |b| = 1 for the forward solve
+            if (!conv[c]) berr[c] = res / (rown[c] * xn + (ADJ ? bn[ADJ ? c : 0] : 1.0));
             conv[c] = conv[c] || berr[c] <= kIterTol;
             all = all && conv[c];
         }
@@ -2230,6 +2251,18 @@ __global__ void __launch_bounds__(kIterQ * LPQ / QPL, MINB) k_bse_iter(const Bse
         const int q = pw[ql];
         const double chi = sx / (a.beta * a.beta);
         const bool ok = isfinite(berr[c]) && berr[c] <= kIterTol;
+        if constexpr (ADJ) {          // the adjoint's z = conj(x) and the flag; no chi, no gamma
+            if (h == 0) {
+                a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
+                if (!ok && a.fail_list) a.fail_list[atomicAdd(a.fail_count, 1)] = q + a.nq * w;
+            }
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                const int i = h * RPL + r;
+                if (i < NL) a.gam[(size_t)q + (size_t)a.nq * (i + (size_t)NL * w)] = cconj(x[c][r]);
+            }
+            continue;
+        }
         if (h == 0) {
             a.chi[(size_t)q + (size_t)a.nq * w] = chi;
             a.flags[(size_t)q + (size_t)a.nq * w] = ok ? 0 : 1;
@@ -2274,6 +2307,8 @@ struct BseAdjArgs {
     double2* ybuf;            // [Nq, N, Nw]   out: y
     double2* zbuf;            // [Nq, N, Nw]   out: z
     int32_t* flags;           // [Nq, Nw]      1: backward error above 1e-12
+    const int32_t* list = nullptr;    // k_bse_adj: only these (q + Nq w), count[0] of them
+    const int32_t* count = nullptr;
 };
 
 template <int N, int T, int MINB>
@@ -2298,17 +2333,15 @@ __global__ void __launch_bounds__(T * T, MINB) k_bse_adj(const BseAdjArgs a) {
     double2* rhs = reinterpret_cast<double2*>(red + 8 * (G / 32) + 2);   // [N] conj(y_bar)
     double2* yfw = rhs + N;                               // [N] forward y
 
-    const int w = blockIdx.y;
-    const int q0 = blockIdx.x * a.qchunk;
-    const int q1 = min(a.nq, q0 + a.qchunk);
-    {
+    auto stage = [&](int w) {
         const double2* Gw = a.Gamma + (size_t)w * N * N;
         for (int e = t; e < N * N; e += blockDim.x) Gsm[e] = Gw[e];
-    }
-    __syncthreads();
+        __syncthreads();
+    };
     const unsigned gmask = (T == 32 ? 0xffffffffu : ((1u << T) - 1u)) << (lane & ~(T - 1));
 
-    for (int q = q0; q < q1; ++q) {
+    // one (q, w) with Gamma(w) staged; every thread of the CTA calls it
+    auto solve = [&](int q, int w) {
         const size_t cq = (size_t)q + (size_t)a.nq * w;
         const double chi = a.chi[cq];
         const double f = 1.0 + a.s * a.U * chi, rf = 1.0 / f;
@@ -2467,7 +2500,21 @@ __global__ void __launch_bounds__(T * T, MINB) k_bse_adj(const BseAdjArgs a) {
             a.zbuf[ci] = z;
         }
         named_barrier(bar, G);
+    };
+    if (a.list) {
+        // the matrices a preconditioned adjoint solve left above its bound, q + Nq w each
+        const int n = min(max(a.count[0], 0), a.nq * a.nw);
+        for (int item = blockIdx.x; item < n; item += gridDim.x) {
+            const int lin = a.list[item];
+            stage(lin / a.nq);
+            solve(lin % a.nq, lin / a.nq);
+        }
+        return;
     }
+    const int q0 = blockIdx.x * a.qchunk;
+    const int q1 = min(a.nq, q0 + a.qchunk);
+    stage(blockIdx.y);
+    for (int q = q0; q < q1; ++q) solve(q, blockIdx.y);
 }
 
 // Gamma_bar(w)[a, b] = -sum_q conj(y[q, a, w]) z[q, b, w], one CTA per (w, 32 x 32 output tile);
@@ -2736,11 +2783,11 @@ int run_warp32(ldga_ctx* ctx, const BseArgs& a0) {
 using BseRun = int (*)(ldga_ctx*, const BseArgs&);
 using BseRunPair = int (*)(ldga_ctx*, const BseArgs&, const BseArgs&);
 template <int N, int LPQ, int MINB, int QPL = 1, bool GSM = true, bool TC = false, bool DM = false, bool P2 = false,
-          bool NS = false, int NL = N>
+          bool NS = false, int NL = N, bool ADJ = false>
 int run_iter_impl(ldga_ctx* ctx, const BseArgs& a, const BseArgs* a_d) {
     if (!ctx->d_qperm) return ctx_fail(ctx, LDGA_ERR_ARG, "preconditioned BSE: q order buffer missing");
     using S = IterSmem<N, GSM, TC, kIterQ * LPQ / QPL / 32, DM, NS>;
-    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2, NS, NL>;
+    auto kern = k_bse_iter<N, LPQ, QPL, MINB, GSM, TC, DM, P2, NS, NL, ADJ>;
     LDGA_CUDA(ctx, set_smem(ctx, kern, S::bytes));
     StageTimer st_(ctx, LDGA_STAGE_BSE);
     // the q order depends on chi0 only: the second channel of the same bubble reuses it
@@ -2893,6 +2940,67 @@ BseArgs bse_args(ldga_ctx* ctx, int channel) {
     return a;
 }
 
+// ---- MIXED adjoint at Nν = 40: the transposed systems (Gamma(w) + diag(1/chi0)) conj(z) = conj(y_bar)
+// by the preconditioned iteration (k_bse_iter<..., ADJ>) on a transposed copy of Gamma, with the
+// pivot-free FP64 LU adjoint (k_bse_adj, list mode) for the matrices it leaves above its bound.
+// The same formulas as k_bse_adj, split around the solve:
+//   k_adj_rhs:     y = gamma chi0 / rf -> ybuf; conj(y_bar) -> zbuf (the right-hand side)
+//   k_bse_iter:    zbuf <- z = conj(x) for the solved matrices, flags 1 for the others
+//   k_adj_chi0bar: chi0_bar from y, z for the unflagged matrices (k_bse_adj writes the others)
+
+// dst[w][i N + j] = src[w][j N + i]
+__global__ void k_transpose_gamma(int n, int nw, const double2* __restrict__ src, double2* __restrict__ dst) {
+    const size_t tot = (size_t)n * n * nw;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t w = e / ((size_t)n * n);
+        const int r = (int)(e - w * n * n), i = r / n, j = r - (r / n) * n;
+        dst[e] = src[w * n * n + (size_t)j * n + i];
+    }
+}
+
+// one thread per (q, w): two sweeps over nu (q fastest in memory, so the warp's loads coalesce)
+__global__ void k_adj_rhs(const BseAdjArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;   // q + Nq w
+    if (e >= a.nq * a.nw) return;
+    const int q = e % a.nq, w = e / a.nq, n = a.nnu;
+    const double f = 1.0 + a.s * a.U * a.chi[e], rf = 1.0 / f;
+    double s1 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)n * w);
+        const double2 c0 = a.chi0[ci];
+        const double2 y = cscale(cmul(a.gam[ci], c0), f);
+        a.ybuf[ci] = y;
+        if (a.gam_bar) {
+            const double2 gb = a.gam_bar[ci], yd = cmul(y, cinv(c0));
+            s1 += gb.x * yd.x + gb.y * yd.y;             // Re(conj(gb) y d)
+        }
+    }
+    const double xbar = (a.chi_bar ? a.chi_bar[e] : 0.0) - a.s * a.U * rf * rf * s1;
+    for (int i = 0; i < n; ++i) {
+        const size_t ci = (size_t)q + (size_t)a.nq * (i + (size_t)n * w);
+        double2 yb = make_double2(xbar / (a.beta * a.beta), 0.0);
+        if (a.gam_bar) yb = cadd(yb, cmul(cconj(cscale(cinv(a.chi0[ci]), rf)), a.gam_bar[ci]));
+        a.zbuf[ci] = cconj(yb);
+    }
+}
+
+// one thread per (q, nu, w) of an unflagged matrix
+__global__ void k_adj_chi0bar(const BseAdjArgs a) {
+    const size_t tot = (size_t)a.nq * a.nnu * a.nw;
+    for (size_t ci = blockIdx.x * (size_t)blockDim.x + threadIdx.x; ci < tot; ci += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(ci % a.nq);
+        const size_t w = ci / ((size_t)a.nq * a.nnu);
+        const size_t cq = (size_t)q + (size_t)a.nq * w;
+        if (a.flags[cq] != 0) continue;
+        const double rf = 1.0 / (1.0 + a.s * a.U * a.chi[cq]);
+        const double2 z = a.zbuf[ci], y = a.ybuf[ci], d = cinv(a.chi0[ci]);
+        double2 db = cscale(cmul(z, cconj(y)), -1.0);
+        if (a.gam_bar) db = cadd(db, cmul(cconj(cscale(y, rf)), a.gam_bar[ci]));
+        const double2 c0b = cscale(cmul(cconj(cmul(d, d)), db), -1.0);
+        a.chi0_bar[ci] = a.accumulate ? cadd(a.chi0_bar[ci], c0b) : c0b;
+    }
+}
+
 }  // namespace
 
 bool bse_has_fast_path(int nnu) {
@@ -3029,6 +3137,42 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
     a.accumulate = accumulate ? 1 : 0;
     a.flags = ctx->d_flags;
     int st = LDGA_OK;
+    if (ctx->prec == LDGA_PREC_MIXED && ctx->Nnu == 40) {
+        // MIXED: the preconditioned iteration on the transposed systems, the LU for what it leaves
+        constexpr int N = 40;
+        const size_t vvw = (size_t)N * N * ctx->Nw;
+        if (!ctx->d_gamma_t) {
+            if (ctx->capturing) return ctx_fail(ctx, LDGA_ERR_STATE, "BSE adjoint: scratch not allocated before capture");
+            LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_gamma_t), vvw * sizeof(double2)));
+        }
+        k_transpose_gamma<<<2 * 148, 256, 0, ctx->stream>>>(N, ctx->Nw, ctx->d_Gamma[channel], ctx->d_gamma_t);
+        LDGA_LAUNCHED(ctx, "k_transpose_gamma");
+        const int nqw = ctx->Nq * ctx->Nw;
+        k_adj_rhs<<<(nqw + 255) / 256, 256, 0, ctx->stream>>>(a);
+        LDGA_LAUNCHED(ctx, "k_adj_rhs");
+        BseArgs b = bse_args(ctx, channel);
+        b.Gamma = ctx->d_gamma_t;
+        b.rhs = zbuf;
+        b.gam = zbuf;
+        b.chi = nullptr;
+        b.stats = nullptr;
+        b.fail_list = ctx->d_list;
+        b.fail_count = ctx->d_count + 2;
+        LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count + 2, 0, sizeof(int32_t), ctx->stream));
+        st = run_iter_impl<N, 8, 2, 2, true, true, true, true, true, N, true>(ctx, b, nullptr);
+        if (st != LDGA_OK) return st;
+        // chi0_bar of the solved matrices first: the LU below clears the flags of those it solves
+        k_adj_chi0bar<<<4 * 148, 256, 0, ctx->stream>>>(a);
+        LDGA_LAUNCHED(ctx, "k_adj_chi0bar");
+        BseAdjArgs al = a;
+        al.list = ctx->d_list;
+        al.count = ctx->d_count + 2;
+        const size_t sm = (size_t)N * N * sizeof(double2) + LuSmem<N, 8>::bytes + 2 * N * sizeof(double2) + 16;
+        auto kern = k_bse_adj<N, 8, 6>;
+        LDGA_CUDA(ctx, set_smem(ctx, kern, sm));
+        kern<<<LDGA_PIVOT_GRID, 64, sm, ctx->stream>>>(al);
+        LDGA_LAUNCHED(ctx, "k_bse_adj");
+    } else {
     switch (ctx->Nnu) {
         case 4: st = run_bse_adj<4, 8, 4>(ctx, a); break;
         case 6: st = run_bse_adj<6, 8, 4>(ctx, a); break;
@@ -3042,6 +3186,7 @@ int launch_bse_adj(ldga_ctx* ctx, int channel, const double* chi_bar, const doub
         case 60: st = run_bse_adj<60, 16, 2>(ctx, a); break;
         default: return ctx_fail(ctx, LDGA_ERR_ARG, "BSE adjoint: fermionic box " + std::to_string(ctx->Nnu) +
                                                         " not built (4..60 even sizes of the tiled kernels)");
+    }
     }
     if (st != LDGA_OK) return st;
     const int n = ctx->Nnu;

@@ -106,6 +106,7 @@ struct ldga_ctx {
     int32_t* d_flags2 = nullptr;   // the d channel's flags when both channels run in one launch
     int32_t* d_list = nullptr;     // compacted fallback list (the m channel's list of a pair launch)
     int32_t* d_list2 = nullptr;    // the d channel's list of a pair launch
+    double2* d_gamma_t = nullptr;  // MIXED BSE adjoint: Gamma(w) transposed [Nnu, Nnu, Nw]
     int32_t* d_count = nullptr;
     double2* d_pivot_scratch = nullptr;   // pivoted fallback matrices in HBM when N (N+1) does not fit shared memory
     int2* d_bub_pairs = nullptr;          // bubble pairs computed directly (pair, conjugate partner or -1)

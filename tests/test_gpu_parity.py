@@ -627,6 +627,27 @@ def test_bse_vjp(case, prec):
     """Adjoint of calc_χγ: against the oracle's FP64 matrix-calculus gradient and against central
     finite differences of the GPU forward along random directions of Γ_r and χ₀."""
     name, inp, ref = case
+    _check_bse_vjp(name, inp, ref, prec)
+
+
+@pytest.mark.parametrize("sweeps", [None, 0])
+def test_bse_vjp_mixed_iteration(sweeps, require_gpu):
+    """MIXED adjoint at Nν = 40: the transposed systems by the preconditioned iteration on a
+    transposed copy of Γ, with general right-hand sides.  Same checks as test_bse_vjp.  With the
+    sweep limit at 0 (LDGA_ITER_SWEEPS=0) every matrix goes to the LU adjoint in list mode, and the
+    forward solve to its pivoted fallback."""
+    import os
+    inp = S.make_input(dim=2, ns=8, beta=12.0, U=1.2, n_iv=20, n_iw=3, seed=340)
+    ref = R.run_chain(inp, lambda_type=None)
+    if sweeps is not None:
+        os.environ["LDGA_ITER_SWEEPS"] = str(sweeps)
+    try:
+        _check_bse_vjp("2d8_n40", inp, ref, L.PREC_MIXED)
+    finally:
+        os.environ.pop("LDGA_ITER_SWEEPS", None)
+
+
+def _check_bse_vjp(name, inp, ref, prec):
     rng = np.random.default_rng(11)
     g = gpu_chain(inp, prec)
     h = g["h"]
