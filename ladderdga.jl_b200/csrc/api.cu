@@ -401,7 +401,7 @@ int ldga_destroy(ldga_ctx* ctx) {
     for (auto& p : ctx->ev_pool) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     if (ctx->io_stream) {
         cudaStreamDestroy(ctx->io_stream);
-        for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_gamma, ctx->ev_loc, ctx->ev_chi, ctx->ev_join})
+        for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_gamma, ctx->ev_loc, ctx->ev_chi, ctx->ev_join, ctx->ev_bub, ctx->ev_l0})
             if (e) cudaEventDestroy(e);
     }
     cudaStreamDestroy(ctx->own_stream);
@@ -1159,6 +1159,19 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     TRY(copy(ctx, ctx->d_sigma_loc, a.sigma_loc, (size_t)a.n_sigma * sizeof(double2)));
     TRY(launch_gloc_transform(ctx, true));                       // a1
     TRY(launch_bubble(ctx));                                     // a2
+    // a5, a6 need χ₀ and the local inputs only: they run on the copy stream beside the BSE and the
+    // λm Newton (8 SMs), and the EoM waits for them.  Their scratch (d_red from 64 on) is theirs.
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_bub, ctx->stream));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(io, ctx->ev_bub, 0));
+    {
+        cudaStream_t main = ctx->stream;
+        ctx->stream = io;
+        const int st = launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp);   // a5
+        const int st2 = st == LDGA_OK ? launch_lambda0(ctx) : st;                      // a6
+        ctx->stream = main;
+        TRY(st2);
+    }
+    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_l0, io));
     LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 4 * sizeof(int32_t), ctx->stream));   // fails, lists
     LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_gamma, 0));
     TRY(launch_bse_pair(ctx, ctx->d_count + 1));                  // a7, both channels
@@ -1167,13 +1180,11 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     if (a.chi_m_out) TRY(cp(a.chi_m_out, ctx->d_chi[0], nX));
     if (a.chi_d_out) TRY(cp(a.chi_d_out, ctx->d_chi[1], nX));
     LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_join, io));
-    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_loc, 0));
-    TRY(launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp));   // a5
-    TRY(launch_lambda0(ctx));                                    // a6
     // λm_correction_full (conditions_new.jl:174-190): rhs = 2 imp_density - sum_kω(chi_d), the Newton, and
     // sum_kω(chi_m, λ = λm) for the EoM's tail, all in the Newton kernel (d_red[56], d_red[16], d_red[8])
     TRY(launch_lambda_m(ctx, 2.0 * a.imp_density, nullptr, ctx->d_red + 16, 100, 1e-13, ctx->d_red + 56,
                         ctx->d_red + 8));
+    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_l0, 0));
     TRY(launch_eom(ctx, numax, 0.0, 0.0, ctx->d_red + 16, nullptr, -1, ctx->d_red + 8, 1, a.chiloc_m_sum,
                    ctx->d_sigma, ctx->Nq, 1));                   // a10 at λm
     TRY(launch_g_ladder(ctx, numax, 1, ctx->mp.mu, ctx->d_red + 24));   // a15: μ fit, energies
@@ -1221,7 +1232,8 @@ int chain_m_submit(ldga_ctx* ctx, const ChainArgs& a, bool use_graph, bool* repl
     if (!ctx->h_stage) LDGA_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&ctx->h_stage), 64 * sizeof(double) + 16));
     if (!ctx->io_stream) {
         LDGA_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
-        for (cudaEvent_t* e : {&ctx->ev_fork, &ctx->ev_gamma, &ctx->ev_loc, &ctx->ev_chi, &ctx->ev_join})
+        for (cudaEvent_t* e : {&ctx->ev_fork, &ctx->ev_gamma, &ctx->ev_loc, &ctx->ev_chi, &ctx->ev_join, &ctx->ev_bub,
+                               &ctx->ev_l0})
             LDGA_CUDA(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     const void* ptrs[] = {a.sigma_loc, a.gamma_m, a.gamma_d, a.chi_loc_m, a.gimp, a.sigma_out, a.chi_m_out, a.chi_d_out};

@@ -132,6 +132,7 @@ struct ldga_ctx {
     // while G and the bubble run, chi_m/chi_d come out there while the λ and EoM stages run
     cudaStream_t io_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_gamma = nullptr, ev_loc = nullptr, ev_chi = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_bub = nullptr, ev_l0 = nullptr;   // χ₀ ready for λ₀ on io_stream; λ₀ ready for the EoM
     bool capturing = false;              // a CUDA graph of the chain is being captured
 
     // fused chain (ldga_chain_m): persistent input buffers and the captured graph
