@@ -374,6 +374,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     if (const char* sw = std::getenv("LDGA_ITER_SWEEPS")) c->iter_sweeps = std::min(std::max(std::atoi(sw), 0), 1000);
     DeviceGuard g(device);
     c->device = device;
+    c->newton_cluster = newton_cluster_size(c->newton_async);
     c->lat = *lat; c->mp = *mp; c->sp = *sp; c->prec = precision;
     c->dim = lat->dim; c->ns = lat->ns;
     c->Nnu = 2 * sp->n_iv; c->Nw = 2 * sp->n_iw + 1;

@@ -86,15 +86,15 @@ constexpr int kClWarps = kClThreads / 32;
 // fewer warps mean fewer partials to exchange and add (measured 0.162 vs 0.172 ms for 100
 // iterations on 39 729 points, 8 x 256 vs 8 x 512 threads).
 constexpr int kNewtonThreads = 256;
-template <int NV, int NW = kClWarps>
+template <int NV, int NW = kClWarps, int CL = kCluster>
 struct ClAll {
     // [slot][source warp][value]: a source's NV values are adjacent, so NV = 2 moves as one
     // 16-byte remote store and one 16-byte shared load
-    alignas(16) double part[2][kCluster * NW][NV];
+    alignas(16) double part[2][CL * NW][NV];
 };
 
-template <int NV, int NW>
-__device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW>& s, int& parity) {
+template <int NV, int NW, int CL>
+__device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW, CL>& s, int& parity) {
     cg::cluster_group cl = cg::this_cluster();
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const int src = (int)cl.block_rank() * NW + w;
@@ -104,8 +104,8 @@ __device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW>& s
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
         v[j] = x;
     }
-    if (l < kCluster) {
-        ClAll<NV, NW>* dst = cl.map_shared_rank(&s, l);
+    if (l < CL) {
+        ClAll<NV, NW, CL>* dst = cl.map_shared_rank(&s, l);
         if constexpr (NV == 2) {
             *reinterpret_cast<double2*>(dst->part[parity][src]) = make_double2(v[0], v[1]);
         } else {
@@ -114,7 +114,7 @@ __device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW>& s
         }
     }
     cl.sync();
-    constexpr int P = kCluster * NW;
+    constexpr int P = CL * NW;
     double x[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) x[j] = 0.0;
@@ -149,16 +149,16 @@ __device__ __forceinline__ void cluster_allsum(double (&v)[NV], ClAll<NV, NW>& s
 // stops its loop and reports NaN.
 constexpr long long kAsyncSpins = 1ll << 22;
 
-template <int NV, int NW>
+template <int NV, int NW, int CL = kCluster>
 struct ClAsync {
-    alignas(16) double part[2][kCluster * NW][NV];
+    alignas(16) double part[2][CL * NW][NV];
     alignas(8) unsigned long long bar[2];
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-template <int NV, int NW>
-__device__ __forceinline__ void async_allsum_init(ClAsync<NV, NW>& s) {
+template <int NV, int NW, int CL>
+__device__ __forceinline__ void async_allsum_init(ClAsync<NV, NW, CL>& s) {
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s.bar[0])), "r"(1) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s.bar[1])), "r"(1) : "memory");
@@ -167,8 +167,8 @@ __device__ __forceinline__ void async_allsum_init(ClAsync<NV, NW>& s) {
     cg::this_cluster().sync();   // every CTA's barriers exist before any remote write
 }
 
-template <int NV, int NW>
-__device__ __forceinline__ bool async_allsum(double (&v)[NV], ClAsync<NV, NW>& s, int iter) {
+template <int NV, int NW, int CL>
+__device__ __forceinline__ bool async_allsum(double (&v)[NV], ClAsync<NV, NW, CL>& s, int iter) {
     static_assert(NV == 2, "the exchange moves one 16-byte value pair per source");
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const int slot = iter & 1;
@@ -182,10 +182,10 @@ __device__ __forceinline__ bool async_allsum(double (&v)[NV], ClAsync<NV, NW>& s
     }
     const uint32_t bar = smem_addr(&s.bar[slot]);
     if (threadIdx.x == 0) {
-        constexpr uint32_t bytes = kCluster * NW * NV * sizeof(double);
+        constexpr uint32_t bytes = CL * NW * NV * sizeof(double);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
     }
-    if (l < kCluster) {
+    if (l < CL) {
         uint32_t raddr, rbar;
         asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(raddr) : "r"(smem_addr(&s.part[slot][src][0])), "r"(l));
         asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rbar) : "r"(bar), "r"(l));
@@ -197,7 +197,7 @@ __device__ __forceinline__ bool async_allsum(double (&v)[NV], ClAsync<NV, NW>& s
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(done) : "r"(bar), "r"(phase) : "memory");
     const bool ok = __all_sync(0xffffffffu, done != 0);
-    constexpr int P = kCluster * NW;
+    constexpr int P = CL * NW;
     double x[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) x[j] = 0.0;
@@ -363,13 +363,17 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 // the trajectory has period p = i - checkpoint and whole periods up to nsteps are skipped; the last
 // < p iterations then run as usual.  xi and i come out bit for bit as from the full loop.
 // out[3], out[4]: the iteration at which the repeat was recognised and p (0, 0: nothing skipped).
-template <int K, bool ASYNC>
-__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kNewtonThreads)
+//
+// CL: CTAs of the cluster, given at launch (cudaLaunchAttributeClusterDimension).  16 (a non-portable
+// size, where the GPU can place it) halves each thread's share of the sums against 8; the exchange
+// costs the same number of steps either way, one st.async per lane and a wider final fold.
+template <int K, bool ASYNC, int CL>
+__global__ void __launch_bounds__(kNewtonThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
            const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out,
            const double* __restrict__ chi_d, double* sum_d_out, double* sum_m_out) {
-    __shared__ ClAll<2, kNewtonThreads / 32> ca;
-    __shared__ ClAsync<2, kNewtonThreads / 32> cs;
+    __shared__ ClAll<2, kNewtonThreads / 32, CL> ca;
+    __shared__ ClAsync<2, kNewtonThreads / 32, CL> cs;
     int parity = 0, iter = 0;
     bool exchange_ok = true;
     if constexpr (ASYNC) async_allsum_init(cs);
@@ -381,7 +385,7 @@ k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__
     const double xmin = xmin_dev[0];
     const double delta = 1e-4;
     const int total = a.nq * a.nw;
-    const int tid = cl_tid(), nth = cl_nth();
+    const int tid = cl_tid(), nth = CL * (int)blockDim.x;
     // finish_kw(s) = (s inv_nk - tail + c) / beta with the tail and constant hoisted out of the loop
     const double tail = w2_tail(a);
     const double cst = (-a.beta * a.beta / 12.0) * a.c2;
@@ -843,6 +847,18 @@ int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2) {
     return LDGA_OK;
 }
 
+using NewtonKern = void (*)(SumArgs, const double*, const double*, double, const double*, const double*, int, double,
+                           double*, const double*, double*, double*);
+
+// Register-resident elements per thread K for `per` (q, ω) terms per thread; K = 0 streams them.
+template <bool AS, int CL>
+NewtonKern pick_newton(int per) {
+    return per <= 2 ? k_lambda_m<2, AS, CL> : per <= 4 ? k_lambda_m<4, AS, CL> : per <= 6 ? k_lambda_m<6, AS, CL>
+         : per <= 8 ? k_lambda_m<8, AS, CL> : per <= 10 ? k_lambda_m<10, AS, CL> : per <= 12 ? k_lambda_m<12, AS, CL>
+         : per <= 16 ? k_lambda_m<16, AS, CL> : per <= 20 ? k_lambda_m<20, AS, CL> : per <= 24 ? k_lambda_m<24, AS, CL>
+         : k_lambda_m<0, AS, CL>;
+}
+
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
     const int w0 = (ctx->Nw + 1) / 2 - 1;   // ω0_index = ceil(Nw/2), 1-based
     StageTimer st_(ctx, LDGA_STAGE_SUMS);
@@ -859,22 +875,65 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
     if (st) return st;
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
     const SumArgs sa = sum_args(ctx);
-    const int per = (sa.nq * sa.nw + kCluster * kNewtonThreads - 1) / (kCluster * kNewtonThreads);
-    const bool as = ctx->newton_async;
-    auto kern = per <= 2 ? (as ? k_lambda_m<2, true> : k_lambda_m<2, false>)
-              : per <= 4 ? (as ? k_lambda_m<4, true> : k_lambda_m<4, false>)
-              : per <= 6 ? (as ? k_lambda_m<6, true> : k_lambda_m<6, false>)
-              : per <= 8 ? (as ? k_lambda_m<8, true> : k_lambda_m<8, false>)
-              : per <= 12 ? (as ? k_lambda_m<12, true> : k_lambda_m<12, false>)
-              : per <= 16 ? (as ? k_lambda_m<16, true> : k_lambda_m<16, false>)
-              : per <= 20 ? (as ? k_lambda_m<20, true> : k_lambda_m<20, false>)
-              : per <= 24 ? (as ? k_lambda_m<24, true> : k_lambda_m<24, false>)
-              : (as ? k_lambda_m<0, true> : k_lambda_m<0, false>);
-    kern<<<kCluster, kNewtonThreads, 0, ctx->stream>>>(sa, ctx->d_chi[LDGA_CH_M], ctx->d_kmult, rhs_const, rhs_sub_dev,
-                                                   d_out + 2, nsteps, atol, d_out,
-                                                   sum_d_out ? ctx->d_chi[LDGA_CH_D] : nullptr, sum_d_out, sum_m_out);
+    const int cl = ctx->newton_cluster;
+    const int per = (sa.nq * sa.nw + cl * kNewtonThreads - 1) / (cl * kNewtonThreads);
+    const NewtonKern kern = cl == 16 ? pick_newton<true, 16>(per)
+                          : ctx->newton_async ? pick_newton<true, kCluster>(per) : pick_newton<false, kCluster>(per);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)cl);
+    cfg.blockDim = dim3(kNewtonThreads);
+    cfg.stream = ctx->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, sa, (const double*)ctx->d_chi[LDGA_CH_M],
+                                             (const double*)ctx->d_kmult, rhs_const, rhs_sub_dev,
+                                             (const double*)(d_out + 2), nsteps, atol, d_out,
+                                             (const double*)(sum_d_out ? ctx->d_chi[LDGA_CH_D] : nullptr),
+                                             sum_d_out, sum_m_out);
+    if (e != cudaSuccess) return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("k_lambda_m launch: ") + cudaGetErrorString(e));
     LDGA_LAUNCHED(ctx, "k_lambda_m");
     return LDGA_OK;
+}
+
+// Cluster size of the λm Newton on the current device: 16 CTAs where the GPU can co-schedule a
+// non-portable 16-CTA cluster of this kernel, else the portable 8.  The barrier form
+// (async = false) keeps 8.  Called by ldga_create with the handle's device current; the
+// environment variable LDGA_NEWTON_CLUSTER=8 keeps 8 for comparison.
+int newton_cluster_size(bool async) {
+    if (!async) return kCluster;
+    if (const char* s = std::getenv("LDGA_NEWTON_CLUSTER"))
+        if (std::atoi(s) == kCluster) return kCluster;
+    const NewtonKern all16[] = {k_lambda_m<2, true, 16>, k_lambda_m<4, true, 16>, k_lambda_m<6, true, 16>,
+                                k_lambda_m<8, true, 16>, k_lambda_m<10, true, 16>, k_lambda_m<12, true, 16>,
+                                k_lambda_m<16, true, 16>, k_lambda_m<20, true, 16>, k_lambda_m<24, true, 16>,
+                                k_lambda_m<0, true, 16>};
+    for (NewtonKern k : all16)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            return kCluster;
+        }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 16;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kNewtonThreads);
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    for (NewtonKern k : all16)
+        if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return kCluster;
+        }
+    return 16;
 }
 
 int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out) {

@@ -152,6 +152,9 @@ struct ldga_ctx {
     // the λm Newton's cluster all-reduce by st.async + mbarrier instead of a cluster barrier per
     // iteration (environment LDGA_NEWTON=barrier at ldga_create selects the barrier form)
     bool newton_async = true;
+    // CTAs of the λm Newton's cluster: 16 where the device can place a non-portable 16-CTA cluster
+    // (chosen by newton_cluster_size at ldga_create; LDGA_NEWTON_CLUSTER=8 keeps 8), else 8
+    int newton_cluster = 8;
     // residual sweeps of MIXED's preconditioned BSE iteration before a matrix is handed to the pivoted
     // FP64 solve (environment LDGA_ITER_SWEEPS at ldga_create, 0..1000; 0 hands every matrix over)
     int iter_sweeps = 40;
@@ -265,6 +268,7 @@ int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const doubl
                double2* out, int out_ld, int add_hartree);
 int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev = nullptr);
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
+int newton_cluster_size(bool async);
 int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2);
 // newton_right's defaults (LambdaCorrection/helpers.jl:133): nsteps 100, atol 1e-13.  sum_d_out given:
 // rhs = rhs_const - sum_kω(chi_d) is formed in the kernel and the sum stored there (rhs_sub_dev unused);

@@ -222,6 +222,25 @@ def test_lambda_m_newton_periodic_skip(case, nsteps, atol):
         _lambda_m_newton(xm, rhs, 0, atol)
 
 
+@pytest.mark.parametrize("cluster", [None, "8"])
+def test_lambda_m_newton_cluster_sizes(case, cluster, monkeypatch):
+    """The λm Newton runs on a 16-CTA cluster where the device can place one (the default) and on
+    the portable 8-CTA cluster with LDGA_NEWTON_CLUSTER=8, read when a handle is created.  The two
+    partition the sums differently; both must give the oracle's λm, and the 8-CTA handle must be
+    bitwise reproducible."""
+    if cluster is not None:
+        monkeypatch.setenv("LDGA_NEWTON_CLUSTER", cluster)
+    name, inp, ref = case
+    g = gpu_chain(inp)
+    rhs = 2 * g["h"].imp_density - L.sum_kω(g["h"].kG, g["chi_d"])
+    lam, its, _ = _lambda_m_newton(g["chi_m"], rhs, 100, 1e-13)
+    lam2, its2, _ = _lambda_m_newton(g["chi_m"], rhs, 100, 1e-13)
+    assert (lam, its) == (lam2, its2)
+    rr = R.lambda_m_correction_full(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"],
+                                    ref["h"])
+    assert abs(lam - rr.lam_m) < ATOL_LAMBDA
+
+
 def test_lambda_m_newton_trajectory_3d32(require_gpu):
     """The benchmark point (3D sc 32³, β = 20, U = 1.5, Nν = 40, Nω = 41, seed 3000).  Its synthetic
     χ_m(q, ω) is negative for every q at large |ω|, so f(λ) = sum_kω χ_λ − rhs has poles above
