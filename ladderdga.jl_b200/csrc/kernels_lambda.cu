@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 
 // newton_right, 1-D (LambdaCorrection/helpers.jl:133-153), iteration for iteration; f and df are the
 // reference's f_c1/df_c1 (conditions_new.jl:152-153): both carry the tail terms of sum_kω.
-// rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0); xmin = xmin_dev[0] (get_λ_min, computed on the stream).
+// rhs = rhs_const - (rhs_sub ? rhs_sub[0] : 0); xmin = get_λ_min(chi), formed at the start (below).
 // K > 0: every thread keeps its K elements of chi and their kMult weights in registers for the whole
 // loop (elements e = tid + j * threads, the order the K = 0 streaming form sums in); the constant
 // tail of sum_kω is formed once.  An iteration is then one or two divisions (the batch inversion
@@ -367,22 +367,40 @@ __global__ void __launch_bounds__(1024) k_lambda_min(int nq, int w0, const doubl
 // CL: CTAs of the cluster, given at launch (cudaLaunchAttributeClusterDimension).  16 (a non-portable
 // size, where the GPU can place it) halves each thread's share of the sums against 8; the exchange
 // costs the same number of steps either way, one st.async per lane and a wider final fold.
+//
+// xmin = get_λ_min(chi) = -min_q 1/chi(q, ω0) (LambdaCorrection/helpers.jl:217-220) is formed by every
+// CTA from the nq values of column w0 (a CTA-local min: fmin is exact, so every CTA gets the same
+// value bit for bit, the value k_lambda_min gives), and CTA 0 stores it to xmin_out.
 template <int K, bool ASYNC, int CL>
 __global__ void __launch_bounds__(kNewtonThreads)
 k_lambda_m(SumArgs a, const double* __restrict__ chi, const double* __restrict__ kmult, double rhs_const,
-           const double* rhs_sub, const double* xmin_dev, int nsteps, double atol, double* out,
+           const double* rhs_sub, int w0, double* xmin_out, int nsteps, double atol, double* out,
            const double* __restrict__ chi_d, double* sum_d_out, double* sum_m_out) {
     __shared__ ClAll<2, kNewtonThreads / 32, CL> ca;
     __shared__ ClAsync<2, kNewtonThreads / 32, CL> cs;
+    __shared__ double s_min[kNewtonThreads / 32];
     int parity = 0, iter = 0;
     bool exchange_ok = true;
-    if constexpr (ASYNC) async_allsum_init(cs);
+    {
+        double mn = INFINITY;
+        for (int q = threadIdx.x; q < a.nq; q += blockDim.x) mn = fmin(mn, 1.0 / chi[(size_t)w0 * a.nq + q]);
+        for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = mn;
+    }
+    if constexpr (ASYNC) async_allsum_init(cs);   // its cluster barrier also orders s_min
+    else __syncthreads();
+    double xmin;
+    {
+        double mn = INFINITY;
+        for (int i = 0; i < kNewtonThreads / 32; ++i) mn = fmin(mn, s_min[i]);
+        xmin = -mn;
+    }
+    if (cg::this_cluster().block_rank() == 0 && threadIdx.x == 0) xmin_out[0] = xmin;
     auto allsum = [&](double (&v)[2]) -> bool {
         if constexpr (ASYNC) return async_allsum(v, cs, iter++);
         cluster_allsum<2>(v, ca, parity);
         return true;
     };
-    const double xmin = xmin_dev[0];
     const double delta = 1e-4;
     const int total = a.nq * a.nw;
     const int tid = cl_tid(), nth = CL * (int)blockDim.x;
@@ -529,14 +547,28 @@ __device__ __forceinline__ double2 g_at(double mu, double eps, double2 sig, int 
 
 // K > 0: the Newton loop keeps every thread's K (q, nu) elements (kMult, eps_q, Sigma, nu_n) in
 // registers; K = 0 streams them from memory each iteration.
-template <int K>
-__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+//
+// CL CTAs of NT threads, the cluster size given at launch.  CL = 16 (NT = 256, where the device can
+// place the non-portable size; the λm Newton's choice) exchanges the sums by st.async into every
+// CTA's shared memory with mbarrier completion (async_allsum) and halves each thread's elements;
+// CL = 8 (NT = 512) keeps one cluster barrier per exchange.
+template <int K, int CL, int NT>
+__global__ void __launch_bounds__(NT)
 k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restrict__ eps,
                 const double2* __restrict__ sigma, int fix_n, double mu_in, double* out) {
-    __shared__ ClAll<2> ca2;
+    constexpr bool ASYNC = CL != kCluster;
+    __shared__ ClAll<2, NT / 32, CL> ca2;
+    __shared__ ClAsync<2, NT / 32, CL> xs;
     __shared__ ClRed<3> cr3;
-    int parity = 0;
+    int parity = 0, iter = 0;
+    bool exchange_ok = true;
+    if constexpr (ASYNC) async_allsum_init(xs);
+    auto allsum = [&](double (&v)[2]) {
+        if constexpr (ASYNC) { if (!async_allsum(v, xs, iter++)) exchange_ok = false; }
+        else cluster_allsum<2>(v, ca2, parity);
+    };
     const int total = a.nq * a.numax;
+    const int cl_n = CL * (int)blockDim.x;
     double mu = mu_in;
     bool failed = false;
     double ck[K > 0 ? K : 1], ce[K > 0 ? K : 1], cw[K > 0 ? K : 1];
@@ -544,7 +576,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
     if (fix_n) {
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            const int e = cl_tid() + j * cl_nth();
+            const int e = cl_tid() + j * cl_n;
             const bool in = e < total;
             const int q = in ? e % a.nq : 0, nn = in ? e / a.nq : 0;
             ck[j] = in ? kmult[q] : 0.0;       // padding elements carry weight 0
@@ -568,14 +600,15 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
                     v[1] = fma(ck[j], -(G.x * G.x - G.y * G.y), v[1]);
                 }
             } else {
-                for (int e = cl_tid(); e < total; e += cl_nth()) {
+                for (int e = cl_tid(); e < total; e += cl_n) {
                     const int q = e % a.nq, nn = e / a.nq;
                     const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
                     v[0] = fma(kmult[q], G.x, v[0]);
                     v[1] = fma(kmult[q], -(G.x * G.x - G.y * G.y), v[1]);
                 }
             }
-            cluster_allsum<2>(v, ca2, parity);
+            allsum(v);
+            if (!exchange_ok) { failed = true; break; }
             const double sG = v[0] * a.inv_nk, dG = v[1] * a.inv_nk;
             const double f = 2.0 * (2.0 * sG / a.beta + 0.5 + mu * a.shell) / (1.0 + a.U * a.shell) - a.n;
             const double df = 2.0 * (2.0 * dG / a.beta + a.shell) / (1.0 + a.U * a.shell);
@@ -596,7 +629,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
     // energies at mu (calc_E with the fitted mu) and the filling
     const double hartree = a.n * a.U / 2.0;
     double v[3] = {0.0, 0.0, 0.0};
-    for (int e = cl_tid(); e < total; e += cl_nth()) {
+    for (int e = cl_tid(); e < total; e += cl_n) {
         const int q = e % a.nq, nn = e / a.nq;
         const double2 G = g_at(mu, eps[q], sigma[e], nn, a.beta);
         const double wn = (2.0 * nn + 1.0) * M_PI / a.beta;
@@ -608,13 +641,23 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
         v[1] = fma(kmult[q], 2.0 * (GS.x - epot_tc * tail), v[1]);
         v[2] = fma(kmult[q], G.x, v[2]);
     }
-    for (int q = cl_tid(); q < a.nq; q += cl_nth()) {     // tail_inv terms, once per q
+    for (int q = cl_tid(); q < a.nq; q += cl_n) {     // tail_inv terms, once per q
         const double ekin_tc = eps[q] + hartree - mu;
         const double epot_tc = a.U * a.U * 0.5 * a.n * (1.0 - 0.5 * a.n) + hartree * (eps[q] + hartree - mu);
         v[0] = fma(kmult[q], (a.beta / 2.0) * eps[q] * (1.0 + -a.beta * ekin_tc), v[0]);
         v[1] = fma(kmult[q], (a.beta / 2.0) * hartree + (a.beta / 2.0) * (-a.beta / 2.0) * epot_tc, v[1]);
     }
-    cluster_sum<3>(v, cr3, parity);
+    if constexpr (ASYNC) {
+        double v01[2] = {v[0], v[1]}, v2[2] = {v[2], 0.0};
+        allsum(v01);
+        allsum(v2);
+        v[0] = v01[0];
+        v[1] = v01[1];
+        v[2] = v2[0];
+        if (!exchange_ok) v[0] = v[1] = v[2] = NAN;
+    } else {
+        cluster_sum<3>(v, cr3, parity);
+    }
     if (cl_tid() == 0) {
         const double sG = v[2] * a.inv_nk;
         out[0] = mu;
@@ -847,7 +890,7 @@ int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2) {
     return LDGA_OK;
 }
 
-using NewtonKern = void (*)(SumArgs, const double*, const double*, double, const double*, const double*, int, double,
+using NewtonKern = void (*)(SumArgs, const double*, const double*, double, const double*, int, double*, int, double,
                            double*, const double*, double*, double*);
 
 // Register-resident elements per thread K for `per` (q, ω) terms per thread; K = 0 streams them.
@@ -857,6 +900,15 @@ NewtonKern pick_newton(int per) {
          : per <= 8 ? k_lambda_m<8, AS, CL> : per <= 10 ? k_lambda_m<10, AS, CL> : per <= 12 ? k_lambda_m<12, AS, CL>
          : per <= 16 ? k_lambda_m<16, AS, CL> : per <= 20 ? k_lambda_m<20, AS, CL> : per <= 24 ? k_lambda_m<24, AS, CL>
          : k_lambda_m<0, AS, CL>;
+}
+
+using MuKern = void (*)(GArgs, const double*, const double*, const double2*, int, double, double*);
+
+template <int CL, int NT>
+MuKern pick_mu(int per) {
+    return per <= 2 ? k_mu_fit_energy<2, CL, NT> : per <= 4 ? k_mu_fit_energy<4, CL, NT>
+         : per <= 6 ? k_mu_fit_energy<6, CL, NT> : per <= 8 ? k_mu_fit_energy<8, CL, NT>
+         : k_mu_fit_energy<0, CL, NT>;
 }
 
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
@@ -871,8 +923,7 @@ int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out) {
 // d_out[2] receives lambda_min; d_out[3..4] the periodic-trajectory skip (iteration, period).
 int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out, int nsteps,
                     double atol, double* sum_d_out, double* sum_m_out) {
-    int st = launch_lambda_min(ctx, LDGA_CH_M, d_out + 2);
-    if (st) return st;
+    const int w0 = (ctx->Nw + 1) / 2 - 1;   // ω0_index = ceil(Nw/2), 1-based; get_λ_min's column
     StageTimer st_(ctx, LDGA_STAGE_LAMBDA_NEWTON);
     const SumArgs sa = sum_args(ctx);
     const int cl = ctx->newton_cluster;
@@ -892,7 +943,7 @@ int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, 
     cfg.numAttrs = 1;
     const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, sa, (const double*)ctx->d_chi[LDGA_CH_M],
                                              (const double*)ctx->d_kmult, rhs_const, rhs_sub_dev,
-                                             (const double*)(d_out + 2), nsteps, atol, d_out,
+                                             w0, d_out + 2, nsteps, atol, d_out,
                                              (const double*)(sum_d_out ? ctx->d_chi[LDGA_CH_D] : nullptr),
                                              sum_d_out, sum_m_out);
     if (e != cudaSuccess) return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("k_lambda_m launch: ") + cudaGetErrorString(e));
@@ -917,6 +968,14 @@ int newton_cluster_size(bool async) {
             cudaGetLastError();
             return kCluster;
         }
+    const MuKern mu16[] = {k_mu_fit_energy<2, 16, kNewtonThreads>, k_mu_fit_energy<4, 16, kNewtonThreads>,
+                           k_mu_fit_energy<6, 16, kNewtonThreads>, k_mu_fit_energy<8, 16, kNewtonThreads>,
+                           k_mu_fit_energy<0, 16, kNewtonThreads>};
+    for (MuKern k : mu16)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            return kCluster;
+        }
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -933,16 +992,35 @@ int newton_cluster_size(bool async) {
             cudaGetLastError();
             return kCluster;
         }
+    for (MuKern k : mu16)
+        if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return kCluster;
+        }
     return 16;
 }
 
 int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out) {
     GArgs a = g_args(ctx, numax, host_G_shell_sum(numax + 1, ctx->mp.beta));
     StageTimer st_(ctx, LDGA_STAGE_GLADDER);
-    const int per = (a.nq * a.numax + kCluster * kClThreads - 1) / (kCluster * kClThreads);
-    auto kern = per <= 2 ? k_mu_fit_energy<2> : per <= 4 ? k_mu_fit_energy<4> : per <= 6 ? k_mu_fit_energy<6>
-              : per <= 8 ? k_mu_fit_energy<8> : k_mu_fit_energy<0>;
-    kern<<<kCluster, kClThreads, 0, ctx->stream>>>(a, ctx->d_kmult, ctx->d_eps, ctx->d_sigma, fix_n, mu_in, d_out);
+    const int cl = ctx->newton_cluster, nt = cl == 16 ? kNewtonThreads : kClThreads;
+    const int per = (a.nq * a.numax + cl * nt - 1) / (cl * nt);
+    const MuKern kern = cl == 16 ? pick_mu<16, kNewtonThreads>(per) : pick_mu<kCluster, kClThreads>(per);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)cl);
+    cfg.blockDim = dim3((unsigned)nt);
+    cfg.stream = ctx->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, (const double*)ctx->d_kmult, (const double*)ctx->d_eps,
+                                             (const double2*)ctx->d_sigma, fix_n, mu_in, d_out);
+    if (e != cudaSuccess)
+        return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("k_mu_fit_energy launch: ") + cudaGetErrorString(e));
     LDGA_LAUNCHED(ctx, "k_mu_fit_energy");
     return LDGA_OK;
 }
