@@ -90,6 +90,9 @@ struct DeviceGuard {
 #define TRY(x) do { int _s = (x); if (_s != LDGA_OK) return _s; } while (0)
 #define NEED(ctx, cond, msg) do { if (!(cond)) return ctx_fail((ctx), LDGA_ERR_STATE, (msg)); } while (0)
 
+// doubles per λdm residual slot (dm_slot); three slots follow the λ₀ scratch at the end of d_red
+constexpr int kDmSlot = 10;
+
 bool supported_grid(int dim, int M) {
     static const int m2[] = {1, 2, 3, 4, 5, 6, 7, 9, 11, 13, 17, 21, 25, 33};
     static const int m3[] = {1, 2, 3, 4, 5, 6, 7, 9, 11, 13, 17};
@@ -159,7 +162,7 @@ int alloc_all(ldga_ctx* c) {
     TRY(dev_alloc(c, &c->d_lambda0, nq * nnu * nw));
     TRY(dev_alloc(c, &c->d_sigma, nq * std::max<size_t>(nnu, 1)));
     TRY(dev_alloc(c, &c->d_gladder, nq * nf));
-    TRY(dev_alloc(c, &c->d_red, 64 + 2 * nnu * nw + 64));
+    TRY(dev_alloc(c, &c->d_red, 64 + 2 * nnu * nw + 64 + 3 * kDmSlot));
     TRY(dev_alloc(c, &c->d_flags, nq * nw));
     TRY(dev_alloc(c, &c->d_list, nq * nw));
     TRY(dev_alloc(c, &c->d_count, 4));
@@ -852,12 +855,15 @@ int eom_inputs_ready(ldga_ctx* ctx) {
 }
 
 // EoM into d_sigma (all on the stream, no sync)
-int eom_device(ldga_ctx* ctx, double lam_m, double lam_d, int numax, int tc, double chiloc_m_sum) {
+// tail_dev: device scalar sum_kω(χ_m^λm) formed earlier on the stream (the EoM tail's); null: formed
+// here into d_red[8]
+int eom_device(ldga_ctx* ctx, double lam_m, double lam_d, int numax, int tc, double chiloc_m_sum,
+               const double* tail_dev = nullptr) {
     if (numax < 1 || numax > ctx->Nnu) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax out of range");
     if (numax > std::abs(ctx->fft_lo) - ctx->sp.n_iw) return ctx_fail(ctx, LDGA_ERR_ARG, "νmax exceeds fft_range");
-    if (tc) TRY(launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8));
-    TRY(launch_eom(ctx, numax, lam_m, lam_d, nullptr, nullptr, -1, ctx->d_red + 8, tc, chiloc_m_sum, ctx->d_sigma,
-                   ctx->Nq, 1));
+    if (tc && !tail_dev) TRY(launch_sum_kw(ctx, LDGA_CH_M, lam_m, 0, ctx->d_red + 8));
+    TRY(launch_eom(ctx, numax, lam_m, lam_d, nullptr, nullptr, -1, tail_dev ? tail_dev : ctx->d_red + 8, tc,
+                   chiloc_m_sum, ctx->d_sigma, ctx->Nq, 1));
     ctx->have_sigma = true;
     ctx->sigma_numax = numax;
     return LDGA_OK;
@@ -1160,19 +1166,26 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     TRY(copy(ctx, ctx->d_sigma_loc, a.sigma_loc, (size_t)a.n_sigma * sizeof(double2)));
     TRY(launch_gloc_transform(ctx, true));                       // a1
     TRY(launch_bubble(ctx));                                     // a2
-    // a5, a6 need χ₀ and the local inputs only: they run on the copy stream beside the BSE and the
-    // λm Newton (8 SMs), and the EoM waits for them.  Their scratch (d_red from 64 on) is theirs.
-    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_bub, ctx->stream));
-    LDGA_CUDA(ctx, cudaStreamWaitEvent(io, ctx->ev_bub, 0));
-    {
+    // a5, a6 need χ₀ and the local inputs only.  A chain alone on the GPU runs them on the copy
+    // stream beside the BSE and the λm Newton (16 SMs), and the EoM waits for them; their scratch
+    // (d_red from 64 on) is theirs.  Chains of a batch (l0_beside false) keep them on their main
+    // stream: with many chains side by side the GPU has no idle SMs to give them, and the batch ran
+    // 37.8 ms with them in line against 43.8 ms beside.
+    if (ctx->l0_beside) {
+        LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_bub, ctx->stream));
+        LDGA_CUDA(ctx, cudaStreamWaitEvent(io, ctx->ev_bub, 0));
         cudaStream_t main = ctx->stream;
         ctx->stream = io;
         const int st = launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp);   // a5
         const int st2 = st == LDGA_OK ? launch_lambda0(ctx) : st;                      // a6
         ctx->stream = main;
         TRY(st2);
+        LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_l0, io));
+    } else {
+        LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_loc, 0));
+        TRY(launch_F_from_chi(ctx, ctx->d_chiloc, ctx->d_gimp, a.n_gimp));   // a5
+        TRY(launch_lambda0(ctx));                                           // a6
     }
-    LDGA_CUDA(ctx, cudaEventRecord(ctx->ev_l0, io));
     LDGA_CUDA(ctx, cudaMemsetAsync(ctx->d_count, 0, 4 * sizeof(int32_t), ctx->stream));   // fails, lists
     LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_gamma, 0));
     TRY(launch_bse_pair(ctx, ctx->d_count + 1));                  // a7, both channels
@@ -1185,7 +1198,7 @@ int chain_m_enqueue(ldga_ctx* ctx, const ChainArgs& a) {
     // sum_kω(chi_m, λ = λm) for the EoM's tail, all in the Newton kernel (d_red[56], d_red[16], d_red[8])
     TRY(launch_lambda_m(ctx, 2.0 * a.imp_density, nullptr, ctx->d_red + 16, 100, 1e-13, ctx->d_red + 56,
                         ctx->d_red + 8));
-    LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_l0, 0));
+    if (ctx->l0_beside) LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_l0, 0));
     TRY(launch_eom(ctx, numax, 0.0, 0.0, ctx->d_red + 16, nullptr, -1, ctx->d_red + 8, 1, a.chiloc_m_sum,
                    ctx->d_sigma, ctx->Nq, 1));                   // a10 at λm
     TRY(launch_g_ladder(ctx, numax, 1, ctx->mp.mu, ctx->d_red + 24));   // a15: μ fit, energies
@@ -1247,7 +1260,8 @@ int chain_m_submit(ldga_ctx* ctx, const ChainArgs& a, bool use_graph, bool* repl
         key.insert(key.end(), {(uint64_t)n_sigma, (uint64_t)n_gimp, dbits(a.imp_density), dbits(a.chiloc_m_sum),
                                dbits(ctx->mp.U), dbits(ctx->mp.mu), dbits(ctx->mp.beta), dbits(ctx->mp.n),
                                dbits(ctx->mp.Ekin_DMFT), (uint64_t)ctx->prec, (uint64_t)(uintptr_t)ctx->stream,
-                               (uint64_t)ctx->profiling, (uint64_t)ctx->prof_mask});
+                               (uint64_t)ctx->profiling, (uint64_t)ctx->prof_mask, (uint64_t)ctx->newton_cluster,
+                               (uint64_t)ctx->l0_beside});
     }
     if (graphable && ctx->graph_exec && key == ctx->graph_key) {
         LDGA_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
@@ -1354,7 +1368,9 @@ int ldga_batch_chain_m(int32_t n, ldga_ctx* const* ctxs, const ldga_chain_io* io
         ChainArgs a{x.sigma_loc, x.gamma_m, x.gamma_d, x.chi_loc_m, x.gimp, x.n_sigma, x.n_gimp, x.imp_density,
                     x.chiloc_m_sum, x.sigma_out, x.chi_m_out, x.chi_d_out};
         bool r = false;
+        c->l0_beside = n == 1;   // λ₀ beside the BSE only for a chain alone on the GPU
         st[i] = chain_m_submit(c, a, use_graph != 0, &r);
+        c->l0_beside = true;
         rep[i] = r;
     }
     int first = LDGA_OK;
@@ -1388,21 +1404,24 @@ struct DmState {
     double last[7];
 };
 
-// residual_vals (conditions_new.jl:250-270): returns false on a CUDA/argument error
-bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
+// One residual's device scalars: [0..3] μ, E_kin, E_pot,1, filling (k_mu_fit_energy), [8] sum_kω(χm^λm)
+// (the EoM tail's), [9] sum_kω(χd^λd).  Slot k of the three a Newton iteration evaluates.
+double* dm_slot(ldga_ctx* ctx, int k) { return ctx->d_red + 128 + 2 * (size_t)ctx->Nnu * ctx->Nw + k * kDmSlot; }
+
+// Enqueue residual_vals (conditions_new.jl:250-270) at (lm, ld) into slot k: the two χ sums in one
+// launch, the EoM, the μ fit and energies.  The μ fit starts from mu_dev (the previous residual's μ on
+// the device) or, when null, from s.mu.
+int dm_enqueue(DmState& s, double lm, double ld, int k, const double* mu_dev) {
     ldga_ctx* ctx = s.ctx;
-    s.evals++;
-    if (lm > 1e5 || ld > 1e5) { F[0] = F[1] = NAN; return true; }
-    int st = eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum);   // d_red[8] = sum_kω(χm^λm), the EoM tail's
-    if (!st) st = launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, ctx->d_red + 24);
-    if (!st && cudaMemcpyAsync(ctx->d_red + 32, ctx->d_red + 8, sizeof(double), cudaMemcpyDeviceToDevice,
-                               ctx->stream) != cudaSuccess)
-        st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaMemcpyAsync");
-    if (!st) st = launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33);
-    double r[10];
-    if (!st) st = copy(ctx, r, ctx->d_red + 24, 10 * sizeof(double));
-    if (!st) st = sync(ctx);
-    if (st) { s.status = st; return false; }
+    double* r = dm_slot(ctx, k);
+    TRY(launch_sum_kw2(ctx, lm, ld, r + 8, r + 9));
+    TRY(eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum, r + 8));
+    return launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, r, mu_dev);
+}
+
+// The residual from a slot's scalars (read back to the host); records μ and the last values in s.
+void dm_finish(DmState& s, const double r[kDmSlot], double F[2]) {
+    ldga_ctx* ctx = s.ctx;
     const double mu = r[0], ek = r[1], ep1 = r[2], n = r[3], xm = r[8], xd = r[9];
     s.mu = mu;
     const double lhs = (xd + xm) / 2.0;
@@ -1412,6 +1431,42 @@ bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
     F[1] = ep1 - ep2;
     s.last[0] = n; s.last[1] = mu; s.last[2] = ek; s.last[3] = ep1; s.last[4] = ep2; s.last[5] = s.rhs_c1;
     s.last[6] = lhs;
+}
+
+// Residuals at n points (n <= 3) in order, with one host synchronisation: each μ fit starts from the
+// μ of the residual evaluated before it, as when they run one by one.  A point above 1e5 is not
+// evaluated (NaN residual), as in the reference's residual_vals guard.  False on a CUDA or argument
+// error (s.status).
+bool dm_residuals(DmState& s, int n, const double (*pts)[2], double (*F)[2]) {
+    ldga_ctx* ctx = s.ctx;
+    bool eval[3] = {false, false, false};
+    const double* mu_src = nullptr;
+    int st = LDGA_OK, last = -1;
+    for (int k = 0; k < n && !st; ++k) {
+        s.evals++;
+        if (pts[k][0] > 1e5 || pts[k][1] > 1e5) continue;
+        st = dm_enqueue(s, pts[k][0], pts[k][1], k, mu_src);
+        eval[k] = true;
+        mu_src = dm_slot(ctx, k);
+        last = k;
+    }
+    double r[3][kDmSlot];
+    if (!st && last >= 0) st = copy(ctx, r, dm_slot(ctx, 0), (size_t)(last + 1) * kDmSlot * sizeof(double));
+    if (!st && last >= 0) st = sync(ctx);
+    if (st) { s.status = st; return false; }
+    for (int k = 0; k < n; ++k) {
+        if (eval[k]) dm_finish(s, r[k], F[k]);
+        else F[k][0] = F[k][1] = NAN;
+    }
+    return true;
+}
+
+bool dm_residual(DmState& s, double lm, double ld, double F[2]) {
+    const double p[1][2] = {{lm, ld}};
+    double f[1][2];
+    if (!dm_residuals(s, 1, p, f)) return false;
+    F[0] = f[0][0];
+    F[1] = f[0][1];
     return true;
 }
 
@@ -1430,19 +1485,20 @@ bool dm_newton(DmState& s, const double start[2], const double xmin[2], double a
     const int max_reset = 5;
     const double reset_backoff = 1.0;
     while (true) {
-        double fi[2], f1[2], J[2][2];
-        if (!dm_residual(s, xi[0], xi[1], fi)) return false;
-        // forward-difference Jacobian.  FiniteDiff evaluates f(x) once more; the residual is a
-        // deterministic function of x (its μ fit converges to |Δn| < 1e-14 from any warm start), so
-        // the value just computed is used
-        const double* f0 = fi;
+        double fi[2], J[2][2];
+        // f at xi and the forward-difference Jacobian's two points, enqueued together (one host
+        // synchronisation).  FiniteDiff evaluates f(x) once more; the residual is a deterministic
+        // function of x (its μ fit converges to |Δn| < 1e-14 from any warm start), so the value
+        // at xi is used
+        const double e[2] = {fd_step(xi[0]), fd_step(xi[1])};
+        const double pts[3][2] = {{xi[0], xi[1]}, {xi[0] + e[0], xi[1]}, {xi[0], xi[1] + e[1]}};
+        double f3[3][2];
+        if (!dm_residuals(s, 3, pts, f3)) return false;
+        fi[0] = f3[0][0];
+        fi[1] = f3[0][1];
         for (int j = 0; j < 2; ++j) {
-            double x1[2] = {xi[0], xi[1]};
-            const double e = fd_step(xi[j]);
-            x1[j] += e;
-            if (!dm_residual(s, x1[0], x1[1], f1)) return false;
-            J[0][j] = (f1[0] - f0[0]) / e;
-            J[1][j] = (f1[1] - f0[1]) / e;
+            J[0][j] = (f3[1 + j][0] - fi[0]) / e[j];
+            J[1][j] = (f3[1 + j][1] - fi[1]) / e[j];
         }
         const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
         const double inv[2][2] = {{J[1][1] / det, -J[0][1] / det}, {-J[1][0] / det, J[0][0] / det}};
@@ -1596,8 +1652,7 @@ int ldga_run_sc(ldga_ctx* ctx, double lam_m, double lam_d, int32_t flags, double
     double lm = lam_m, ld = lam_d;
     auto sums = [&](double* lhs, double* ep2) -> int {
         double r[2];
-        TRY(launch_sum_kw(ctx, LDGA_CH_M, lm, 0, ctx->d_red + 32));
-        TRY(launch_sum_kw(ctx, LDGA_CH_D, ld, 0, ctx->d_red + 33));
+        TRY(launch_sum_kw2(ctx, lm, ld, ctx->d_red + 32, ctx->d_red + 33));
         TRY(copy(ctx, r, ctx->d_red + 32, 2 * sizeof(double)));
         TRY(sync(ctx));
         *lhs = (r[1] + r[0]) / 2.0;

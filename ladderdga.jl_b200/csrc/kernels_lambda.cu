@@ -555,7 +555,7 @@ __device__ __forceinline__ double2 g_at(double mu, double eps, double2 sig, int 
 template <int K, int CL, int NT>
 __global__ void __launch_bounds__(NT)
 k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restrict__ eps,
-                const double2* __restrict__ sigma, int fix_n, double mu_in, double* out) {
+                const double2* __restrict__ sigma, int fix_n, double mu_in, const double* mu_dev, double* out) {
     constexpr bool ASYNC = CL != kCluster;
     __shared__ ClAll<2, NT / 32, CL> ca2;
     __shared__ ClAsync<2, NT / 32, CL> xs;
@@ -569,7 +569,7 @@ k_mu_fit_energy(GArgs a, const double* __restrict__ kmult, const double* __restr
     };
     const int total = a.nq * a.numax;
     const int cl_n = CL * (int)blockDim.x;
-    double mu = mu_in;
+    double mu = mu_dev ? mu_dev[0] : mu_in;   // the start: a value written earlier on the stream, or mu_in
     bool failed = false;
     double ck[K > 0 ? K : 1], ce[K > 0 ? K : 1], cw[K > 0 ? K : 1];
     double2 cs[K > 0 ? K : 1];
@@ -871,6 +871,41 @@ int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_ou
     return LDGA_OK;
 }
 
+namespace {
+
+// sum_kω(χ_m^λm) -> out_m[0] and sum_kω(χ_d^λd) -> out_d[0] in one launch: the same per-thread
+// order and reduction as two k_sum_kw (mode 0) launches, so the values are the same bit for bit
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kClThreads)
+k_sum_kw2(SumArgs a, const double* __restrict__ chi_m, const double* __restrict__ chi_d,
+          const double* __restrict__ kmult, double lam_m, double lam_d, double* out_m, double* out_d) {
+    __shared__ ClRed<2> cr;
+    int parity = 0;
+    double v[2] = {0.0, 0.0};
+    const int total = a.nq * a.nw;
+    for (int e = cl_tid(); e < total; e += cl_nth()) {
+        const double km = kmult[e % a.nq];
+        const double xm = chi_m[e], xd = chi_d[e];
+        v[0] = fma(km, lam_m != 0.0 ? xm / (lam_m * xm + 1.0) : xm, v[0]);
+        v[1] = fma(km, lam_d != 0.0 ? xd / (lam_d * xd + 1.0) : xd, v[1]);
+    }
+    cluster_sum<2>(v, cr, parity);
+    if (cl_tid() == 0) {
+        out_m[0] = finish_kw(a, v[0]);
+        out_d[0] = finish_kw(a, v[1]);
+    }
+    cg::this_cluster().sync();
+}
+
+}  // namespace
+
+int launch_sum_kw2(ldga_ctx* ctx, double lam_m, double lam_d, double* d_out_m, double* d_out_d) {
+    StageTimer st_(ctx, LDGA_STAGE_SUMS);
+    k_sum_kw2<<<kCluster, kClThreads, 0, ctx->stream>>>(sum_args(ctx), ctx->d_chi[LDGA_CH_M], ctx->d_chi[LDGA_CH_D],
+                                                        ctx->d_kmult, lam_m, lam_d, d_out_m, d_out_d);
+    LDGA_LAUNCHED(ctx, "k_sum_kw2");
+    return LDGA_OK;
+}
+
 // update_tail! (DataTypes.jl:315-345) of the c2/(i w)^2 tail: chi[:, w] += Re((c2_new - c2_old)/(i w_m)^2)
 // = -(c2_new - c2_old)/w_m^2 for every w_m = 2 pi m / beta != 0.
 __global__ void k_chi_tail_shift(int nq, int nw, int n_iw, double beta, double dc2, double* __restrict__ chi) {
@@ -902,7 +937,7 @@ NewtonKern pick_newton(int per) {
          : k_lambda_m<0, AS, CL>;
 }
 
-using MuKern = void (*)(GArgs, const double*, const double*, const double2*, int, double, double*);
+using MuKern = void (*)(GArgs, const double*, const double*, const double2*, int, double, const double*, double*);
 
 template <int CL, int NT>
 MuKern pick_mu(int per) {
@@ -1000,7 +1035,7 @@ int newton_cluster_size(bool async) {
     return 16;
 }
 
-int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out) {
+int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out, const double* mu_dev) {
     GArgs a = g_args(ctx, numax, host_G_shell_sum(numax + 1, ctx->mp.beta));
     StageTimer st_(ctx, LDGA_STAGE_GLADDER);
     const int cl = ctx->newton_cluster, nt = cl == 16 ? kNewtonThreads : kClThreads;
@@ -1018,7 +1053,7 @@ int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d
     cfg.attrs = at;
     cfg.numAttrs = 1;
     const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, (const double*)ctx->d_kmult, (const double*)ctx->d_eps,
-                                             (const double2*)ctx->d_sigma, fix_n, mu_in, d_out);
+                                             (const double2*)ctx->d_sigma, fix_n, mu_in, mu_dev, d_out);
     if (e != cudaSuccess)
         return ctx_fail(ctx, LDGA_ERR_CUDA, std::string("k_mu_fit_energy launch: ") + cudaGetErrorString(e));
     LDGA_LAUNCHED(ctx, "k_mu_fit_energy");

@@ -133,6 +133,7 @@ struct ldga_ctx {
     cudaStream_t io_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_gamma = nullptr, ev_loc = nullptr, ev_chi = nullptr, ev_join = nullptr;
     cudaEvent_t ev_bub = nullptr, ev_l0 = nullptr;   // χ₀ ready for λ₀ on io_stream; λ₀ ready for the EoM
+    bool l0_beside = true;               // the chain's λ₀ on io_stream (false: in line, for batched chains)
     bool capturing = false;              // a CUDA graph of the chain is being captured
 
     // fused chain (ldga_chain_m): persistent input buffers and the captured graph
@@ -268,6 +269,8 @@ int launch_eom(ldga_ctx* ctx, int numax, double lam_m, double lam_d, const doubl
                double2* out, int out_ld, int add_hartree);
 int launch_sum_kw(ldga_ctx* ctx, int channel, double lam, int mode, double* d_out, const double* lam_dev = nullptr);
 int launch_lambda_min(ldga_ctx* ctx, int channel, double* d_out);
+// sum_kω(χ_m^λm) and sum_kω(χ_d^λd) (mode 0 of launch_sum_kw) in one launch
+int launch_sum_kw2(ldga_ctx* ctx, double lam_m, double lam_d, double* d_out_m, double* d_out_d);
 int newton_cluster_size(bool async);
 int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2);
 // newton_right's defaults (LambdaCorrection/helpers.jl:133): nsteps 100, atol 1e-13.  sum_d_out given:
@@ -276,7 +279,9 @@ int launch_chi_tail_shift(ldga_ctx* ctx, int channel, double dc2);
 int launch_lambda_m(ldga_ctx* ctx, double rhs_const, const double* rhs_sub_dev, double* d_out /*[5]*/,
                     int nsteps = 100, double atol = 1e-13, double* sum_d_out = nullptr,
                     double* sum_m_out = nullptr);
-int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[4]*/);
+// mu_dev (may be null): device scalar the μ fit starts from instead of mu_in
+int launch_g_ladder(ldga_ctx* ctx, int numax, int fix_n, double mu_in, double* d_out /*[4]*/,
+                    const double* mu_dev = nullptr);
 int launch_g_ladder_full(ldga_ctx* ctx, int numax, const double* mu_dev);
 int launch_calc_E(ldga_ctx* ctx, const double2* G, int ldg, const double2* sigma, int numax, double mu,
                   double* d_out);
