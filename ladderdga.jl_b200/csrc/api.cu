@@ -210,7 +210,8 @@ void free_all(ldga_ctx* c) {
     void* ptrs[] = {c->d_kmult, c->d_eps, c->d_ghat, c->d_gloc, c->d_sigma_loc, c->d_chi0, c->d_Gamma[0],
                     c->d_Gamma[1], c->d_chi[0], c->d_chi[1], c->d_gam[0], c->d_gam[1], c->d_F, c->d_lambda0,
                     c->d_sigma, c->d_gladder, c->d_partial, c->d_red, c->d_flags, c->d_flags2, c->d_list, c->d_list2, c->d_gamma_t, c->d_count,
-                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats};
+                    c->d_pivot_scratch, c->d_bub_pairs, c->d_arena, c->d_qperm, c->d_iter_stats,
+                    c->dm_partial[0], c->dm_partial[1], c->dm_sigma[0], c->dm_sigma[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -374,6 +375,7 @@ int ldga_create(const ldga_lattice* lat, const ldga_model* mp, const ldga_sim* s
     if (!c) return ctx_fail(nullptr, LDGA_ERR_ARG, "out of host memory");
     if (const char* tr = std::getenv("LDGA_TRANSFORM")) c->transform_tc = std::strcmp(tr, "tc") == 0;
     if (const char* nw = std::getenv("LDGA_NEWTON")) c->newton_async = std::strcmp(nw, "barrier") != 0;
+    if (const char* dl = std::getenv("LDGA_DM_LANES")) c->dm_lanes = std::strcmp(dl, "0") != 0;
     if (const char* sw = std::getenv("LDGA_ITER_SWEEPS")) c->iter_sweeps = std::min(std::max(std::atoi(sw), 0), 1000);
     DeviceGuard g(device);
     c->device = device;
@@ -408,6 +410,10 @@ int ldga_destroy(ldga_ctx* ctx) {
         for (cudaEvent_t e : {ctx->ev_fork, ctx->ev_gamma, ctx->ev_loc, ctx->ev_chi, ctx->ev_join, ctx->ev_bub, ctx->ev_l0})
             if (e) cudaEventDestroy(e);
     }
+    for (cudaStream_t st : ctx->dm_stream)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t e : {ctx->dm_ev[0], ctx->dm_ev[1], ctx->dm_ev[2], ctx->dm_fork})
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return LDGA_OK;
@@ -1408,17 +1414,6 @@ struct DmState {
 // (the EoM tail's), [9] sum_kω(χd^λd).  Slot k of the three a Newton iteration evaluates.
 double* dm_slot(ldga_ctx* ctx, int k) { return ctx->d_red + 128 + 2 * (size_t)ctx->Nnu * ctx->Nw + k * kDmSlot; }
 
-// Enqueue residual_vals (conditions_new.jl:250-270) at (lm, ld) into slot k: the two χ sums in one
-// launch, the EoM, the μ fit and energies.  The μ fit starts from mu_dev (the previous residual's μ on
-// the device) or, when null, from s.mu.
-int dm_enqueue(DmState& s, double lm, double ld, int k, const double* mu_dev) {
-    ldga_ctx* ctx = s.ctx;
-    double* r = dm_slot(ctx, k);
-    TRY(launch_sum_kw2(ctx, lm, ld, r + 8, r + 9));
-    TRY(eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum, r + 8));
-    return launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, r, mu_dev);
-}
-
 // The residual from a slot's scalars (read back to the host); records μ and the last values in s.
 void dm_finish(DmState& s, const double r[kDmSlot], double F[2]) {
     ldga_ctx* ctx = s.ctx;
@@ -1433,27 +1428,107 @@ void dm_finish(DmState& s, const double r[kDmSlot], double F[2]) {
     s.last[6] = lhs;
 }
 
-// Residuals at n points (n <= 3) in order, with one host synchronisation: each μ fit starts from the
-// μ of the residual evaluated before it, as when they run one by one.  A point above 1e5 is not
-// evaluated (NaN residual), as in the reference's residual_vals guard.  False on a CUDA or argument
-// error (s.status).
+// Streams, events and buffers of the residual lanes 1 and 2, made on first use (outside any capture:
+// the λdm entry points are not captured).  Lane buffers match the handle's own.
+int dm_lanes_ready(ldga_ctx* ctx) {
+    if (ctx->dm_stream[0]) return LDGA_OK;
+    for (cudaStream_t& st : ctx->dm_stream) LDGA_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ctx->dm_ev[0], &ctx->dm_ev[1], &ctx->dm_ev[2], &ctx->dm_fork})
+        LDGA_CUDA(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    const size_t nsig = (size_t)ctx->Nq * std::max(ctx->Nnu, 1);
+    for (int j = 0; j < 2; ++j) {
+        LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->dm_sigma[j]), nsig * sizeof(double2)));
+        if (ctx->partial_elems) {
+            LDGA_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->dm_partial[j]), ctx->partial_elems * sizeof(double2)));
+            ctx->dm_partial_elems[j] = ctx->partial_elems;
+        }
+    }
+    return LDGA_OK;
+}
+
+// Lane k's stream, Σ and partial-sum buffers put into the handle (lane 0: the handle's own) by
+// lane_enter, and the handle's put back by lane_leave (keeping a lane buffer the EoM may have grown).
+struct LaneSave {
+    cudaStream_t stream;
+    double2 *sigma, *partial;
+    size_t partial_elems;
+};
+
+void lane_enter(ldga_ctx* ctx, int k, LaneSave& sv) {
+    sv = {ctx->stream, ctx->d_sigma, ctx->d_partial, ctx->partial_elems};
+    if (k == 0) return;
+    const int j = k - 1;
+    ctx->stream = ctx->dm_stream[j];
+    ctx->d_sigma = ctx->dm_sigma[j];
+    ctx->d_partial = ctx->dm_partial[j];
+    ctx->partial_elems = ctx->dm_partial_elems[j];
+}
+
+void lane_leave(ldga_ctx* ctx, int k, const LaneSave& sv) {
+    if (k == 0) return;
+    const int j = k - 1;
+    ctx->dm_partial[j] = ctx->d_partial;
+    ctx->dm_partial_elems[j] = ctx->partial_elems;
+    ctx->stream = sv.stream;
+    ctx->d_sigma = sv.sigma;
+    ctx->d_partial = sv.partial;
+    ctx->partial_elems = sv.partial_elems;
+}
+
+// residual_vals (conditions_new.jl:250-270) at (lm, ld) into slot k on the current stream: the two χ
+// sums in one launch, the EoM, then the μ fit and energies after event `after` (if given), from the
+// μ at mu_dev (the previous residual's, on the device) or s.mu
+int dm_enqueue(DmState& s, double lm, double ld, int k, cudaEvent_t after, const double* mu_dev) {
+    ldga_ctx* ctx = s.ctx;
+    double* r = dm_slot(ctx, k);
+    TRY(launch_sum_kw2(ctx, lm, ld, r + 8, r + 9));
+    TRY(eom_device(ctx, lm, ld, s.numax, 1, s.chiloc_m_sum, r + 8));
+    if (after) LDGA_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, after, 0));
+    return launch_g_ladder(ctx, s.numax, s.fix_n, s.mu, r, mu_dev);
+}
+
+// Residuals at n points (n <= 3) in order, with one host synchronisation.  Residual k runs on lane k:
+// its χ sums and EoM overlap the other lanes' work, and its μ fit waits for the μ fit of the residual
+// evaluated before it and starts from that μ, as when they run one by one, so the values are the
+// same.  A point above 1e5 is not evaluated (NaN residual), as in the reference's residual_vals
+// guard.  False on a CUDA or argument error (s.status).
 bool dm_residuals(DmState& s, int n, const double (*pts)[2], double (*F)[2]) {
     ldga_ctx* ctx = s.ctx;
     bool eval[3] = {false, false, false};
     const double* mu_src = nullptr;
-    int st = LDGA_OK, last = -1;
+    int st = n > 1 ? dm_lanes_ready(ctx) : LDGA_OK, last = -1;
+    if (!st && n > 1) {
+        if (cudaEventRecord(ctx->dm_fork, ctx->stream) != cudaSuccess) st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaEventRecord");
+        for (int j = 0; j < 2 && !st; ++j)
+            if (cudaStreamWaitEvent(ctx->dm_stream[j], ctx->dm_fork, 0) != cudaSuccess)
+                st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaStreamWaitEvent");
+    }
     for (int k = 0; k < n && !st; ++k) {
         s.evals++;
         if (pts[k][0] > 1e5 || pts[k][1] > 1e5) continue;
-        st = dm_enqueue(s, pts[k][0], pts[k][1], k, mu_src);
+        LaneSave sv;
+        lane_enter(ctx, k, sv);
+        st = dm_enqueue(s, pts[k][0], pts[k][1], k, last >= 0 ? ctx->dm_ev[last] : nullptr, mu_src);
+        if (!st && n > 1 && cudaEventRecord(ctx->dm_ev[k], ctx->stream) != cudaSuccess)
+            st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaEventRecord");
+        lane_leave(ctx, k, sv);
         eval[k] = true;
         mu_src = dm_slot(ctx, k);
         last = k;
     }
+    for (int k = 1; k < n && !st; ++k)   // join the lanes before the read-back
+        if (eval[k] && cudaStreamWaitEvent(ctx->stream, ctx->dm_ev[k], 0) != cudaSuccess)
+            st = ctx_fail(ctx, LDGA_ERR_CUDA, "cudaStreamWaitEvent");
     double r[3][kDmSlot];
     if (!st && last >= 0) st = copy(ctx, r, dm_slot(ctx, 0), (size_t)(last + 1) * kDmSlot * sizeof(double));
     if (!st && last >= 0) st = sync(ctx);
-    if (st) { s.status = st; return false; }
+    if (st) {
+        if (n > 1)   // nothing of this call stays in flight on the lanes
+            for (cudaStream_t ls : ctx->dm_stream)
+                if (ls) cudaStreamSynchronize(ls);
+        s.status = st;
+        return false;
+    }
     for (int k = 0; k < n; ++k) {
         if (eval[k]) dm_finish(s, r[k], F[k]);
         else F[k][0] = F[k][1] = NAN;
@@ -1493,7 +1568,12 @@ bool dm_newton(DmState& s, const double start[2], const double xmin[2], double a
         const double e[2] = {fd_step(xi[0]), fd_step(xi[1])};
         const double pts[3][2] = {{xi[0], xi[1]}, {xi[0] + e[0], xi[1]}, {xi[0], xi[1] + e[1]}};
         double f3[3][2];
-        if (!dm_residuals(s, 3, pts, f3)) return false;
+        if (s.ctx->dm_lanes) {
+            if (!dm_residuals(s, 3, pts, f3)) return false;
+        } else {
+            for (int k = 0; k < 3; ++k)
+                if (!dm_residuals(s, 1, pts + k, f3 + k)) return false;
+        }
         fi[0] = f3[0][0];
         fi[1] = f3[0][1];
         for (int j = 0; j < 2; ++j) {

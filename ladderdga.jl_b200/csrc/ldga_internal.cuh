@@ -134,6 +134,15 @@ struct ldga_ctx {
     cudaEvent_t ev_fork = nullptr, ev_gamma = nullptr, ev_loc = nullptr, ev_chi = nullptr, ev_join = nullptr;
     cudaEvent_t ev_bub = nullptr, ev_l0 = nullptr;   // χ₀ ready for λ₀ on io_stream; λ₀ ready for the EoM
     bool l0_beside = true;               // the chain's λ₀ on io_stream (false: in line, for batched chains)
+    // λdm residual lanes 1 and 2 (lane 0 is the handle's own stream and buffers): a stream, the
+    // EoM's partial sums and Σ of each, and one event per lane marking its μ fit
+    bool dm_lanes = true;                // false (LDGA_DM_LANES=0 at ldga_create): residuals one by one
+    cudaStream_t dm_stream[2] = {nullptr, nullptr};
+    cudaEvent_t dm_ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t dm_fork = nullptr;
+    double2* dm_partial[2] = {nullptr, nullptr};
+    size_t dm_partial_elems[2] = {0, 0};
+    double2* dm_sigma[2] = {nullptr, nullptr};
     bool capturing = false;              // a CUDA graph of the chain is being captured
 
     // fused chain (ldga_chain_m): persistent input buffers and the captured graph

@@ -290,6 +290,23 @@ def test_lambda_dm_correction(case):
     assert abs(res_g.EPot_p1 - res_g.EPot_p2) < 1e-8
 
 
+def test_lambda_dm_lanes_bitwise(case, monkeypatch):
+    """The λdm Newton evaluates the three residuals of an iteration on three streams (each μ fit
+    after the previous one, from its μ); with LDGA_DM_LANES=0 they run one by one.  Both orders must
+    give the same λm, λd, μ and Σ_ladder bit for bit."""
+    name, inp, ref = case
+    if name != "2d16":
+        pytest.skip("λdm root is checked on configuration 1")
+    out = []
+    for lanes in ("1", "0"):
+        monkeypatch.setenv("LDGA_DM_LANES", lanes)
+        g = gpu_chain(inp)
+        r = L.λdm_correction(g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], g["h"])
+        out.append((r.λm, r.λd, r.μ, np.array(r.Σ_ladder)))
+    assert out[0][:3] == out[1][:3]
+    assert np.array_equal(out[0][3], out[1][3])
+
+
 def test_fused_chain_matches_stepwise(case):
     """ldga_chain_m (one call, CUDA graph on replay) gives the step-by-step API's λm result."""
     import ctypes as C
