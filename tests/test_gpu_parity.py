@@ -239,6 +239,12 @@ def test_lambda_m_newton_cluster_sizes(case, cluster, monkeypatch):
     rr = R.lambda_m_correction_full(ref["chi_m"], ref["gamma_m"], ref["chi_d"], ref["gamma_d"], ref["lambda0"],
                                     ref["h"])
     assert abs(lam - rr.lam_m) < ATOL_LAMBDA
+    # the μ fit and energies run on the same cluster size
+    res = L.λ_correction("m", g["chi_m"], g["gamma_m"], g["chi_d"], g["gamma_d"], g["lambda0"], g["h"])
+    assert abs(res.μ - rr.mu) < 1e-10
+    assert rel(res.Σ_ladder, rr.Sigma_ladder) < RTOL
+    for a, b in ((res.EKin, rr.EKin), (res.EPot_p1, rr.EPot_p1)):
+        assert abs(a - b) <= RTOL * max(1.0, abs(b))
 
 
 def test_lambda_m_newton_trajectory_3d32(require_gpu):
